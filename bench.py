@@ -1,0 +1,305 @@
+#!/usr/bin/env python
+"""Benchmark: exact Matern log-likelihood evaluations per second on B200.
+
+One step = one evaluation of the hot path (generate Sigma(theta) -> tiled
+Cholesky with fused log-det and solve -> log-likelihood) for the N = 100,000
+univariate Matern field (317 x 317 jittered unit-square grid truncated to
+1e5 points, theta = (1.0, 0.05, 0.5), z = L e from the reference's
+generator).  The covariance (40 GB of lower tiles) is far larger than L2, so
+no explicit L2 flush is needed between steps.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--n N] [--impl ours|reference]
+
+With N > 1 GPUs (torchrun) every rank evaluates its own replica field (the
+single-field path does not shard); value = all ranks' evaluations / max time.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "exact Matern log-likelihood evaluations per second (N=100000, FP64)"
+UNIT = "loglik-evals/s"
+THETA = [1.0, 0.05, 0.5]
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=3)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--n", type=int, default=100000)
+    ap.add_argument("--ts", type=int, default=512)
+    ap.add_argument("--seed", type=int, default=0)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--cpu-seconds", type=float, default=12.0, help="target CPU time of the oracle sample")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    return ap.parse_args()
+
+
+def workload(n):
+    side = 1
+    while side * side < n:
+        side += 1
+    return "univariate Matern exact loglik, N=%d (%dx%d jittered grid truncated), theta=(%g, %g, %g), FP64" % (
+        n, side, side, *THETA)
+
+
+# ---------------------------------------------------------------- clocks ----
+class ClockSampler:
+    """nvidia-smi samples during the timed region."""
+
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.hw_slowdown,"
+         "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+         "clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index):
+        self.index = index
+        self.proc = None
+        self.lines = []
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.index), "--query-gpu=" + self.Q,
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except OSError:
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def stop(self):
+        if not self.proc:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        sm, smax, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            f = [v.strip() for v in ln.split(",")]
+            if len(f) < 8:
+                continue
+            try:
+                sm.append(float(f[1]))
+                smax = float(f[2])
+            except ValueError:
+                continue
+            for nm, v in zip(names, f[4:8]):
+                if v.lower() == "active":
+                    reasons.add(nm)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": smax, "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+# ------------------------------------------------------- CPU (oracle) leg ----
+def cpu_sample(n_target, seconds):
+    """Time the oracle (the C restatement of the reference CPU path, all host
+    threads) on a bounded sample: one full evaluation at N_s, grown until it
+    takes a few seconds, then scaled to N_target by N^2 (generation, solve)
+    and N^3 (Cholesky)."""
+    import oracle
+
+    oracle.build()
+    threads = os.cpu_count() or 1
+    oracle.set_threads(threads)
+    n = 4000
+    while True:
+        x, y = oracle.generate_xy_loc(n, 0)
+        import numpy as np
+
+        z = np.random.default_rng(0).standard_normal(n)
+        t0 = time.perf_counter()
+        _, _, _, (tg, tc, tsv) = oracle.dmle(x, y, z, THETA)
+        wall = time.perf_counter() - t0
+        if wall * 8 > seconds or n >= 32000:
+            break
+        n *= 2
+    s = n_target / n
+    t_full = tg * s * s + tc * s ** 3 + tsv * s * s
+    return {"value": 1.0 / t_full, "unit": UNIT, "cores": threads, "kind": "port",
+            "sample": "oracle loglik at N=%d (gen %.3fs, chol %.3fs, solve %.3fs) on %d threads, scaled to N=%d "
+                      "by N^2 (gen, solve) and N^3 (chol)" % (n, tg, tc, tsv, threads, n_target),
+            "seconds_per_eval_extrapolated": t_full, "sample_n": n}
+
+
+def run_reference(args):
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return
+    samples = []
+    for i in range(args.warmup + args.steps):
+        cb = cpu_sample(args.n, args.cpu_seconds)
+        if i >= args.warmup:
+            samples.append(cb)
+    value = statistics.median(c["value"] for c in samples)
+    cb = dict(samples[-1])
+    cb["value"] = value
+    line = {"impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 / value, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": {"workload": workload(args.n), "sample": cb["sample"]},
+            "cpu_baseline": cb, "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0,
+                                        "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+# ----------------------------------------------------------- our arm -----
+def measured_dgemm_tflops(torch):
+    """cuBLAS DGEMM (torch.matmul, float64, 8192^3) best of 5 -- the FP64
+    tensor-core denominator (MEASURED_PEAKS.json has no FP64 entry)."""
+    n = 8192
+    a = torch.randn(n, n, dtype=torch.float64, device="cuda")
+    b = torch.randn(n, n, dtype=torch.float64, device="cuda")
+    c = torch.empty_like(a)
+    best = 0.0
+    for _ in range(6):
+        s, e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        s.record()
+        torch.matmul(a, b, out=c)
+        e.record()
+        e.synchronize()
+        best = max(best, 2 * n ** 3 / (s.elapsed_time(e) * 1e-3) / 1e12)
+    del a, b, c
+    torch.cuda.empty_cache()
+    return best
+
+
+def read_traffic_per_flop():
+    p = os.path.join(ROOT, "profiles", "xg_syrk_gemm_kernel.md")
+    if not os.path.exists(p):
+        return None
+    for ln in open(p):
+        if ln.startswith("dram_bytes_per_flop:"):
+            return float(ln.split(":")[1])
+    return None
+
+
+def main():
+    args = parse()
+    if args.impl == "reference":
+        run_reference(args)
+        return
+    import numpy as np
+    import torch
+
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    dist = None
+    if world > 1:
+        import datetime
+
+        import torch.distributed as dist
+
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
+    os.environ.setdefault("EXAGEOSTAT_B200_SILENT", "1")
+    import exageostat_b200 as xg
+    from exageostat_b200 import build as xgbuild
+    from exageostat_b200.synthetic import dlarnv
+
+    if not os.path.exists(xg.LIB_PATH):
+        xgbuild.build()
+    peak = measured_dgemm_tflops(torch)
+    xg.init(args.ts)
+    N = args.n
+    x, y = xg.generate_xy_loc(N, args.seed)
+    e = dlarnv(args.seed, N)
+    sess = xg.Session(x, y, dts=args.ts)
+    sess.zvg(THETA, e)
+    z = sess.z()
+
+    def barrier():
+        if dist is not None:
+            dist.barrier()
+        torch.cuda.synchronize()
+
+    for _ in range(args.warmup):
+        sess.loglik(THETA)
+    sess.set_profiling(True)
+    barrier()
+    clk = ClockSampler(local)
+    clk.start()
+    t0 = time.perf_counter()
+    lls = [sess.loglik(THETA) for _ in range(args.steps)]
+    wall = time.perf_counter() - t0
+    barrier()
+    clocks = clk.stop()
+    prof = sess.profile()
+    sess.set_profiling(False)
+    dev_time = prof["t_gen"] + prof["t_potrf"] + prof["t_trsm"] + prof["t_gemm"]
+    t_max = dev_time
+    if dist is not None:
+        t = torch.tensor([dev_time], device="cuda", dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        t_max = float(t.item())
+    value = world * args.steps / t_max
+
+    # e2e: through the public C ABI from pinned host buffers: upload x, y, z,
+    # MLE_alg, loglik back to the host
+    px = torch.from_numpy(x).pin_memory()
+    py = torch.from_numpy(y).pin_memory()
+    pz = torch.from_numpy(z).pin_memory()
+    e2e_steps = max(1, min(args.steps, 2))
+    barrier()
+    t0 = time.perf_counter()
+    for _ in range(e2e_steps):
+        sess.set_data(px.numpy(), py.numpy(), pz.numpy())
+        ll_e2e = sess.mle_alg(THETA)
+    e2e_wall = time.perf_counter() - t0
+    if dist is not None:
+        t = torch.tensor([e2e_wall], device="cuda", dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        e2e_wall = float(t.item())
+    e2e = {"value": world * e2e_steps / e2e_wall, "unit": UNIT, "h2d_bytes_per_step": 3 * N * 8,
+           "d2h_bytes_per_step": 8 + 5 * 8, "path": "exageostat_b200_set_data + MLE_alg (C ABI), wall clock"}
+
+    launches_per_eval = prof["launches"] / max(prof["evals"], 1)
+    gemm_launches = prof["nt"] - 1
+    achieved = prof["gemm_flops"] / prof["t_gemm"] / 1e12
+    tpf = read_traffic_per_flop()
+    flops_per_launch = prof["gemm_flops"] / max(prof["evals"], 1) / max(gemm_launches, 1)
+    roofline = {"bound": "tensor", "kernel": "xg_syrk_gemm_kernel (FP64 DMMA trailing update)",
+                "achieved": achieved, "peak": peak, "unit": "TFLOP/s", "frac": achieved / peak,
+                "peak_source": "cuBLAS DGEMM 8192^3 measured in this process (of measured)",
+                "traffic": (tpf * flops_per_launch) if tpf else None,
+                "algorithmic_flops_per_launch": flops_per_launch,
+                "share_of_step": prof["t_gemm"] / dev_time,
+                "phases_s_per_eval": {k: prof[k] / prof["evals"] for k in ("t_gen", "t_potrf", "t_trsm", "t_gemm")}}
+    line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": 1e3 * t_max / args.steps, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": {"workload": workload(N), "tile": int(prof["ts"]), "tiles_per_side": int(prof["nt"]),
+                       "parallelism": "replicas" if world > 1 else "single-gpu",
+                       "l2": "inputs larger than L2 (40 GB of covariance tiles per step)",
+                       "loglik": lls[-1], "loglik_e2e": ll_e2e, "wall_s_timed": wall},
+            "roofline": roofline, "e2e": e2e, "clocks": clocks,
+            "gpu_launches": int(round(launches_per_eval * args.steps))}
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        line["cpu_baseline"] = cpu_sample(N, args.cpu_seconds)
+    sess.close()
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    if dist is not None:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

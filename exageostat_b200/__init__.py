@@ -1,0 +1,345 @@
+"""exageostat_b200 -- Python bindings over the C ABI (include/exageostat_b200.h).
+
+The library ``exageostat_b200/lib/libexageostat_b200.so`` is built in-tree by
+``python -m exageostat_b200.build``.  There is no CPU fallback: loading
+raises if the library is missing, and every compute call runs on the GPU.
+
+``MLEData`` / ``Location`` / ``Output`` mirror the reference structures
+(misc/include/MLE_misc.h:111-328) field for field; ``check_abi()`` compares
+their layout with the compiled library.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "lib", "libexageostat_b200.so")
+
+_D = ctypes.c_double
+_I = ctypes.c_int
+_PD = ctypes.POINTER(ctypes.c_double)
+_VP = ctypes.c_void_p
+_CP = ctypes.c_char_p
+
+
+class Location(ctypes.Structure):
+    _fields_ = [("x", _PD), ("y", _PD), ("z", _PD)]
+
+
+_OUTPUT_FIELDS = [
+    ("problem_size", _I), ("computation", _CP), ("kernel", _CP), ("ds_type", _CP), ("precision", _CP),
+    ("z_sample", _I), ("dense_ts", _I), ("lr_ts", _I), ("lr_acc", _I), ("lr_maxrank", _I), ("ncores", _I),
+    ("ngpus", _I), ("p", _I), ("q", _I), ("num_params", _I), ("initial_theta", _PD), ("starting_theta", _PD),
+    ("estimated_theta", _PD), ("final_loglik", _D), ("time_per_iteration", _D), ("cholesky_per_iter", _D),
+    ("flops_per_iteration", _D), ("generation_per_iter", _D), ("solve_per_iter", _D), ("total_mle_time", _D),
+    ("avg_exec_time_gen_stage", _D), ("avg_flops_gen_stage", _D), ("mse_pred1", _D), ("mse_pred2", _D),
+    ("mse_pred3", _D), ("mse_pred", _D), ("trace_pred_sum", _D), ("trace_pred_mean", _D), ("total_pred_time", _D),
+    ("total_pred_flops", _D), ("mloe", _D), ("mmom", _D), ("mloe_exec", _CP), ("total_mloe_mmom_time", _D),
+    ("matrix_gen_mloe_mmom_time", _D), ("cho_fact_mloe_mmom_time", _D), ("loop_mloe_mmom_time", _D),
+    ("total_mloe_mmom_flops", _D), ("fisher_00", _D), ("fisher_11", _D), ("fisher_22", _D), ("fisher_time", _D),
+]
+
+
+class Output(ctypes.Structure):
+    _fields_ = _OUTPUT_FIELDS
+
+
+_MLE_FIELDS = (
+    [("variance", _D), ("variance1", _D), ("variance2", _D), ("variance3", _D), ("computation", _CP),
+     ("c_fun", _CP), ("test", _I), ("async", _I), ("iter_count", _I), ("l1", Location), ("lmiss", Location),
+     ("lobs", Location), ("lm", Location)]
+    + [(n, _VP) for n in ("descC", "descsubC11", "descsubC12", "descsubC21", "descsubC22", "descZ", "descZ1",
+                          "descZ2", "descZ3")]
+    + [("Adense", _PD), ("Adense2", _PD)]
+    + [(n, _VP) for n in ("descZcpy", "descdet", "descsum", "descproduct", "descproduct1", "descproduct2",
+                          "descproduct3", "descZmiss", "descC11", "descC21", "descC12", "descC22", "descZactual",
+                          "descZobs", "descmse", "descmse1", "descmse2", "descmse3", "descZtrace", "sequence",
+                          "request")]
+    + [("verbose", _I), ("check", _I), ("log", _I)]
+    + [(n, _D) for n in ("avg_exec_time_per_iter", "total_exec_time", "avg_flops_per_iter",
+                         "avg_generation_per_iter", "avg_solve_per_iter", "avg_cholesky_per_iter",
+                         "avg_exec_time_gen_stage", "avg_flops_gen_stage", "final_loglik")]
+    + [(n, _CP) for n in ("locsFPath", "timeFPath", "obsFPath", "obsFPath2", "obsFPath3", "actualZFPath",
+                          "actualZFPath2", "actualZFPath3", "actualZLocFPath", "actualTimeFPath")]
+    + [(n, _D) for n in ("det", "sum", "dotp", "dotp1", "dotp2", "dotp3")]
+    + [("sdotp", ctypes.c_float)]
+    + [(n, _D) for n in ("mserror", "mserror1", "mserror2", "mserror3")]
+    + [("dm", _CP), ("diag_thick", _I), ("nFileLog", _CP), ("pFileLog", _VP), ("hicma_maxrank", _I),
+       ("hicma_data_type", _I)]
+    + [(n, _VP) for n in ("hicma_descC", "hicma_descZ", "hicma_descCD", "hicma_descCUV", "hicma_descCrk",
+                          "hicma_descZcpy", "hicma_descdet", "hicma_descproduct", "hicma_descC12D",
+                          "hicma_descC12UV", "hicma_descC12rk", "hicma_descC22D", "hicma_descC22UV",
+                          "hicma_descC22rk")]
+    + [("hicma_acc", _D), ("hsequence", _VP), ("hrequest", _VP), ("opt_tol", _I), ("opt_max_iters", _I),
+       ("ooc", _I), ("kernel_fun", _CP), ("precision", _I)]
+    + [(n, _VP) for n in ("desctemp", "desctemp22", "desck_t", "desck_a", "desck_ttmp", "desck_atmp", "descK_t",
+                          "descK_a", "descexpr1", "descexpr2", "descexpr3", "descexpr4", "descestimatedalpha",
+                          "desctruthalpha", "desc_mloe_mmom", "descmloe", "descmmom")]
+    + [(n, _D) for n in ("expr1", "expr2", "expr3", "expr4", "mloe", "mmom")]
+    + [("mloe_mmom", _I), ("mloe_mmom_async", _I), ("mspe", _I), ("recovery_file", _CP),
+       ("checkpoint_file", _CP), ("time_slots", _I), ("idw", _I), ("fisher", _I), ("descr", _VP),
+       ("descrcpy", _VP), ("seed", _I)]
+)
+
+
+class MLEData(ctypes.Structure):
+    _fields_ = _MLE_FIELDS
+
+
+# error codes (include/exageostat_b200.h)
+XG_OK, XG_ERR_NOT_INITIALIZED, XG_ERR_BAD_ARGUMENT, XG_ERR_CUDA, XG_ERR_NOT_SPD, XG_ERR_TIMEOUT, \
+    XG_ERR_UNSUPPORTED, XG_ERR_NO_MEMORY = range(8)
+
+EXPORTED_SYMBOLS = [
+    "exageostat_init", "EXAGEOSTAT_init", "exageostat_finalize", "EXAGEOSTAT_dmle_Call", "MORSE_dmle_Call",
+    "MLE_zvg", "MLE_alg", "EXAGEOSTAT_dmle_Tile", "MORSE_dmle_Tile", "MLE_get_zobs", "prediction_init",
+    "EXAGEOSTAT_dmle_Predict_Allocate", "EXAGEOSTAT_dmle_Predict_Tile", "MORSE_dmle_Predict_Tile",
+    "prediction_finalize", "MLE_Finalize", "GenerateXYLoc", "uniform_distribution", "shuffle",
+    "locations_obs_zsort_inplace", "pick_random_points", "exageostat_b200_loglik", "exageostat_last_error",
+    "exageostat_b200_abi_version", "exageostat_b200_sizeof_MLE_data", "exageostat_b200_sizeof_output",
+    "exageostat_b200_offsetof_MLE_data", "exageostat_b200_dmle_host", "exageostat_b200_bessel_knu",
+    "exageostat_b200_matern_pairs", "exageostat_b200_covariance_dense", "exageostat_b200_set_data",
+    "exageostat_b200_set_profiling", "exageostat_b200_get_profile", "results",
+]
+
+_lib = None
+
+
+class XgError(RuntimeError):
+    def __init__(self, code: int, msg: str):
+        super().__init__("exageostat_b200 error %d: %s" % (code, msg))
+        self.code = code
+
+
+def lib():
+    """Load the compiled library (raises if it has not been built)."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(LIB_PATH):
+        raise RuntimeError("%s is missing: build it with `python -m exageostat_b200.build` "
+                           "(there is no CPU fallback)" % LIB_PATH)
+    L = ctypes.CDLL(LIB_PATH)
+    PM = ctypes.POINTER(MLEData)
+    sig = {
+        "exageostat_init": (None, [ctypes.POINTER(_I)] * 4),
+        "exageostat_finalize": (None, []),
+        "EXAGEOSTAT_dmle_Call": (None, [PM, _I, _I, _I, _I, _I, _I, _I, _I]),
+        "MLE_zvg": (None, [PM, _PD, _PD, _I, _I, _I, _I, _I]),
+        "MLE_alg": (_D, [ctypes.c_uint, _PD, _PD, _VP]),
+        "EXAGEOSTAT_dmle_Tile": (_D, [ctypes.c_uint, _PD, _PD, _VP]),
+        "MLE_get_zobs": (None, [PM, _PD, _I]),
+        "prediction_init": (None, [PM, _I, _I, _I, _I, _I, _I]),
+        "EXAGEOSTAT_dmle_Predict_Tile": (_D, [PM, _PD, _I, _I, _PD, _PD, _PD, _I]),
+        "prediction_finalize": (None, [PM]),
+        "MLE_Finalize": (None, [PM]),
+        "GenerateXYLoc": (ctypes.POINTER(Location), [_I, _I]),
+        "uniform_distribution": (_D, [_D, _D]),
+        "locations_obs_zsort_inplace": (_I, [_I, ctypes.POINTER(Location), _PD]),
+        "pick_random_points": (None, [PM, _PD, _PD, _I, _I, _I]),
+        "exageostat_b200_loglik": (_I, [PM, _PD, _PD, _PD]),
+        "exageostat_last_error": (_CP, []),
+        "exageostat_b200_abi_version": (_I, []),
+        "exageostat_b200_sizeof_MLE_data": (ctypes.c_size_t, []),
+        "exageostat_b200_sizeof_output": (ctypes.c_size_t, []),
+        "exageostat_b200_offsetof_MLE_data": (ctypes.c_long, [_CP]),
+        "exageostat_b200_dmle_host": (_I, [_I, _PD, _PD, _PD, _PD, _I, _I, _I, _PD]),
+        "exageostat_b200_bessel_knu": (_I, [_I, _PD, _PD, _PD]),
+        "exageostat_b200_matern_pairs": (_I, [_I, _PD, _PD, _PD, _PD, _PD, _I, _I, _PD]),
+        "exageostat_b200_covariance_dense": (_I, [_I, _PD, _PD, _PD, _I, _I, _I, _I, _PD]),
+        "exageostat_b200_set_data": (_I, [PM, _PD, _PD, _PD]),
+        "exageostat_b200_set_profiling": (_I, [PM, _I]),
+        "exageostat_b200_get_profile": (_I, [PM, _PD, _I]),
+    }
+    for name, (res, args) in sig.items():
+        f = getattr(L, name)
+        f.restype = res
+        f.argtypes = args
+    _lib = L
+    return L
+
+
+def _p(a: np.ndarray):
+    return a.ctypes.data_as(_PD)
+
+
+def _f64(a) -> np.ndarray:
+    return np.ascontiguousarray(a, dtype=np.float64)
+
+
+def last_error() -> str:
+    return lib().exageostat_last_error().decode()
+
+
+def _check(rc: int):
+    if rc != XG_OK:
+        raise XgError(rc, last_error())
+
+
+def check_abi() -> None:
+    """Raise if the ctypes mirrors disagree with the compiled structures."""
+    L = lib()
+    if L.exageostat_b200_sizeof_MLE_data() != ctypes.sizeof(MLEData):
+        raise RuntimeError("sizeof(MLE_data) %d != ctypes %d" % (L.exageostat_b200_sizeof_MLE_data(),
+                                                                 ctypes.sizeof(MLEData)))
+    if L.exageostat_b200_sizeof_output() != ctypes.sizeof(Output):
+        raise RuntimeError("sizeof(output) mismatch")
+    for name, _ in _MLE_FIELDS:
+        off = L.exageostat_b200_offsetof_MLE_data(name.encode())
+        if off >= 0 and off != getattr(MLEData, name).offset:
+            raise RuntimeError("offsetof(MLE_data, %s) %d != ctypes %d" % (name, off, getattr(MLEData, name).offset))
+
+
+def init(dts: int = 0) -> None:
+    """exageostat_init(ncores=1, gpus=1, dts, lts=0)."""
+    a, b, c, d = _I(1), _I(1), _I(int(dts)), _I(0)
+    lib().exageostat_init(ctypes.byref(a), ctypes.byref(b), ctypes.byref(c), ctypes.byref(d))
+
+
+def finalize() -> None:
+    lib().exageostat_finalize()
+
+
+KERNELS = {0: b"univariate_matern_stationary", 1: b"univariate_matern_nuggets_stationary"}
+
+
+def bessel_knu(nu, x) -> np.ndarray:
+    nu, x = _f64(nu), _f64(x)
+    nu, x = np.broadcast_arrays(nu, x)
+    nu, x = _f64(nu), _f64(x)
+    out = np.empty(x.size)
+    _check(lib().exageostat_b200_bessel_knu(x.size, _p(nu), _p(x), _p(out)))
+    return out
+
+
+def matern_pairs(x1, y1, x2, y2, theta, kernel=0, metric=0) -> np.ndarray:
+    a = [_f64(v) for v in (x1, y1, x2, y2)]
+    out = np.empty(a[0].size)
+    _check(lib().exageostat_b200_matern_pairs(a[0].size, *[_p(v) for v in a], _p(_f64(theta)), kernel, metric,
+                                              _p(out)))
+    return out
+
+
+def covariance_dense(x, y, theta, kernel=0, metric=0, ts=0, factor=False) -> np.ndarray:
+    x, y = _f64(x), _f64(y)
+    n = x.size
+    out = np.empty((n, n))
+    _check(lib().exageostat_b200_covariance_dense(n, _p(x), _p(y), _p(_f64(theta)), kernel, metric, ts,
+                                                  1 if factor else 0, _p(out)))
+    return out
+
+
+def dmle_host(x, y, z, theta, kernel=0, metric=0, ts=0):
+    """One-shot log-likelihood on host arrays: (loglik, logdet, dotp)."""
+    x, y, z = _f64(x), _f64(y), _f64(z)
+    out = np.empty(3)
+    _check(lib().exageostat_b200_dmle_host(x.size, _p(x), _p(y), _p(z), _p(_f64(theta)), kernel, metric, ts,
+                                           _p(out)))
+    return tuple(out)
+
+
+class Session:
+    """One MLE_data driven through the reference entry points, as the
+    reference driver (examples/synthetic_dmle_test.c) does."""
+
+    def __init__(self, x, y, kernel: int = 0, dm: str = "ed", dts: int = 0, precision: int = 0,
+                 diag_thick: int = 1):
+        self.L = lib()
+        self.x, self.y = _f64(x).copy(), _f64(y).copy()
+        self.N = self.x.size
+        self.kernel = kernel
+        self.nparams = 4 if kernel == 1 else 3
+        d = MLEData()
+        d.computation = b"exact"
+        d.kernel_fun = KERNELS[kernel]
+        d.dm = dm.encode()
+        d.precision = precision
+        d.diag_thick = diag_thick
+        d.recovery_file = b""
+        d.checkpoint_file = b""
+        d.l1.x = _p(self.x)
+        d.l1.y = _p(self.y)
+        self._keep = []
+        self.data = d
+        self.L.EXAGEOSTAT_dmle_Call(ctypes.byref(d), 1, 1, dts, 1, 1, self.N, self.N, 0)
+        if not d.descC:
+            raise XgError(XG_ERR_CUDA, last_error())
+
+    def zvg(self, theta0, nrand) -> None:
+        t = _f64(theta0)
+        e = _f64(nrand)
+        self.L.MLE_zvg(ctypes.byref(self.data), _p(e), _p(t), self.N, 0, 0, 1, 1)
+
+    def z(self) -> np.ndarray:
+        out = np.empty(self.N)
+        self.L.MLE_get_zobs(ctypes.byref(self.data), _p(out), self.N)
+        return out
+
+    def loglik(self, theta, grad: bool = False):
+        t = _f64(theta)
+        ll = _D()
+        g = np.empty(self.nparams) if grad else None
+        _check(self.L.exageostat_b200_loglik(ctypes.byref(self.data), _p(t), ctypes.byref(ll),
+                                             _p(g) if grad else None))
+        return (ll.value, g) if grad else ll.value
+
+    def mle_alg(self, theta) -> float:
+        t = _f64(theta)
+        return self.L.MLE_alg(self.nparams, _p(t), None, ctypes.cast(ctypes.byref(self.data), _VP))
+
+    def predict(self, theta, x_miss, y_miss, x_obs, y_obs, z_obs, z_actual=None):
+        """EXAGEOSTAT_dmle_Predict_Tile: returns (mse, zmiss)."""
+        xm, ym, xo, yo, zo = (_f64(a).copy() for a in (x_miss, y_miss, x_obs, y_obs, z_obs))
+        za = None if z_actual is None else _f64(z_actual).copy()
+        self._keep = [xm, ym, xo, yo]
+        d = self.data
+        d.lmiss.x, d.lmiss.y = _p(xm), _p(ym)
+        d.lobs.x, d.lobs.y = _p(xo), _p(yo)
+        zmiss = np.empty(xm.size)
+        t = _f64(theta)
+        mse = self.L.EXAGEOSTAT_dmle_Predict_Tile(ctypes.byref(d), _p(t), xm.size, xo.size, _p(zo),
+                                                  None if za is None else _p(za), _p(zmiss), self.N)
+        return mse, zmiss
+
+    def set_data(self, x=None, y=None, z=None) -> None:
+        arrs = [None if a is None else _f64(a) for a in (x, y, z)]
+        _check(self.L.exageostat_b200_set_data(ctypes.byref(self.data),
+                                               *[None if a is None else _p(a) for a in arrs]))
+
+    def set_profiling(self, on: bool = True) -> None:
+        _check(self.L.exageostat_b200_set_profiling(ctypes.byref(self.data), 1 if on else 0))
+
+    def profile(self) -> dict:
+        out = np.zeros(10)
+        _check(self.L.exageostat_b200_get_profile(ctypes.byref(self.data), _p(out), 10))
+        keys = ["t_gen", "t_potrf", "t_trsm", "t_gemm", "gemm_flops", "launches", "evals", "ts", "nt", "N"]
+        return dict(zip(keys, out.tolist()))
+
+    def close(self) -> None:
+        if self.data.descC22:
+            self.L.prediction_finalize(ctypes.byref(self.data))
+        if self.data.descC:
+            self.L.MLE_Finalize(ctypes.byref(self.data))
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+
+def generate_xy_loc(n: int, seed: int):
+    """GenerateXYLoc through the library (host code; consumes libc rand())."""
+    L = lib()
+    p = L.GenerateXYLoc(int(n), int(seed))
+    x = np.ctypeslib.as_array(p.contents.x, shape=(n,)).copy()
+    y = np.ctypeslib.as_array(p.contents.y, shape=(n,)).copy()
+    libc = ctypes.CDLL(None)
+    libc.free.argtypes = [_VP]
+    libc.free(ctypes.cast(p.contents.x, _VP))
+    libc.free(ctypes.cast(p.contents.y, _VP))
+    libc.free(ctypes.cast(p, _VP))
+    return x, y

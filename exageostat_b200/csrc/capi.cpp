@@ -1,0 +1,499 @@
+/*
+ * The reference's C API (include/exageostat_b200.h) on top of the engine.
+ *
+ * Argument meaning, side effects on MLE_data / results and the per-iterate
+ * log line follow the cited reference functions; where the reference calls
+ * exit() this layer returns an error value instead.
+ */
+#include <math.h>
+#include <stddef.h>
+#include <stdio.h>
+#include <stdlib.h>
+#include <string.h>
+
+#include "../../include/exageostat_b200.h"
+#include "xg_engine.h"
+
+/* misc/include/MLE_misc.h:350 / examples/examples.c:24 */
+__attribute__((weak)) output results;
+
+static bool xg_quiet()
+{
+    const char *s = getenv("EXAGEOSTAT_B200_SILENT");
+    return s && *s && strcmp(s, "0") != 0;
+}
+
+/* kernel_fun -> (kernel id, number of parameters); the exact path of this
+ * library covers the two univariate stationary Matern kernels
+ * (MLE_dexact.c:272-298 lists the reference's set). */
+static int xg_kernel_of(const MLE_data *data, int *kernel, int *nparams)
+{
+    const char *k = data->kernel_fun ? data->kernel_fun : "univariate_matern_stationary";
+    if (strcmp(k, "univariate_matern_stationary") == 0) {
+        *kernel = 0;
+        *nparams = 3;
+        return XG_OK;
+    }
+    if (strcmp(k, "univariate_matern_nuggets_stationary") == 0) {
+        *kernel = 1;
+        *nparams = 4;
+        return XG_OK;
+    }
+    return xg_fail(XG_ERR_UNSUPPORTED, "kernel_fun \"%s\" is not supported (univariate_matern_stationary and "
+                                       "univariate_matern_nuggets_stationary are)", k);
+}
+
+static int xg_metric_of(const MLE_data *data)
+{
+    return (data->dm && (strcmp(data->dm, "gc") == 0 || strcmp(data->dm, "gcd") == 0)) ? 1 : 0;
+}
+
+static bool xg_is_exact(const MLE_data *data)
+{
+    return data->computation == NULL || strcmp(data->computation, "exact") == 0;
+}
+
+/* ------------------------------------------------------------------------- */
+/* init / finalize                                                           */
+/* ------------------------------------------------------------------------- */
+
+extern "C" void exageostat_init(int *ncores, int *gpus, int *dts, int *lts)
+{
+    (void)ncores;
+    (void)lts;
+    if (g_xg.initialized) {
+        printf("Another instance of Chameleon is already running...!");
+        return;
+    }
+    if (gpus && *gpus > 1) fprintf(stderr, "exageostat_b200: one GPU per field; using the current device only\n");
+    int rc = xg_context_start(dts ? *dts : 0);
+    if (rc) fprintf(stderr, "exageostat_b200: init failed: %s\n", exageostat_last_error());
+}
+
+extern "C" void EXAGEOSTAT_init(int *ncores, int *gpus, int *dts, int *lts) { exageostat_init(ncores, gpus, dts, lts); }
+
+extern "C" void exageostat_finalize(void)
+{
+    if (!g_xg.initialized) {
+        printf("No active instance oh Chameleon...please use exageostat_init() function to initiate a new instance!\n");
+        return;
+    }
+    cudaStreamSynchronize(g_xg.stream);
+    cudaStreamDestroy(g_xg.stream);
+    g_xg.stream = nullptr;
+    g_xg.initialized = false;
+}
+
+/* ------------------------------------------------------------------------- */
+/* descriptors                                                               */
+/* ------------------------------------------------------------------------- */
+
+static XgField *xg_field_of(MLE_data *data) { return data ? (XgField *)data->descC : nullptr; }
+
+extern "C" void EXAGEOSTAT_dmle_Call(MLE_data *data, int ncores, int gpus, int dts, int p_grid, int q_grid, int N,
+                                     int nZobs, int nZmiss)
+{
+    (void)ncores;
+    (void)gpus;
+    (void)p_grid;
+    (void)q_grid;
+    (void)nZobs;
+    (void)nZmiss;
+    int kernel = 0, np = 0;
+    if (xg_kernel_of(data, &kernel, &np)) {
+        fprintf(stderr, "EXAGEOSTAT_dmle_Call: %s\n", exageostat_last_error());
+        return;
+    }
+    if (data->descC) MLE_Finalize(data);
+    XgField *f = nullptr;
+    const int ts = dts > 0 ? dts : g_xg.dts;
+    if (xg_field_create(&f, N, ts, data->l1.x, data->l1.y, kernel, xg_metric_of(data))) {
+        fprintf(stderr, "EXAGEOSTAT_dmle_Call: %s\n", exageostat_last_error());
+        return;
+    }
+    data->descC = f;
+    data->descZ = f;
+    data->descZcpy = f;
+    data->descdet = &data->det;
+    data->descproduct = &data->dotp;
+    data->sequence = NULL;
+    data->request = NULL;
+}
+
+extern "C" void MORSE_dmle_Call(MLE_data *data, int ncores, int gpus, int dts, int p_grid, int q_grid, int N,
+                                int nZobs, int nZmiss)
+{
+    EXAGEOSTAT_dmle_Call(data, ncores, gpus, dts, p_grid, q_grid, N, nZobs, nZmiss);
+}
+
+extern "C" void MLE_Finalize(MLE_data *data)
+{
+    if (!data) return;
+    XgField *f = xg_field_of(data);
+    if (f) xg_field_destroy(f);
+    data->descC = data->descZ = data->descZcpy = NULL;
+    data->descdet = data->descproduct = NULL;
+}
+
+/* ------------------------------------------------------------------------- */
+/* synthetic z                                                               */
+/* ------------------------------------------------------------------------- */
+
+extern "C" void MLE_zvg(MLE_data *data, double *Nrand, double *initial_theta, int n, int ts, int log, int p_grid,
+                        int q_grid)
+{
+    (void)ts;
+    (void)log;
+    (void)p_grid;
+    (void)q_grid;
+    data->iter_count = 0;
+    XgField *f = xg_field_of(data);
+    if (!f) {
+        xg_fail(XG_ERR_NOT_INITIALIZED, "MLE_zvg before EXAGEOSTAT_dmle_Call");
+        fprintf(stderr, "MLE_zvg: %s\n", exageostat_last_error());
+        return;
+    }
+    if (!xg_is_exact(data) || (data->precision != 0 && data->precision != 2)) {
+        xg_fail(XG_ERR_UNSUPPORTED, "MLE_zvg: computation=%s precision=%d", data->computation, data->precision);
+        fprintf(stderr, "%s\n", exageostat_last_error());
+        return;
+    }
+    if (n != f->N) {
+        xg_fail(XG_ERR_BAD_ARGUMENT, "MLE_zvg: n = %d but the descriptors hold N = %d", n, f->N);
+        fprintf(stderr, "%s\n", exageostat_last_error());
+        return;
+    }
+    double times[2] = {0, 0};
+    if (xg_field_zvg(f, initial_theta, Nrand, times)) {
+        fprintf(stderr, "MLE_zvg: %s\n", exageostat_last_error());
+        return;
+    }
+    data->avg_exec_time_gen_stage = times[1];
+    const double flops = (double)n * n * n / 3.0;
+    data->avg_flops_gen_stage = times[1] > 0 ? flops / 1e9 / times[1] : 0.0;
+}
+
+extern "C" void MLE_get_zobs(MLE_data *data, double *z, int n)
+{
+    XgField *f = xg_field_of(data);
+    if (!f || xg_field_get_z(f, z, n)) fprintf(stderr, "MLE_get_zobs: %s\n", exageostat_last_error());
+}
+
+/* ------------------------------------------------------------------------- */
+/* the likelihood                                                            */
+/* ------------------------------------------------------------------------- */
+
+/* recover(), misc/compute/MLE_misc.c:2037-2074: a line "iter theta... loglik"
+ * of the recovery file replays that iteration's value. */
+static bool xg_recover(const char *path, int iter, int np, double *loglik)
+{
+    FILE *fp = fopen(path, "r");
+    if (!fp) return false;
+    char line[4096];
+    bool found = false;
+    while (fgets(line, sizeof line, fp)) {
+        char *save = NULL;
+        char *tok = strtok_r(line, " \n", &save);
+        if (!tok || atoi(tok) != iter) continue;
+        int i = 0;
+        for (; i < np && (tok = strtok_r(NULL, " \n", &save)); ++i) {
+        }
+        tok = strtok_r(NULL, " \n", &save);
+        if (i == np && tok) {
+            *loglik = atof(tok);
+            found = true;
+        }
+        break;
+    }
+    fclose(fp);
+    return found;
+}
+
+/* checkpointing(), misc/compute/MLE_misc.c:2014-2035 */
+static void xg_checkpoint(const char *path, int iter, const double *theta, int np, double loglik)
+{
+    FILE *fp = fopen(path, "a");
+    if (!fp) return;
+    fprintf(fp, "%d ", iter);
+    for (int i = 0; i < np; ++i) fprintf(fp, "%.17g ", theta[i]);
+    fprintf(fp, "%.17g \n", loglik);
+    fclose(fp);
+}
+
+extern "C" int exageostat_b200_loglik(MLE_data *data, const double *theta, double *loglik, double *grad)
+{
+    XgField *f = xg_field_of(data);
+    if (!f) return xg_fail(XG_ERR_NOT_INITIALIZED, "no descriptors: call EXAGEOSTAT_dmle_Call first");
+    int kernel = 0, np = 0;
+    int rc = xg_kernel_of(data, &kernel, &np);
+    if (rc) return rc;
+    if (!xg_is_exact(data)) return xg_fail(XG_ERR_UNSUPPORTED, "computation \"%s\"", data->computation);
+    if (data->precision != 0) return xg_fail(XG_ERR_UNSUPPORTED, "precision %d", data->precision);
+    double res[3], times[2];
+    data->det = 0;
+    data->dotp = 0;
+    double t_gen = 0, t_fact = 0;
+    if (data->recovery_file && data->recovery_file[0] &&
+        xg_recover(data->recovery_file, data->iter_count, np, loglik)) {
+        rc = XG_OK;
+    } else {
+        rc = xg_field_loglik(f, theta, res, times);
+        if (rc == XG_OK) {
+            *loglik = res[0];
+            data->det = 0.5 * res[1];
+            data->dotp = res[2];
+            t_gen = times[0];
+            t_fact = times[1];
+        }
+    }
+    if (rc == XG_OK && grad) {
+        for (int i = 0; i < np; ++i) grad[i] = NAN;
+        rc = xg_fail(XG_ERR_UNSUPPORTED, "the gradient is not available in this build");
+    }
+    if (rc != XG_OK && rc != XG_ERR_UNSUPPORTED) *loglik = -INFINITY;
+    /* per-iterate record, MLE_dexact.c:441-488 */
+    if (!xg_quiet()) {
+        fprintf(stderr, " %3d- Model Parameters (", data->iter_count + 1);
+        for (int i = 0; i < np; ++i) fprintf(stderr, "%.8f%s", theta[i], i < np - 1 ? "," : "");
+        fprintf(stderr, ")----> LogLi: %.18f\n", *loglik);
+        fprintf(stderr, " ---- Facto Time: %6.2f\n", t_fact);
+        fprintf(stderr, " ---- Matrix Generation Time: %6.2f\n", t_gen);
+        fprintf(stderr, " ---- Total Time: %6.2f\n", t_gen + t_fact);
+    }
+    if (data->log == 1 && data->pFileLog) {
+        fprintf(data->pFileLog, " %3d- Model Parameters (", data->iter_count + 1);
+        for (int i = 0; i < np; ++i) fprintf(data->pFileLog, "%.8f, ", theta[i]);
+        fprintf(data->pFileLog, ")----> LogLi: %.18f\n", *loglik);
+    }
+    if (data->checkpoint_file && data->checkpoint_file[0])
+        xg_checkpoint(data->checkpoint_file, data->iter_count, theta, np, *loglik);
+    if (results.estimated_theta)
+        for (int i = 0; i < np; ++i) results.estimated_theta[i] = theta[i];
+    data->iter_count++;
+    const double n = f->N;
+    data->avg_exec_time_per_iter += t_fact;
+    if (t_fact > 0) data->avg_flops_per_iter += (n * n * n / 3.0 + n * n) / 1e9 / t_fact;
+    data->avg_generation_per_iter += t_gen;
+    data->avg_cholesky_per_iter += t_fact;
+    data->final_loglik = *loglik;
+    data->variance = theta[0];
+    results.final_loglik = *loglik;
+    return rc;
+}
+
+extern "C" double EXAGEOSTAT_dmle_Tile(unsigned n, const double *theta, double *grad, void *vdata)
+{
+    (void)n;
+    double ll = -INFINITY;
+    int rc = exageostat_b200_loglik((MLE_data *)vdata, theta, &ll, grad);
+    if (rc && rc != XG_ERR_NOT_SPD) fprintf(stderr, "EXAGEOSTAT_dmle_Tile: %s\n", exageostat_last_error());
+    return ll;
+}
+
+extern "C" double MORSE_dmle_Tile(unsigned n, const double *theta, double *grad, void *data)
+{
+    return EXAGEOSTAT_dmle_Tile(n, theta, grad, data);
+}
+
+extern "C" double MLE_alg(unsigned n, const double *theta, double *grad, void *vdata)
+{
+    MLE_data *data = (MLE_data *)vdata;
+    if (!xg_is_exact(data)) {
+        fprintf(stderr, "MLE_alg: computation \"%s\" is not provided by this library\n", data->computation);
+        return 0;
+    }
+    if (data->precision == 0) return EXAGEOSTAT_dmle_Tile(n, theta, grad, vdata);
+    fprintf(stderr, "MLE_alg: precision %d is not provided by this build\n", data->precision);
+    return 0;
+}
+
+/* ------------------------------------------------------------------------- */
+/* prediction                                                                */
+/* ------------------------------------------------------------------------- */
+
+extern "C" void EXAGEOSTAT_dmle_Predict_Allocate(MLE_data *data, int nZmiss, int nZobs, int dts, int p_grid,
+                                                 int q_grid, int mse_flag)
+{
+    (void)p_grid;
+    (void)q_grid;
+    if (nZmiss <= 0) {
+        fprintf(stderr, " Number of missing values should be positive value\n");
+        return;
+    }
+    if (data->descC22) prediction_finalize(data);
+    XgPredict *q = nullptr;
+    if (xg_predict_create(&q, nZmiss, nZobs, dts > 0 ? dts : g_xg.dts)) {
+        fprintf(stderr, "EXAGEOSTAT_dmle_Predict_Allocate: %s\n", exageostat_last_error());
+        return;
+    }
+    q->mse_flag = mse_flag;
+    data->descC22 = q;
+    data->descC12 = q;
+    data->descZobs = q;
+    data->descZmiss = q;
+    data->descZactual = q;
+    data->descmse = &data->mserror;
+}
+
+extern "C" void prediction_init(MLE_data *data, int nZmiss, int nZobs, int ts, int p_grid, int q_grid, int mse_flag)
+{
+    if (data->precision == 0 || data->precision == 2)
+        EXAGEOSTAT_dmle_Predict_Allocate(data, nZmiss, nZobs, ts, p_grid, q_grid, mse_flag);
+}
+
+extern "C" double EXAGEOSTAT_dmle_Predict_Tile(MLE_data *data, double *theta, int nZmiss, int nZobs, double *Zobs,
+                                               double *Zactual, double *Zmiss, int n)
+{
+    (void)n;
+    data->mserror = 0;
+    if (nZmiss <= 0) {
+        fprintf(stderr, " Number of missing values should be positive value\n");
+        return -1;
+    }
+    int kernel = 0, np = 0;
+    if (xg_kernel_of(data, &kernel, &np)) {
+        fprintf(stderr, "EXAGEOSTAT_dmle_Predict_Tile: %s\n", exageostat_last_error());
+        return -1;
+    }
+    XgPredict *q = (XgPredict *)data->descC22;
+    if (!q || q->nmiss != nZmiss || q->nobs != nZobs) {
+        if (q) prediction_finalize(data);
+        EXAGEOSTAT_dmle_Predict_Allocate(data, nZmiss, nZobs, 0, 1, 1, Zactual != NULL);
+        q = (XgPredict *)data->descC22;
+        if (!q) return -1;
+    }
+    if (!xg_quiet()) {
+        printf("estimated parameters:");
+        for (int i = 0; i < np; ++i) printf("%.8f,", theta[i]);
+        printf(")\n");
+    }
+    double mse = -1;
+    const double t0 = 0;
+    int rc = xg_predict_run(q, theta, kernel, xg_metric_of(data), data->lmiss.x, data->lmiss.y, data->lobs.x,
+                            data->lobs.y, Zobs, Zactual, Zmiss, &mse);
+    (void)t0;
+    if (rc) {
+        fprintf(stderr, "EXAGEOSTAT_dmle_Predict_Tile: %s\n", exageostat_last_error());
+        data->mserror = rc == XG_ERR_NOT_SPD ? -2 : -1;
+        return data->mserror;
+    }
+    data->mserror = mse;
+    results.mse_pred = mse;
+    return mse;
+}
+
+extern "C" double MORSE_dmle_Predict_Tile(MLE_data *data, double *theta, int nZmiss, int nZobs, double *Zobs,
+                                          double *Zactual, double *Zmiss, int n)
+{
+    return EXAGEOSTAT_dmle_Predict_Tile(data, theta, nZmiss, nZobs, Zobs, Zactual, Zmiss, n);
+}
+
+extern "C" void prediction_finalize(MLE_data *data)
+{
+    XgPredict *q = (XgPredict *)data->descC22;
+    if (q) xg_predict_destroy(q);
+    data->descC22 = data->descC12 = data->descZobs = data->descZmiss = data->descZactual = NULL;
+    data->descmse = NULL;
+}
+
+/* ------------------------------------------------------------------------- */
+/* one-shot and diagnostic entry points                                      */
+/* ------------------------------------------------------------------------- */
+
+extern "C" int exageostat_b200_dmle_host(int n, const double *x, const double *y, const double *z,
+                                         const double *theta, int kernel, int metric, int ts, double *out)
+{
+    if (kernel != 0 && kernel != 1) return xg_fail(XG_ERR_BAD_ARGUMENT, "kernel %d", kernel);
+    XgField *f = nullptr;
+    int rc = xg_field_create(&f, n, ts, x, y, kernel, metric);
+    if (rc) return rc;
+    rc = xg_field_set_z(f, z);
+    double res[3];
+    if (!rc) rc = xg_field_loglik(f, theta, res, nullptr);
+    if (!rc) memcpy(out, res, sizeof res);
+    xg_field_destroy(f);
+    return rc;
+}
+
+extern "C" int exageostat_b200_bessel_knu(int n, const double *nu, const double *x, double *out)
+{
+    return xg_bessel_knu_host(n, nu, x, out);
+}
+
+extern "C" int exageostat_b200_matern_pairs(int n, const double *x1, const double *y1, const double *x2,
+                                            const double *y2, const double *theta, int kernel, int metric,
+                                            double *out)
+{
+    return xg_matern_pairs_host(n, x1, y1, x2, y2, theta, kernel, metric, out);
+}
+
+extern "C" int exageostat_b200_covariance_dense(int n, const double *x, const double *y, const double *theta,
+                                                int kernel, int metric, int ts, int factor, double *out)
+{
+    return xg_covariance_dense(n, x, y, theta, kernel, metric, ts, factor, out);
+}
+
+extern "C" int exageostat_b200_set_data(MLE_data *data, const double *x, const double *y, const double *z)
+{
+    XgField *f = xg_field_of(data);
+    if (!f) return xg_fail(XG_ERR_NOT_INITIALIZED, "no descriptors: call EXAGEOSTAT_dmle_Call first");
+    return xg_field_set_data(f, x, y, z);
+}
+
+extern "C" int exageostat_b200_set_profiling(MLE_data *data, int on)
+{
+    XgField *f = xg_field_of(data);
+    if (!f) return xg_fail(XG_ERR_NOT_INITIALIZED, "no descriptors: call EXAGEOSTAT_dmle_Call first");
+    return xg_field_set_profiling(f, on);
+}
+
+extern "C" int exageostat_b200_get_profile(MLE_data *data, double *out, int n)
+{
+    XgField *f = xg_field_of(data);
+    if (!f) return xg_fail(XG_ERR_NOT_INITIALIZED, "no descriptors: call EXAGEOSTAT_dmle_Call first");
+    double info[10] = {f->prof[0], f->prof[1], f->prof[2], f->prof[3], f->prof[4], f->prof[5], f->prof[6],
+                       (double)f->C.ts, (double)f->C.nt, (double)f->N};
+    for (int i = 0; i < n && i < 10; ++i) out[i] = info[i];
+    return XG_OK;
+}
+
+extern "C" int exageostat_b200_abi_version(void) { return 1; }
+extern "C" size_t exageostat_b200_sizeof_MLE_data(void) { return sizeof(MLE_data); }
+extern "C" size_t exageostat_b200_sizeof_output(void) { return sizeof(output); }
+
+extern "C" long exageostat_b200_offsetof_MLE_data(const char *field)
+{
+#define XG_OFF(name)                                                                                                   \
+    if (strcmp(field, #name) == 0) return (long)offsetof(MLE_data, name)
+    XG_OFF(variance);
+    XG_OFF(computation);
+    XG_OFF(iter_count);
+    XG_OFF(l1);
+    XG_OFF(lmiss);
+    XG_OFF(lobs);
+    XG_OFF(descC);
+    XG_OFF(descZcpy);
+    XG_OFF(descC22);
+    XG_OFF(verbose);
+    XG_OFF(log);
+    XG_OFF(avg_exec_time_per_iter);
+    XG_OFF(final_loglik);
+    XG_OFF(det);
+    XG_OFF(dotp);
+    XG_OFF(sdotp);
+    XG_OFF(mserror);
+    XG_OFF(dm);
+    XG_OFF(diag_thick);
+    XG_OFF(pFileLog);
+    XG_OFF(hicma_acc);
+    XG_OFF(opt_tol);
+    XG_OFF(kernel_fun);
+    XG_OFF(precision);
+    XG_OFF(expr1);
+    XG_OFF(mloe_mmom);
+    XG_OFF(recovery_file);
+    XG_OFF(checkpoint_file);
+    XG_OFF(seed);
+#undef XG_OFF
+    return -1;
+}

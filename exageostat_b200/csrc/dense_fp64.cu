@@ -1,0 +1,608 @@
+/*
+ * FP64 kernels of the exact Matern log-likelihood path on sm_100a.
+ *
+ * Storage ("lower tile" layout): an N x N covariance is padded to
+ * Np = nt * ts (the padding is the identity, so it adds log 1 = 0 to the
+ * log-determinant and 0 to the quadratic form) and only the nt (nt + 1) / 2
+ * lower tiles are kept, each ts x ts row-major, packed column by column
+ * (xg_tile_index).  Row-major tiles make both operands of the trailing
+ * update A_ij -= L_ik L_jk^T K-major, which is the layout TMA's 128-byte
+ * swizzle and the DMMA fragments want.
+ *
+ * Reference steps these kernels replace (paths inside the reference tree):
+ *   xg_gen_matern_kernel      core_dcmg / core_dcmg_nuggets
+ *                             (exageostat_exact/cpu_core/compute/core_zcmg.c:963-994,
+ *                              core_zcmg_nuggets.c:107-156), tile loop of
+ *                             EXAGEOSTAT_MLE_dcmg_Tile_Async (runtime/starpu/codelets/codelet_zcmg.c:316-342)
+ *   xg_potrf_diag_kernel      POTRF(k,k) of CHAMELEON_dpotrf_Tile (MLE_dexact.c:372) fused with
+ *                             core_dmdet (cpu_core/compute/core_zmdet.c:50-59) and the diagonal block of
+ *                             CHAMELEON_dtrsm_Tile on Z (MLE_dexact.c:391)
+ *   xg_trsm_panel_kernel      TRSM(m,k) of dpotrf fused with the off-diagonal GEMV of the Z solve
+ *   xg_syrk_gemm_kernel       SYRK/GEMM trailing updates of dpotrf (algorithm shown in-tree by
+ *                             exageostat_exact/src/compute/psdportf.c:85-186 with an infinite band)
+ *   xg_finalize_kernel        dot product (MLE_dexact.c:399) and the log-likelihood formula (:426)
+ */
+#include <math.h>
+#include <stdint.h>
+
+#include "kbessel.cuh"
+#include "xg_common.cuh"
+#include "xg_kernels.h"
+
+/* ========================================================================== */
+/* Matern tile generation                                                     */
+/* ========================================================================== */
+
+__device__ inline double xg_deg2rad(double d) { return d * (XG_PI / 180.0); }
+
+/* Distance between (x1, y1) [row location] and (x2, y2) [column location].
+ * Euclidean: sqrt(pow(x2 - x1, 2) + pow(y2 - y1, 2)) as core_zcmg.c:84, with
+ * explicit round-to-nearest products and sum so no FMA contraction changes
+ * the rounding.  Great circle (dm = "gc"): haversine in km on (lat, lon) in
+ * degrees, as distanceEarth (core_zcmg.c:51-60). */
+__device__ inline double xg_distance(double x1, double y1, double x2, double y2, int metric)
+{
+    if (metric == 1) {
+        const double lat1 = xg_deg2rad(x1), lon1 = xg_deg2rad(y1);
+        const double lat2 = xg_deg2rad(x2), lon2 = xg_deg2rad(y2);
+        const double u = sin((lat2 - lat1) / 2), v = sin((lon2 - lon1) / 2);
+        return 2.0 * 6371.0 * asin(sqrt(u * u + cos(lat1) * cos(lat2) * v * v));
+    }
+    const double dx = x2 - x1, dy = y2 - y1;
+    return sqrt(__dadd_rn(__dmul_rn(dx, dx), __dmul_rn(dy, dy)));
+}
+
+__device__ inline double xg_matern_value(double d, const XgMaternParams &p)
+{
+    const double r = d / p.beta;
+    if (r == 0.0) return p.sigma2 + p.nugget;
+    if (p.half_integer >= 0) return xg_matern_half_integer(r, p.sigma2, p.half_integer);
+    return xg_matern_general(r, p.nu, p.con);
+}
+
+/* One CTA fills XG_GEN_ROWS rows of one tile; threads stride the columns so
+ * the row-major stores and the column-location loads are coalesced. */
+#define XG_GEN_ROWS 8
+__global__ void __launch_bounds__(256) xg_gen_matern_kernel(XgTileArgs T, const int2 *__restrict__ tile_ij,
+                                                            const double *__restrict__ xr, const double *__restrict__ yr,
+                                                            const double *__restrict__ xc, const double *__restrict__ yc,
+                                                            int n_rows, int n_cols, XgMaternParams p, int metric,
+                                                            int identity_pad)
+{
+    const int strips = T.ts / XG_GEN_ROWS;
+    const long long t = blockIdx.x / strips;
+    const int strip = blockIdx.x % strips;
+    const int2 ij = tile_ij[t];
+    double *tile = T.data + t * (long long)T.ts * T.ts;
+    for (int rr = 0; rr < XG_GEN_ROWS; ++rr) {
+        const int r = strip * XG_GEN_ROWS + rr;
+        const int R = ij.x * T.ts + r;
+        const bool row_ok = R < n_rows;
+        const double x1 = row_ok ? xr[R] : 0.0, y1 = row_ok ? yr[R] : 0.0;
+        for (int c = threadIdx.x; c < T.ts; c += blockDim.x) {
+            const int C = ij.y * T.ts + c;
+            double val;
+            if (row_ok && C < n_cols)
+                val = xg_matern_value(xg_distance(x1, y1, xc[C], yc[C], metric), p);
+            else
+                val = (identity_pad && R == C) ? 1.0 : 0.0;
+            tile[(long long)r * T.ts + c] = val;
+        }
+    }
+}
+
+/* ========================================================================== */
+/* POTRF of a diagonal tile, fused with log-det and the z block solve         */
+/* ========================================================================== */
+
+/* Panel of width NB (32, or 16 when ts = 1024) staged in shared memory with a
+ * leading dimension NB + 4: row-per-thread access then costs one extra
+ * wavefront but the DMMA fragment loads are conflict-free. */
+#define XG_POTRF_THREADS 512
+
+template <int NB>
+__global__ void __launch_bounds__(XG_POTRF_THREADS) xg_potrf_diag_kernel(XgTileArgs T, int k, double *__restrict__ v,
+                                                                         double *__restrict__ part_logdet,
+                                                                         double *__restrict__ part_dot, int with_rhs,
+                                                                         int *status, int *info)
+{
+    constexpr int LDP = NB + 4;
+    extern __shared__ __align__(16) double xg_smem_d[];
+    double *P = xg_smem_d;                 /* [ts][LDP] */
+    double *vs = P + (size_t)T.ts * LDP;   /* [ts] */
+    __shared__ int s_fail;
+    __shared__ double s_logdet;
+    const int ts = T.ts;
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    if (xg_cta_should_skip(status)) return;
+    double *A = T.data + xg_tile_index(k, k, T.nt) * (long long)ts * ts;
+    double *vk = v + (long long)k * ts;
+    if (tid == 0) {
+        s_fail = 0;
+        s_logdet = 0.0;
+    }
+    if (with_rhs)
+        for (int r = tid; r < ts; r += blockDim.x) vs[r] = vk[r];
+    double logdet_lane = 0.0;
+    for (int c0 = 0; c0 < ts; c0 += NB) {
+        const int rows = ts - c0;
+        __syncthreads();
+        for (int idx = tid; idx < rows * NB; idx += blockDim.x) {
+            const int r = idx / NB, c = idx - r * NB;
+            P[r * LDP + c] = A[(long long)(c0 + r) * ts + c0 + c];
+        }
+        __syncthreads();
+        /* unblocked Cholesky of the NB x NB diagonal block, one lane per row */
+        if (warp == 0) {
+            for (int j = 0; j < NB; ++j) {
+                double d = 0.0;
+                if (lane == j) {
+                    d = P[j * LDP + j];
+                    if (!(d > 0.0)) {
+                        s_fail = c0 + j + 1;
+                        d = 1.0;
+                    }
+                    d = sqrt(d);
+                    P[j * LDP + j] = d;
+                    logdet_lane += log(d);
+                }
+                d = __shfl_sync(0xffffffffu, d, j);
+                if (lane > j && lane < NB) P[lane * LDP + j] /= d;
+                __syncwarp();
+                if (lane > j && lane < NB) {
+                    const double lij = P[lane * LDP + j];
+                    for (int c = j + 1; c <= lane; ++c) P[lane * LDP + c] -= lij * P[c * LDP + j];
+                }
+                __syncwarp();
+            }
+        }
+        __syncthreads();
+        if (s_fail) {
+            if (tid == 0) {
+                atomicCAS(info, 0, k * ts + s_fail);
+                atomicOr(status, XG_ST_NOT_SPD);
+            }
+            return;
+        }
+        /* rows below the diagonal block: X = B L_D^-T, one thread per row */
+        for (int r = NB + tid; r < rows; r += blockDim.x) {
+            double row[NB];
+#pragma unroll
+            for (int j = 0; j < NB; ++j) row[j] = P[r * LDP + j];
+#pragma unroll
+            for (int j = 0; j < NB; ++j) {
+                double s = row[j];
+#pragma unroll
+                for (int q = 0; q < j; ++q) s -= row[q] * P[j * LDP + q];
+                row[j] = s / P[j * LDP + j];
+            }
+#pragma unroll
+            for (int j = 0; j < NB; ++j) P[r * LDP + j] = row[j];
+        }
+        /* z block solve L_D w = vs[c0:c0+NB] (warp 0, forward substitution) */
+        if (with_rhs && warp == 0) {
+            double w = (lane < NB) ? vs[c0 + lane] : 0.0;
+            for (int j = 0; j < NB; ++j) {
+                if (lane == j) w = w / P[j * LDP + j];
+                const double wj = __shfl_sync(0xffffffffu, w, j);
+                if (lane > j && lane < NB) w -= P[lane * LDP + j] * wj;
+            }
+            if (lane < NB) vs[c0 + lane] = w;
+        }
+        __syncthreads();
+        /* vs[below] -= P[below] . w ; write the panel back (upper of the
+         * diagonal block zeroed, so the stored factor is exactly L) */
+        if (with_rhs)
+            for (int r = NB + tid; r < rows; r += blockDim.x) {
+                double s = vs[c0 + r];
+#pragma unroll
+                for (int j = 0; j < NB; ++j) s -= P[r * LDP + j] * vs[c0 + j];
+                vs[c0 + r] = s;
+            }
+        for (int idx = tid; idx < rows * NB; idx += blockDim.x) {
+            const int rr = idx / NB, c = idx - rr * NB;
+            A[(long long)(c0 + rr) * ts + c0 + c] = (rr < c) ? 0.0 : P[rr * LDP + c];
+        }
+        /* trailing update of the tile: A[t][t] -= Pb Pb^T on the lower part,
+         * 32 x 32 output blocks per warp iteration, DMMA m16n8k4 */
+        const int R = rows - NB;
+        if (R > 0) {
+            const int nbr = (R + 31) / 32;
+            const int nblk = nbr * (nbr + 1) / 2;
+            const int g = lane >> 2, tq = lane & 3;
+            const double *Pb = P + NB * LDP;
+            double *At = A + (long long)(c0 + NB) * ts + (c0 + NB);
+            for (int blk = warp; blk < nblk; blk += XG_POTRF_THREADS / 32) {
+                int bi = (int)((sqrtf(8.0f * blk + 1.0f) - 1.0f) * 0.5f);
+                while ((bi + 1) * (bi + 2) / 2 <= blk) ++bi;
+                while (bi * (bi + 1) / 2 > blk) --bi;
+                const int bj = blk - bi * (bi + 1) / 2;
+                const int r0 = bi * 32, cb0 = bj * 32;
+                double acc[2][4][4];
+#pragma unroll
+                for (int mi = 0; mi < 2; ++mi)
+#pragma unroll
+                    for (int ni = 0; ni < 4; ++ni)
+#pragma unroll
+                        for (int e = 0; e < 4; ++e) acc[mi][ni][e] = 0.0;
+#pragma unroll
+                for (int p0 = 0; p0 < NB; p0 += 4) {
+                    double a[2][2], b[4];
+#pragma unroll
+                    for (int mi = 0; mi < 2; ++mi) {
+                        const int ra = r0 + mi * 16 + g;
+                        a[mi][0] = (ra < R) ? Pb[ra * LDP + p0 + tq] : 0.0;
+                        a[mi][1] = (ra + 8 < R) ? Pb[(ra + 8) * LDP + p0 + tq] : 0.0;
+                    }
+#pragma unroll
+                    for (int ni = 0; ni < 4; ++ni) {
+                        const int cbn = cb0 + ni * 8 + g;
+                        b[ni] = (cbn < R) ? Pb[cbn * LDP + p0 + tq] : 0.0;
+                    }
+#pragma unroll
+                    for (int mi = 0; mi < 2; ++mi)
+#pragma unroll
+                        for (int ni = 0; ni < 4; ++ni)
+                            xg_dmma_16x8x4(acc[mi][ni][0], acc[mi][ni][1], acc[mi][ni][2], acc[mi][ni][3], a[mi][0],
+                                           a[mi][1], b[ni]);
+                }
+#pragma unroll
+                for (int mi = 0; mi < 2; ++mi)
+#pragma unroll
+                    for (int ni = 0; ni < 4; ++ni) {
+                        const int cc = cb0 + ni * 8 + 2 * tq;
+#pragma unroll
+                        for (int h = 0; h < 2; ++h) {
+                            const int rr = r0 + mi * 16 + g + 8 * h;
+                            if (rr < R && cc < R) {
+                                double2 *pc = reinterpret_cast<double2 *>(At + (long long)rr * ts + cc);
+                                double2 cv = *pc;
+                                cv.x -= acc[mi][ni][2 * h];
+                                cv.y -= acc[mi][ni][2 * h + 1];
+                                *pc = cv;
+                            }
+                        }
+                    }
+            }
+        }
+    }
+    __syncthreads();
+    /* deterministic reductions: log-det over lanes of warp 0, dot over vs */
+    if (warp == 0) {
+        double s = logdet_lane;
+        for (int off = 16; off > 0; off >>= 1) s += __shfl_xor_sync(0xffffffffu, s, off);
+        if (lane == 0) s_logdet = s;
+    }
+    if (with_rhs)
+        for (int rr = tid; rr < ts; rr += blockDim.x) vk[rr] = vs[rr];
+    __syncthreads();
+    if (tid == 0) part_logdet[k] = s_logdet;
+    if (with_rhs && warp == 0) {
+        double s = 0.0;
+        for (int rr = lane; rr < ts; rr += 32) s += vs[rr] * vs[rr];
+        for (int off = 16; off > 0; off >>= 1) s += __shfl_xor_sync(0xffffffffu, s, off);
+        if (lane == 0) part_dot[k] = s;
+    }
+}
+
+/* ========================================================================== */
+/* Panel TRSM: L_ik = A_ik L_kk^-T, fused with v_i -= L_ik v_k                */
+/* ========================================================================== */
+
+#define XG_TRSM_THREADS 512
+#define XG_TRSM_SR 32 /* rows of A_ik per CTA */
+
+__global__ void __launch_bounds__(XG_TRSM_THREADS) xg_trsm_panel_kernel(XgTileArgs T, int k, double *__restrict__ v,
+                                                                        int with_rhs, const int *status)
+{
+    const int ts = T.ts, LDS = ts + 4;
+    extern __shared__ __align__(16) double xg_smem_d[];
+    double *S = xg_smem_d;                  /* [SR][LDS] */
+    double *LD = S + XG_TRSM_SR * LDS;      /* [32][33] */
+    if (xg_cta_should_skip(status)) return;
+    const int strips = ts / XG_TRSM_SR;
+    const int i = k + 1 + blockIdx.x / strips;
+    const int strip = blockIdx.x % strips;
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    const int g = lane >> 2, tq = lane & 3;
+    double *B = T.data + xg_tile_index(i, k, T.nt) * (long long)ts * ts + (long long)strip * XG_TRSM_SR * ts;
+    const double *L = T.data + xg_tile_index(k, k, T.nt) * (long long)ts * ts;
+    for (int idx = tid; idx < XG_TRSM_SR * ts; idx += blockDim.x) {
+        const int r = idx / ts, c = idx - r * ts;
+        S[r * LDS + c] = B[(long long)r * ts + c];
+    }
+    for (int cb = 0; cb < ts; cb += 32) {
+        for (int idx = tid; idx < 32 * 32; idx += blockDim.x) {
+            const int r = idx >> 5, c = idx & 31;
+            LD[r * 33 + c] = L[(long long)(cb + r) * ts + cb + c];
+        }
+        __syncthreads();
+        if (warp == 0) { /* lane = row of the strip */
+            double row[32];
+#pragma unroll
+            for (int j = 0; j < 32; ++j) row[j] = S[lane * LDS + cb + j];
+#pragma unroll
+            for (int j = 0; j < 32; ++j) {
+                double s = row[j];
+#pragma unroll
+                for (int q = 0; q < j; ++q) s -= row[q] * LD[j * 33 + q];
+                row[j] = s / LD[j * 33 + j];
+            }
+#pragma unroll
+            for (int j = 0; j < 32; ++j) S[lane * LDS + cb + j] = row[j];
+        }
+        __syncthreads();
+        /* S[:, cb+32:] -= S[:, cb:cb+32] L[cb+32:, cb:cb+32]^T, 32-column groups */
+        const int ncol = ts - cb - 32;
+        const int ngrp = ncol / 32;
+        for (int grp = warp; grp < ngrp; grp += XG_TRSM_THREADS / 32) {
+            const int c0 = cb + 32 + grp * 32;
+            double acc[2][4][4];
+#pragma unroll
+            for (int mi = 0; mi < 2; ++mi)
+#pragma unroll
+                for (int ni = 0; ni < 4; ++ni)
+#pragma unroll
+                    for (int e = 0; e < 4; ++e) acc[mi][ni][e] = 0.0;
+#pragma unroll
+            for (int p0 = 0; p0 < 32; p0 += 4) {
+                double a[2][2], b[4];
+#pragma unroll
+                for (int mi = 0; mi < 2; ++mi) {
+                    a[mi][0] = S[(mi * 16 + g) * LDS + cb + p0 + tq];
+                    a[mi][1] = S[(mi * 16 + g + 8) * LDS + cb + p0 + tq];
+                }
+#pragma unroll
+                for (int ni = 0; ni < 4; ++ni) b[ni] = __ldg(L + (long long)(c0 + ni * 8 + g) * ts + cb + p0 + tq);
+#pragma unroll
+                for (int mi = 0; mi < 2; ++mi)
+#pragma unroll
+                    for (int ni = 0; ni < 4; ++ni)
+                        xg_dmma_16x8x4(acc[mi][ni][0], acc[mi][ni][1], acc[mi][ni][2], acc[mi][ni][3], a[mi][0],
+                                       a[mi][1], b[ni]);
+            }
+#pragma unroll
+            for (int mi = 0; mi < 2; ++mi)
+#pragma unroll
+                for (int ni = 0; ni < 4; ++ni)
+#pragma unroll
+                    for (int h = 0; h < 2; ++h) {
+                        double *ps = S + (mi * 16 + g + 8 * h) * LDS + c0 + ni * 8 + 2 * tq;
+                        ps[0] -= acc[mi][ni][2 * h];
+                        ps[1] -= acc[mi][ni][2 * h + 1];
+                    }
+        }
+        __syncthreads();
+    }
+    for (int idx = tid; idx < XG_TRSM_SR * ts; idx += blockDim.x) {
+        const int r = idx / ts, c = idx - r * ts;
+        B[(long long)r * ts + c] = S[r * LDS + c];
+    }
+    if (with_rhs) {
+        const double *vk = v + (long long)k * ts;
+        double *vi = v + (long long)i * ts + strip * XG_TRSM_SR;
+        for (int r = warp; r < XG_TRSM_SR; r += XG_TRSM_THREADS / 32) {
+            double s = 0.0;
+            for (int c = lane; c < ts; c += 32) s += S[r * LDS + c] * vk[c];
+            for (int off = 16; off > 0; off >>= 1) s += __shfl_xor_sync(0xffffffffu, s, off);
+            if (lane == 0) vi[r] -= s;
+        }
+    }
+}
+
+/* ========================================================================== */
+/* Trailing update A_ij -= L_ik L_jk^T on FP64 tensor cores (DMMA), TMA fed   */
+/* ========================================================================== */
+
+/* 128 x 128 output block per CTA, K streamed in 16-wide slabs through a
+ * 4-stage TMA ring (128-byte swizzle).  Warps 0-7 compute (2 x 4 warps of
+ * 64 x 32), warp 8 is the TMA producer. */
+#define XG_G_BM 128
+#define XG_G_BK 16
+#define XG_G_STAGES 4
+#define XG_G_THREADS 288
+#define XG_G_STAGE_BYTES (2 * XG_G_BM * XG_G_BK * 8)
+
+__global__ void __launch_bounds__(XG_G_THREADS, 1) xg_syrk_gemm_kernel(const __grid_constant__ CUtensorMap map,
+                                                                       XgTileArgs T, int k, int *status)
+{
+    extern __shared__ __align__(1024) unsigned char xg_smem_raw[];
+    unsigned char *smem = (unsigned char *)(((uintptr_t)xg_smem_raw + 1023) & ~(uintptr_t)1023);
+    uint64_t *full = (uint64_t *)(smem + XG_G_STAGES * XG_G_STAGE_BYTES);
+    uint64_t *empty = full + XG_G_STAGES;
+    const int ts = T.ts;
+    const int bpt = ts / XG_G_BM; /* blocks per tile side */
+    const long long pair = blockIdx.x / (bpt * bpt);
+    const int blk = blockIdx.x % (bpt * bpt);
+    const int bi = blk / bpt, bj = blk % bpt;
+    int ii, jj;
+    xg_pair_decode(pair, &ii, &jj);
+    const int i = k + 1 + ii, j = k + 1 + jj;
+    if (xg_cta_should_skip(status, i == j && bj > bi)) return;
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    if (tid == 0) {
+        for (int s = 0; s < XG_G_STAGES; ++s) {
+            xg_mbar_init(&full[s], 1);
+            xg_mbar_init(&empty[s], 8);
+        }
+        xg_fence_barrier_init();
+    }
+    __syncthreads();
+    const int KT = ts / XG_G_BK;
+    const int rowA = (int)(xg_tile_index(i, k, T.nt) * ts + bi * XG_G_BM);
+    const int rowB = (int)(xg_tile_index(j, k, T.nt) * ts + bj * XG_G_BM);
+    if (warp == 8) {
+        if (lane == 0) {
+            xg_prefetch_tensormap(&map);
+            int issued = 0;
+            bool ok = true;
+            for (int kb = 0; kb < KT; ++kb) {
+                const int s = kb % XG_G_STAGES;
+                if (kb >= XG_G_STAGES && !xg_mbar_wait(&empty[s], ((kb / XG_G_STAGES) - 1) & 1)) {
+                    ok = false;
+                    break;
+                }
+                unsigned char *sa = smem + s * XG_G_STAGE_BYTES;
+                xg_mbar_arrive_expect_tx(&full[s], XG_G_STAGE_BYTES);
+                xg_tma_load_2d(sa, &map, kb * XG_G_BK, rowA, &full[s]);
+                xg_tma_load_2d(sa + XG_G_BM * XG_G_BK * 8, &map, kb * XG_G_BK, rowB, &full[s]);
+                ++issued;
+            }
+            if (!ok) atomicOr(status, XG_ST_TIMEOUT);
+            /* every issued copy has landed before the CTA may exit */
+            for (int kb = (issued > XG_G_STAGES ? issued - XG_G_STAGES : 0); kb < issued; ++kb)
+                if (!xg_mbar_wait(&full[kb % XG_G_STAGES], (kb / XG_G_STAGES) & 1)) atomicOr(status, XG_ST_TIMEOUT);
+        }
+        return;
+    }
+    const int wm = warp >> 2, wn = warp & 3;
+    const int g = lane >> 2, tq = lane & 3;
+    double acc[4][4][4];
+#pragma unroll
+    for (int mi = 0; mi < 4; ++mi)
+#pragma unroll
+        for (int ni = 0; ni < 4; ++ni)
+#pragma unroll
+            for (int e = 0; e < 4; ++e) acc[mi][ni][e] = 0.0;
+    bool ok = true;
+    for (int kb = 0; kb < KT; ++kb) {
+        const int s = kb % XG_G_STAGES;
+        if (!xg_mbar_wait(&full[s], (kb / XG_G_STAGES) & 1)) {
+            ok = false;
+            break;
+        }
+        const unsigned char *sa = smem + s * XG_G_STAGE_BYTES;
+        const unsigned char *sb = sa + XG_G_BM * XG_G_BK * 8;
+#pragma unroll
+        for (int ks = 0; ks < XG_G_BK / 4; ++ks) {
+            const int kk = ks * 4 + tq;
+            double a[4][2], b[4];
+#pragma unroll
+            for (int mi = 0; mi < 4; ++mi) {
+                const int r = wm * 64 + mi * 16 + g;
+                a[mi][0] = *(const double *)(sa + xg_swz128_off(r, kk));
+                a[mi][1] = *(const double *)(sa + xg_swz128_off(r + 8, kk));
+            }
+#pragma unroll
+            for (int ni = 0; ni < 4; ++ni) b[ni] = *(const double *)(sb + xg_swz128_off(wn * 32 + ni * 8 + g, kk));
+#pragma unroll
+            for (int mi = 0; mi < 4; ++mi)
+#pragma unroll
+                for (int ni = 0; ni < 4; ++ni)
+                    xg_dmma_16x8x4(acc[mi][ni][0], acc[mi][ni][1], acc[mi][ni][2], acc[mi][ni][3], a[mi][0], a[mi][1],
+                                   b[ni]);
+        }
+        __syncwarp();
+        if (lane == 0) xg_mbar_arrive(&empty[s]);
+    }
+    if (!ok) {
+        if (lane == 0) atomicOr(status, XG_ST_TIMEOUT);
+        return;
+    }
+    double *C = T.data + xg_tile_index(i, j, T.nt) * (long long)ts * ts + (long long)(bi * XG_G_BM) * ts + bj * XG_G_BM;
+#pragma unroll
+    for (int mi = 0; mi < 4; ++mi)
+#pragma unroll
+        for (int ni = 0; ni < 4; ++ni)
+#pragma unroll
+            for (int h = 0; h < 2; ++h) {
+                const int r = wm * 64 + mi * 16 + g + 8 * h;
+                const int c = wn * 32 + ni * 8 + 2 * tq;
+                double2 *pc = reinterpret_cast<double2 *>(C + (long long)r * ts + c);
+                double2 cv = *pc;
+                cv.x -= acc[mi][ni][2 * h];
+                cv.y -= acc[mi][ni][2 * h + 1];
+                *pc = cv;
+            }
+}
+
+/* ========================================================================== */
+/* Log-likelihood assembly                                                    */
+/* ========================================================================== */
+
+/* loglik = -0.5 dotp - 0.5 logdet - (N / 2.0) log(2 pi)  (MLE_dexact.c:426),
+ * with logdet = 2 sum log L_ii (MLE_dexact.c:384) summed in tile order. */
+__global__ void xg_finalize_kernel(const double *part_logdet, const double *part_dot, int nt, int N, double *out,
+                                   const int *status, const int *info)
+{
+    if (threadIdx.x != 0) return;
+    double det = 0.0, dot = 0.0;
+    for (int k = 0; k < nt; ++k) {
+        det += part_logdet[k];
+        dot += part_dot[k];
+    }
+    const double logdet = 2.0 * det;
+    out[0] = -0.5 * dot - 0.5 * logdet - (double)(N / 2.0) * log(2.0 * 3.141592653589793);
+    out[1] = logdet;
+    out[2] = dot;
+    out[3] = (double)(*status);
+    out[4] = (double)(*info);
+}
+
+/* ========================================================================== */
+/* Host launchers                                                             */
+/* ========================================================================== */
+
+static int xg_potrf_nb(int ts) { return ts > 512 ? 16 : 32; }
+
+size_t xg_potrf_smem_bytes(int ts) { return ((size_t)ts * (xg_potrf_nb(ts) + 4) + ts) * sizeof(double); }
+size_t xg_trsm_smem_bytes(int ts) { return ((size_t)XG_TRSM_SR * (ts + 4) + 32 * 33) * sizeof(double); }
+size_t xg_gemm_smem_bytes() { return (size_t)XG_G_STAGES * XG_G_STAGE_BYTES + 2 * XG_G_STAGES * 8 + 1024; }
+
+cudaError_t xg_kernels_configure()
+{
+    cudaError_t e;
+    e = cudaFuncSetAttribute(xg_potrf_diag_kernel<32>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             (int)xg_potrf_smem_bytes(512));
+    if (e != cudaSuccess) return e;
+    e = cudaFuncSetAttribute(xg_trsm_panel_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             (int)xg_trsm_smem_bytes(XG_MAX_TS));
+    if (e != cudaSuccess) return e;
+    e = cudaFuncSetAttribute(xg_syrk_gemm_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             (int)xg_gemm_smem_bytes());
+    return e;
+}
+
+void xg_launch_gen(const XgTileArgs &T, const int2 *tile_ij, long long ntiles, const double *xr, const double *yr,
+                   const double *xc, const double *yc, int n_rows, int n_cols, const XgMaternParams &p, int metric,
+                   int identity_pad, cudaStream_t st)
+{
+    const long long blocks = ntiles * (T.ts / XG_GEN_ROWS);
+    xg_gen_matern_kernel<<<(unsigned)blocks, 256, 0, st>>>(T, tile_ij, xr, yr, xc, yc, n_rows, n_cols, p, metric,
+                                                            identity_pad);
+}
+
+void xg_launch_potrf_diag(const XgTileArgs &T, int k, double *v, double *part_logdet, double *part_dot, int with_rhs,
+                          int *status, int *info, cudaStream_t st)
+{
+    const size_t smem = xg_potrf_smem_bytes(T.ts);
+    if (xg_potrf_nb(T.ts) == 16)
+        xg_potrf_diag_kernel<16><<<1, XG_POTRF_THREADS, smem, st>>>(T, k, v, part_logdet, part_dot, with_rhs, status,
+                                                                     info);
+    else
+        xg_potrf_diag_kernel<32><<<1, XG_POTRF_THREADS, smem, st>>>(T, k, v, part_logdet, part_dot, with_rhs, status,
+                                                                     info);
+}
+
+void xg_launch_trsm_panel(const XgTileArgs &T, int k, double *v, int with_rhs, const int *status, cudaStream_t st)
+{
+    const int n = T.nt - k - 1;
+    if (n <= 0) return;
+    xg_trsm_panel_kernel<<<n * (T.ts / XG_TRSM_SR), XG_TRSM_THREADS, xg_trsm_smem_bytes(T.ts), st>>>(T, k, v, with_rhs,
+                                                                                                   status);
+}
+
+void xg_launch_syrk_gemm(const CUtensorMap &map, const XgTileArgs &T, int k, int *status, cudaStream_t st)
+{
+    const long long n = T.nt - k - 1;
+    if (n <= 0) return;
+    const int bpt = T.ts / XG_G_BM;
+    const long long blocks = n * (n + 1) / 2 * bpt * bpt;
+    xg_syrk_gemm_kernel<<<(unsigned)blocks, XG_G_THREADS, xg_gemm_smem_bytes(), st>>>(map, T, k, status);
+}
+
+void xg_launch_finalize(const double *part_logdet, const double *part_dot, int nt, int N, double *out,
+                        const int *status, const int *info, cudaStream_t st)
+{
+    xg_finalize_kernel<<<1, 32, 0, st>>>(part_logdet, part_dot, nt, N, out, status, info);
+}

@@ -1,0 +1,609 @@
+/*
+ * Host engine behind the reference C API (capi.cpp).
+ *
+ * One process-wide context (exageostat_init) owns the CUDA stream.  Each
+ * MLE_data owns one XgField (stored in data->descC): the device locations,
+ * z, the lower-tile covariance / factor and the solve buffers.  An
+ * evaluation is a fixed launch sequence on the context stream:
+ *
+ *   generate Sigma(theta) tiles -> for k: POTRF(k,k) [+ log-det, + z block
+ *   solve] -> TRSM panel k [+ z update] -> trailing update k -> finalize
+ *
+ * and one device-to-host copy of the result.  Nothing here calls exit().
+ */
+#include <math.h>
+#include <stdarg.h>
+#include <stdio.h>
+#include <stdlib.h>
+#include <string.h>
+#include <sys/time.h>
+
+#include <mutex>
+#include <string>
+
+#include "../../include/exageostat_b200.h"
+#include "xg_common.cuh"
+#include "xg_engine.h"
+#include "xg_kernels.h"
+
+/* ------------------------------------------------------------------------- */
+/* errors                                                                    */
+/* ------------------------------------------------------------------------- */
+
+static thread_local std::string g_last_error;
+
+int xg_fail(int code, const char *fmt, ...)
+{
+    char buf[512];
+    va_list ap;
+    va_start(ap, fmt);
+    vsnprintf(buf, sizeof buf, fmt, ap);
+    va_end(ap);
+    g_last_error = buf;
+    return code;
+}
+
+static int xg_cuda_fail(cudaError_t e, const char *what)
+{
+    return xg_fail(XG_ERR_CUDA, "%s: %s", what, cudaGetErrorString(e));
+}
+
+#define XG_CU(call)                                                                                                    \
+    do {                                                                                                               \
+        cudaError_t _e = (call);                                                                                       \
+        if (_e != cudaSuccess) return xg_cuda_fail(_e, #call);                                                         \
+    } while (0)
+
+extern "C" const char *exageostat_last_error(void) { return g_last_error.c_str(); }
+
+static bool xg_silent()
+{
+    const char *s = getenv("EXAGEOSTAT_B200_SILENT");
+    return s && *s && strcmp(s, "0") != 0;
+}
+
+static double xg_wtime()
+{
+    struct timeval tp;
+    gettimeofday(&tp, NULL);
+    return tp.tv_sec + 1e-6 * tp.tv_usec;
+}
+
+/* ------------------------------------------------------------------------- */
+/* context                                                                   */
+/* ------------------------------------------------------------------------- */
+
+XgContext g_xg;
+
+typedef CUresult (*XgEncodeTiledFn)(CUtensorMap *, CUtensorMapDataType, cuuint32_t, void *, const cuuint64_t *,
+                                     const cuuint64_t *, const cuuint32_t *, const cuuint32_t *, CUtensorMapInterleave,
+                                     CUtensorMapSwizzle, CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
+static XgEncodeTiledFn g_encode = nullptr;
+
+int xg_context_start(int dts)
+{
+    std::lock_guard<std::mutex> lk(g_xg.mu);
+    if (g_xg.initialized) return XG_OK;
+    int dev = 0;
+    XG_CU(cudaGetDevice(&dev));
+    cudaDeviceProp prop;
+    XG_CU(cudaGetDeviceProperties(&prop, dev));
+    if (prop.major != 10)
+        return xg_fail(XG_ERR_UNSUPPORTED, "device %d (%s, sm_%d%d) is not a B200-class sm_100 GPU", dev, prop.name,
+                       prop.major, prop.minor);
+    XG_CU(cudaStreamCreateWithFlags(&g_xg.stream, cudaStreamNonBlocking));
+    cudaDriverEntryPointQueryResult q;
+    void *fn = nullptr;
+    XG_CU(cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &fn, cudaEnableDefault, &q));
+    if (!fn || q != cudaDriverEntryPointSuccess)
+        return xg_fail(XG_ERR_CUDA, "cuTensorMapEncodeTiled is not available from the driver");
+    g_encode = (XgEncodeTiledFn)fn;
+    cudaError_t e = xg_kernels_configure();
+    if (e != cudaSuccess) return xg_cuda_fail(e, "kernel attribute setup");
+    g_xg.device = dev;
+    g_xg.sm_count = prop.multiProcessorCount;
+    g_xg.dts = dts;
+    g_xg.initialized = true;
+    return XG_OK;
+}
+
+int xg_context_require()
+{
+    if (g_xg.initialized) return XG_OK;
+    /* The reference requires exageostat_init first; starting lazily keeps
+     * the one-shot entry points usable on their own. */
+    return xg_context_start(0);
+}
+
+/* tile size: a multiple of 128 in [128, XG_MAX_TS]; 0 picks by problem size */
+int xg_choose_ts(int N, int dts)
+{
+    if (dts <= 0) {
+        if (N <= 1024) return 128;
+        if (N <= 8192) return 256;
+        return 512;
+    }
+    int ts = ((dts + 127) / 128) * 128;
+    if (ts < 128) ts = 128;
+    if (ts > XG_MAX_TS) ts = XG_MAX_TS;
+    return ts;
+}
+
+/* ------------------------------------------------------------------------- */
+/* lower-tile matrices                                                       */
+/* ------------------------------------------------------------------------- */
+
+int xg_tm_alloc(XgTileMatrix &M, int N, int ts)
+{
+    M.N = N;
+    M.ts = ts;
+    M.nt = (N + ts - 1) / ts;
+    M.ntiles = xg_num_lower_tiles(M.nt);
+    const size_t bytes = (size_t)M.ntiles * ts * ts * sizeof(double);
+    cudaError_t e = cudaMalloc(&M.d, bytes);
+    if (e != cudaSuccess) {
+        M.d = nullptr;
+        return xg_fail(XG_ERR_NO_MEMORY, "cannot allocate %.2f GB for %lld covariance tiles: %s", bytes / 1e9,
+                       M.ntiles, cudaGetErrorString(e));
+    }
+    int2 *hij = (int2 *)malloc(sizeof(int2) * M.ntiles);
+    for (int j = 0; j < M.nt; ++j)
+        for (int i = j; i < M.nt; ++i) hij[xg_tile_index(i, j, M.nt)] = make_int2(i, j);
+    e = cudaMalloc(&M.ij, sizeof(int2) * M.ntiles);
+    if (e == cudaSuccess) e = cudaMemcpy(M.ij, hij, sizeof(int2) * M.ntiles, cudaMemcpyHostToDevice);
+    free(hij);
+    if (e != cudaSuccess) return xg_cuda_fail(e, "tile index table");
+    /* TMA view: a 2-D FP64 tensor [ntiles * ts rows][ts columns], boxes of
+     * 128 rows x 16 columns (128 bytes, swizzled) */
+    cuuint64_t dims[2] = {(cuuint64_t)ts, (cuuint64_t)M.ntiles * ts};
+    cuuint64_t strides[1] = {(cuuint64_t)ts * sizeof(double)};
+    cuuint32_t box[2] = {16, 128};
+    cuuint32_t estr[2] = {1, 1};
+    CUresult r = g_encode(&M.map, CU_TENSOR_MAP_DATA_TYPE_FLOAT64, 2, M.d, dims, strides, box, estr,
+                          CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+                          CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+    if (r != CUDA_SUCCESS) return xg_fail(XG_ERR_CUDA, "cuTensorMapEncodeTiled failed (%d)", (int)r);
+    return XG_OK;
+}
+
+void xg_tm_free(XgTileMatrix &M)
+{
+    if (M.d) cudaFree(M.d);
+    if (M.ij) cudaFree(M.ij);
+    M.d = nullptr;
+    M.ij = nullptr;
+}
+
+XgMaternParams xg_params(const double *theta, int kernel)
+{
+    XgMaternParams p;
+    p.sigma2 = theta[0];
+    p.beta = theta[1];
+    p.nu = theta[2];
+    p.nugget = (kernel == 1) ? theta[3] : 0.0;
+    /* core_zcmg.c:976-978 */
+    double con = pow(2, (theta[2] - 1)) * tgamma(theta[2]);
+    con = 1.0 / con;
+    p.con = theta[0] * con;
+    p.half_integer = (theta[2] == 0.5) ? 0 : (theta[2] == 1.5) ? 1 : (theta[2] == 2.5) ? 2 : -1;
+    return p;
+}
+
+int xg_check_theta(const double *theta, int kernel)
+{
+    const int np = kernel == 1 ? 4 : 3;
+    for (int i = 0; i < np; ++i)
+        if (!isfinite(theta[i])) return xg_fail(XG_ERR_BAD_ARGUMENT, "theta[%d] is not finite", i);
+    if (!(theta[0] > 0) || !(theta[1] > 0) || !(theta[2] > 0))
+        return xg_fail(XG_ERR_BAD_ARGUMENT, "theta = (%g, %g, %g) must be positive", theta[0], theta[1], theta[2]);
+    if (theta[2] > 25.0)
+        return xg_fail(XG_ERR_BAD_ARGUMENT, "smoothness nu = %g is above the supported maximum 25", theta[2]);
+    if (kernel == 1 && theta[3] < 0) return xg_fail(XG_ERR_BAD_ARGUMENT, "nugget %g must be >= 0", theta[3]);
+    return XG_OK;
+}
+
+/* Cholesky of M in place; with v != nullptr also v <- L^-1 v and the per-tile
+ * partial sums (log-det in part[0:nt], |v_k|^2 in part[nt:2nt]). */
+void xg_factor(XgTileMatrix &M, double *v, double *part, int *status, int *info, cudaStream_t st, cudaEvent_t *pev)
+{
+    XgTileArgs T{M.d, M.ts, M.nt};
+    for (int k = 0; k < M.nt; ++k) {
+        if (pev) cudaEventRecord(pev[3 * k], st);
+        xg_launch_potrf_diag(T, k, v, part, part + M.nt, v != nullptr, status, info, st);
+        if (pev) cudaEventRecord(pev[3 * k + 1], st);
+        xg_launch_trsm_panel(T, k, v, v != nullptr, status, st);
+        if (pev) cudaEventRecord(pev[3 * k + 2], st);
+        xg_launch_syrk_gemm(M.map, T, k, status, st);
+    }
+    if (pev) cudaEventRecord(pev[3 * M.nt], st);
+}
+
+/* Algorithmic flops of the trailing update after step k: a GEMM (2 ts^3) per
+ * off-diagonal tile pair and a SYRK (ts^2 (ts + 1)) per diagonal tile. */
+double xg_trailing_flops(int nt, int ts, int k)
+{
+    const double n = nt - k - 1;
+    const double t = ts;
+    return n * (n - 1) / 2 * 2 * t * t * t + n * t * t * (t + 1);
+}
+
+int xg_field_set_profiling(XgField *f, int on)
+{
+    if (on && !f->pev) {
+        const int n = 3 * f->C.nt + 1;
+        f->pev = (cudaEvent_t *)calloc(n, sizeof(cudaEvent_t));
+        for (int i = 0; i < n; ++i)
+            if (cudaEventCreate(&f->pev[i]) != cudaSuccess) return xg_fail(XG_ERR_CUDA, "profiling events");
+    }
+    f->profiling = on != 0;
+    for (int i = 0; i < 8; ++i) f->prof[i] = 0;
+    return XG_OK;
+}
+
+static void xg_field_collect_profile(XgField *f)
+{
+    float ms = 0;
+    const int nt = f->C.nt;
+    cudaEventElapsedTime(&ms, f->ev[0], f->ev[1]);
+    f->prof[0] += ms * 1e-3;
+    for (int k = 0; k < nt; ++k) {
+        cudaEventElapsedTime(&ms, f->pev[3 * k], f->pev[3 * k + 1]);
+        f->prof[1] += ms * 1e-3;
+        cudaEventElapsedTime(&ms, f->pev[3 * k + 1], f->pev[3 * k + 2]);
+        f->prof[2] += ms * 1e-3;
+        cudaEventElapsedTime(&ms, f->pev[3 * k + 2], (k + 1 < nt) ? f->pev[3 * k + 3] : f->pev[3 * nt]);
+        f->prof[3] += ms * 1e-3;
+        f->prof[4] += xg_trailing_flops(nt, f->C.ts, k);
+    }
+    /* launches: generation, per step POTRF (+ TRSM + trailing when k < nt-1), finalize */
+    f->prof[5] += 1 + nt + 2.0 * (nt - 1) + 1;
+    f->prof[6] += 1;
+}
+
+int xg_field_set_data(XgField *f, const double *x, const double *y, const double *z)
+{
+    cudaStream_t st = g_xg.stream;
+    if (x) XG_CU(cudaMemcpyAsync(f->x, x, f->N * sizeof(double), cudaMemcpyHostToDevice, st));
+    if (y) XG_CU(cudaMemcpyAsync(f->y, y, f->N * sizeof(double), cudaMemcpyHostToDevice, st));
+    if (z) XG_CU(cudaMemcpyAsync(f->z, z, f->N * sizeof(double), cudaMemcpyHostToDevice, st));
+    XG_CU(cudaStreamSynchronize(st));
+    if (z) f->have_z = true;
+    return XG_OK;
+}
+
+/* ------------------------------------------------------------------------- */
+/* fields                                                                    */
+/* ------------------------------------------------------------------------- */
+
+static int xg_dev_alloc(double **p, size_t n)
+{
+    cudaError_t e = cudaMalloc(p, n * sizeof(double));
+    if (e != cudaSuccess) return xg_fail(XG_ERR_NO_MEMORY, "cudaMalloc(%zu doubles): %s", n, cudaGetErrorString(e));
+    return cudaMemset(*p, 0, n * sizeof(double)) == cudaSuccess ? XG_OK : XG_ERR_CUDA;
+}
+
+void xg_field_destroy(XgField *f)
+{
+    if (!f) return;
+    xg_tm_free(f->C);
+    double *bufs[] = {f->x, f->y, f->z, f->v, f->e, f->part, f->out};
+    for (double *b : bufs)
+        if (b) cudaFree(b);
+    if (f->status) cudaFree(f->status);
+    if (f->h_out) cudaFreeHost(f->h_out);
+    if (f->pev) {
+        for (int i = 0; i < 3 * f->C.nt + 1; ++i)
+            if (f->pev[i]) cudaEventDestroy(f->pev[i]);
+        free(f->pev);
+    }
+    for (int i = 0; i < 4; ++i)
+        if (f->ev[i]) cudaEventDestroy(f->ev[i]);
+    delete f;
+}
+
+int xg_field_create(XgField **out, int N, int ts, const double *x, const double *y, int kernel, int metric)
+{
+    *out = nullptr;
+    int rc = xg_context_require();
+    if (rc) return rc;
+    if (N <= 0) return xg_fail(XG_ERR_BAD_ARGUMENT, "N = %d must be positive", N);
+    if (!x || !y) return xg_fail(XG_ERR_BAD_ARGUMENT, "locations are NULL");
+    XgField *f = new XgField();
+    f->N = N;
+    f->kernel = kernel;
+    f->metric = metric;
+    rc = xg_tm_alloc(f->C, N, xg_choose_ts(N, ts));
+    const size_t Np = (size_t)f->C.nt * f->C.ts;
+    if (!rc) rc = xg_dev_alloc(&f->x, Np);
+    if (!rc) rc = xg_dev_alloc(&f->y, Np);
+    if (!rc) rc = xg_dev_alloc(&f->z, Np);
+    if (!rc) rc = xg_dev_alloc(&f->v, Np);
+    if (!rc) rc = xg_dev_alloc(&f->e, Np);
+    if (!rc) rc = xg_dev_alloc(&f->part, 2 * (size_t)f->C.nt);
+    if (!rc) rc = xg_dev_alloc(&f->out, 8);
+    if (!rc && cudaMalloc(&f->status, 2 * sizeof(int)) != cudaSuccess) rc = xg_fail(XG_ERR_NO_MEMORY, "status word");
+    if (!rc && cudaMallocHost(&f->h_out, 8 * sizeof(double)) != cudaSuccess)
+        rc = xg_fail(XG_ERR_NO_MEMORY, "pinned result buffer");
+    for (int i = 0; i < 4 && !rc; ++i)
+        if (cudaEventCreate(&f->ev[i]) != cudaSuccess) rc = xg_fail(XG_ERR_CUDA, "event");
+    if (!rc && cudaMemcpy(f->x, x, N * sizeof(double), cudaMemcpyHostToDevice) != cudaSuccess)
+        rc = xg_fail(XG_ERR_CUDA, "upload x");
+    if (!rc && cudaMemcpy(f->y, y, N * sizeof(double), cudaMemcpyHostToDevice) != cudaSuccess)
+        rc = xg_fail(XG_ERR_CUDA, "upload y");
+    if (rc) {
+        xg_field_destroy(f);
+        return rc;
+    }
+    f->info = f->status + 1;
+    *out = f;
+    return XG_OK;
+}
+
+int xg_field_set_z(XgField *f, const double *z)
+{
+    cudaStream_t st = g_xg.stream;
+    XG_CU(cudaMemcpyAsync(f->z, z, f->N * sizeof(double), cudaMemcpyHostToDevice, st));
+    XG_CU(cudaStreamSynchronize(st));
+    f->have_z = true;
+    return XG_OK;
+}
+
+static int xg_read_status(XgField *f)
+{
+    const int st = (int)f->h_out[3];
+    if (st & XG_ST_NOT_SPD)
+        return xg_fail(XG_ERR_NOT_SPD, "the covariance is not positive definite (pivot %d)", (int)f->h_out[4]);
+    if (st & XG_ST_TIMEOUT) return xg_fail(XG_ERR_TIMEOUT, "a device pipeline wait timed out");
+    if (st) return xg_fail(XG_ERR_CUDA, "device status word 0x%x", st);
+    return XG_OK;
+}
+
+/* log-likelihood at theta; res[0..2] = loglik, logdet, dotp; times[0..1] =
+ * generation and factorisation+solve seconds (CUDA events). */
+int xg_field_loglik(XgField *f, const double *theta, double *res, double *times)
+{
+    int rc = xg_check_theta(theta, f->kernel);
+    if (rc) return rc;
+    if (!f->have_z) return xg_fail(XG_ERR_BAD_ARGUMENT, "no observations: call MLE_zvg or set z first");
+    cudaStream_t st = g_xg.stream;
+    XgTileArgs T{f->C.d, f->C.ts, f->C.nt};
+    const XgMaternParams p = xg_params(theta, f->kernel);
+    const size_t Np = (size_t)f->C.nt * f->C.ts;
+    XG_CU(cudaMemsetAsync(f->status, 0, 2 * sizeof(int), st));
+    XG_CU(cudaMemcpyAsync(f->v, f->z, Np * sizeof(double), cudaMemcpyDeviceToDevice, st));
+    XG_CU(cudaEventRecord(f->ev[0], st));
+    xg_launch_gen(T, f->C.ij, f->C.ntiles, f->x, f->y, f->x, f->y, f->N, f->N, p, f->metric, 1, st);
+    XG_CU(cudaEventRecord(f->ev[1], st));
+    xg_factor(f->C, f->v, f->part, f->status, f->info, st, f->profiling ? f->pev : nullptr);
+    xg_launch_finalize(f->part, f->part + f->C.nt, f->C.nt, f->N, f->out, f->status, f->info, st);
+    XG_CU(cudaEventRecord(f->ev[2], st));
+    XG_CU(cudaMemcpyAsync(f->h_out, f->out, 5 * sizeof(double), cudaMemcpyDeviceToHost, st));
+    XG_CU(cudaGetLastError());
+    XG_CU(cudaStreamSynchronize(st));
+    if (times) {
+        float a = 0, b = 0;
+        cudaEventElapsedTime(&a, f->ev[0], f->ev[1]);
+        cudaEventElapsedTime(&b, f->ev[1], f->ev[2]);
+        times[0] = a * 1e-3;
+        times[1] = b * 1e-3;
+    }
+    if (f->profiling) xg_field_collect_profile(f);
+    rc = xg_read_status(f);
+    if (rc) return rc;
+    res[0] = f->h_out[0];
+    res[1] = f->h_out[1];
+    res[2] = f->h_out[2];
+    return XG_OK;
+}
+
+/* z = chol(Sigma(theta)) e, e = nrand (N host doubles) */
+int xg_field_zvg(XgField *f, const double *theta, const double *nrand, double *times)
+{
+    int rc = xg_check_theta(theta, f->kernel);
+    if (rc) return rc;
+    cudaStream_t st = g_xg.stream;
+    XgTileArgs T{f->C.d, f->C.ts, f->C.nt};
+    const XgMaternParams p = xg_params(theta, f->kernel);
+    XG_CU(cudaMemsetAsync(f->status, 0, 2 * sizeof(int), st));
+    XG_CU(cudaMemcpyAsync(f->e, nrand, f->N * sizeof(double), cudaMemcpyHostToDevice, st));
+    XG_CU(cudaEventRecord(f->ev[0], st));
+    xg_launch_gen(T, f->C.ij, f->C.ntiles, f->x, f->y, f->x, f->y, f->N, f->N, p, f->metric, 1, st);
+    XG_CU(cudaEventRecord(f->ev[1], st));
+    xg_factor(f->C, nullptr, f->part, f->status, f->info, st);
+    xg_launch_trmv_lower(T, f->e, f->z, f->status, st);
+    XG_CU(cudaEventRecord(f->ev[2], st));
+    XG_CU(cudaGetLastError());
+    XG_CU(cudaStreamSynchronize(st));
+    /* status and info are ints on the device: widen them into the slots
+     * xg_read_status reads */
+    int sv[2];
+    XG_CU(cudaMemcpy(sv, f->status, sizeof sv, cudaMemcpyDeviceToHost));
+    f->h_out[3] = sv[0];
+    f->h_out[4] = sv[1];
+    if (times) {
+        float a = 0, b = 0;
+        cudaEventElapsedTime(&a, f->ev[0], f->ev[1]);
+        cudaEventElapsedTime(&b, f->ev[1], f->ev[2]);
+        times[0] = a * 1e-3;
+        times[1] = b * 1e-3;
+    }
+    rc = xg_read_status(f);
+    if (rc) return rc;
+    f->have_z = true;
+    return XG_OK;
+}
+
+int xg_field_get_z(XgField *f, double *z, int n)
+{
+    if (!f->have_z) return xg_fail(XG_ERR_BAD_ARGUMENT, "no observations generated yet");
+    if (n > f->N) n = f->N;
+    XG_CU(cudaMemcpy(z, f->z, n * sizeof(double), cudaMemcpyDeviceToHost));
+    return XG_OK;
+}
+
+/* ------------------------------------------------------------------------- */
+/* kriging                                                                   */
+/* ------------------------------------------------------------------------- */
+
+void xg_predict_destroy(XgPredict *q)
+{
+    if (!q) return;
+    xg_tm_free(q->C22);
+    double *bufs[] = {q->xm, q->ym, q->xo, q->yo, q->v, q->zact, q->zmiss, q->part, q->out};
+    for (double *b : bufs)
+        if (b) cudaFree(b);
+    if (q->status) cudaFree(q->status);
+    delete q;
+}
+
+int xg_predict_create(XgPredict **out, int nmiss, int nobs, int ts)
+{
+    *out = nullptr;
+    int rc = xg_context_require();
+    if (rc) return rc;
+    if (nmiss <= 0 || nobs <= 0) return xg_fail(XG_ERR_BAD_ARGUMENT, "nZmiss = %d, nZobs = %d", nmiss, nobs);
+    XgPredict *q = new XgPredict();
+    q->nmiss = nmiss;
+    q->nobs = nobs;
+    rc = xg_tm_alloc(q->C22, nobs, xg_choose_ts(nobs, ts));
+    const size_t Np = (size_t)q->C22.nt * q->C22.ts;
+    if (!rc) rc = xg_dev_alloc(&q->xo, Np);
+    if (!rc) rc = xg_dev_alloc(&q->yo, Np);
+    if (!rc) rc = xg_dev_alloc(&q->v, Np);
+    if (!rc) rc = xg_dev_alloc(&q->xm, nmiss);
+    if (!rc) rc = xg_dev_alloc(&q->ym, nmiss);
+    if (!rc) rc = xg_dev_alloc(&q->zact, nmiss);
+    if (!rc) rc = xg_dev_alloc(&q->zmiss, nmiss);
+    if (!rc) rc = xg_dev_alloc(&q->part, 2 * (size_t)q->C22.nt);
+    if (!rc) rc = xg_dev_alloc(&q->out, 8);
+    if (!rc && cudaMalloc(&q->status, 2 * sizeof(int)) != cudaSuccess) rc = xg_fail(XG_ERR_NO_MEMORY, "status");
+    if (rc) {
+        xg_predict_destroy(q);
+        return rc;
+    }
+    *out = q;
+    return XG_OK;
+}
+
+int xg_predict_run(XgPredict *q, const double *theta, int kernel, int metric, const double *xm, const double *ym,
+                   const double *xo, const double *yo, const double *zobs, const double *zactual, double *zmiss,
+                   double *mse)
+{
+    int rc = xg_check_theta(theta, kernel);
+    if (rc) return rc;
+    cudaStream_t st = g_xg.stream;
+    const int nmiss = q->nmiss, nobs = q->nobs;
+    XgTileArgs T{q->C22.d, q->C22.ts, q->C22.nt};
+    const XgMaternParams p = xg_params(theta, kernel);
+    const size_t Np = (size_t)q->C22.nt * q->C22.ts;
+    XG_CU(cudaMemsetAsync(q->status, 0, 2 * sizeof(int), st));
+    XG_CU(cudaMemsetAsync(q->v, 0, Np * sizeof(double), st));
+    XG_CU(cudaMemcpyAsync(q->xo, xo, nobs * sizeof(double), cudaMemcpyHostToDevice, st));
+    XG_CU(cudaMemcpyAsync(q->yo, yo, nobs * sizeof(double), cudaMemcpyHostToDevice, st));
+    XG_CU(cudaMemcpyAsync(q->v, zobs, nobs * sizeof(double), cudaMemcpyHostToDevice, st));
+    XG_CU(cudaMemcpyAsync(q->xm, xm, nmiss * sizeof(double), cudaMemcpyHostToDevice, st));
+    XG_CU(cudaMemcpyAsync(q->ym, ym, nmiss * sizeof(double), cudaMemcpyHostToDevice, st));
+    if (zactual) XG_CU(cudaMemcpyAsync(q->zact, zactual, nmiss * sizeof(double), cudaMemcpyHostToDevice, st));
+    /* C22 = Sigma(obs, obs); POSV: L L^T alpha = zobs */
+    xg_launch_gen(T, q->C22.ij, q->C22.ntiles, q->xo, q->yo, q->xo, q->yo, nobs, nobs, p, metric, 1, st);
+    xg_factor(q->C22, q->v, q->part, q->status, q->info(), st);
+    for (int k = q->C22.nt - 1; k >= 0; --k) xg_launch_trsv_lower_t_step(T, k, q->v, q->status, st);
+    /* zmiss = Sigma(miss, obs) alpha, C12 generated on the fly */
+    xg_launch_predict_cross(q->xm, q->ym, nmiss, q->xo, q->yo, nobs, q->v, p, metric, q->zmiss, st);
+    if (zactual) xg_launch_mse(q->zact, q->zmiss, nmiss, q->out, st);
+    XG_CU(cudaGetLastError());
+    int sv[2];
+    XG_CU(cudaMemcpyAsync(sv, q->status, sizeof sv, cudaMemcpyDeviceToHost, st));
+    XG_CU(cudaMemcpyAsync(zmiss, q->zmiss, nmiss * sizeof(double), cudaMemcpyDeviceToHost, st));
+    double m = -1;
+    if (zactual) XG_CU(cudaMemcpyAsync(&m, q->out, sizeof(double), cudaMemcpyDeviceToHost, st));
+    XG_CU(cudaStreamSynchronize(st));
+    if (sv[0] & XG_ST_NOT_SPD) return xg_fail(XG_ERR_NOT_SPD, "C22 is not positive definite (pivot %d)", sv[1]);
+    if (sv[0]) return xg_fail(XG_ERR_TIMEOUT, "device status word 0x%x", sv[0]);
+    *mse = zactual ? m : -1.0;
+    return XG_OK;
+}
+
+/* ------------------------------------------------------------------------- */
+/* dense diagnostics                                                         */
+/* ------------------------------------------------------------------------- */
+
+int xg_covariance_dense(int n, const double *x, const double *y, const double *theta, int kernel, int metric, int ts,
+                        int factor, double *out)
+{
+    XgField *f = nullptr;
+    int rc = xg_check_theta(theta, kernel);
+    if (rc) return rc;
+    rc = xg_field_create(&f, n, ts, x, y, kernel, metric);
+    if (rc) return rc;
+    cudaStream_t st = g_xg.stream;
+    XgTileArgs T{f->C.d, f->C.ts, f->C.nt};
+    const XgMaternParams p = xg_params(theta, kernel);
+    cudaMemsetAsync(f->status, 0, 2 * sizeof(int), st);
+    xg_launch_gen(T, f->C.ij, f->C.ntiles, f->x, f->y, f->x, f->y, n, n, p, metric, 1, st);
+    if (factor) xg_factor(f->C, nullptr, f->part, f->status, f->info, st);
+    const int tsz = f->C.ts;
+    const size_t tile_elems = (size_t)tsz * tsz;
+    double *h = (double *)malloc(f->C.ntiles * tile_elems * sizeof(double));
+    int sv[2] = {0, 0};
+    cudaError_t e = cudaMemcpyAsync(h, f->C.d, f->C.ntiles * tile_elems * sizeof(double), cudaMemcpyDeviceToHost, st);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(sv, f->status, sizeof sv, cudaMemcpyDeviceToHost, st);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+    if (e != cudaSuccess) rc = xg_cuda_fail(e, "covariance download");
+    if (!rc && (sv[0] & XG_ST_NOT_SPD)) rc = xg_fail(XG_ERR_NOT_SPD, "not positive definite (pivot %d)", sv[1]);
+    if (!rc) {
+        for (int r = 0; r < n; ++r)
+            for (int c = 0; c < n; ++c) {
+                double val = 0.0;
+                if (c <= r) {
+                    const int i = r / tsz, j = c / tsz;
+                    val = h[xg_tile_index(i, j, f->C.nt) * tile_elems + (size_t)(r % tsz) * tsz + (c % tsz)];
+                }
+                out[(size_t)r * n + c] = val;
+            }
+    }
+    free(h);
+    xg_field_destroy(f);
+    return rc;
+}
+
+int xg_bessel_knu_host(int n, const double *nu, const double *x, double *out)
+{
+    int rc = xg_context_require();
+    if (rc) return rc;
+    if (n <= 0) return XG_OK;
+    double *d = nullptr;
+    XG_CU(cudaMalloc(&d, 3 * (size_t)n * sizeof(double)));
+    cudaStream_t st = g_xg.stream;
+    cudaMemcpyAsync(d, nu, n * sizeof(double), cudaMemcpyHostToDevice, st);
+    cudaMemcpyAsync(d + n, x, n * sizeof(double), cudaMemcpyHostToDevice, st);
+    xg_launch_bessel(d, d + n, n, d + 2 * (size_t)n, st);
+    cudaMemcpyAsync(out, d + 2 * (size_t)n, n * sizeof(double), cudaMemcpyDeviceToHost, st);
+    cudaError_t e = cudaStreamSynchronize(st);
+    cudaFree(d);
+    if (e != cudaSuccess) return xg_cuda_fail(e, "bessel");
+    return XG_OK;
+}
+
+int xg_matern_pairs_host(int n, const double *x1, const double *y1, const double *x2, const double *y2,
+                         const double *theta, int kernel, int metric, double *out)
+{
+    int rc = xg_context_require();
+    if (rc) return rc;
+    rc = xg_check_theta(theta, kernel);
+    if (rc) return rc;
+    if (n <= 0) return XG_OK;
+    double *d = nullptr;
+    XG_CU(cudaMalloc(&d, 5 * (size_t)n * sizeof(double)));
+    cudaStream_t st = g_xg.stream;
+    const double *src[4] = {x1, y1, x2, y2};
+    for (int i = 0; i < 4; ++i)
+        cudaMemcpyAsync(d + (size_t)i * n, src[i], n * sizeof(double), cudaMemcpyHostToDevice, st);
+    xg_launch_matern_pairs(d, d + n, d + 2 * (size_t)n, d + 3 * (size_t)n, n, xg_params(theta, kernel), metric,
+                           d + 4 * (size_t)n, st);
+    cudaMemcpyAsync(out, d + 4 * (size_t)n, n * sizeof(double), cudaMemcpyDeviceToHost, st);
+    cudaError_t e = cudaStreamSynchronize(st);
+    cudaFree(d);
+    if (e != cudaSuccess) return xg_cuda_fail(e, "matern pairs");
+    return XG_OK;
+}

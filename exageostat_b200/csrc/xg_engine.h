@@ -1,0 +1,97 @@
+/*
+ * Host engine: device objects behind the MLE_data handles.
+ */
+#ifndef EXAGEOSTAT_B200_ENGINE_H
+#define EXAGEOSTAT_B200_ENGINE_H
+
+#include <cuda.h>
+#include <cuda_runtime.h>
+
+#include <mutex>
+
+#include "xg_kernels.h"
+
+struct XgContext {
+    bool initialized = false;
+    int device = 0;
+    int sm_count = 0;
+    int dts = 0;
+    cudaStream_t stream = nullptr;
+    std::mutex mu;
+};
+extern XgContext g_xg;
+
+struct XgTileMatrix {
+    int N = 0, ts = 0, nt = 0;
+    long long ntiles = 0;
+    double *d = nullptr;
+    int2 *ij = nullptr; /* (i, j) of every packed tile */
+    CUtensorMap map;    /* TMA view for the trailing-update kernel */
+};
+
+/* One dataset: locations, observations and the covariance / factor. */
+struct XgField {
+    int N = 0;
+    int kernel = 0; /* 0 Matern, 1 Matern + nugget */
+    int metric = 0; /* 0 Euclidean, 1 great circle */
+    XgTileMatrix C;
+    double *x = nullptr, *y = nullptr; /* padded to nt * ts */
+    double *z = nullptr;               /* observations (zero padded); never modified by evaluations */
+    double *v = nullptr;               /* solve work vector */
+    double *e = nullptr;               /* N(0,1) draws for MLE_zvg */
+    double *part = nullptr;            /* per-tile log-det / dot partials (2 nt) */
+    double *out = nullptr;             /* device result record */
+    int *status = nullptr, *info = nullptr;
+    double *h_out = nullptr; /* pinned copy of out */
+    cudaEvent_t ev[4] = {nullptr, nullptr, nullptr, nullptr};
+    bool have_z = false;
+    /* optional per-kernel-class timing (exageostat_b200_set_profiling) */
+    bool profiling = false;
+    cudaEvent_t *pev = nullptr; /* 3 nt + 1 events around the factorisation kernels */
+    double prof[8] = {0, 0, 0, 0, 0, 0, 0, 0}; /* gen, potrf, trsm, gemm seconds; gemm flops; launches; evals */
+};
+
+struct XgPredict {
+    int nmiss = 0, nobs = 0;
+    int mse_flag = 1;
+    XgTileMatrix C22;
+    double *xm = nullptr, *ym = nullptr, *xo = nullptr, *yo = nullptr;
+    double *v = nullptr, *zact = nullptr, *zmiss = nullptr, *part = nullptr, *out = nullptr;
+    int *status = nullptr;
+    int *info() { return status + 1; }
+};
+
+int xg_fail(int code, const char *fmt, ...);
+int xg_context_start(int dts);
+int xg_context_require();
+int xg_choose_ts(int N, int dts);
+int xg_tm_alloc(XgTileMatrix &M, int N, int ts);
+void xg_tm_free(XgTileMatrix &M);
+XgMaternParams xg_params(const double *theta, int kernel);
+int xg_check_theta(const double *theta, int kernel);
+void xg_factor(XgTileMatrix &M, double *v, double *part, int *status, int *info, cudaStream_t st,
+               cudaEvent_t *pev = nullptr);
+double xg_trailing_flops(int nt, int ts, int k);
+int xg_field_set_data(XgField *f, const double *x, const double *y, const double *z);
+int xg_field_set_profiling(XgField *f, int on);
+
+int xg_field_create(XgField **out, int N, int ts, const double *x, const double *y, int kernel, int metric);
+void xg_field_destroy(XgField *f);
+int xg_field_set_z(XgField *f, const double *z);
+int xg_field_loglik(XgField *f, const double *theta, double *res, double *times);
+int xg_field_zvg(XgField *f, const double *theta, const double *nrand, double *times);
+int xg_field_get_z(XgField *f, double *z, int n);
+
+int xg_predict_create(XgPredict **out, int nmiss, int nobs, int ts);
+void xg_predict_destroy(XgPredict *q);
+int xg_predict_run(XgPredict *q, const double *theta, int kernel, int metric, const double *xm, const double *ym,
+                   const double *xo, const double *yo, const double *zobs, const double *zactual, double *zmiss,
+                   double *mse);
+
+int xg_covariance_dense(int n, const double *x, const double *y, const double *theta, int kernel, int metric, int ts,
+                        int factor, double *out);
+int xg_matern_pairs_host(int n, const double *x1, const double *y1, const double *x2, const double *y2,
+                         const double *theta, int kernel, int metric, double *out);
+int xg_bessel_knu_host(int n, const double *nu, const double *x, double *out);
+
+#endif

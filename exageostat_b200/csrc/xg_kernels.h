@@ -1,0 +1,62 @@
+/*
+ * Internal interface between the host engine and the CUDA kernels.
+ */
+#ifndef EXAGEOSTAT_B200_KERNELS_H
+#define EXAGEOSTAT_B200_KERNELS_H
+
+#include <cuda.h>
+#include <cuda_runtime.h>
+#include <stddef.h>
+
+/* Tile sizes are multiples of 128 up to XG_MAX_TS: the panel TRSM stages
+ * 32 x ts doubles in shared memory. */
+#define XG_MAX_TS 512
+
+/* A lower-tile FP64 matrix on the device (see dense_fp64.cu for the layout). */
+struct XgTileArgs {
+    double *data;
+    int ts; /* tile size */
+    int nt; /* tiles per side */
+};
+
+/* Matern parameters of one covariance evaluation.  con = sigma^2 /
+ * (2^(nu-1) Gamma(nu)) is computed on the host exactly as core_zcmg.c:976-978;
+ * half_integer = 0, 1, 2 selects the closed form for nu = 0.5, 1.5, 2.5
+ * (exact match of nu), -1 the general Bessel path. */
+struct XgMaternParams {
+    double sigma2;
+    double beta;
+    double nu;
+    double nugget; /* tau^2, added on the zero-distance branch only */
+    double con;
+    int half_integer;
+};
+
+cudaError_t xg_kernels_configure();
+size_t xg_potrf_smem_bytes(int ts);
+size_t xg_trsm_smem_bytes(int ts);
+size_t xg_gemm_smem_bytes();
+
+void xg_launch_gen(const XgTileArgs &T, const int2 *tile_ij, long long ntiles, const double *xr, const double *yr,
+                   const double *xc, const double *yc, int n_rows, int n_cols, const XgMaternParams &p, int metric,
+                   int identity_pad, cudaStream_t st);
+void xg_launch_potrf_diag(const XgTileArgs &T, int k, double *v, double *part_logdet, double *part_dot, int with_rhs,
+                          int *status, int *info, cudaStream_t st);
+void xg_launch_trsm_panel(const XgTileArgs &T, int k, double *v, int with_rhs, const int *status, cudaStream_t st);
+void xg_launch_syrk_gemm(const CUtensorMap &map, const XgTileArgs &T, int k, int *status, cudaStream_t st);
+void xg_launch_finalize(const double *part_logdet, const double *part_dot, int nt, int N, double *out,
+                        const int *status, const int *info, cudaStream_t st);
+
+/* solve.cu */
+void xg_launch_trmv_lower(const XgTileArgs &T, const double *e, double *z, const int *status, cudaStream_t st);
+void xg_launch_trsv_lower_t_step(const XgTileArgs &T, int k, double *v, const int *status, cudaStream_t st);
+void xg_launch_predict_cross(const double *xm, const double *ym, int nmiss, const double *xo, const double *yo,
+                             int nobs, const double *alpha, const XgMaternParams &p, int metric, double *zmiss,
+                             cudaStream_t st);
+void xg_launch_mse(const double *zactual, const double *zmiss, int nmiss, double *out, cudaStream_t st);
+void xg_launch_matern_pairs(const double *x1, const double *y1, const double *x2, const double *y2, int n,
+                            const XgMaternParams &p, int metric, double *out, cudaStream_t st);
+
+void xg_launch_bessel(const double *nu, const double *x, int n, double *out, cudaStream_t st);
+
+#endif

@@ -1,0 +1,378 @@
+/*
+ * exageostat_b200 -- C ABI of the B200 (sm_100a) exact Matern MLE library.
+ *
+ * Drop-in for the exact (exageostat_exact) maximum-likelihood path of
+ * ExaGeoStat 1.2: the same entry points, the same MLE_data / location /
+ * output structures (field for field, so drivers that poke fields keep
+ * working) and the same argument meaning.  Paths in the citations are inside
+ * the reference project.  Differences from the reference are listed per
+ * function; the main one is that no function calls exit(): failures are
+ * reported through return values, data fields and exageostat_last_error().
+ *
+ * Everything runs on one CUDA device (the current device at
+ * exageostat_init).  All pointers in these signatures are HOST pointers.
+ */
+#ifndef EXAGEOSTAT_B200_H
+#define EXAGEOSTAT_B200_H
+
+#include <stddef.h>
+#include <stdio.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---- data structures: layout-identical to misc/include/MLE_misc.h:111-328 ---- */
+
+/* misc/include/MLE_misc.h:111-115 */
+typedef struct {
+    double *x; /* first coordinate (x, or latitude for dm = "gc") */
+    double *y; /* second coordinate */
+    double *z; /* third coordinate; NULL for 2-D locations (the only case handled here) */
+} location;
+
+/* misc/include/MLE_misc.h:130-178; the library writes final_loglik and
+ * estimated_theta (when allocated) like the reference. */
+typedef struct {
+    int problem_size;
+    char *computation;
+    char *kernel;
+    char *ds_type;
+    char *precision;
+    int z_sample;
+    int dense_ts;
+    int lr_ts;
+    int lr_acc;
+    int lr_maxrank;
+    int ncores;
+    int ngpus;
+    int p;
+    int q;
+    int num_params;
+    double *initial_theta;
+    double *starting_theta;
+    double *estimated_theta;
+    double final_loglik;
+    double time_per_iteration;
+    double cholesky_per_iter;
+    double flops_per_iteration;
+    double generation_per_iter;
+    double solve_per_iter;
+    double total_mle_time;
+    double avg_exec_time_gen_stage;
+    double avg_flops_gen_stage;
+    double mse_pred1;
+    double mse_pred2;
+    double mse_pred3;
+    double mse_pred;
+    double trace_pred_sum;
+    double trace_pred_mean;
+    double total_pred_time;
+    double total_pred_flops;
+    double mloe;
+    double mmom;
+    char *mloe_exec;
+    double total_mloe_mmom_time;
+    double matrix_gen_mloe_mmom_time;
+    double cho_fact_mloe_mmom_time;
+    double loop_mloe_mmom_time;
+    double total_mloe_mmom_flops;
+    double fisher_00;
+    double fisher_11;
+    double fisher_22;
+    double fisher_time;
+} output;
+
+/* misc/include/MLE_misc.h:184-328.  Fields this library reads: computation
+ * ("exact"), kernel_fun, dm ("ed" | "gc"), precision (0 FP64, 2 mixed),
+ * diag_thick (mixed band, in tiles), l1 / lobs / lmiss, verbose, log,
+ * pFileLog, recovery_file, checkpoint_file.  The desc* handles hold this
+ * library's device objects (opaque). */
+typedef struct {
+    double variance;
+    double variance1;
+    double variance2;
+    double variance3;
+    char *computation;
+    char *c_fun;
+    int test;
+    int async;
+    int iter_count;
+    location l1;
+    location lmiss;
+    location lobs;
+    location lm;
+    void *descC;
+    void *descsubC11;
+    void *descsubC12;
+    void *descsubC21;
+    void *descsubC22;
+    void *descZ;
+    void *descZ1;
+    void *descZ2;
+    void *descZ3;
+    double *Adense;
+    double *Adense2;
+    void *descZcpy;
+    void *descdet;
+    void *descsum;
+    void *descproduct;
+    void *descproduct1;
+    void *descproduct2;
+    void *descproduct3;
+    void *descZmiss;
+    void *descC11;
+    void *descC21;
+    void *descC12;
+    void *descC22;
+    void *descZactual;
+    void *descZobs;
+    void *descmse;
+    void *descmse1;
+    void *descmse2;
+    void *descmse3;
+    void *descZtrace;
+    void *sequence;
+    void *request;
+    int verbose;
+    int check;
+    int log;
+    double avg_exec_time_per_iter;
+    double total_exec_time;
+    double avg_flops_per_iter;
+    double avg_generation_per_iter;
+    double avg_solve_per_iter;
+    double avg_cholesky_per_iter;
+    double avg_exec_time_gen_stage;
+    double avg_flops_gen_stage;
+    double final_loglik;
+    char *locsFPath;
+    char *timeFPath;
+    char *obsFPath;
+    char *obsFPath2;
+    char *obsFPath3;
+    char *actualZFPath;
+    char *actualZFPath2;
+    char *actualZFPath3;
+    char *actualZLocFPath;
+    char *actualTimeFPath;
+    double det;
+    double sum;
+    double dotp;
+    double dotp1;
+    double dotp2;
+    double dotp3;
+    float sdotp;
+    double mserror;
+    double mserror1;
+    double mserror2;
+    double mserror3;
+    char *dm;
+    int diag_thick;
+    char *nFileLog;
+    FILE *pFileLog;
+    int hicma_maxrank;
+    int hicma_data_type;
+    void *hicma_descC;
+    void *hicma_descZ;
+    void *hicma_descCD;
+    void *hicma_descCUV;
+    void *hicma_descCrk;
+    void *hicma_descZcpy;
+    void *hicma_descdet;
+    void *hicma_descproduct;
+    void *hicma_descC12D;
+    void *hicma_descC12UV;
+    void *hicma_descC12rk;
+    void *hicma_descC22D;
+    void *hicma_descC22UV;
+    void *hicma_descC22rk;
+    double hicma_acc;
+    void *hsequence;
+    void *hrequest;
+    int opt_tol;
+    int opt_max_iters;
+    int ooc;
+    char *kernel_fun;
+    int precision;
+    void *desctemp;
+    void *desctemp22;
+    void *desck_t;
+    void *desck_a;
+    void *desck_ttmp;
+    void *desck_atmp;
+    void *descK_t;
+    void *descK_a;
+    void *descexpr1;
+    void *descexpr2;
+    void *descexpr3;
+    void *descexpr4;
+    void *descestimatedalpha;
+    void *desctruthalpha;
+    void *desc_mloe_mmom;
+    void *descmloe;
+    void *descmmom;
+    double expr1;
+    double expr2;
+    double expr3;
+    double expr4;
+    double mloe;
+    double mmom;
+    int mloe_mmom;
+    int mloe_mmom_async;
+    int mspe;
+    char *recovery_file;
+    char *checkpoint_file;
+    int time_slots;
+    int idw;
+    int fisher;
+    void *descr;
+    void *descrcpy;
+    int seed;
+} MLE_data;
+
+/* The reference's global result record (misc/include/MLE_misc.h:350, defined
+ * by the driver in examples/examples.c:24).  Defined weakly here so a driver
+ * that defines its own keeps working. */
+extern output results;
+
+/* ---- reference entry points ---- */
+
+/* src/include/MLE.h:54-55 (src/compute/MLE.c:233-260).  Selects the CUDA
+ * device (the current one), creates the stream and records *dts as the
+ * default tile size (0 = choose automatically).  ncores and lts are
+ * accepted and ignored; *gpus must be 0 or 1 (one GPU per field).  A second
+ * call prints the reference's warning and keeps the first context. */
+void exageostat_init(int *ncores, int *gpus, int *dts, int *lts);
+void EXAGEOSTAT_init(int *ncores, int *gpus, int *dts, int *lts); /* alias */
+
+/* src/include/MLE.h:57 (src/compute/MLE.c:263-281). */
+void exageostat_finalize(void);
+
+/* exageostat_exact/src/include/MLE_exact.h:60-62 (MLE_dexact.c:1938-2017).
+ * Allocates the device covariance (lower tiles of size dts), z and the
+ * solve buffers for N locations and uploads data->l1.x / l1.y.  Handles are
+ * stored in data->descC / descZ / descZcpy.  On failure data->descC stays
+ * NULL and exageostat_last_error() says why.  MORSE_dmle_Call is the
+ * MORSE-era name of the same function. */
+void EXAGEOSTAT_dmle_Call(MLE_data *data, int ncores, int gpus, int dts, int p_grid, int q_grid, int N, int nZobs,
+                          int nZmiss);
+void MORSE_dmle_Call(MLE_data *data, int ncores, int gpus, int dts, int p_grid, int q_grid, int N, int nZobs,
+                     int nZmiss);
+
+/* src/include/MLE.h:40-42 (src/compute/MLE.c:38-92 -> MLE_dexact.c:25-148).
+ * z = chol(Sigma(initial_theta)) * Nrand on the device; Nrand is n host
+ * doubles.  Resets data->iter_count.  `log` writes nothing here. */
+void MLE_zvg(MLE_data *data, double *Nrand, double *initial_theta, int n, int ts, int log, int p_grid, int q_grid);
+
+/* src/include/MLE.h:48-49 (src/compute/MLE.c:138-193): NLopt objective,
+ * dispatching on data->precision (0: FP64, 2: banded mixed precision).
+ * Returns the log-likelihood.  New: when grad != NULL it receives d loglik /
+ * d theta (the reference ignores grad).  A non-positive-definite covariance
+ * returns -INFINITY (the reference exits). */
+double MLE_alg(unsigned n, const double *theta, double *grad, void *data);
+
+/* exageostat_exact/src/include/MLE_exact.h:43-44 (MLE_dexact.c:231-489). */
+double EXAGEOSTAT_dmle_Tile(unsigned n, const double *theta, double *grad, void *data);
+double MORSE_dmle_Tile(unsigned n, const double *theta, double *grad, void *data);
+
+/* src/include/MLE.h:67 (src/compute/MLE.c:420-430): copies the synthetic z
+ * (n doubles) to host memory. */
+void MLE_get_zobs(MLE_data *data, double *z, int n);
+
+/* src/include/MLE.h:59-61 (src/compute/MLE.c:284-306 -> MLE_dexact.c:613-685). */
+void prediction_init(MLE_data *data, int nZmiss, int nZobs, int ts, int p_grid, int q_grid, int mse_flag);
+void EXAGEOSTAT_dmle_Predict_Allocate(MLE_data *data, int nZmiss, int nZobs, int dts, int p_grid, int q_grid,
+                                      int mse_flag);
+
+/* exageostat_exact/src/include/MLE_exact.h:49-51 (MLE_dexact.c:688-874).
+ * Kriging of the nZmiss locations data->lmiss from the nZobs observations
+ * Zobs at data->lobs.  Writes Zmiss; returns the MSE against Zactual, or -1
+ * when Zactual is NULL or nZmiss <= 0 (as the reference), -2 on a
+ * non-positive-definite C22. */
+double EXAGEOSTAT_dmle_Predict_Tile(MLE_data *data, double *theta, int nZmiss, int nZobs, double *Zobs,
+                                    double *Zactual, double *Zmiss, int n);
+double MORSE_dmle_Predict_Tile(MLE_data *data, double *theta, int nZmiss, int nZobs, double *Zobs, double *Zactual,
+                               double *Zmiss, int n);
+
+/* src/include/MLE.h:63 and :65. */
+void prediction_finalize(MLE_data *data);
+void MLE_Finalize(MLE_data *data);
+
+/* ---- host-side synthetic data helpers (misc/include/MLE_misc.h) ---- */
+
+/* misc/compute/MLE_misc.c:763-792: srand(seed), jittered ceil(sqrt(n))^2
+ * grid, Morton sort with uint16 quantisation.  Returns a malloc'd location
+ * whose x / y are malloc'd n-arrays (free with free()). */
+location *GenerateXYLoc(int n, int seed);
+/* misc/compute/MLE_misc.c:753-761 */
+double uniform_distribution(double rangeLow, double rangeHigh);
+/* misc/compute/MLE_misc.c:1238-1259 */
+void shuffle(double *array, location *locations, size_t n);
+/* misc/compute/MLE_misc.c:453-534 */
+int locations_obs_zsort_inplace(int n, location *locations, double *z);
+/* misc/compute/MLE_misc.c:1700-1741: splits the synthetic z (from the
+ * device) into missing / observed sets with the libc rand() stream;
+ * data->lmiss.x / .y are malloc'd N-arrays and data->lobs points into them
+ * at offset nZmiss, as in the reference. */
+void pick_random_points(MLE_data *data, double *Zobs, double *Zactual, int nZmiss, int nZobs, int N);
+
+/* ---- new entry points (no counterpart in the reference) ---- */
+
+/* Status-returning form of MLE_alg: 0 on success, else an XG_ERR_* code;
+ * loglik receives the value, grad (may be NULL) the gradient. */
+int exageostat_b200_loglik(MLE_data *data, const double *theta, double *loglik, double *grad);
+
+/* Text of the last error on the calling thread ("" if none). */
+const char *exageostat_last_error(void);
+
+#define XG_OK 0
+#define XG_ERR_NOT_INITIALIZED 1
+#define XG_ERR_BAD_ARGUMENT 2
+#define XG_ERR_CUDA 3
+#define XG_ERR_NOT_SPD 4
+#define XG_ERR_TIMEOUT 5
+#define XG_ERR_UNSUPPORTED 6
+#define XG_ERR_NO_MEMORY 7
+
+/* Library / ABI introspection (used by the bindings' layout checks). */
+int exageostat_b200_abi_version(void);
+size_t exageostat_b200_sizeof_MLE_data(void);
+size_t exageostat_b200_sizeof_output(void);
+long exageostat_b200_offsetof_MLE_data(const char *field);
+
+/* One-shot evaluation on host arrays (no MLE_data): uploads x, y, z (n
+ * doubles each), evaluates the log-likelihood at theta (3 values, or 4 for
+ * kernel 1 = Matern + nugget) with tile size ts (0 = automatic) and copies
+ * the result back.  out[0..2] = loglik, logdet, z^T Sigma^-1 z. */
+int exageostat_b200_dmle_host(int n, const double *x, const double *y, const double *z, const double *theta,
+                              int kernel, int metric, int ts, double *out);
+
+/* Replaces the locations and/or observations (N host doubles each; NULL
+ * keeps the current array) of an allocated MLE_data, e.g. for a new dataset
+ * of the same size, without reallocating the device covariance. */
+int exageostat_b200_set_data(MLE_data *data, const double *x, const double *y, const double *z);
+
+/* Per-kernel-class CUDA-event timing of the log-likelihood evaluations of
+ * one MLE_data.  set_profiling(on) resets the counters; get_profile fills
+ * out[0..9] = seconds in generation, diagonal POTRF, panel TRSM, trailing
+ * update; trailing-update algorithmic flops; kernel launches; evaluations;
+ * tile size; tiles per side; N. */
+int exageostat_b200_set_profiling(MLE_data *data, int on);
+int exageostat_b200_get_profile(MLE_data *data, double *out, int n);
+
+/* Diagnostics used by the parity tests.  All run on the GPU. */
+int exageostat_b200_bessel_knu(int n, const double *nu, const double *x, double *out);
+int exageostat_b200_matern_pairs(int n, const double *x1, const double *y1, const double *x2, const double *y2,
+                                 const double *theta, int kernel, int metric, double *out);
+/* Dense lower-triangular Sigma (factor = 0) or its Cholesky factor L
+ * (factor = 1) for n locations, row-major n x n with zeros above the
+ * diagonal, computed with tile size ts. */
+int exageostat_b200_covariance_dense(int n, const double *x, const double *y, const double *theta, int kernel,
+                                     int metric, int ts, int factor, double *out);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif

@@ -1,0 +1,167 @@
+"""CPU oracle for the exact Matern log-likelihood path (TEST INFRASTRUCTURE).
+
+Only the tests, the smoke check and the benchmark's CPU-baseline leg use this
+package, and only as the checker.  The product library never imports it.
+
+It wraps ``oracle/_build/liboracle.so`` (built from ``oracle.c`` by
+``oracle/Makefile``), a C restatement of the reference algorithm with the
+reference file:line of every function in its header comment.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+import subprocess
+
+import numpy as np
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+_LIB_PATH = os.path.join(_HERE, "_build", "liboracle.so")
+_lib = None
+
+_D = ctypes.c_double
+_I = ctypes.c_int
+_PD = ctypes.POINTER(ctypes.c_double)
+
+
+def build(force: bool = False) -> str:
+    """Compile the oracle with its Makefile (gcc + numpy's OpenBLAS)."""
+    if force or not os.path.exists(_LIB_PATH):
+        subprocess.run(["make", "-s", "-C", _HERE], check=True)
+    return _LIB_PATH
+
+
+def lib():
+    global _lib
+    if _lib is None:
+        if not os.path.exists(_LIB_PATH):
+            build()
+        L = ctypes.CDLL(_LIB_PATH)
+        L.ora_bessel_knu.restype = _D
+        L.ora_bessel_knu.argtypes = [_D, _D]
+        L.ora_generate_xy_loc.argtypes = [_I, _I, _PD, _PD]
+        L.ora_rand_replay.argtypes = [_I, ctypes.c_long]
+        L.ora_pick_random_points.argtypes = [_I, _PD, _PD, _PD, _I, _PD, _PD, _PD, _PD, _PD, _PD]
+        L.ora_locations_obs_zsort_inplace.argtypes = [_I, _PD, _PD, _PD]
+        L.ora_core_dcmg.argtypes = [_PD, _I, _I, _I, _I, _PD, _PD, _PD, _PD, _PD, _I]
+        L.ora_gen_lower_dense.argtypes = [_PD, _I, _PD, _PD, _PD, _I]
+        L.ora_dlarnv.argtypes = [_I, _I, _PD]
+        L.ora_dzvg.argtypes = [_I, _PD, _PD, _PD, _I, _PD, _PD]
+        L.ora_dmle.argtypes = [_I, _PD, _PD, _PD, _PD, _I, _PD, _PD, _PD, _PD]
+        L.ora_dpredict.restype = _D
+        L.ora_dpredict.argtypes = [_I, _I, _PD, _PD, _PD, _PD, _PD, _PD, _PD, _I, _PD]
+        L.ora_set_threads.argtypes = [_I]
+        L.ora_get_max_threads.restype = _I
+        _lib = L
+    return _lib
+
+
+def _p(a: np.ndarray):
+    return a.ctypes.data_as(_PD)
+
+
+def _f64(a) -> np.ndarray:
+    return np.ascontiguousarray(a, dtype=np.float64)
+
+
+def set_threads(n: int) -> None:
+    lib().ora_set_threads(int(n))
+
+
+def max_threads() -> int:
+    return int(lib().ora_get_max_threads())
+
+
+def bessel_knu(nu: float, x: float) -> float:
+    return float(lib().ora_bessel_knu(float(nu), float(x)))
+
+
+def generate_xy_loc(n: int, seed: int):
+    x = np.empty(n)
+    y = np.empty(n)
+    lib().ora_generate_xy_loc(int(n), int(seed), _p(x), _p(y))
+    return x, y
+
+
+def rand_replay(seed: int, skip: int) -> None:
+    lib().ora_rand_replay(int(seed), int(skip))
+
+
+def pick_random_points(x, y, z, n_miss: int, seed: int | None = None, skip: int | None = None):
+    """Hold-out split.  With ``seed`` the libc stream is first replayed to the
+    state GenerateXYLoc(N, seed) leaves it in (2 N draws)."""
+    x, y, z = _f64(x), _f64(y), _f64(z)
+    N = x.size
+    if seed is not None:
+        rand_replay(seed, 2 * N if skip is None else skip)
+    n_obs = N - n_miss
+    out = [np.empty(n_miss), np.empty(n_miss), np.empty(n_miss), np.empty(n_obs), np.empty(n_obs), np.empty(n_obs)]
+    lib().ora_pick_random_points(N, _p(x), _p(y), _p(z), int(n_miss), *[_p(a) for a in out])
+    xm, ym, za, xo, yo, zo = out
+    return dict(x_miss=xm, y_miss=ym, z_actual=za, x_obs=xo, y_obs=yo, z_obs=zo)
+
+
+def core_dcmg(m, n, m0, n0, x1, y1, x2, y2, theta, kernel=0) -> np.ndarray:
+    """Column-major m x n tile, returned as an (m, n) array."""
+    A = np.empty((n, m))  # column-major storage == C-order (n, m)
+    x1, y1, x2, y2, th = _f64(x1), _f64(y1), _f64(x2), _f64(y2), _f64(theta)
+    lib().ora_core_dcmg(_p(A), m, n, m0, n0, _p(x1), _p(y1), _p(x2), _p(y2), _p(th), int(kernel))
+    return A.T.copy()
+
+
+def covariance_lower(x, y, theta, kernel=0) -> np.ndarray:
+    """Lower triangle of Sigma(theta) (upper part left as zeros)."""
+    x, y, th = _f64(x), _f64(y), _f64(theta)
+    N = x.size
+    C = np.zeros((N, N))  # column-major buffer; transposed on return
+    lib().ora_gen_lower_dense(_p(C), N, _p(x), _p(y), _p(th), int(kernel))
+    return C.T.copy()
+
+
+def dlarnv(seed: int, n: int) -> np.ndarray:
+    out = np.empty(n)
+    info = lib().ora_dlarnv(int(seed), int(n), _p(out))
+    if info != 0:
+        raise RuntimeError("dlarnv failed: %d" % info)
+    return out
+
+
+def dzvg(x, y, theta, nrand, kernel=0) -> np.ndarray:
+    x, y, th, e = _f64(x), _f64(y), _f64(theta), _f64(nrand)
+    z = np.empty(x.size)
+    info = lib().ora_dzvg(x.size, _p(x), _p(y), _p(th), int(kernel), _p(e), _p(z))
+    if info != 0:
+        raise RuntimeError("oracle dzvg: dpotrf info=%d" % info)
+    return z
+
+
+def dmle(x, y, z, theta, kernel=0):
+    """Returns (loglik, logdet, dotp, (t_gen, t_chol, t_solve))."""
+    x, y, z, th = _f64(x), _f64(y), _f64(z), _f64(theta)
+    ll, ld, dp = _D(), _D(), _D()
+    times = np.zeros(3)
+    info = lib().ora_dmle(x.size, _p(x), _p(y), _p(z), _p(th), int(kernel), ctypes.byref(ll), ctypes.byref(ld),
+                          ctypes.byref(dp), _p(times))
+    if info != 0:
+        raise RuntimeError("oracle dmle: dpotrf info=%d" % info)
+    return ll.value, ld.value, dp.value, tuple(times)
+
+
+def dpredict(x_miss, y_miss, x_obs, y_obs, z_obs, z_actual, theta, kernel=0):
+    """Returns (mse, zmiss)."""
+    xm, ym, xo, yo, zo, th = (_f64(a) for a in (x_miss, y_miss, x_obs, y_obs, z_obs, theta))
+    za = None if z_actual is None else _f64(z_actual)
+    zmiss = np.empty(xm.size)
+    mse = lib().ora_dpredict(xm.size, xo.size, _p(xm), _p(ym), _p(xo), _p(yo), _p(zo),
+                             None if za is None else _p(za), _p(th), int(kernel), _p(zmiss))
+    return float(mse), zmiss
+
+
+def synthetic_field(N: int, seed: int, theta, kernel=0):
+    """The reference's synthetic workflow (synthetic_dmle_test.c:103-147,278):
+    e = dlarnv(3, {seed,seed,seed,1}), locations = GenerateXYLoc(N, seed),
+    z = L(theta) e."""
+    e = dlarnv(seed, N)
+    x, y = generate_xy_loc(N, seed)
+    z = dzvg(x, y, theta, e, kernel)
+    return x, y, z, e
