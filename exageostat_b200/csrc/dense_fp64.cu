@@ -266,6 +266,13 @@ __global__ void __launch_bounds__(XG_POTRF_THREADS) xg_potrf_diag_kernel(XgTileA
             }
         }
     }
+    /* zero the strict upper triangle outside the NB-wide diagonal blocks (the
+     * panel write-back zeroed the part inside them), so the stored tile is
+     * exactly L_kk and consumers may read it as a full tile */
+    for (long long idx = tid; idx < (long long)ts * ts; idx += blockDim.x) {
+        const int r = (int)(idx / ts), c = (int)(idx - (long long)r * ts);
+        if (c >= (r / NB + 1) * NB) A[idx] = 0.0;
+    }
     __syncthreads();
     /* deterministic reductions: log-det over lanes of warp 0, dot over vs */
     if (warp == 0) {

@@ -75,6 +75,23 @@ def test_cholesky_factor_matches_lapack(gpu, ora, n, ts):
     assert res < 60
 
 
+def test_zvg_matches_oracle_across_tile_sizes(gpu, ora):
+    """z = L e (TRMV over full stored tiles): exercises the zeroed upper
+    triangle of the diagonal tiles."""
+    from exageostat_b200.synthetic import dlarnv
+
+    N = 1000
+    x, y = ora.generate_xy_loc(N, 6)
+    e = dlarnv(6, N)
+    th = [1.0, 0.1, 0.5]
+    zref = ora.dzvg(x, y, th, e)
+    for ts in (128, 256, 512):
+        with gpu.Session(x, y, dts=ts) as s:
+            s.zvg(th, e)
+            z = s.z()
+        assert np.linalg.norm(z - zref) / np.linalg.norm(zref) < 1e-11, ts
+
+
 @pytest.mark.parametrize("case", _ll_cases(), ids=lambda c: c["name"])
 @pytest.mark.parametrize("ts", [128, 256])
 def test_loglik_matches_mpmath_golden(gpu, case, ts):
