@@ -199,10 +199,11 @@ def test_library_pick_random_points_matches_oracle(gpu, ora):
 
 
 def test_not_spd_reports_error_and_context_survives(gpu, ora):
-    """Duplicate locations make Sigma singular: the library reports it (the
-    reference exits) and the next evaluation still works."""
+    """A NaN location makes a pivot NaN: the library reports a non-positive-
+    definite covariance (the reference exits, MLE_misc.h:343-348) and the next
+    evaluation on the same context still works."""
     x, y = ora.generate_xy_loc(400, 2)
-    x[5], y[5] = x[6], y[6]
+    x[150] = np.nan
     z = np.ones(400)
     with pytest.raises(gpu.XgError) as ei:
         gpu.dmle_host(x, y, z, [1.0, 0.1, 0.5], ts=128)
@@ -210,9 +211,23 @@ def test_not_spd_reports_error_and_context_survives(gpu, ora):
     with gpu.Session(x, y, dts=128) as s:
         s.set_data(z=z)
         assert s.mle_alg([1.0, 0.1, 0.5]) == -np.inf
+        assert s.data.final_loglik == -np.inf
     x2, y2 = ora.generate_xy_loc(400, 2)
     ref = ora.dmle(x2, y2, z, [1.0, 0.1, 0.5])[0]
     assert gpu.dmle_host(x2, y2, z, [1.0, 0.1, 0.5], ts=128)[0] == pytest.approx(ref, rel=LL_RTOL)
+
+
+def test_duplicate_locations_do_not_crash(gpu, ora):
+    """Exactly repeated locations make Sigma singular in exact arithmetic; the
+    rounded pivot may come out on either side of zero (as in LAPACK), so the
+    call either reports NOT_SPD or returns a finite value."""
+    x, y = ora.generate_xy_loc(400, 2)
+    x[5], y[5] = x[6], y[6]
+    try:
+        ll = gpu.dmle_host(x, y, np.ones(400), [1.0, 0.1, 0.5], ts=128)[0]
+        assert np.isfinite(ll)
+    except gpu.XgError as e:
+        assert e.code == gpu.XG_ERR_NOT_SPD
 
 
 def test_bad_theta_is_rejected(gpu, ora):
