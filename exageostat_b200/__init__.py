@@ -102,7 +102,8 @@ EXPORTED_SYMBOLS = [
     "exageostat_b200_abi_version", "exageostat_b200_sizeof_MLE_data", "exageostat_b200_sizeof_output",
     "exageostat_b200_offsetof_MLE_data", "exageostat_b200_dmle_host", "exageostat_b200_bessel_knu",
     "exageostat_b200_matern_pairs", "exageostat_b200_covariance_dense", "exageostat_b200_set_data",
-    "exageostat_b200_set_profiling", "exageostat_b200_get_profile", "results",
+    "exageostat_b200_set_profiling", "exageostat_b200_get_profile", "exageostat_b200_dmle_device_noalloc",
+    "results",
 ]
 
 _lib = None
@@ -153,6 +154,7 @@ def lib():
         "exageostat_b200_set_data": (_I, [PM, _PD, _PD, _PD]),
         "exageostat_b200_set_profiling": (_I, [PM, _I]),
         "exageostat_b200_get_profile": (_I, [PM, _PD, _I]),
+        "exageostat_b200_dmle_device_noalloc": (_I, [_I, _PD, _PD, _PD, _PD, _I, _I, _PD, _VP]),
     }
     for name, (res, args) in sig.items():
         f = getattr(L, name)

@@ -361,6 +361,22 @@ int exageostat_b200_set_data(MLE_data *data, const double *x, const double *y, c
 int exageostat_b200_set_profiling(MLE_data *data, int on);
 int exageostat_b200_get_profile(MLE_data *data, double *out, int n);
 
+/* No counterpart in the reference.  The log-likelihood of
+ * exageostat_b200_dmle_host for callers that cannot call cudaMalloc (code
+ * running inside another framework's allocator or memory pool, or with the
+ * device heap exhausted).  Inputs and the result are DEVICE pointers owned by
+ * the caller: d_x, d_y, d_z (n doubles each) and d_out (3 doubles: loglik,
+ * logdet, z^T Sigma^-1 z); theta (3 or 4 values) is a host pointer; stream is
+ * a cudaStream_t (NULL = default stream); the call returns after the stream
+ * work completes.  The library works in one static device array of about
+ * 18 MB that every GPU loading the library holds until exit, so n is at most
+ * 2048 (larger n returns XG_ERR_BAD_ARGUMENT).  The first call on a device
+ * looks up that array's device address and sets up the kernels: make it
+ * before any stream capture.  All calls share the array; calls that overlap
+ * on the GPU race and must be serialised by the caller. */
+int exageostat_b200_dmle_device_noalloc(int n, const double *d_x, const double *d_y, const double *d_z,
+                                        const double *theta, int kernel, int metric, double *d_out, void *stream);
+
 /* Diagnostics used by the parity tests.  All run on the GPU. */
 int exageostat_b200_bessel_knu(int n, const double *nu, const double *x, double *out);
 int exageostat_b200_matern_pairs(int n, const double *x1, const double *y1, const double *x2, const double *y2,
