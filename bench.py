@@ -243,7 +243,7 @@ def main():
     clocks = clk.stop()
     prof = sess.profile()
     sess.set_profiling(False)
-    dev_time = prof["t_gen"] + prof["t_potrf"] + prof["t_trsm"] + prof["t_gemm"]
+    dev_time = prof["t_total"]
     t_max = dev_time
     if dist is not None:
         t = torch.tensor([dev_time], device="cuda", dtype=torch.float64)
@@ -271,7 +271,7 @@ def main():
            "d2h_bytes_per_step": 8 + 5 * 8, "path": "exageostat_b200_set_data + MLE_alg (C ABI), wall clock"}
 
     launches_per_eval = prof["launches"] / max(prof["evals"], 1)
-    gemm_launches = prof["nt"] - 1
+    gemm_launches = 2 * (prof["nt"] - 1) - 1
     achieved = prof["gemm_flops"] / prof["t_gemm"] / 1e12
     tpf = read_traffic_per_flop()
     flops_per_launch = prof["gemm_flops"] / max(prof["evals"], 1) / max(gemm_launches, 1)
@@ -281,6 +281,9 @@ def main():
                 "traffic": (tpf * flops_per_launch) if tpf else None,
                 "algorithmic_flops_per_launch": flops_per_launch,
                 "share_of_step": prof["t_gemm"] / dev_time,
+                "note": "achieved = algorithmic flops of both trailing-update launches of each step / their "
+                        "summed CUDA-event time; the lookahead panel (POTRF + TRSM) runs concurrently on a "
+                        "high-priority stream and is included in that time",
                 "phases_s_per_eval": {k: prof[k] / prof["evals"] for k in ("t_gen", "t_potrf", "t_trsm", "t_gemm")}}
     line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": 1e3 * t_max / args.steps, "higher_is_better": True,

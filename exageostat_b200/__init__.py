@@ -315,9 +315,10 @@ class Session:
         _check(self.L.exageostat_b200_set_profiling(ctypes.byref(self.data), 1 if on else 0))
 
     def profile(self) -> dict:
-        out = np.zeros(10)
-        _check(self.L.exageostat_b200_get_profile(ctypes.byref(self.data), _p(out), 10))
-        keys = ["t_gen", "t_potrf", "t_trsm", "t_gemm", "gemm_flops", "launches", "evals", "ts", "nt", "N"]
+        out = np.zeros(11)
+        _check(self.L.exageostat_b200_get_profile(ctypes.byref(self.data), _p(out), 11))
+        keys = ["t_gen", "t_potrf", "t_trsm", "t_gemm", "gemm_flops", "launches", "evals", "t_total", "ts", "nt",
+                "N"]
         return dict(zip(keys, out.tolist()))
 
     def close(self) -> None:

@@ -410,8 +410,11 @@ __global__ void __launch_bounds__(XG_TRSM_THREADS) xg_trsm_panel_kernel(XgTileAr
 #define XG_G_THREADS 288
 #define XG_G_STAGE_BYTES (2 * XG_G_BM * XG_G_BK * 8)
 
-__global__ void __launch_bounds__(XG_G_THREADS, 1) xg_syrk_gemm_kernel(const __grid_constant__ CUtensorMap map,
-                                                                       XgTileArgs T, int k, int *status)
+/* Updates the tiles (i, j), j0 <= j <= i < nt, with panel column k.  With
+ * single_col the launch covers column j0 only (the lookahead split: the next
+ * panel's column first, the rest of the trailing matrix in a second launch). */
+__global__ void __maxnreg__(224) xg_syrk_gemm_kernel(const __grid_constant__ CUtensorMap map, XgTileArgs T, int k,
+                                                    int j0, int single_col, int *status)
 {
     extern __shared__ __align__(1024) unsigned char xg_smem_raw[];
     unsigned char *smem = (unsigned char *)(((uintptr_t)xg_smem_raw + 1023) & ~(uintptr_t)1023);
@@ -423,8 +426,13 @@ __global__ void __launch_bounds__(XG_G_THREADS, 1) xg_syrk_gemm_kernel(const __g
     const int blk = blockIdx.x % (bpt * bpt);
     const int bi = blk / bpt, bj = blk % bpt;
     int ii, jj;
-    xg_pair_decode(pair, &ii, &jj);
-    const int i = k + 1 + ii, j = k + 1 + jj;
+    if (single_col) {
+        ii = (int)pair;
+        jj = 0;
+    } else {
+        xg_pair_decode(pair, &ii, &jj);
+    }
+    const int i = j0 + ii, j = j0 + jj;
     if (xg_cta_should_skip(status, i == j && bj > bi)) return;
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     if (tid == 0) {
@@ -464,13 +472,22 @@ __global__ void __launch_bounds__(XG_G_THREADS, 1) xg_syrk_gemm_kernel(const __g
     }
     const int wm = warp >> 2, wn = warp & 3;
     const int g = lane >> 2, tq = lane & 3;
+    double *C = T.data + xg_tile_index(i, j, T.nt) * (long long)ts * ts + (long long)(bi * XG_G_BM) * ts + bj * XG_G_BM;
+    /* accumulators start at -C (loaded while the TMA ring fills), the main
+     * loop adds L_ik L_jk^T and the epilogue stores -acc = C - L_ik L_jk^T */
     double acc[4][4][4];
 #pragma unroll
     for (int mi = 0; mi < 4; ++mi)
 #pragma unroll
         for (int ni = 0; ni < 4; ++ni)
 #pragma unroll
-            for (int e = 0; e < 4; ++e) acc[mi][ni][e] = 0.0;
+            for (int h = 0; h < 2; ++h) {
+                const int r = wm * 64 + mi * 16 + g + 8 * h;
+                const int c = wn * 32 + ni * 8 + 2 * tq;
+                const double2 cv = *reinterpret_cast<const double2 *>(C + (long long)r * ts + c);
+                acc[mi][ni][2 * h] = -cv.x;
+                acc[mi][ni][2 * h + 1] = -cv.y;
+            }
     bool ok = true;
     for (int kb = 0; kb < KT; ++kb) {
         const int s = kb % XG_G_STAGES;
@@ -480,24 +497,34 @@ __global__ void __launch_bounds__(XG_G_THREADS, 1) xg_syrk_gemm_kernel(const __g
         }
         const unsigned char *sa = smem + s * XG_G_STAGE_BYTES;
         const unsigned char *sb = sa + XG_G_BM * XG_G_BK * 8;
+        /* k permutation inside the 16-wide slab: at MMA step ks, lane slot t
+         * holds k = 4 t + ks.  A thread's four k values of a row are then
+         * contiguous (two 16-byte chunks), read with conflict-free LDS.128
+         * under the 128-byte swizzle. */
 #pragma unroll
-        for (int ks = 0; ks < XG_G_BK / 4; ++ks) {
-            const int kk = ks * 4 + tq;
-            double a[4][2], b[4];
+        for (int half = 0; half < 2; ++half) {
+            const int chunk = 2 * tq + half; /* k = 4 tq + 2 half + {0, 1} */
+            double2 a[4][2], b[4];
 #pragma unroll
             for (int mi = 0; mi < 4; ++mi) {
                 const int r = wm * 64 + mi * 16 + g;
-                a[mi][0] = *(const double *)(sa + xg_swz128_off(r, kk));
-                a[mi][1] = *(const double *)(sa + xg_swz128_off(r + 8, kk));
+                a[mi][0] = *(const double2 *)(sa + (r << 7) + ((chunk ^ (r & 7)) << 4));
+                a[mi][1] = *(const double2 *)(sa + ((r + 8) << 7) + ((chunk ^ ((r + 8) & 7)) << 4));
             }
 #pragma unroll
-            for (int ni = 0; ni < 4; ++ni) b[ni] = *(const double *)(sb + xg_swz128_off(wn * 32 + ni * 8 + g, kk));
+            for (int ni = 0; ni < 4; ++ni) {
+                const int r = wn * 32 + ni * 8 + g;
+                b[ni] = *(const double2 *)(sb + (r << 7) + ((chunk ^ (r & 7)) << 4));
+            }
 #pragma unroll
             for (int mi = 0; mi < 4; ++mi)
 #pragma unroll
-                for (int ni = 0; ni < 4; ++ni)
-                    xg_dmma_16x8x4(acc[mi][ni][0], acc[mi][ni][1], acc[mi][ni][2], acc[mi][ni][3], a[mi][0], a[mi][1],
-                                   b[ni]);
+                for (int ni = 0; ni < 4; ++ni) {
+                    xg_dmma_16x8x4(acc[mi][ni][0], acc[mi][ni][1], acc[mi][ni][2], acc[mi][ni][3], a[mi][0].x,
+                                   a[mi][1].x, b[ni].x);
+                    xg_dmma_16x8x4(acc[mi][ni][0], acc[mi][ni][1], acc[mi][ni][2], acc[mi][ni][3], a[mi][0].y,
+                                   a[mi][1].y, b[ni].y);
+                }
         }
         __syncwarp();
         if (lane == 0) xg_mbar_arrive(&empty[s]);
@@ -506,7 +533,6 @@ __global__ void __launch_bounds__(XG_G_THREADS, 1) xg_syrk_gemm_kernel(const __g
         if (lane == 0) atomicOr(status, XG_ST_TIMEOUT);
         return;
     }
-    double *C = T.data + xg_tile_index(i, j, T.nt) * (long long)ts * ts + (long long)(bi * XG_G_BM) * ts + bj * XG_G_BM;
 #pragma unroll
     for (int mi = 0; mi < 4; ++mi)
 #pragma unroll
@@ -515,11 +541,8 @@ __global__ void __launch_bounds__(XG_G_THREADS, 1) xg_syrk_gemm_kernel(const __g
             for (int h = 0; h < 2; ++h) {
                 const int r = wm * 64 + mi * 16 + g + 8 * h;
                 const int c = wn * 32 + ni * 8 + 2 * tq;
-                double2 *pc = reinterpret_cast<double2 *>(C + (long long)r * ts + c);
-                double2 cv = *pc;
-                cv.x -= acc[mi][ni][2 * h];
-                cv.y -= acc[mi][ni][2 * h + 1];
-                *pc = cv;
+                *reinterpret_cast<double2 *>(C + (long long)r * ts + c) =
+                    make_double2(-acc[mi][ni][2 * h], -acc[mi][ni][2 * h + 1]);
             }
 }
 
@@ -599,13 +622,17 @@ void xg_launch_trsm_panel(const XgTileArgs &T, int k, double *v, int with_rhs, c
                                                                                                    status);
 }
 
-void xg_launch_syrk_gemm(const CUtensorMap &map, const XgTileArgs &T, int k, int *status, cudaStream_t st)
+void xg_launch_syrk_gemm(const CUtensorMap &map, const XgTileArgs &T, int k, int *status, cudaStream_t st, int part)
 {
-    const long long n = T.nt - k - 1;
+    /* part: 0 = every trailing column, 1 = column k+1 only, 2 = columns >= k+2 */
+    const int j0 = (part == 2) ? k + 2 : k + 1;
+    const long long n = T.nt - j0;
     if (n <= 0) return;
     const int bpt = T.ts / XG_G_BM;
-    const long long blocks = n * (n + 1) / 2 * bpt * bpt;
-    xg_syrk_gemm_kernel<<<(unsigned)blocks, XG_G_THREADS, xg_gemm_smem_bytes(), st>>>(map, T, k, status);
+    const long long pairs = (part == 1) ? n : n * (n + 1) / 2;
+    const long long blocks = pairs * bpt * bpt;
+    xg_syrk_gemm_kernel<<<(unsigned)blocks, XG_G_THREADS, xg_gemm_smem_bytes(), st>>>(map, T, k, j0, part == 1,
+                                                                                       status);
 }
 
 void xg_launch_finalize(const double *part_logdet, const double *part_dot, int nt, int N, double *out,

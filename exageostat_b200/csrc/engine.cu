@@ -92,6 +92,9 @@ int xg_context_start(int dts)
         return xg_fail(XG_ERR_UNSUPPORTED, "device %d (%s, sm_%d%d) is not a B200-class sm_100 GPU", dev, prop.name,
                        prop.major, prop.minor);
     XG_CU(cudaStreamCreateWithFlags(&g_xg.stream, cudaStreamNonBlocking));
+    int prio_least = 0, prio_greatest = 0;
+    XG_CU(cudaDeviceGetStreamPriorityRange(&prio_least, &prio_greatest));
+    XG_CU(cudaStreamCreateWithPriority(&g_xg.stream_hi, cudaStreamNonBlocking, prio_greatest));
     cudaDriverEntryPointQueryResult q;
     void *fn = nullptr;
     XG_CU(cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &fn, cudaEnableDefault, &q));
@@ -204,18 +207,55 @@ int xg_check_theta(const double *theta, int kernel)
 
 /* Cholesky of M in place; with v != nullptr also v <- L^-1 v and the per-tile
  * partial sums (log-det in part[0:nt], |v_k|^2 in part[nt:2nt]). */
-void xg_factor(XgTileMatrix &M, double *v, double *part, int *status, int *info, cudaStream_t st, cudaEvent_t *pev)
+/* Right-looking tile Cholesky with the fused z solve.  Per step k:
+ *   panel   : POTRF(k,k) [+ log-det, + L_kk v_k = v_k]  ->  TRSM(i,k) [+ v_i -= L_ik v_k]
+ *   trailing: A_ij -= L_ik L_jk^T, j >= k+1
+ * With fs.st_hi the panel of step k+1 runs on the high-priority stream as soon
+ * as column k+1 has received the step-k update (the trailing update is split
+ * into "column k+1" and "the rest"), so it overlaps the rest of step k.
+ * Profiling events (5 per step): panel start, after POTRF, after TRSM,
+ * trailing start, trailing end. */
+void xg_factor_lookahead(XgTileMatrix &M, double *v, double *part, int *status, int *info, const XgFactorStreams &fs)
 {
     XgTileArgs T{M.d, M.ts, M.nt};
-    for (int k = 0; k < M.nt; ++k) {
-        if (pev) cudaEventRecord(pev[3 * k], st);
-        xg_launch_potrf_diag(T, k, v, part, part + M.nt, v != nullptr, status, info, st);
-        if (pev) cudaEventRecord(pev[3 * k + 1], st);
-        xg_launch_trsm_panel(T, k, v, v != nullptr, status, st);
-        if (pev) cudaEventRecord(pev[3 * k + 2], st);
-        xg_launch_syrk_gemm(M.map, T, k, status, st);
+    const bool la = fs.st_hi != nullptr;
+    cudaStream_t sp = la ? fs.st_hi : fs.st; /* panel stream */
+    cudaEvent_t *pev = fs.pev;
+    const int rhs = v != nullptr;
+    if (la) {
+        cudaEventRecord(fs.ev_upd, fs.st); /* the generated matrix */
     }
-    if (pev) cudaEventRecord(pev[3 * M.nt], st);
+    for (int k = 0; k < M.nt; ++k) {
+        if (la) cudaStreamWaitEvent(sp, fs.ev_upd, 0);
+        if (pev) cudaEventRecord(pev[5 * k], sp);
+        xg_launch_potrf_diag(T, k, v, part, part + M.nt, rhs, status, info, sp);
+        if (pev) cudaEventRecord(pev[5 * k + 1], sp);
+        xg_launch_trsm_panel(T, k, v, rhs, status, sp);
+        if (pev) cudaEventRecord(pev[5 * k + 2], sp);
+        if (la) {
+            cudaEventRecord(fs.ev_panel, sp);
+            cudaStreamWaitEvent(fs.st, fs.ev_panel, 0);
+        }
+        if (pev) cudaEventRecord(pev[5 * k + 3], fs.st);
+        if (k + 1 < M.nt) {
+            if (la) {
+                xg_launch_syrk_gemm(M.map, T, k, status, fs.st, 1);
+                cudaEventRecord(fs.ev_upd, fs.st);
+                xg_launch_syrk_gemm(M.map, T, k, status, fs.st, 2);
+            } else {
+                xg_launch_syrk_gemm(M.map, T, k, status, fs.st, 0);
+            }
+        }
+        if (pev) cudaEventRecord(pev[5 * k + 4], fs.st);
+    }
+}
+
+void xg_factor(XgTileMatrix &M, double *v, double *part, int *status, int *info, cudaStream_t st, cudaEvent_t *pev)
+{
+    XgFactorStreams fs;
+    fs.st = st;
+    fs.pev = pev;
+    xg_factor_lookahead(M, v, part, status, info, fs);
 }
 
 /* Algorithmic flops of the trailing update after step k: a GEMM (2 ts^3) per
@@ -230,7 +270,7 @@ double xg_trailing_flops(int nt, int ts, int k)
 int xg_field_set_profiling(XgField *f, int on)
 {
     if (on && !f->pev) {
-        const int n = 3 * f->C.nt + 1;
+        const int n = 5 * f->C.nt;
         f->pev = (cudaEvent_t *)calloc(n, sizeof(cudaEvent_t));
         for (int i = 0; i < n; ++i)
             if (cudaEventCreate(&f->pev[i]) != cudaSuccess) return xg_fail(XG_ERR_CUDA, "profiling events");
@@ -247,16 +287,24 @@ static void xg_field_collect_profile(XgField *f)
     cudaEventElapsedTime(&ms, f->ev[0], f->ev[1]);
     f->prof[0] += ms * 1e-3;
     for (int k = 0; k < nt; ++k) {
-        cudaEventElapsedTime(&ms, f->pev[3 * k], f->pev[3 * k + 1]);
+        cudaEventElapsedTime(&ms, f->pev[5 * k], f->pev[5 * k + 1]);
         f->prof[1] += ms * 1e-3;
-        cudaEventElapsedTime(&ms, f->pev[3 * k + 1], f->pev[3 * k + 2]);
+        cudaEventElapsedTime(&ms, f->pev[5 * k + 1], f->pev[5 * k + 2]);
         f->prof[2] += ms * 1e-3;
-        cudaEventElapsedTime(&ms, f->pev[3 * k + 2], (k + 1 < nt) ? f->pev[3 * k + 3] : f->pev[3 * nt]);
-        f->prof[3] += ms * 1e-3;
-        f->prof[4] += xg_trailing_flops(nt, f->C.ts, k);
+        if (k + 1 < nt) {
+            cudaEventElapsedTime(&ms, f->pev[5 * k + 3], f->pev[5 * k + 4]);
+            f->prof[3] += ms * 1e-3;
+            f->prof[4] += xg_trailing_flops(nt, f->C.ts, k);
+        }
     }
-    /* launches: generation, per step POTRF (+ TRSM + trailing when k < nt-1), finalize */
-    f->prof[5] += 1 + nt + 2.0 * (nt - 1) + 1;
+    cudaEventElapsedTime(&ms, f->ev[0], f->ev[2]);
+    f->prof[7] += ms * 1e-3;
+    /* launches: generation, POTRF per step, TRSM and two trailing launches per
+     * step but the last (the first trailing launch of the last step but one
+     * covers one column and the second is empty), finalize */
+    double launches = 1 + nt + 1;
+    for (int k = 0; k + 1 < nt; ++k) launches += 1 + 1 + (k + 2 < nt ? 1 : 0);
+    f->prof[5] += launches;
     f->prof[6] += 1;
 }
 
@@ -292,10 +340,12 @@ void xg_field_destroy(XgField *f)
     if (f->status) cudaFree(f->status);
     if (f->h_out) cudaFreeHost(f->h_out);
     if (f->pev) {
-        for (int i = 0; i < 3 * f->C.nt + 1; ++i)
+        for (int i = 0; i < 5 * f->C.nt; ++i)
             if (f->pev[i]) cudaEventDestroy(f->pev[i]);
         free(f->pev);
     }
+    if (f->ev_panel) cudaEventDestroy(f->ev_panel);
+    if (f->ev_upd) cudaEventDestroy(f->ev_upd);
     for (int i = 0; i < 4; ++i)
         if (f->ev[i]) cudaEventDestroy(f->ev[i]);
     delete f;
@@ -326,6 +376,9 @@ int xg_field_create(XgField **out, int N, int ts, const double *x, const double 
         rc = xg_fail(XG_ERR_NO_MEMORY, "pinned result buffer");
     for (int i = 0; i < 4 && !rc; ++i)
         if (cudaEventCreate(&f->ev[i]) != cudaSuccess) rc = xg_fail(XG_ERR_CUDA, "event");
+    if (!rc && (cudaEventCreateWithFlags(&f->ev_panel, cudaEventDisableTiming) != cudaSuccess ||
+                cudaEventCreateWithFlags(&f->ev_upd, cudaEventDisableTiming) != cudaSuccess))
+        rc = xg_fail(XG_ERR_CUDA, "lookahead events");
     if (!rc && cudaMemcpy(f->x, x, N * sizeof(double), cudaMemcpyHostToDevice) != cudaSuccess)
         rc = xg_fail(XG_ERR_CUDA, "upload x");
     if (!rc && cudaMemcpy(f->y, y, N * sizeof(double), cudaMemcpyHostToDevice) != cudaSuccess)
@@ -374,7 +427,13 @@ int xg_field_loglik(XgField *f, const double *theta, double *res, double *times)
     XG_CU(cudaEventRecord(f->ev[0], st));
     xg_launch_gen(T, f->C.ij, f->C.ntiles, f->x, f->y, f->x, f->y, f->N, f->N, p, f->metric, 1, st);
     XG_CU(cudaEventRecord(f->ev[1], st));
-    xg_factor(f->C, f->v, f->part, f->status, f->info, st, f->profiling ? f->pev : nullptr);
+    XgFactorStreams fs;
+    fs.st = st;
+    fs.st_hi = g_xg.stream_hi;
+    fs.ev_panel = f->ev_panel;
+    fs.ev_upd = f->ev_upd;
+    fs.pev = f->profiling ? f->pev : nullptr;
+    xg_factor_lookahead(f->C, f->v, f->part, f->status, f->info, fs);
     xg_launch_finalize(f->part, f->part + f->C.nt, f->C.nt, f->N, f->out, f->status, f->info, st);
     XG_CU(cudaEventRecord(f->ev[2], st));
     XG_CU(cudaMemcpyAsync(f->h_out, f->out, 5 * sizeof(double), cudaMemcpyDeviceToHost, st));
@@ -409,7 +468,12 @@ int xg_field_zvg(XgField *f, const double *theta, const double *nrand, double *t
     XG_CU(cudaEventRecord(f->ev[0], st));
     xg_launch_gen(T, f->C.ij, f->C.ntiles, f->x, f->y, f->x, f->y, f->N, f->N, p, f->metric, 1, st);
     XG_CU(cudaEventRecord(f->ev[1], st));
-    xg_factor(f->C, nullptr, f->part, f->status, f->info, st);
+    XgFactorStreams fs;
+    fs.st = st;
+    fs.st_hi = g_xg.stream_hi;
+    fs.ev_panel = f->ev_panel;
+    fs.ev_upd = f->ev_upd;
+    xg_factor_lookahead(f->C, nullptr, f->part, f->status, f->info, fs);
     xg_launch_trmv_lower(T, f->e, f->z, f->status, st);
     XG_CU(cudaEventRecord(f->ev[2], st));
     XG_CU(cudaGetLastError());
@@ -453,6 +517,8 @@ void xg_predict_destroy(XgPredict *q)
     for (double *b : bufs)
         if (b) cudaFree(b);
     if (q->status) cudaFree(q->status);
+    if (q->ev_panel) cudaEventDestroy(q->ev_panel);
+    if (q->ev_upd) cudaEventDestroy(q->ev_upd);
     delete q;
 }
 
@@ -477,6 +543,9 @@ int xg_predict_create(XgPredict **out, int nmiss, int nobs, int ts)
     if (!rc) rc = xg_dev_alloc(&q->part, 2 * (size_t)q->C22.nt);
     if (!rc) rc = xg_dev_alloc(&q->out, 8);
     if (!rc && cudaMalloc(&q->status, 2 * sizeof(int)) != cudaSuccess) rc = xg_fail(XG_ERR_NO_MEMORY, "status");
+    if (!rc && (cudaEventCreateWithFlags(&q->ev_panel, cudaEventDisableTiming) != cudaSuccess ||
+                cudaEventCreateWithFlags(&q->ev_upd, cudaEventDisableTiming) != cudaSuccess))
+        rc = xg_fail(XG_ERR_CUDA, "lookahead events");
     if (rc) {
         xg_predict_destroy(q);
         return rc;
@@ -506,7 +575,12 @@ int xg_predict_run(XgPredict *q, const double *theta, int kernel, int metric, co
     if (zactual) XG_CU(cudaMemcpyAsync(q->zact, zactual, nmiss * sizeof(double), cudaMemcpyHostToDevice, st));
     /* C22 = Sigma(obs, obs); POSV: L L^T alpha = zobs */
     xg_launch_gen(T, q->C22.ij, q->C22.ntiles, q->xo, q->yo, q->xo, q->yo, nobs, nobs, p, metric, 1, st);
-    xg_factor(q->C22, q->v, q->part, q->status, q->info(), st);
+    XgFactorStreams fs;
+    fs.st = st;
+    fs.st_hi = g_xg.stream_hi;
+    fs.ev_panel = q->ev_panel;
+    fs.ev_upd = q->ev_upd;
+    xg_factor_lookahead(q->C22, q->v, q->part, q->status, q->info(), fs);
     for (int k = q->C22.nt - 1; k >= 0; --k) xg_launch_trsv_lower_t_step(T, k, q->v, q->status, st);
     /* zmiss = Sigma(miss, obs) alpha, C12 generated on the fly */
     xg_launch_predict_cross(q->xm, q->ym, nmiss, q->xo, q->yo, nobs, q->v, p, metric, q->zmiss, st);

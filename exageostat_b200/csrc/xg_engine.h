@@ -16,8 +16,19 @@ struct XgContext {
     int device = 0;
     int sm_count = 0;
     int dts = 0;
-    cudaStream_t stream = nullptr;
+    cudaStream_t stream = nullptr;    /* trailing updates, generation, solves */
+    cudaStream_t stream_hi = nullptr; /* high priority: the lookahead panel (POTRF + TRSM) */
     std::mutex mu;
+};
+
+/* Streams and events of one factorisation.  With st_hi == nullptr the steps
+ * run in order on st; otherwise panel k+1 (POTRF, TRSM on st_hi) overlaps the
+ * trailing update of step k (st), ordered by the two events. */
+struct XgFactorStreams {
+    cudaStream_t st = nullptr;
+    cudaStream_t st_hi = nullptr;
+    cudaEvent_t ev_panel = nullptr, ev_upd = nullptr;
+    cudaEvent_t *pev = nullptr; /* optional profiling events, 4 per step + 1 */
 };
 extern XgContext g_xg;
 
@@ -45,10 +56,12 @@ struct XgField {
     double *h_out = nullptr; /* pinned copy of out */
     cudaEvent_t ev[4] = {nullptr, nullptr, nullptr, nullptr};
     bool have_z = false;
+    cudaEvent_t ev_panel = nullptr, ev_upd = nullptr; /* lookahead ordering */
     /* optional per-kernel-class timing (exageostat_b200_set_profiling) */
     bool profiling = false;
-    cudaEvent_t *pev = nullptr; /* 3 nt + 1 events around the factorisation kernels */
-    double prof[8] = {0, 0, 0, 0, 0, 0, 0, 0}; /* gen, potrf, trsm, gemm seconds; gemm flops; launches; evals */
+    cudaEvent_t *pev = nullptr; /* 4 nt + 1 events around the factorisation kernels */
+    /* gen, potrf, trsm, trailing seconds; trailing flops; launches; evals; total seconds */
+    double prof[8] = {0, 0, 0, 0, 0, 0, 0, 0};
 };
 
 struct XgPredict {
@@ -58,6 +71,7 @@ struct XgPredict {
     double *xm = nullptr, *ym = nullptr, *xo = nullptr, *yo = nullptr;
     double *v = nullptr, *zact = nullptr, *zmiss = nullptr, *part = nullptr, *out = nullptr;
     int *status = nullptr;
+    cudaEvent_t ev_panel = nullptr, ev_upd = nullptr;
     int *info() { return status + 1; }
 };
 
@@ -71,6 +85,7 @@ XgMaternParams xg_params(const double *theta, int kernel);
 int xg_check_theta(const double *theta, int kernel);
 void xg_factor(XgTileMatrix &M, double *v, double *part, int *status, int *info, cudaStream_t st,
                cudaEvent_t *pev = nullptr);
+void xg_factor_lookahead(XgTileMatrix &M, double *v, double *part, int *status, int *info, const XgFactorStreams &fs);
 double xg_trailing_flops(int nt, int ts, int k);
 int xg_field_set_data(XgField *f, const double *x, const double *y, const double *z);
 int xg_field_set_profiling(XgField *f, int on);

@@ -43,7 +43,8 @@ void xg_launch_gen(const XgTileArgs &T, const int2 *tile_ij, long long ntiles, c
 void xg_launch_potrf_diag(const XgTileArgs &T, int k, double *v, double *part_logdet, double *part_dot, int with_rhs,
                           int *status, int *info, cudaStream_t st);
 void xg_launch_trsm_panel(const XgTileArgs &T, int k, double *v, int with_rhs, const int *status, cudaStream_t st);
-void xg_launch_syrk_gemm(const CUtensorMap &map, const XgTileArgs &T, int k, int *status, cudaStream_t st);
+void xg_launch_syrk_gemm(const CUtensorMap &map, const XgTileArgs &T, int k, int *status, cudaStream_t st,
+                         int part = 0);
 void xg_launch_finalize(const double *part_logdet, const double *part_dot, int nt, int N, double *out,
                         const int *status, const int *info, cudaStream_t st);
 

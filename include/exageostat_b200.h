@@ -355,9 +355,11 @@ int exageostat_b200_set_data(MLE_data *data, const double *x, const double *y, c
 
 /* Per-kernel-class CUDA-event timing of the log-likelihood evaluations of
  * one MLE_data.  set_profiling(on) resets the counters; get_profile fills
- * out[0..9] = seconds in generation, diagonal POTRF, panel TRSM, trailing
- * update; trailing-update algorithmic flops; kernel launches; evaluations;
- * tile size; tiles per side; N. */
+ * out[0..10] = seconds in generation, diagonal POTRF, panel TRSM, trailing
+ * update (the panel overlaps the trailing update, so these may add up to
+ * more than the total); trailing-update algorithmic flops; kernel launches;
+ * evaluations; total seconds (generation to result); tile size; tiles per
+ * side; N. */
 int exageostat_b200_set_profiling(MLE_data *data, int on);
 int exageostat_b200_get_profile(MLE_data *data, double *out, int n);
 
