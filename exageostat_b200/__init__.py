@@ -103,7 +103,7 @@ EXPORTED_SYMBOLS = [
     "exageostat_b200_offsetof_MLE_data", "exageostat_b200_dmle_host", "exageostat_b200_bessel_knu",
     "exageostat_b200_matern_pairs", "exageostat_b200_covariance_dense", "exageostat_b200_set_data",
     "exageostat_b200_set_profiling", "exageostat_b200_get_profile", "exageostat_b200_dmle_device_noalloc",
-    "results",
+    "exageostat_b200_bobyqa", "results",
 ]
 
 _lib = None
@@ -155,6 +155,7 @@ def lib():
         "exageostat_b200_set_profiling": (_I, [PM, _I]),
         "exageostat_b200_get_profile": (_I, [PM, _PD, _I]),
         "exageostat_b200_dmle_device_noalloc": (_I, [_I, _PD, _PD, _PD, _PD, _I, _I, _PD, _VP]),
+        "exageostat_b200_bobyqa": (_I, [_I, _PD, _PD, _PD, _D, _D, _D, _I, _VP, _VP, _PD]),
     }
     for name, (res, args) in sig.items():
         f = getattr(L, name)
@@ -288,6 +289,14 @@ class Session:
                                              _p(g) if grad else None))
         return (ll.value, g) if grad else ll.value
 
+    def fit_bobyqa(self, lb, ub, x0=None, ftol_abs=1e-9, maxeval=0, rhobeg=0.0):
+        """MLE with the derivative-free maximiser driving MLE_alg through the C
+        ABI, as the reference driver does with NLopt (start = lower bounds,
+        examples/examples.c:263-264).  Returns (theta_hat, loglik, evals)."""
+        x0 = _f64(lb).copy() if x0 is None else _f64(x0)
+        return bobyqa_maximize(None, x0, lb, ub, rhobeg=rhobeg, ftol_abs=ftol_abs, maxeval=maxeval,
+                               c_objective=self.L.MLE_alg, c_data=ctypes.cast(ctypes.byref(self.data), _VP))
+
     def mle_alg(self, theta) -> float:
         t = _f64(theta)
         return self.L.MLE_alg(self.nparams, _p(t), None, ctypes.cast(ctypes.byref(self.data), _VP))
@@ -332,6 +341,35 @@ class Session:
 
     def __exit__(self, *a):
         self.close()
+
+
+NLOPT_FUNC = ctypes.CFUNCTYPE(_D, ctypes.c_uint, _PD, _PD, _VP)
+
+
+def bobyqa_maximize(fun, x0, lb, ub, rhobeg=0.0, rhoend=0.0, ftol_abs=1e-9, maxeval=0, c_objective=None,
+                    c_data=None):
+    """Maximise with the library's bound-constrained derivative-free method.
+
+    ``fun(x) -> float`` is a Python objective; alternatively pass a C function
+    pointer (``c_objective``, e.g. ``lib().MLE_alg``) and its ``c_data``.
+    Returns (x_max, f_max, evaluations)."""
+    x = _f64(x0).copy()
+    lb, ub = _f64(lb), _f64(ub)
+    if c_objective is None:
+        def _cb(n, xp, gp, data):
+            return float(fun(np.ctypeslib.as_array(xp, shape=(n,)).copy()))
+
+        cfun = NLOPT_FUNC(_cb)
+        fptr = ctypes.cast(cfun, _VP)
+    else:
+        cfun = None
+        fptr = ctypes.cast(c_objective, _VP)
+    fmax = _D()
+    ev = lib().exageostat_b200_bobyqa(x.size, _p(x), _p(lb), _p(ub), rhobeg, rhoend, ftol_abs, maxeval, fptr,
+                                      c_data, ctypes.byref(fmax))
+    if ev < 0:
+        raise XgError(-ev, "bobyqa: bad arguments")
+    return x, fmax.value, ev
 
 
 def generate_xy_loc(n: int, seed: int):

@@ -402,18 +402,20 @@ __global__ void __launch_bounds__(XG_TRSM_THREADS) xg_trsm_panel_kernel(XgTileAr
 /* ========================================================================== */
 
 /* 128 x 128 output block per CTA, K streamed in 16-wide slabs through a
- * 4-stage TMA ring (128-byte swizzle).  Warps 0-7 compute (2 x 4 warps of
- * 64 x 32), warp 8 is the TMA producer. */
+ * 4-stage TMA ring (128-byte swizzle).  Eight warps compute (2 x 4 warps of
+ * 64 x 32); thread 0 also issues the TMA loads, refilling a stage once all
+ * eight warps have released it.  (A separate producer warp would make 9 warps,
+ * which caps a 1-CTA kernel at 168 registers; 8 warps may use 255.) */
 #define XG_G_BM 128
 #define XG_G_BK 16
 #define XG_G_STAGES 4
-#define XG_G_THREADS 288
+#define XG_G_THREADS 256
 #define XG_G_STAGE_BYTES (2 * XG_G_BM * XG_G_BK * 8)
 
 /* Updates the tiles (i, j), j0 <= j <= i < nt, with panel column k.  With
  * single_col the launch covers column j0 only (the lookahead split: the next
  * panel's column first, the rest of the trailing matrix in a second launch). */
-__global__ void __maxnreg__(224) xg_syrk_gemm_kernel(const __grid_constant__ CUtensorMap map, XgTileArgs T, int k,
+__global__ void __launch_bounds__(XG_G_THREADS, 1) xg_syrk_gemm_kernel(const __grid_constant__ CUtensorMap map, XgTileArgs T, int k,
                                                     int j0, int single_col, int *status)
 {
     extern __shared__ __align__(1024) unsigned char xg_smem_raw[];
@@ -446,29 +448,15 @@ __global__ void __maxnreg__(224) xg_syrk_gemm_kernel(const __grid_constant__ CUt
     const int KT = ts / XG_G_BK;
     const int rowA = (int)(xg_tile_index(i, k, T.nt) * ts + bi * XG_G_BM);
     const int rowB = (int)(xg_tile_index(j, k, T.nt) * ts + bj * XG_G_BM);
-    if (warp == 8) {
-        if (lane == 0) {
-            xg_prefetch_tensormap(&map);
-            int issued = 0;
-            bool ok = true;
-            for (int kb = 0; kb < KT; ++kb) {
-                const int s = kb % XG_G_STAGES;
-                if (kb >= XG_G_STAGES && !xg_mbar_wait(&empty[s], ((kb / XG_G_STAGES) - 1) & 1)) {
-                    ok = false;
-                    break;
-                }
-                unsigned char *sa = smem + s * XG_G_STAGE_BYTES;
-                xg_mbar_arrive_expect_tx(&full[s], XG_G_STAGE_BYTES);
-                xg_tma_load_2d(sa, &map, kb * XG_G_BK, rowA, &full[s]);
-                xg_tma_load_2d(sa + XG_G_BM * XG_G_BK * 8, &map, kb * XG_G_BK, rowB, &full[s]);
-                ++issued;
-            }
-            if (!ok) atomicOr(status, XG_ST_TIMEOUT);
-            /* every issued copy has landed before the CTA may exit */
-            for (int kb = (issued > XG_G_STAGES ? issued - XG_G_STAGES : 0); kb < issued; ++kb)
-                if (!xg_mbar_wait(&full[kb % XG_G_STAGES], (kb / XG_G_STAGES) & 1)) atomicOr(status, XG_ST_TIMEOUT);
+    int issued = 0;
+    if (tid == 0) {
+        xg_prefetch_tensormap(&map);
+        for (; issued < XG_G_STAGES && issued < KT; ++issued) {
+            unsigned char *sa = smem + issued * XG_G_STAGE_BYTES;
+            xg_mbar_arrive_expect_tx(&full[issued], XG_G_STAGE_BYTES);
+            xg_tma_load_2d(sa, &map, issued * XG_G_BK, rowA, &full[issued]);
+            xg_tma_load_2d(sa + XG_G_BM * XG_G_BK * 8, &map, issued * XG_G_BK, rowB, &full[issued]);
         }
-        return;
     }
     const int wm = warp >> 2, wn = warp & 3;
     const int g = lane >> 2, tq = lane & 3;
@@ -504,33 +492,51 @@ __global__ void __maxnreg__(224) xg_syrk_gemm_kernel(const __grid_constant__ CUt
 #pragma unroll
         for (int half = 0; half < 2; ++half) {
             const int chunk = 2 * tq + half; /* k = 4 tq + 2 half + {0, 1} */
-            double2 a[4][2], b[4];
-#pragma unroll
-            for (int mi = 0; mi < 4; ++mi) {
-                const int r = wm * 64 + mi * 16 + g;
-                a[mi][0] = *(const double2 *)(sa + (r << 7) + ((chunk ^ (r & 7)) << 4));
-                a[mi][1] = *(const double2 *)(sa + ((r + 8) << 7) + ((chunk ^ ((r + 8) & 7)) << 4));
-            }
+            double2 b[4];
 #pragma unroll
             for (int ni = 0; ni < 4; ++ni) {
                 const int r = wn * 32 + ni * 8 + g;
                 b[ni] = *(const double2 *)(sb + (r << 7) + ((chunk ^ (r & 7)) << 4));
             }
+            /* one m-tile's A fragments at a time keeps the kernel within the
+             * 168 registers a 288-thread CTA may use */
 #pragma unroll
-            for (int mi = 0; mi < 4; ++mi)
+            for (int mi = 0; mi < 4; ++mi) {
+                const int r = wm * 64 + mi * 16 + g;
+                const double2 a0 = *(const double2 *)(sa + (r << 7) + ((chunk ^ (r & 7)) << 4));
+                const double2 a1 = *(const double2 *)(sa + ((r + 8) << 7) + ((chunk ^ ((r + 8) & 7)) << 4));
 #pragma unroll
                 for (int ni = 0; ni < 4; ++ni) {
-                    xg_dmma_16x8x4(acc[mi][ni][0], acc[mi][ni][1], acc[mi][ni][2], acc[mi][ni][3], a[mi][0].x,
-                                   a[mi][1].x, b[ni].x);
-                    xg_dmma_16x8x4(acc[mi][ni][0], acc[mi][ni][1], acc[mi][ni][2], acc[mi][ni][3], a[mi][0].y,
-                                   a[mi][1].y, b[ni].y);
+                    xg_dmma_16x8x4(acc[mi][ni][0], acc[mi][ni][1], acc[mi][ni][2], acc[mi][ni][3], a0.x, a1.x,
+                                   b[ni].x);
+                    xg_dmma_16x8x4(acc[mi][ni][0], acc[mi][ni][1], acc[mi][ni][2], acc[mi][ni][3], a0.y, a1.y,
+                                   b[ni].y);
                 }
+            }
         }
         __syncwarp();
         if (lane == 0) xg_mbar_arrive(&empty[s]);
+        /* refill this stage with slab kb + STAGES once every warp released it */
+        if (tid == 0 && issued < KT) {
+            if (xg_mbar_wait(&empty[s], (kb / XG_G_STAGES) & 1)) {
+                unsigned char *sa = smem + s * XG_G_STAGE_BYTES;
+                xg_mbar_arrive_expect_tx(&full[s], XG_G_STAGE_BYTES);
+                xg_tma_load_2d(sa, &map, issued * XG_G_BK, rowA, &full[s]);
+                xg_tma_load_2d(sa + XG_G_BM * XG_G_BK * 8, &map, issued * XG_G_BK, rowB, &full[s]);
+                ++issued;
+            } else {
+                ok = false;
+            }
+        }
+        __syncwarp();
+        if (!ok) break;
     }
     if (!ok) {
-        if (lane == 0) atomicOr(status, XG_ST_TIMEOUT);
+        atomicOr(status, XG_ST_TIMEOUT);
+        /* every copy thread 0 issued lands before the CTA may exit */
+        if (tid == 0)
+            for (int q = (issued > XG_G_STAGES ? issued - XG_G_STAGES : 0); q < issued; ++q)
+                xg_mbar_wait(&full[q % XG_G_STAGES], (q / XG_G_STAGES) & 1);
         return;
     }
 #pragma unroll

@@ -616,6 +616,13 @@ int xg_covariance_dense(int n, const double *x, const double *y, const double *t
     cudaMemsetAsync(f->status, 0, 2 * sizeof(int), st);
     xg_launch_gen(T, f->C.ij, f->C.ntiles, f->x, f->y, f->x, f->y, n, n, p, metric, 1, st);
     if (factor) xg_factor(f->C, nullptr, f->part, f->status, f->info, st);
+    {
+        cudaError_t le = cudaGetLastError();
+        if (le != cudaSuccess) {
+            xg_field_destroy(f);
+            return xg_cuda_fail(le, "covariance launch");
+        }
+    }
     const int tsz = f->C.ts;
     const size_t tile_elems = (size_t)tsz * tsz;
     double *h = (double *)malloc(f->C.ntiles * tile_elems * sizeof(double));
@@ -675,6 +682,10 @@ int xg_matern_pairs_host(int n, const double *x1, const double *y1, const double
         cudaMemcpyAsync(d + (size_t)i * n, src[i], n * sizeof(double), cudaMemcpyHostToDevice, st);
     xg_launch_matern_pairs(d, d + n, d + 2 * (size_t)n, d + 3 * (size_t)n, n, xg_params(theta, kernel), metric,
                            d + 4 * (size_t)n, st);
+    if (cudaGetLastError() != cudaSuccess) {
+        cudaFree(d);
+        return xg_fail(XG_ERR_CUDA, "matern pairs launch failed");
+    }
     cudaMemcpyAsync(out, d + 4 * (size_t)n, n * sizeof(double), cudaMemcpyDeviceToHost, st);
     cudaError_t e = cudaStreamSynchronize(st);
     cudaFree(d);

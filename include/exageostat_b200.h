@@ -317,6 +317,21 @@ int locations_obs_zsort_inplace(int n, location *locations, double *z);
  * at offset nZmiss, as in the reference. */
 void pick_random_points(MLE_data *data, double *Zobs, double *Zactual, int nZmiss, int nZobs, int N);
 
+/* ---- MLE driver ---- */
+
+/* Bound-constrained derivative-free maximiser standing in for NLopt's
+ * LN_BOBYQA, which the reference driver uses (examples/synthetic_dmle_test.c:
+ * 140-142, 283-284; nlopt_set_ftol_abs / bounds in init_optimizer,
+ * misc/compute/MLE_misc.c:1352-1366).  f has NLopt's objective signature, so
+ * MLE_alg plugs in with data = the MLE_data pointer.  x holds the start and
+ * receives the maximiser; rhobeg <= 0 picks a quarter of the smallest bound
+ * range; ftol_abs > 0 stops when an accepted step changes f by less;
+ * maxeval <= 0 means no limit.  Returns the number of evaluations (or
+ * -XG_ERR_BAD_ARGUMENT); *fmax receives the best value. */
+int exageostat_b200_bobyqa(int n, double *x, const double *lb, const double *ub, double rhobeg, double rhoend,
+                           double ftol_abs, int maxeval, double (*f)(unsigned, const double *, double *, void *),
+                           void *data, double *fmax);
+
 /* ---- new entry points (no counterpart in the reference) ---- */
 
 /* Status-returning form of MLE_alg: 0 on success, else an XG_ERR_* code;
