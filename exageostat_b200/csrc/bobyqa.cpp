@@ -144,6 +144,16 @@ struct Model {
                     H[i * n + j] += rhs[a] * (Y[a * n + i] - xb[i]) * (Y[a * n + j] - xb[j]);
         return true;
     }
+    /* moves the base point to x (the model itself is unchanged): keeps the
+     * KKT system well scaled as the points cluster around the optimum */
+    void rebase(const double *x)
+    {
+        std::vector<double> gx((size_t)n);
+        grad(x, gx.data());
+        c = value(x);
+        g = gx;
+        xb.assign(x, x + n);
+    }
     /* values of all m Lagrange functions at x */
     bool lagrange(const double *x, std::vector<double> &out) const
     {
@@ -256,7 +266,9 @@ double norm2(const double *a, const double *b, int n)
  * maximiser).  f has NLopt's nlopt_func signature (MLE_alg fits).  Stops when
  * the trust-region resolution reaches rhoend, when an accepted step changes
  * the value by less than ftol_abs (> 0), or after maxeval evaluations
- * (<= 0: no limit).  Returns the number of evaluations, or a negative
+ * (<= 0: no limit).  The ftol test needs two accepted steps in a row below
+ * the threshold, so one lucky tiny step on a flat stretch does not end the
+ * search.  Returns the number of evaluations, or a negative
  * XG_ERR_* code; *fmax receives the best value found. */
 extern "C" int exageostat_b200_bobyqa(int n, double *x, const double *lb, const double *ub, double rhobeg,
                                       double rhoend, double ftol_abs, int maxeval,
@@ -337,15 +349,19 @@ extern "C" int exageostat_b200_bobyqa(int n, double *x, const double *lb, const 
         if (M.F[a] < M.F[kopt]) kopt = a;
     std::vector<double> s, xnew((size_t)n), lag;
     bool stop_ftol = false;
-    int fails_at_rho = 0;
+    int small_steps = 0;
     while (P.evals < P.maxeval && !stop_ftol) {
+        M.rebase(&M.Y[kopt * n]);
         const double *xo = &M.Y[kopt * n];
         trust_region_step(M, xo, lb, ub, delta, s);
         double snorm = 0;
         for (int i = 0; i < n; ++i) snorm += s[i] * s[i];
         snorm = sqrt(snorm);
-        bool improved = false;
-        if (snorm >= 0.5 * rho) {
+        if (snorm < 0.5 * rho) {
+            /* the model's step is too short to be worth a function value */
+            delta = std::max(0.1 * delta, rho);
+            if (delta <= 1.5 * rho) delta = rho;
+        } else {
             for (int i = 0; i < n; ++i) xnew[i] = std::min(ub[i], std::max(lb[i], xo[i] + s[i]));
             const double qred = M.value(xo) - M.value(xnew.data());
             const double fnew = P.eval(xnew.data());
@@ -363,10 +379,11 @@ extern "C" int exageostat_b200_bobyqa(int n, double *x, const double *lb, const 
             if (M.lagrange(xnew.data(), lag)) {
                 double best = -1;
                 for (int a = 0; a < m; ++a) {
+                    if (a == kopt) continue;
                     const double d = norm2(&M.Y[a * n], fnew < fold ? xnew.data() : xo, n);
                     const double w = std::max(1.0, (d / delta) * (d / delta));
                     const double sc = fabs(lag[a]) * w * w;
-                    if (a != kopt && sc > best) {
+                    if (sc > best) {
                         best = sc;
                         t = a;
                     }
@@ -378,15 +395,13 @@ extern "C" int exageostat_b200_bobyqa(int n, double *x, const double *lb, const 
             M.update();
             if (fnew < fold) {
                 kopt = t;
-                improved = true;
-                if (ftol_abs > 0 && fold - fnew < ftol_abs) stop_ftol = true;
+                /* two accepted steps in a row that change f by < ftol_abs */
+                small_steps = (ftol_abs > 0 && fold - fnew < ftol_abs) ? small_steps + 1 : 0;
+                if (small_steps >= 2) stop_ftol = true;
             }
-            if (ratio > 0.1) {
-                fails_at_rho = 0;
-                continue;
-            }
+            if (ratio > 0.1) continue;
         }
-        /* geometry: move the point farthest from the best one if it is far */
+        /* failure at this radius: improve the geometry if a point is far */
         int far = -1;
         double dmax = 0;
         for (int a = 0; a < m; ++a) {
@@ -396,22 +411,24 @@ extern "C" int exageostat_b200_bobyqa(int n, double *x, const double *lb, const 
                 far = a;
             }
         }
-        if (!improved && far >= 0 && dmax > 2.0 * delta && P.evals < P.maxeval) {
-            /* candidates on the box-clipped ball of radius rho around x_opt:
-             * the coordinate directions and the direction to the far point;
-             * keep the one where the far point's Lagrange function is largest */
+        if (far >= 0 && dmax > 2.0 * delta && P.evals < P.maxeval) {
+            /* candidates on the box-clipped ball of radius max(rho, delta/10)
+             * around x_opt: the coordinate directions and the direction to the
+             * far point; keep the one where the far point's Lagrange function
+             * is largest */
+            const double rad = std::max(rho, 0.1 * delta);
             const double *xo2 = &M.Y[kopt * n];
             std::vector<double> cand((size_t)n), bestc((size_t)n);
             double bestv = -1;
             for (int dir = 0; dir <= 2 * n; ++dir) {
                 for (int i = 0; i < n; ++i) cand[i] = xo2[i];
                 if (dir < 2 * n) {
-                    cand[dir / 2] += (dir & 1) ? -rho : rho;
+                    cand[dir / 2] += (dir & 1) ? -rad : rad;
                 } else {
-                    for (int i = 0; i < n; ++i) cand[i] += rho * (M.Y[far * n + i] - xo2[i]) / dmax;
+                    for (int i = 0; i < n; ++i) cand[i] += rad * (M.Y[far * n + i] - xo2[i]) / dmax;
                 }
                 for (int i = 0; i < n; ++i) cand[i] = std::min(ub[i], std::max(lb[i], cand[i]));
-                if (norm2(cand.data(), xo2, n) < 1e-3 * rho) continue;
+                if (norm2(cand.data(), xo2, n) < 1e-3 * rad) continue;
                 if (!M.lagrange(cand.data(), lag)) continue;
                 if (fabs(lag[far]) > bestv) {
                     bestv = fabs(lag[far]);
@@ -427,12 +444,9 @@ extern "C" int exageostat_b200_bobyqa(int n, double *x, const double *lb, const 
                 continue;
             }
         }
-        if (improved) continue;
-        /* no progress at this resolution: refine rho */
-        if (rho <= rhoend) {
-            if (++fails_at_rho >= 2) break;
-            continue;
-        }
+        /* retry with the reduced radius before refining the resolution */
+        if (std::max(delta, snorm) > rho) continue;
+        if (rho <= rhoend) break;
         const double ratio = rho / rhoend;
         const double rho_old = rho;
         if (ratio <= 16.0)

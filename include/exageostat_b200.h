@@ -325,7 +325,8 @@ void pick_random_points(MLE_data *data, double *Zobs, double *Zactual, int nZmis
  * misc/compute/MLE_misc.c:1352-1366).  f has NLopt's objective signature, so
  * MLE_alg plugs in with data = the MLE_data pointer.  x holds the start and
  * receives the maximiser; rhobeg <= 0 picks a quarter of the smallest bound
- * range; ftol_abs > 0 stops when an accepted step changes f by less;
+ * range; ftol_abs > 0 stops after two accepted steps in a row that change f
+ * by less;
  * maxeval <= 0 means no limit.  Returns the number of evaluations (or
  * -XG_ERR_BAD_ARGUMENT); *fmax receives the best value. */
 int exageostat_b200_bobyqa(int n, double *x, const double *lb, const double *ub, double rhobeg, double rhoend,

@@ -40,7 +40,10 @@ def test_matern_mle_on_oracle_objective(xg, ora):
     lb, ub = [0.01] * 3, [5.0] * 3
     th, fm, ev = xg.bobyqa_maximize(f, lb, lb, ub, ftol_abs=1e-9)
     assert fm >= f(theta0) - 1e-6
-    assert ev < 2000
-    # a second start reaches the same maximum
-    th2, fm2, _ = xg.bobyqa_maximize(f, [2.0, 1.0, 1.0], lb, ub, ftol_abs=1e-9)
-    assert abs(fm - fm2) < 1e-4 * abs(fm)
+    assert ev < 600
+    # a gradient-based maximiser from an interior start finds the same point
+    from scipy.optimize import minimize
+
+    r = minimize(lambda t: -f(t), [0.5, 0.5, 0.5], bounds=list(zip(lb, ub)), method="L-BFGS-B")
+    assert abs(fm + r.fun) < 1e-6 * abs(fm)
+    assert np.allclose(th, r.x, rtol=1e-3)
