@@ -229,7 +229,7 @@ extern "C" int exageostat_b200_loglik(MLE_data *data, const double *theta, doubl
     if (rc) return rc;
     if (!xg_is_exact(data)) return xg_fail(XG_ERR_UNSUPPORTED, "computation \"%s\"", data->computation);
     if (data->precision != 0) return xg_fail(XG_ERR_UNSUPPORTED, "precision %d", data->precision);
-    double res[3], times[2];
+    double res[3], times[3] = {0, 0, 0};
     data->det = 0;
     data->dotp = 0;
     double t_gen = 0, t_fact = 0;
@@ -237,7 +237,7 @@ extern "C" int exageostat_b200_loglik(MLE_data *data, const double *theta, doubl
         xg_recover(data->recovery_file, data->iter_count, np, loglik)) {
         rc = XG_OK;
     } else {
-        rc = xg_field_loglik(f, theta, res, times);
+        rc = grad ? xg_field_loglik_grad(f, theta, res, grad, times) : xg_field_loglik(f, theta, res, times);
         if (rc == XG_OK) {
             *loglik = res[0];
             data->det = 0.5 * res[1];
@@ -246,11 +246,11 @@ extern "C" int exageostat_b200_loglik(MLE_data *data, const double *theta, doubl
             t_fact = times[1];
         }
     }
-    if (rc == XG_OK && grad) {
-        for (int i = 0; i < np; ++i) grad[i] = NAN;
-        rc = xg_fail(XG_ERR_UNSUPPORTED, "the gradient is not available in this build");
+    if (rc != XG_OK) {
+        *loglik = -INFINITY;
+        if (grad)
+            for (int i = 0; i < np; ++i) grad[i] = NAN;
     }
-    if (rc != XG_OK && rc != XG_ERR_UNSUPPORTED) *loglik = -INFINITY;
     /* per-iterate record, MLE_dexact.c:441-488 */
     if (!xg_quiet()) {
         fprintf(stderr, " %3d- Model Parameters (", data->iter_count + 1);

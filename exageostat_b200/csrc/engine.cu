@@ -102,6 +102,7 @@ int xg_context_start(int dts)
         return xg_fail(XG_ERR_CUDA, "cuTensorMapEncodeTiled is not available from the driver");
     g_encode = (XgEncodeTiledFn)fn;
     cudaError_t e = xg_kernels_configure();
+    if (e == cudaSuccess) e = xg_gradient_kernels_configure();
     if (e != cudaSuccess) return xg_cuda_fail(e, "kernel attribute setup");
     g_xg.device = dev;
     g_xg.sm_count = prop.multiProcessorCount;
@@ -346,6 +347,9 @@ void xg_field_destroy(XgField *f)
     }
     if (f->ev_panel) cudaEventDestroy(f->ev_panel);
     if (f->ev_upd) cudaEventDestroy(f->ev_upd);
+    xg_tm_free(f->X);
+    if (f->gpart) cudaFree(f->gpart);
+    if (f->gout) cudaFree(f->gout);
     for (int i = 0; i < 4; ++i)
         if (f->ev[i]) cudaEventDestroy(f->ev[i]);
     delete f;
@@ -494,6 +498,68 @@ int xg_field_zvg(XgField *f, const double *theta, const double *nrand, double *t
     rc = xg_read_status(f);
     if (rc) return rc;
     f->have_z = true;
+    return XG_OK;
+}
+
+/* digamma: upward recurrence to x >= 10, then the asymptotic series
+ * psi(x) = ln x - 1/(2x) - sum_k B_2k / (2k x^2k) (Abramowitz & Stegun 6.3.18) */
+double xg_digamma(double x)
+{
+    double r = 0.0;
+    while (x < 10.0) {
+        r -= 1.0 / x;
+        x += 1.0;
+    }
+    const double i2 = 1.0 / (x * x);
+    const double series =
+        i2 * (1.0 / 12 - i2 * (1.0 / 120 - i2 * (1.0 / 252 - i2 * (1.0 / 240 - i2 * (1.0 / 132 - i2 * (691.0 / 32760 - i2 / 12))))));
+    return r + log(x) - 0.5 / x - series;
+}
+
+/* log-likelihood and its gradient (see gradient_fp64.cu for the steps);
+ * grad has 3 entries (4 for the nugget kernel) */
+int xg_field_loglik_grad(XgField *f, const double *theta, double *res, double *grad, double *times)
+{
+    if (!f->X.d) {
+        int rc = xg_tm_alloc(f->X, f->N, f->C.ts);
+        if (rc) return rc;
+        const long long blocks = xg_grad_contract_blocks(f->C.ntiles, f->C.ts);
+        if (cudaMalloc(&f->gpart, 4 * (size_t)blocks * sizeof(double)) != cudaSuccess ||
+            cudaMalloc(&f->gout, 4 * sizeof(double)) != cudaSuccess)
+            return xg_fail(XG_ERR_NO_MEMORY, "gradient workspace");
+    }
+    int rc = xg_field_loglik(f, theta, res, times);
+    if (rc) return rc;
+    cudaStream_t st = g_xg.stream;
+    XgTileArgs T{f->C.d, f->C.ts, f->C.nt};
+    const XgMaternParams p = xg_params(theta, f->kernel);
+    const double dlogcon = -(log(2.0) + xg_digamma(theta[2]));
+    XG_CU(cudaEventRecord(f->ev[0], st));
+    for (int k = f->C.nt - 1; k >= 0; --k) xg_launch_trsv_lower_t_step(T, k, f->v, f->status, st);
+    xg_launch_inverse_factor(f->X.map, f->C.map, f->X.d, f->C.d, f->C.nt, f->C.ts, f->status, st);
+    xg_launch_inverse_syrk(f->X.map, f->C.d, f->C.nt, f->C.ts, f->status, st);
+    xg_launch_grad_contract(f->C.d, f->C.ij, f->C.ntiles, f->C.nt, f->C.ts, f->x, f->y, f->v, f->N, p, f->kernel,
+                            f->metric, dlogcon, f->gpart, f->gout, st);
+    XG_CU(cudaEventRecord(f->ev[3], st));
+    double g4[4];
+    int sv[2];
+    XG_CU(cudaGetLastError());
+    XG_CU(cudaMemcpyAsync(g4, f->gout, sizeof g4, cudaMemcpyDeviceToHost, st));
+    XG_CU(cudaMemcpyAsync(sv, f->status, sizeof sv, cudaMemcpyDeviceToHost, st));
+    XG_CU(cudaStreamSynchronize(st));
+    if (sv[0]) {
+        f->h_out[3] = sv[0];
+        f->h_out[4] = sv[1];
+        return xg_read_status(f);
+    }
+    if (times) {
+        float ms = 0;
+        cudaEventElapsedTime(&ms, f->ev[0], f->ev[3]);
+        times[2] = ms * 1e-3;
+    }
+    const int np = f->kernel == 1 ? 4 : 3;
+    for (int i = 0; i < np; ++i) grad[i] = g4[i];
+    /* the contraction kernel accumulates the nugget term in slot 3 */
     return XG_OK;
 }
 

@@ -57,6 +57,10 @@ struct XgField {
     cudaEvent_t ev[4] = {nullptr, nullptr, nullptr, nullptr};
     bool have_z = false;
     cudaEvent_t ev_panel = nullptr, ev_upd = nullptr; /* lookahead ordering */
+    /* gradient workspace, allocated on the first gradient request */
+    XgTileMatrix X;              /* X = L^-T (lower-tile slots, X_IK at slot (K, I)) */
+    double *gpart = nullptr;     /* per-CTA contraction partials */
+    double *gout = nullptr;      /* 4 gradient sums */
     /* optional per-kernel-class timing (exageostat_b200_set_profiling) */
     bool profiling = false;
     cudaEvent_t *pev = nullptr; /* 4 nt + 1 events around the factorisation kernels */
@@ -95,6 +99,8 @@ void xg_field_destroy(XgField *f);
 int xg_field_set_z(XgField *f, const double *z);
 int xg_field_loglik(XgField *f, const double *theta, double *res, double *times);
 int xg_field_zvg(XgField *f, const double *theta, const double *nrand, double *times);
+int xg_field_loglik_grad(XgField *f, const double *theta, double *res, double *grad, double *times);
+double xg_digamma(double x);
 int xg_field_get_z(XgField *f, double *z, int n);
 
 int xg_predict_create(XgPredict **out, int nmiss, int nobs, int ts);

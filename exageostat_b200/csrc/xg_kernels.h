@@ -60,4 +60,14 @@ void xg_launch_matern_pairs(const double *x1, const double *y1, const double *x2
 
 void xg_launch_bessel(const double *nu, const double *x, int n, double *out, cudaStream_t st);
 
+/* gradient_fp64.cu */
+cudaError_t xg_gradient_kernels_configure();
+void xg_launch_inverse_factor(const CUtensorMap &mapX, const CUtensorMap &mapL, double *X, const double *L, int nt,
+                              int ts, int *status, cudaStream_t st);
+void xg_launch_inverse_syrk(const CUtensorMap &mapX, double *S, int nt, int ts, int *status, cudaStream_t st);
+long long xg_grad_contract_blocks(long long ntiles, int ts);
+void xg_launch_grad_contract(const double *S, const int2 *tile_ij, long long ntiles, int nt, int ts, const double *x,
+                             const double *y, const double *alpha, int N, const XgMaternParams &mp, int kernel,
+                             int metric, double dlogcon, double *part, double *out, cudaStream_t st);
+
 #endif
