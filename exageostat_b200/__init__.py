@@ -103,7 +103,8 @@ EXPORTED_SYMBOLS = [
     "exageostat_b200_offsetof_MLE_data", "exageostat_b200_dmle_host", "exageostat_b200_bessel_knu",
     "exageostat_b200_matern_pairs", "exageostat_b200_covariance_dense", "exageostat_b200_set_data",
     "exageostat_b200_set_profiling", "exageostat_b200_get_profile", "exageostat_b200_dmle_device_noalloc",
-    "exageostat_b200_bobyqa", "results",
+    "exageostat_b200_bobyqa", "EXAGEOSTAT_sdmle_Tile", "exageostat_b200_set_mixed",
+    "exageostat_b200_dmle_host_mixed", "exageostat_b200_mixed_factor_dense", "results",
 ]
 
 _lib = None
@@ -156,6 +157,10 @@ def lib():
         "exageostat_b200_get_profile": (_I, [PM, _PD, _I]),
         "exageostat_b200_dmle_device_noalloc": (_I, [_I, _PD, _PD, _PD, _PD, _I, _I, _PD, _VP]),
         "exageostat_b200_bobyqa": (_I, [_I, _PD, _PD, _PD, _D, _D, _D, _I, _VP, _VP, _PD]),
+        "EXAGEOSTAT_sdmle_Tile": (_D, [ctypes.c_uint, _PD, _PD, _VP]),
+        "exageostat_b200_set_mixed": (_I, [PM, _I, _I]),
+        "exageostat_b200_dmle_host_mixed": (_I, [_I, _PD, _PD, _PD, _PD, _I, _I, _I, _I, _I, _PD]),
+        "exageostat_b200_mixed_factor_dense": (_I, [_I, _PD, _PD, _PD, _I, _I, _I, _I, _I, _PD]),
     }
     for name, (res, args) in sig.items():
         f = getattr(L, name)
@@ -232,6 +237,24 @@ def covariance_dense(x, y, theta, kernel=0, metric=0, ts=0, factor=False) -> np.
     out = np.empty((n, n))
     _check(lib().exageostat_b200_covariance_dense(n, _p(x), _p(y), _p(_f64(theta)), kernel, metric, ts,
                                                   1 if factor else 0, _p(out)))
+    return out
+
+
+def dmle_host_mixed(x, y, z, theta, kernel=0, metric=0, ts=512, band=1, passes=3):
+    """One-shot banded mixed-precision log-likelihood: (loglik, logdet, dotp)."""
+    x, y, z = _f64(x), _f64(y), _f64(z)
+    out = np.empty(3)
+    _check(lib().exageostat_b200_dmle_host_mixed(x.size, _p(x), _p(y), _p(z), _p(_f64(theta)), kernel, metric, ts,
+                                                 band, passes, _p(out)))
+    return tuple(out)
+
+
+def mixed_factor_dense(x, y, theta, kernel=0, metric=0, ts=512, band=1, passes=3) -> np.ndarray:
+    x, y = _f64(x), _f64(y)
+    n = x.size
+    out = np.empty((n, n))
+    _check(lib().exageostat_b200_mixed_factor_dense(n, _p(x), _p(y), _p(_f64(theta)), kernel, metric, ts, band,
+                                                    passes, _p(out)))
     return out
 
 
@@ -319,6 +342,14 @@ class Session:
         arrs = [None if a is None else _f64(a) for a in (x, y, z)]
         _check(self.L.exageostat_b200_set_data(ctypes.byref(self.data),
                                                *[None if a is None else _p(a) for a in arrs]))
+
+    def set_mixed(self, band: int = 1, passes: int = 3) -> None:
+        """Switch MLE_alg / loglik to the banded mixed-precision path."""
+        _check(self.L.exageostat_b200_set_mixed(ctypes.byref(self.data), band, passes))
+        self.data.precision = 2
+
+    def set_fp64(self) -> None:
+        self.data.precision = 0
 
     def set_profiling(self, on: bool = True) -> None:
         _check(self.L.exageostat_b200_set_profiling(ctypes.byref(self.data), 1 if on else 0))

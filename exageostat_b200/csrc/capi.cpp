@@ -228,7 +228,15 @@ extern "C" int exageostat_b200_loglik(MLE_data *data, const double *theta, doubl
     int rc = xg_kernel_of(data, &kernel, &np);
     if (rc) return rc;
     if (!xg_is_exact(data)) return xg_fail(XG_ERR_UNSUPPORTED, "computation \"%s\"", data->computation);
-    if (data->precision != 0) return xg_fail(XG_ERR_UNSUPPORTED, "precision %d", data->precision);
+    if (data->precision != 0 && data->precision != 2)
+        return xg_fail(XG_ERR_UNSUPPORTED, "precision %d (0 = FP64 and 2 = banded mixed are supported)",
+                       data->precision);
+    const bool mixed = data->precision == 2;
+    if (mixed && grad) return xg_fail(XG_ERR_UNSUPPORTED, "the gradient is computed in FP64 only (precision 0)");
+    if (mixed && (!f->mx || f->mx->band != (data->diag_thick > 0 ? data->diag_thick : 1))) {
+        rc = xg_field_set_mixed(f, data->diag_thick > 0 ? data->diag_thick : 1, f->mx ? f->mx->passes : 3);
+        if (rc) return rc;
+    }
     double res[3], times[3] = {0, 0, 0};
     data->det = 0;
     data->dotp = 0;
@@ -237,7 +245,9 @@ extern "C" int exageostat_b200_loglik(MLE_data *data, const double *theta, doubl
         xg_recover(data->recovery_file, data->iter_count, np, loglik)) {
         rc = XG_OK;
     } else {
-        rc = grad ? xg_field_loglik_grad(f, theta, res, grad, times) : xg_field_loglik(f, theta, res, times);
+        rc = mixed  ? xg_field_loglik_mixed(f, theta, res, times)
+             : grad ? xg_field_loglik_grad(f, theta, res, grad, times)
+                    : xg_field_loglik(f, theta, res, times);
         if (rc == XG_OK) {
             *loglik = res[0];
             data->det = 0.5 * res[1];
@@ -295,6 +305,18 @@ extern "C" double MORSE_dmle_Tile(unsigned n, const double *theta, double *grad,
     return EXAGEOSTAT_dmle_Tile(n, theta, grad, data);
 }
 
+/* EXAGEOSTAT_sdmle_Tile (MLE_sdexact.c:172-357): the banded mixed-precision
+ * objective; data->diag_thick is the band width in tiles */
+extern "C" double EXAGEOSTAT_sdmle_Tile(unsigned n, const double *theta, double *grad, void *vdata)
+{
+    MLE_data *data = (MLE_data *)vdata;
+    const int saved = data->precision;
+    data->precision = 2;
+    const double ll = EXAGEOSTAT_dmle_Tile(n, theta, grad, vdata);
+    data->precision = saved;
+    return ll;
+}
+
 extern "C" double MLE_alg(unsigned n, const double *theta, double *grad, void *vdata)
 {
     MLE_data *data = (MLE_data *)vdata;
@@ -302,8 +324,8 @@ extern "C" double MLE_alg(unsigned n, const double *theta, double *grad, void *v
         fprintf(stderr, "MLE_alg: computation \"%s\" is not provided by this library\n", data->computation);
         return 0;
     }
-    if (data->precision == 0) return EXAGEOSTAT_dmle_Tile(n, theta, grad, vdata);
-    fprintf(stderr, "MLE_alg: precision %d is not provided by this build\n", data->precision);
+    if (data->precision == 0 || data->precision == 2) return EXAGEOSTAT_dmle_Tile(n, theta, grad, vdata);
+    fprintf(stderr, "MLE_alg: precision %d is not provided by this library\n", data->precision);
     return 0;
 }
 
@@ -413,6 +435,37 @@ extern "C" int exageostat_b200_dmle_host(int n, const double *x, const double *y
     if (!rc) memcpy(out, res, sizeof res);
     xg_field_destroy(f);
     return rc;
+}
+
+extern "C" int exageostat_b200_set_mixed(MLE_data *data, int band, int passes)
+{
+    XgField *f = xg_field_of(data);
+    if (!f) return xg_fail(XG_ERR_NOT_INITIALIZED, "no descriptors: call EXAGEOSTAT_dmle_Call first");
+    data->diag_thick = band;
+    return xg_field_set_mixed(f, band, passes);
+}
+
+extern "C" int exageostat_b200_dmle_host_mixed(int n, const double *x, const double *y, const double *z,
+                                               const double *theta, int kernel, int metric, int ts, int band,
+                                               int passes, double *out)
+{
+    if (kernel != 0 && kernel != 1) return xg_fail(XG_ERR_BAD_ARGUMENT, "kernel %d", kernel);
+    XgField *f = nullptr;
+    int rc = xg_field_create(&f, n, ts > 0 ? ts : 512, x, y, kernel, metric);
+    if (rc) return rc;
+    rc = xg_field_set_z(f, z);
+    if (!rc) rc = xg_field_set_mixed(f, band, passes);
+    double res[3];
+    if (!rc) rc = xg_field_loglik_mixed(f, theta, res, nullptr);
+    if (!rc) memcpy(out, res, sizeof res);
+    xg_field_destroy(f);
+    return rc;
+}
+
+extern "C" int exageostat_b200_mixed_factor_dense(int n, const double *x, const double *y, const double *theta,
+                                                  int kernel, int metric, int ts, int band, int passes, double *out)
+{
+    return xg_mixed_factor_dense(n, x, y, theta, kernel, metric, ts, band, passes, out);
 }
 
 extern "C" int exageostat_b200_bessel_knu(int n, const double *nu, const double *x, double *out)

@@ -115,7 +115,7 @@ __global__ void __launch_bounds__(XG_POTRF_THREADS) xg_potrf_diag_kernel(XgTileA
     const int ts = T.ts;
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     if (xg_cta_should_skip(status)) return;
-    double *A = T.data + xg_tile_index(k, k, T.nt) * (long long)ts * ts;
+    double *A = T.data + xg_slot64(T, k, k) * (long long)ts * ts;
     double *vk = v + (long long)k * ts;
     if (tid == 0) {
         s_fail = 0;
@@ -312,8 +312,8 @@ __global__ void __launch_bounds__(XG_TRSM_THREADS) xg_trsm_panel_kernel(XgTileAr
     const int strip = blockIdx.x % strips;
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     const int g = lane >> 2, tq = lane & 3;
-    double *B = T.data + xg_tile_index(i, k, T.nt) * (long long)ts * ts + (long long)strip * XG_TRSM_SR * ts;
-    const double *L = T.data + xg_tile_index(k, k, T.nt) * (long long)ts * ts;
+    double *B = T.data + xg_slot64(T, i, k) * (long long)ts * ts + (long long)strip * XG_TRSM_SR * ts;
+    const double *L = T.data + xg_slot64(T, k, k) * (long long)ts * ts;
     for (int idx = tid; idx < XG_TRSM_SR * ts; idx += blockDim.x) {
         const int r = idx / ts, c = idx - r * ts;
         S[r * LDS + c] = B[(long long)r * ts + c];
@@ -427,15 +427,24 @@ __global__ void __launch_bounds__(XG_G_THREADS, 1) xg_syrk_gemm_kernel(const __g
     const long long pair = blockIdx.x / (bpt * bpt);
     const int blk = blockIdx.x % (bpt * bpt);
     const int bi = blk / bpt, bj = blk % bpt;
-    int ii, jj;
-    if (single_col) {
-        ii = (int)pair;
-        jj = 0;
+    int i, j;
+    if (T.band) {
+        /* band targets (i, j), 0 <= i - j < band, j from j0 */
+        j = j0 + (int)(pair / T.band);
+        i = j + (int)(pair % T.band);
+        if (single_col && j != j0) i = T.nt; /* outside the launch */
     } else {
-        xg_pair_decode(pair, &ii, &jj);
+        int ii, jj;
+        if (single_col) {
+            ii = (int)pair;
+            jj = 0;
+        } else {
+            xg_pair_decode(pair, &ii, &jj);
+        }
+        i = j0 + ii;
+        j = j0 + jj;
     }
-    const int i = j0 + ii, j = j0 + jj;
-    if (xg_cta_should_skip(status, i == j && bj > bi)) return;
+    if (xg_cta_should_skip(status, (i == j && bj > bi) || i >= T.nt)) return;
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     if (tid == 0) {
         for (int s = 0; s < XG_G_STAGES; ++s) {
@@ -446,8 +455,9 @@ __global__ void __launch_bounds__(XG_G_THREADS, 1) xg_syrk_gemm_kernel(const __g
     }
     __syncthreads();
     const int KT = ts / XG_G_BK;
-    const int rowA = (int)(xg_tile_index(i, k, T.nt) * ts + bi * XG_G_BM);
-    const int rowB = (int)(xg_tile_index(j, k, T.nt) * ts + bj * XG_G_BM);
+    /* operands: packed tiles (i, k), (j, k), or rows of the FP64 panel copy in mixed mode */
+    const int rowA = T.band ? i * ts + bi * XG_G_BM : (int)(xg_tile_index(i, k, T.nt) * ts + bi * XG_G_BM);
+    const int rowB = T.band ? j * ts + bj * XG_G_BM : (int)(xg_tile_index(j, k, T.nt) * ts + bj * XG_G_BM);
     int issued = 0;
     if (tid == 0) {
         xg_prefetch_tensormap(&map);
@@ -460,7 +470,7 @@ __global__ void __launch_bounds__(XG_G_THREADS, 1) xg_syrk_gemm_kernel(const __g
     }
     const int wm = warp >> 2, wn = warp & 3;
     const int g = lane >> 2, tq = lane & 3;
-    double *C = T.data + xg_tile_index(i, j, T.nt) * (long long)ts * ts + (long long)(bi * XG_G_BM) * ts + bj * XG_G_BM;
+    double *C = T.data + xg_slot64(T, i, j) * (long long)ts * ts + (long long)(bi * XG_G_BM) * ts + bj * XG_G_BM;
     /* accumulators start at -C (loaded while the TMA ring fills), the main
      * loop adds L_ik L_jk^T and the epilogue stores -acc = C - L_ik L_jk^T */
     double acc[4][4][4];
@@ -620,9 +630,12 @@ void xg_launch_potrf_diag(const XgTileArgs &T, int k, double *v, double *part_lo
                                                                      info);
 }
 
-void xg_launch_trsm_panel(const XgTileArgs &T, int k, double *v, int with_rhs, const int *status, cudaStream_t st)
+void xg_launch_trsm_panel(const XgTileArgs &T, int k, double *v, int with_rhs, const int *status, cudaStream_t st,
+                          int i1)
 {
-    const int n = T.nt - k - 1;
+    /* tiles i = k+1 .. i1-1 (i1 < 0: to the last tile) */
+    const int last = (i1 < 0 || i1 > T.nt) ? T.nt : i1;
+    const int n = last - k - 1;
     if (n <= 0) return;
     xg_trsm_panel_kernel<<<n * (T.ts / XG_TRSM_SR), XG_TRSM_THREADS, xg_trsm_smem_bytes(T.ts), st>>>(T, k, v, with_rhs,
                                                                                                    status);
@@ -638,6 +651,20 @@ void xg_launch_syrk_gemm(const CUtensorMap &map, const XgTileArgs &T, int k, int
     const long long pairs = (part == 1) ? n : n * (n + 1) / 2;
     const long long blocks = pairs * bpt * bpt;
     xg_syrk_gemm_kernel<<<(unsigned)blocks, XG_G_THREADS, xg_gemm_smem_bytes(), st>>>(map, T, k, j0, part == 1,
+                                                                                       status);
+}
+
+/* band targets of the trailing update in mixed mode: part 1 = column k+1,
+ * part 2 = columns >= k+2, part 0 = all */
+void xg_launch_band_gemm(const CUtensorMap &p64map, const XgTileArgs &T, int k, int part, int *status,
+                         cudaStream_t st)
+{
+    const int j0 = (part == 2) ? k + 2 : k + 1;
+    const long long ncol = (part == 1) ? 1 : T.nt - j0;
+    if (j0 >= T.nt || ncol <= 0) return;
+    const int bpt = T.ts / XG_G_BM;
+    const long long blocks = ncol * T.band * bpt * bpt;
+    xg_syrk_gemm_kernel<<<(unsigned)blocks, XG_G_THREADS, xg_gemm_smem_bytes(), st>>>(p64map, T, k, j0, part == 1,
                                                                                        status);
 }
 

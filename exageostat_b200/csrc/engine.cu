@@ -20,6 +20,7 @@
 
 #include <mutex>
 #include <string>
+#include <vector>
 
 #include "../../include/exageostat_b200.h"
 #include "xg_common.cuh"
@@ -103,6 +104,7 @@ int xg_context_start(int dts)
     g_encode = (XgEncodeTiledFn)fn;
     cudaError_t e = xg_kernels_configure();
     if (e == cudaSuccess) e = xg_gradient_kernels_configure();
+    if (e == cudaSuccess) e = xg_mixed_kernels_configure();
     if (e != cudaSuccess) return xg_cuda_fail(e, "kernel attribute setup");
     g_xg.device = dev;
     g_xg.sm_count = prop.multiProcessorCount;
@@ -309,6 +311,10 @@ static void xg_field_collect_profile(XgField *f)
     f->prof[6] += 1;
 }
 
+/* mixed: the same event layout; flops split into band (FP64) and off-band
+ * (TF32) parts, prof[4] counts all trailing-update flops */
+void xg_field_collect_profile_mixed(XgField *f) { xg_field_collect_profile(f); }
+
 int xg_field_set_data(XgField *f, const double *x, const double *y, const double *z)
 {
     cudaStream_t st = g_xg.stream;
@@ -348,6 +354,7 @@ void xg_field_destroy(XgField *f)
     if (f->ev_panel) cudaEventDestroy(f->ev_panel);
     if (f->ev_upd) cudaEventDestroy(f->ev_upd);
     xg_tm_free(f->X);
+    if (f->mx) xg_mixed_destroy(f->mx);
     if (f->gpart) cudaFree(f->gpart);
     if (f->gout) cudaFree(f->gout);
     for (int i = 0; i < 4; ++i)
@@ -561,6 +568,238 @@ int xg_field_loglik_grad(XgField *f, const double *theta, double *res, double *g
     for (int i = 0; i < np; ++i) grad[i] = g4[i];
     /* the contraction kernel accumulates the nugget term in slot 3 */
     return XG_OK;
+}
+
+/* ------------------------------------------------------------------------- */
+/* banded mixed precision                                                    */
+/* ------------------------------------------------------------------------- */
+
+static int xg_encode(CUtensorMap *map, CUtensorMapDataType dt, size_t esize, void *base, cuuint64_t cols,
+                     cuuint64_t rows, cuuint32_t box_cols, cuuint32_t box_rows)
+{
+    cuuint64_t dims[2] = {cols, rows};
+    cuuint64_t strides[1] = {cols * esize};
+    cuuint32_t box[2] = {box_cols, box_rows};
+    cuuint32_t estr[2] = {1, 1};
+    CUresult r = g_encode(map, dt, 2, base, dims, strides, box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE,
+                          CU_TENSOR_MAP_SWIZZLE_128B, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+                          CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+    return r == CUDA_SUCCESS ? XG_OK : xg_fail(XG_ERR_CUDA, "cuTensorMapEncodeTiled failed (%d)", (int)r);
+}
+
+void xg_mixed_destroy(XgMixed *m)
+{
+    if (!m) return;
+    if (m->T.data) cudaFree(m->T.data);
+    if (m->T.data32) cudaFree(m->T.data32);
+    for (int b = 0; b < 2; ++b) {
+        if (m->p64[b]) cudaFree(m->p64[b]);
+        if (m->phi[b]) cudaFree(m->phi[b]);
+        if (m->plo[b]) cudaFree(m->plo[b]);
+    }
+    delete m;
+}
+
+static int xg_mixed_create(XgMixed **out, int N, int ts, int band, int passes)
+{
+    *out = nullptr;
+    if (ts % 256 != 0) return xg_fail(XG_ERR_BAD_ARGUMENT, "mixed precision needs a tile size multiple of 256 (got %d)", ts);
+    if (band < 1) band = 1;
+    if (passes != 1 && passes != 3) return xg_fail(XG_ERR_BAD_ARGUMENT, "TF32 passes must be 1 or 3 (got %d)", passes);
+    XgMixed *m = new XgMixed();
+    const int nt = (N + ts - 1) / ts;
+    if (band > nt) band = nt;
+    m->band = band;
+    m->passes = passes;
+    m->T.ts = ts;
+    m->T.nt = nt;
+    m->T.band = band;
+    const size_t tile = (size_t)ts * ts;
+    const size_t np = (size_t)nt * ts;
+    int rc = XG_OK;
+    double *d64 = nullptr;
+    float *d32 = nullptr;
+    const long long noff = xg_num_offband_tiles(nt, band);
+    if (cudaMalloc(&d64, (size_t)nt * band * tile * sizeof(double)) != cudaSuccess)
+        rc = xg_fail(XG_ERR_NO_MEMORY, "mixed band tiles");
+    if (!rc && noff > 0 && cudaMalloc(&d32, (size_t)noff * tile * sizeof(float)) != cudaSuccess)
+        rc = xg_fail(XG_ERR_NO_MEMORY, "mixed off-band tiles (%.2f GB)", noff * tile * 4.0 / 1e9);
+    m->T.data = d64;
+    m->T.data32 = d32;
+    for (int b = 0; b < 2 && !rc; ++b) {
+        if (cudaMalloc(&m->p64[b], np * ts * sizeof(double)) != cudaSuccess ||
+            cudaMalloc(&m->phi[b], np * ts * sizeof(float)) != cudaSuccess ||
+            cudaMalloc(&m->plo[b], np * ts * sizeof(float)) != cudaSuccess) {
+            rc = xg_fail(XG_ERR_NO_MEMORY, "mixed panel buffers");
+            break;
+        }
+        rc = xg_encode(&m->maps[b].p64, CU_TENSOR_MAP_DATA_TYPE_FLOAT64, 8, m->p64[b], ts, np, 16, 128);
+        if (!rc) rc = xg_encode(&m->maps[b].ahi, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 4, m->phi[b], ts, np, 32, 128);
+        if (!rc) rc = xg_encode(&m->maps[b].bhi, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 4, m->phi[b], ts, np, 32, 256);
+        if (!rc) rc = xg_encode(&m->maps[b].alo, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 4, m->plo[b], ts, np, 32, 128);
+        if (!rc) rc = xg_encode(&m->maps[b].blo, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 4, m->plo[b], ts, np, 32, 256);
+    }
+    if (rc) {
+        xg_mixed_destroy(m);
+        return rc;
+    }
+    *out = m;
+    return XG_OK;
+}
+
+/* Mixed factorisation with the z solve fused (v), lookahead as in the FP64
+ * path: the panel of step k+1 (POTRF, band TRSM, FP32 TRSM, panel prep) runs
+ * on the high-priority stream under the rest of step k's trailing update. */
+static void xg_factor_mixed(XgMixed *m, double *v, double *part, int *status, int *info, const XgFactorStreams &fs)
+{
+    const XgTileArgs &T = m->T;
+    const int nt = T.nt;
+    const bool la = fs.st_hi != nullptr;
+    cudaStream_t sp = la ? fs.st_hi : fs.st;
+    cudaEvent_t *pev = fs.pev;
+    if (la) cudaEventRecord(fs.ev_upd, fs.st);
+    for (int k = 0; k < nt; ++k) {
+        const int b = k & 1;
+        if (la) cudaStreamWaitEvent(sp, fs.ev_upd, 0);
+        if (pev) cudaEventRecord(pev[5 * k], sp);
+        xg_launch_potrf_diag(T, k, v, part, part + nt, v != nullptr, status, info, sp);
+        if (pev) cudaEventRecord(pev[5 * k + 1], sp);
+        xg_launch_trsm_panel(T, k, v, v != nullptr, status, sp, k + T.band);
+        xg_launch_trsm_panel32(T, k, v, v != nullptr, status, sp);
+        if (k + 1 < nt) xg_launch_panel_prep(T, k, m->p64[b], m->phi[b], m->plo[b], m->passes, status, sp);
+        if (pev) cudaEventRecord(pev[5 * k + 2], sp);
+        if (la) {
+            cudaEventRecord(fs.ev_panel, sp);
+            cudaStreamWaitEvent(fs.st, fs.ev_panel, 0);
+        }
+        if (pev) cudaEventRecord(pev[5 * k + 3], fs.st);
+        if (k + 1 < nt) {
+            if (la) {
+                xg_launch_band_gemm(m->maps[b].p64, T, k, 1, status, fs.st);
+                xg_launch_offband_gemm(m->maps[b], T, k, 1, m->passes, g_xg.sm_count, status, fs.st);
+                cudaEventRecord(fs.ev_upd, fs.st);
+                xg_launch_band_gemm(m->maps[b].p64, T, k, 2, status, fs.st);
+                xg_launch_offband_gemm(m->maps[b], T, k, 2, m->passes, g_xg.sm_count, status, fs.st);
+            } else {
+                xg_launch_band_gemm(m->maps[b].p64, T, k, 0, status, fs.st);
+                xg_launch_offband_gemm(m->maps[b], T, k, 0, m->passes, g_xg.sm_count, status, fs.st);
+            }
+        }
+        if (pev) cudaEventRecord(pev[5 * k + 4], fs.st);
+    }
+}
+
+int xg_field_set_mixed(XgField *f, int band, int passes)
+{
+    if (f->mx && f->mx->band == band && f->mx->passes == passes) return XG_OK;
+    if (f->mx) {
+        xg_mixed_destroy(f->mx);
+        f->mx = nullptr;
+    }
+    return xg_mixed_create(&f->mx, f->N, f->C.ts, band, passes);
+}
+
+int xg_field_loglik_mixed(XgField *f, const double *theta, double *res, double *times)
+{
+    int rc = xg_check_theta(theta, f->kernel);
+    if (rc) return rc;
+    if (!f->have_z) return xg_fail(XG_ERR_BAD_ARGUMENT, "no observations: call MLE_zvg or set z first");
+    if (!f->mx) {
+        rc = xg_field_set_mixed(f, 1, 3);
+        if (rc) return rc;
+    }
+    XgMixed *m = f->mx;
+    cudaStream_t st = g_xg.stream;
+    const XgMaternParams p = xg_params(theta, f->kernel);
+    const size_t Np = (size_t)f->C.nt * f->C.ts;
+    XG_CU(cudaMemsetAsync(f->status, 0, 2 * sizeof(int), st));
+    XG_CU(cudaMemcpyAsync(f->v, f->z, Np * sizeof(double), cudaMemcpyDeviceToDevice, st));
+    XG_CU(cudaEventRecord(f->ev[0], st));
+    xg_launch_gen_mixed(m->T, f->C.ij, f->C.ntiles, f->x, f->y, f->N, p, f->metric, st);
+    XG_CU(cudaEventRecord(f->ev[1], st));
+    XgFactorStreams fs;
+    fs.st = st;
+    fs.st_hi = g_xg.stream_hi;
+    fs.ev_panel = f->ev_panel;
+    fs.ev_upd = f->ev_upd;
+    fs.pev = f->profiling ? f->pev : nullptr;
+    xg_factor_mixed(m, f->v, f->part, f->status, f->info, fs);
+    xg_launch_finalize(f->part, f->part + f->C.nt, f->C.nt, f->N, f->out, f->status, f->info, st);
+    XG_CU(cudaEventRecord(f->ev[2], st));
+    XG_CU(cudaMemcpyAsync(f->h_out, f->out, 5 * sizeof(double), cudaMemcpyDeviceToHost, st));
+    XG_CU(cudaGetLastError());
+    XG_CU(cudaStreamSynchronize(st));
+    if (times) {
+        float a = 0, b = 0;
+        cudaEventElapsedTime(&a, f->ev[0], f->ev[1]);
+        cudaEventElapsedTime(&b, f->ev[1], f->ev[2]);
+        times[0] = a * 1e-3;
+        times[1] = b * 1e-3;
+    }
+    if (f->profiling) xg_field_collect_profile_mixed(f);
+    rc = xg_read_status(f);
+    if (rc) return rc;
+    res[0] = f->h_out[0];
+    res[1] = f->h_out[1];
+    res[2] = f->h_out[2];
+    return XG_OK;
+}
+
+/* Dense mixed factor L (row-major n x n, zeros above the diagonal) for the
+ * parity tests: FP64 band tiles and FP32 off-band tiles widened. */
+int xg_mixed_factor_dense(int n, const double *x, const double *y, const double *theta, int kernel, int metric, int ts,
+                          int band, int passes, double *out)
+{
+    XgField *f = nullptr;
+    int rc = xg_check_theta(theta, kernel);
+    if (rc) return rc;
+    rc = xg_field_create(&f, n, ts, x, y, kernel, metric);
+    if (rc) return rc;
+    rc = xg_field_set_mixed(f, band, passes);
+    if (rc) {
+        xg_field_destroy(f);
+        return rc;
+    }
+    XgMixed *m = f->mx;
+    cudaStream_t st = g_xg.stream;
+    cudaMemsetAsync(f->status, 0, 2 * sizeof(int), st);
+    xg_launch_gen_mixed(m->T, f->C.ij, f->C.ntiles, f->x, f->y, n, xg_params(theta, kernel), metric, st);
+    XgFactorStreams fs;
+    fs.st = st;
+    fs.st_hi = g_xg.stream_hi;
+    fs.ev_panel = f->ev_panel;
+    fs.ev_upd = f->ev_upd;
+    xg_factor_mixed(m, nullptr, f->part, f->status, f->info, fs);
+    cudaError_t e = cudaGetLastError();
+    const int nt = m->T.nt, tsz = m->T.ts;
+    const size_t tile = (size_t)tsz * tsz;
+    std::vector<double> h64((size_t)nt * m->band * tile);
+    const long long noff = xg_num_offband_tiles(nt, m->band);
+    std::vector<float> h32((size_t)noff * tile);
+    int sv[2] = {0, 0};
+    if (e == cudaSuccess) e = cudaMemcpyAsync(h64.data(), m->T.data, h64.size() * sizeof(double), cudaMemcpyDeviceToHost, st);
+    if (e == cudaSuccess && noff)
+        e = cudaMemcpyAsync(h32.data(), m->T.data32, h32.size() * sizeof(float), cudaMemcpyDeviceToHost, st);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(sv, f->status, sizeof sv, cudaMemcpyDeviceToHost, st);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+    if (e != cudaSuccess) rc = xg_cuda_fail(e, "mixed factor");
+    if (!rc && sv[0]) rc = xg_fail(sv[0] & XG_ST_NOT_SPD ? XG_ERR_NOT_SPD : XG_ERR_TIMEOUT, "status 0x%x", sv[0]);
+    if (!rc)
+        for (int r = 0; r < n; ++r)
+            for (int c = 0; c < n; ++c) {
+                double val = 0.0;
+                if (c <= r) {
+                    const int i = r / tsz, j = c / tsz;
+                    const size_t off = (size_t)(r % tsz) * tsz + (c % tsz);
+                    if (i - j < m->band)
+                        val = h64[(size_t)xg_slot64(m->T, i, j) * tile + off];
+                    else
+                        val = h32[(size_t)xg_slot32(i, j, nt, m->band) * tile + off];
+                }
+                out[(size_t)r * n + c] = val;
+            }
+    xg_field_destroy(f);
+    return rc;
 }
 
 int xg_field_get_z(XgField *f, double *z, int n)

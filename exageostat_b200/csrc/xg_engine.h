@@ -40,6 +40,16 @@ struct XgTileMatrix {
     CUtensorMap map;    /* TMA view for the trailing-update kernel */
 };
 
+/* Banded mixed-precision workspace (mixed.cu): compact FP64 band tiles,
+ * compact FP32 off-band tiles, double-buffered panel copies. */
+struct XgMixed {
+    int band = 1, passes = 3;
+    XgTileArgs T;
+    double *p64[2] = {nullptr, nullptr};
+    float *phi[2] = {nullptr, nullptr}, *plo[2] = {nullptr, nullptr};
+    XgMixedMaps maps[2];
+};
+
 /* One dataset: locations, observations and the covariance / factor. */
 struct XgField {
     int N = 0;
@@ -59,6 +69,7 @@ struct XgField {
     cudaEvent_t ev_panel = nullptr, ev_upd = nullptr; /* lookahead ordering */
     /* gradient workspace, allocated on the first gradient request */
     XgTileMatrix X;              /* X = L^-T (lower-tile slots, X_IK at slot (K, I)) */
+    XgMixed *mx = nullptr;       /* mixed-precision workspace (precision 2) */
     double *gpart = nullptr;     /* per-CTA contraction partials */
     double *gout = nullptr;      /* 4 gradient sums */
     /* optional per-kernel-class timing (exageostat_b200_set_profiling) */
@@ -100,7 +111,13 @@ int xg_field_set_z(XgField *f, const double *z);
 int xg_field_loglik(XgField *f, const double *theta, double *res, double *times);
 int xg_field_zvg(XgField *f, const double *theta, const double *nrand, double *times);
 int xg_field_loglik_grad(XgField *f, const double *theta, double *res, double *grad, double *times);
+int xg_field_set_mixed(XgField *f, int band, int passes);
+int xg_field_loglik_mixed(XgField *f, const double *theta, double *res, double *times);
+void xg_mixed_destroy(XgMixed *m);
+int xg_mixed_factor_dense(int n, const double *x, const double *y, const double *theta, int kernel, int metric, int ts,
+                          int band, int passes, double *out);
 double xg_digamma(double x);
+void xg_field_collect_profile_mixed(XgField *f);
 int xg_field_get_z(XgField *f, double *z, int n);
 
 int xg_predict_create(XgPredict **out, int nmiss, int nobs, int ts);

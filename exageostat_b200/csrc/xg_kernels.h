@@ -12,12 +12,37 @@
  * 32 x ts doubles in shared memory. */
 #define XG_MAX_TS 512
 
-/* A lower-tile FP64 matrix on the device (see dense_fp64.cu for the layout). */
+/* A lower-tile matrix on the device (see dense_fp64.cu for the layout).
+ * band == 0: every lower tile is FP64 in data, packed (xg_tile_index).
+ * band  > 0: banded mixed precision -- data holds only the FP64 band tiles
+ * (0 <= i - j < band, compact: slot j * band + (i - j)), data32 the FP32
+ * off-band tiles (compact, xg_slot32). */
 struct XgTileArgs {
     double *data;
     int ts; /* tile size */
     int nt; /* tiles per side */
+    int band = 0;
+    float *data32 = nullptr;
 };
+
+__host__ __device__ inline long long xg_slot64(const XgTileArgs &T, int i, int j)
+{
+    if (T.band) return (long long)j * T.band + (i - j);
+    return (long long)j * T.nt - (long long)j * (j - 1) / 2 + (i - j);
+}
+
+/* off-band tile (i, j), i - j >= band: column j holds nt - j - band tiles */
+__host__ __device__ inline long long xg_slot32(int i, int j, int nt, int band)
+{
+    const long long M = nt - band;
+    return (long long)j * M - (long long)j * (j - 1) / 2 + (i - j - band);
+}
+
+__host__ __device__ inline long long xg_num_offband_tiles(int nt, int band)
+{
+    const long long M = nt - band;
+    return M > 0 ? M * (M + 1) / 2 : 0;
+}
 
 /* Matern parameters of one covariance evaluation.  con = sigma^2 /
  * (2^(nu-1) Gamma(nu)) is computed on the host exactly as core_zcmg.c:976-978;
@@ -42,9 +67,27 @@ void xg_launch_gen(const XgTileArgs &T, const int2 *tile_ij, long long ntiles, c
                    int identity_pad, cudaStream_t st);
 void xg_launch_potrf_diag(const XgTileArgs &T, int k, double *v, double *part_logdet, double *part_dot, int with_rhs,
                           int *status, int *info, cudaStream_t st);
-void xg_launch_trsm_panel(const XgTileArgs &T, int k, double *v, int with_rhs, const int *status, cudaStream_t st);
+void xg_launch_trsm_panel(const XgTileArgs &T, int k, double *v, int with_rhs, const int *status, cudaStream_t st,
+                          int i1 = -1);
 void xg_launch_syrk_gemm(const CUtensorMap &map, const XgTileArgs &T, int k, int *status, cudaStream_t st,
                          int part = 0);
+
+/* mixed.cu: banded mixed precision */
+struct XgMixedMaps {
+    CUtensorMap p64;           /* FP64 panel copy, boxes 128 x 16 (DMMA band targets) */
+    CUtensorMap ahi, bhi;      /* TF32 "hi" panel, boxes 128 x 32 and 256 x 32 (FP32) */
+    CUtensorMap alo, blo;      /* TF32 "lo" panel */
+};
+cudaError_t xg_mixed_kernels_configure();
+void xg_launch_gen_mixed(const XgTileArgs &T, const int2 *tile_ij, long long ntiles, const double *x, const double *y,
+                         int n, const XgMaternParams &p, int metric, cudaStream_t st);
+void xg_launch_trsm_panel32(const XgTileArgs &T, int k, double *v, int with_rhs, const int *status, cudaStream_t st);
+void xg_launch_panel_prep(const XgTileArgs &T, int k, double *p64, float *phi, float *plo, int passes,
+                          const int *status, cudaStream_t st);
+void xg_launch_band_gemm(const CUtensorMap &p64map, const XgTileArgs &T, int k, int part, int *status,
+                         cudaStream_t st);
+void xg_launch_offband_gemm(const XgMixedMaps &maps, const XgTileArgs &T, int k, int part, int passes, int sm_count,
+                            int *status, cudaStream_t st);
 void xg_launch_finalize(const double *part_logdet, const double *part_dot, int nt, int N, double *out,
                         const int *status, const int *info, cudaStream_t st);
 

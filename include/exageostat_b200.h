@@ -274,6 +274,13 @@ double MLE_alg(unsigned n, const double *theta, double *grad, void *data);
 
 /* exageostat_exact/src/include/MLE_exact.h:43-44 (MLE_dexact.c:231-489). */
 double EXAGEOSTAT_dmle_Tile(unsigned n, const double *theta, double *grad, void *data);
+
+/* The banded mixed-precision objective (EXAGEOSTAT_sdmle_Tile,
+ * exageostat_exact/src/compute/MLE_sdexact.c:172-357): tiles within
+ * data->diag_thick tiles of the diagonal in FP64, the others stored FP32 and
+ * updated on the TF32 tensor cores (three passes by default, see
+ * exageostat_b200_set_mixed).  grad must be NULL (the gradient is FP64 only). */
+double EXAGEOSTAT_sdmle_Tile(unsigned n, const double *theta, double *grad, void *data);
 double MORSE_dmle_Tile(unsigned n, const double *theta, double *grad, void *data);
 
 /* src/include/MLE.h:67 (src/compute/MLE.c:420-430): copies the synthetic z
@@ -364,6 +371,16 @@ long exageostat_b200_offsetof_MLE_data(const char *field);
 int exageostat_b200_dmle_host(int n, const double *x, const double *y, const double *z, const double *theta,
                               int kernel, int metric, int ts, double *out);
 
+/* Band width (tiles kept in FP64, >= 1; also written to data->diag_thick) and
+ * number of TF32 passes (1, or 3 for the hi/lo split with FP32-class
+ * products) of the mixed-precision path (precision = 2). */
+int exageostat_b200_set_mixed(MLE_data *data, int band, int passes);
+
+/* One-shot mixed-precision log-likelihood on host arrays (as
+ * exageostat_b200_dmle_host; ts must be a multiple of 256, 0 = 512). */
+int exageostat_b200_dmle_host_mixed(int n, const double *x, const double *y, const double *z, const double *theta,
+                                    int kernel, int metric, int ts, int band, int passes, double *out);
+
 /* Replaces the locations and/or observations (N host doubles each; NULL
  * keeps the current array) of an allocated MLE_data, e.g. for a new dataset
  * of the same size, without reallocating the device covariance. */
@@ -404,6 +421,10 @@ int exageostat_b200_matern_pairs(int n, const double *x1, const double *y1, cons
  * diagonal, computed with tile size ts. */
 int exageostat_b200_covariance_dense(int n, const double *x, const double *y, const double *theta, int kernel,
                                      int metric, int ts, int factor, double *out);
+/* The mixed-precision factor L (band tiles FP64, off-band FP32 widened),
+ * row-major n x n with zeros above the diagonal. */
+int exageostat_b200_mixed_factor_dense(int n, const double *x, const double *y, const double *theta, int kernel,
+                                       int metric, int ts, int band, int passes, double *out);
 
 #ifdef __cplusplus
 }
