@@ -5,8 +5,10 @@ One step = one evaluation of the hot path (generate Sigma(theta) -> tiled
 Cholesky with fused log-det and solve -> log-likelihood) for the N = 100,000
 univariate Matern field (317 x 317 jittered unit-square grid truncated to
 1e5 points, theta = (1.0, 0.05, 0.5), z = L e from the reference's
-generator).  The covariance (40 GB of lower tiles) is far larger than L2, so
-no explicit L2 flush is needed between steps.
+generator).  Two legs are timed: plain FP64 and banded mixed precision (the
+headline value; its |dl|/|l| against the FP64 leg is in the line).  The
+covariance (20-40 GB of tiles) is far larger than L2, so no explicit L2 flush
+is needed between steps.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--n N] [--impl ours|reference]
 
@@ -27,7 +29,8 @@ import time
 ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
-METRIC = "exact Matern log-likelihood evaluations per second (N=100000, FP64)"
+METRIC = ("exact Matern log-likelihood evaluations per second, N=100000, 1 B200: banded mixed precision "
+          "(FP64 band, FP32 off-band on TF32 tensor cores) vs plain FP64")
 UNIT = "loglik-evals/s"
 THETA = [1.0, 0.05, 0.5]
 
@@ -43,6 +46,8 @@ def parse():
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--cpu-seconds", type=float, default=12.0, help="target CPU time of the oracle sample")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--band", type=int, default=2, help="FP64 band width in tiles (mixed leg)")
+    ap.add_argument("--passes", type=int, default=3, help="TF32 passes of the off-band update (1 or 3)")
     return ap.parse_args()
 
 
@@ -190,6 +195,29 @@ def read_traffic_per_flop():
     return None
 
 
+def peak_bf16_tflops():
+    """Measured dense bf16 peak from MEASURED_PEAKS.json (driver-written), if present."""
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    try:
+        with open(p) as f:
+            d = json.load(f)
+        return float(d["bf16_tflops"]), float(d.get("bf16_tflops_sustained", d["bf16_tflops"])), "MEASURED_PEAKS.json"
+    except (OSError, KeyError, ValueError):
+        return 1590.0, 1400.0, "fallback"
+
+
+def timed_leg(sess, theta, steps, warmup, barrier):
+    for _ in range(warmup):
+        sess.loglik(theta)
+    sess.set_profiling(True)
+    barrier()
+    lls = [sess.loglik(theta) for _ in range(steps)]
+    barrier()
+    prof = sess.profile()
+    sess.set_profiling(False)
+    return lls, prof
+
+
 def main():
     args = parse()
     if args.impl == "reference":
@@ -216,7 +244,9 @@ def main():
 
     if not os.path.exists(xg.LIB_PATH):
         xgbuild.build()
-    peak = measured_dgemm_tflops(torch)
+    fp64_peak = measured_dgemm_tflops(torch)
+    bf16_peak, bf16_sust, bf16_src = peak_bf16_tflops()
+    tf32_peak = bf16_peak / 2.0  # dense TF32 runs at half the BF16 rate on B200
     xg.init(args.ts)
     N = args.n
     x, y = xg.generate_xy_loc(N, args.seed)
@@ -230,29 +260,39 @@ def main():
             dist.barrier()
         torch.cuda.synchronize()
 
+    def max_over_ranks(v):
+        if dist is None:
+            return v
+        t = torch.tensor([v], device="cuda", dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        return float(t.item())
+
+    # ---- plain FP64 leg ----
+    lls64, p64 = timed_leg(sess, THETA, args.steps, args.warmup, barrier)
+    t64 = max_over_ranks(p64["t_total"])
+    fp64_value = world * args.steps / t64
+    ach64 = p64["gemm_flops"] / p64["t_gemm"] / 1e12
+
+    # ---- banded mixed-precision leg (the headline) ----
+    sess.set_mixed(band=args.band, passes=args.passes)
+    clk = ClockSampler(local)
     for _ in range(args.warmup):
         sess.loglik(THETA)
     sess.set_profiling(True)
     barrier()
-    clk = ClockSampler(local)
     clk.start()
     t0 = time.perf_counter()
-    lls = [sess.loglik(THETA) for _ in range(args.steps)]
+    llsmx = [sess.loglik(THETA) for _ in range(args.steps)]
     wall = time.perf_counter() - t0
     barrier()
     clocks = clk.stop()
-    prof = sess.profile()
+    pmx = sess.profile()
     sess.set_profiling(False)
-    dev_time = prof["t_total"]
-    t_max = dev_time
-    if dist is not None:
-        t = torch.tensor([dev_time], device="cuda", dtype=torch.float64)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        t_max = float(t.item())
-    value = world * args.steps / t_max
+    tmx = max_over_ranks(pmx["t_total"])
+    value = world * args.steps / tmx
+    rel_err = abs(llsmx[-1] - lls64[-1]) / abs(lls64[-1])
 
-    # e2e: through the public C ABI from pinned host buffers: upload x, y, z,
-    # MLE_alg, loglik back to the host
+    # ---- end to end: C ABI from pinned host buffers (mixed path) ----
     px = torch.from_numpy(x).pin_memory()
     py = torch.from_numpy(y).pin_memory()
     pz = torch.from_numpy(z).pin_memory()
@@ -262,38 +302,47 @@ def main():
     for _ in range(e2e_steps):
         sess.set_data(px.numpy(), py.numpy(), pz.numpy())
         ll_e2e = sess.mle_alg(THETA)
-    e2e_wall = time.perf_counter() - t0
-    if dist is not None:
-        t = torch.tensor([e2e_wall], device="cuda", dtype=torch.float64)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        e2e_wall = float(t.item())
+    e2e_wall = max_over_ranks(time.perf_counter() - t0)
     e2e = {"value": world * e2e_steps / e2e_wall, "unit": UNIT, "h2d_bytes_per_step": 3 * N * 8,
-           "d2h_bytes_per_step": 8 + 5 * 8, "path": "exageostat_b200_set_data + MLE_alg (C ABI), wall clock"}
+           "d2h_bytes_per_step": 5 * 8,
+           "path": "exageostat_b200_set_data + MLE_alg (C ABI, precision 2), wall clock"}
 
-    launches_per_eval = prof["launches"] / max(prof["evals"], 1)
-    gemm_launches = 2 * (prof["nt"] - 1) - 1
-    achieved = prof["gemm_flops"] / prof["t_gemm"] / 1e12
+    passes = args.passes
+    t_off = pmx["t_offband"]
+    mma_flops = pmx["offband_flops"] * passes
+    ach_mx = mma_flops / t_off / 1e12 if t_off > 0 else 0.0
+    roofline = {"bound": "tensor", "kernel": "xg_offband_gemm_kernel (tcgen05 kind::tf32, %d pass%s, TMEM)" % (
+                    passes, "es" if passes > 1 else ""),
+                "achieved": ach_mx, "peak": tf32_peak, "unit": "TFLOP/s", "frac": ach_mx / tf32_peak,
+                "peak_source": "dense TF32 = bf16 / 2, bf16 from %s (of measured)" % bf16_src,
+                "traffic": None,
+                "algorithmic_flops_per_launch": pmx["offband_flops"] * passes / max(pmx["evals"], 1) /
+                max(2 * (pmx["nt"] - 1), 1),
+                "useful_fp32_tflops": pmx["offband_flops"] / t_off / 1e12 if t_off > 0 else 0.0,
+                "share_of_step": t_off / pmx["t_total"],
+                "phases_s_per_eval": {k: pmx[k] / pmx["evals"] for k in
+                                      ("t_gen", "t_potrf", "t_trsm", "t_gemm", "t_offband", "t_band")}}
     tpf = read_traffic_per_flop()
-    flops_per_launch = prof["gemm_flops"] / max(prof["evals"], 1) / max(gemm_launches, 1)
-    roofline = {"bound": "tensor", "kernel": "xg_syrk_gemm_kernel (FP64 DMMA trailing update)",
-                "achieved": achieved, "peak": peak, "unit": "TFLOP/s", "frac": achieved / peak,
-                "peak_source": "cuBLAS DGEMM 8192^3 measured in this process (of measured)",
-                "traffic": (tpf * flops_per_launch) if tpf else None,
-                "algorithmic_flops_per_launch": flops_per_launch,
-                "share_of_step": prof["t_gemm"] / dev_time,
-                "note": "achieved = algorithmic flops of both trailing-update launches of each step / their "
-                        "summed CUDA-event time; the lookahead panel (POTRF + TRSM) runs concurrently on a "
-                        "high-priority stream and is included in that time",
-                "phases_s_per_eval": {k: prof[k] / prof["evals"] for k in ("t_gen", "t_potrf", "t_trsm", "t_gemm")}}
+    fp64 = {"value": fp64_value, "unit": UNIT, "ms_per_step": 1e3 * t64 / args.steps, "loglik": lls64[-1],
+            "roofline": {"bound": "tensor", "kernel": "xg_syrk_gemm_kernel (FP64 DMMA trailing update)",
+                         "achieved": ach64, "peak": fp64_peak, "unit": "TFLOP/s", "frac": ach64 / fp64_peak,
+                         "peak_source": "cuBLAS DGEMM 8192^3 measured in this process (of measured)",
+                         "traffic": (tpf * p64["gemm_flops"] / p64["evals"] / max(2 * (p64["nt"] - 1) - 1, 1))
+                         if tpf else None,
+                         "share_of_step": p64["t_gemm"] / p64["t_total"]}}
     line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
-            "warmup": args.warmup, "ms_per_step": 1e3 * t_max / args.steps, "higher_is_better": True,
-            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-            "config": {"workload": workload(N), "tile": int(prof["ts"]), "tiles_per_side": int(prof["nt"]),
+            "warmup": args.warmup, "ms_per_step": 1e3 * tmx / args.steps, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None,
+            "dtype": "f64 band + f32 off-band (tf32x%d tensor cores)" % passes, "data": "synthetic",
+            "config": {"workload": workload(N), "tile": int(pmx["ts"]), "tiles_per_side": int(pmx["nt"]),
+                       "band_tiles": args.band, "tf32_passes": passes,
                        "parallelism": "replicas" if world > 1 else "single-gpu",
-                       "l2": "inputs larger than L2 (40 GB of covariance tiles per step)",
-                       "loglik": lls[-1], "loglik_e2e": ll_e2e, "wall_s_timed": wall},
+                       "l2": "inputs larger than L2 (20-40 GB of covariance tiles per step)",
+                       "loglik_mixed": llsmx[-1], "loglik_fp64": lls64[-1], "rel_err_vs_fp64": rel_err,
+                       "loglik_e2e": ll_e2e, "wall_s_timed": wall},
+            "fp64": fp64, "speedup_vs_fp64": value / fp64_value,
             "roofline": roofline, "e2e": e2e, "clocks": clocks,
-            "gpu_launches": int(round(launches_per_eval * args.steps))}
+            "gpu_launches": int(round(pmx["launches"] / max(pmx["evals"], 1) * args.steps))}
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         line["cpu_baseline"] = cpu_sample(N, args.cpu_seconds)
     sess.close()

@@ -355,10 +355,10 @@ class Session:
         _check(self.L.exageostat_b200_set_profiling(ctypes.byref(self.data), 1 if on else 0))
 
     def profile(self) -> dict:
-        out = np.zeros(11)
-        _check(self.L.exageostat_b200_get_profile(ctypes.byref(self.data), _p(out), 11))
+        out = np.zeros(15)
+        _check(self.L.exageostat_b200_get_profile(ctypes.byref(self.data), _p(out), 15))
         keys = ["t_gen", "t_potrf", "t_trsm", "t_gemm", "gemm_flops", "launches", "evals", "t_total", "ts", "nt",
-                "N"]
+                "N", "t_offband", "offband_flops", "t_band", "band_flops"]
         return dict(zip(keys, out.tolist()))
 
     def close(self) -> None:

@@ -504,9 +504,10 @@ extern "C" int exageostat_b200_get_profile(MLE_data *data, double *out, int n)
 {
     XgField *f = xg_field_of(data);
     if (!f) return xg_fail(XG_ERR_NOT_INITIALIZED, "no descriptors: call EXAGEOSTAT_dmle_Call first");
-    double info[11] = {f->prof[0], f->prof[1], f->prof[2], f->prof[3], f->prof[4], f->prof[5],
-                       f->prof[6], f->prof[7], (double)f->C.ts, (double)f->C.nt, (double)f->N};
-    for (int i = 0; i < n && i < 11; ++i) out[i] = info[i];
+    double info[15] = {f->prof[0], f->prof[1], f->prof[2], f->prof[3], f->prof[4],  f->prof[5],
+                       f->prof[6], f->prof[7], (double)f->C.ts, (double)f->C.nt, (double)f->N,
+                       f->prof[8], f->prof[9], f->prof[10], f->prof[11]};
+    for (int i = 0; i < n && i < 15; ++i) out[i] = info[i];
     return XG_OK;
 }
 

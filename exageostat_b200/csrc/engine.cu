@@ -273,13 +273,13 @@ double xg_trailing_flops(int nt, int ts, int k)
 int xg_field_set_profiling(XgField *f, int on)
 {
     if (on && !f->pev) {
-        const int n = 5 * f->C.nt;
+        const int n = 8 * f->C.nt;
         f->pev = (cudaEvent_t *)calloc(n, sizeof(cudaEvent_t));
         for (int i = 0; i < n; ++i)
             if (cudaEventCreate(&f->pev[i]) != cudaSuccess) return xg_fail(XG_ERR_CUDA, "profiling events");
     }
     f->profiling = on != 0;
-    for (int i = 0; i < 8; ++i) f->prof[i] = 0;
+    for (int i = 0; i < 12; ++i) f->prof[i] = 0;
     return XG_OK;
 }
 
@@ -310,10 +310,6 @@ static void xg_field_collect_profile(XgField *f)
     f->prof[5] += launches;
     f->prof[6] += 1;
 }
-
-/* mixed: the same event layout; flops split into band (FP64) and off-band
- * (TF32) parts, prof[4] counts all trailing-update flops */
-void xg_field_collect_profile_mixed(XgField *f) { xg_field_collect_profile(f); }
 
 int xg_field_set_data(XgField *f, const double *x, const double *y, const double *z)
 {
@@ -347,7 +343,7 @@ void xg_field_destroy(XgField *f)
     if (f->status) cudaFree(f->status);
     if (f->h_out) cudaFreeHost(f->h_out);
     if (f->pev) {
-        for (int i = 0; i < 5 * f->C.nt; ++i)
+        for (int i = 0; i < 8 * f->C.nt; ++i)
             if (f->pev[i]) cudaEventDestroy(f->pev[i]);
         free(f->pev);
     }
@@ -656,37 +652,101 @@ static void xg_factor_mixed(XgMixed *m, double *v, double *part, int *status, in
     const int nt = T.nt;
     const bool la = fs.st_hi != nullptr;
     cudaStream_t sp = la ? fs.st_hi : fs.st;
+    /* profiling events, 8 per step: panel start, after POTRF, after TRSM and
+     * panel prep, trailing start, after band part 1, after off-band part 1,
+     * after band part 2, trailing end */
     cudaEvent_t *pev = fs.pev;
+    auto rec = [&](int k, int e, cudaStream_t s) {
+        if (pev) cudaEventRecord(pev[8 * k + e], s);
+    };
     if (la) cudaEventRecord(fs.ev_upd, fs.st);
     for (int k = 0; k < nt; ++k) {
         const int b = k & 1;
         if (la) cudaStreamWaitEvent(sp, fs.ev_upd, 0);
-        if (pev) cudaEventRecord(pev[5 * k], sp);
+        rec(k, 0, sp);
         xg_launch_potrf_diag(T, k, v, part, part + nt, v != nullptr, status, info, sp);
-        if (pev) cudaEventRecord(pev[5 * k + 1], sp);
+        rec(k, 1, sp);
         xg_launch_trsm_panel(T, k, v, v != nullptr, status, sp, k + T.band);
         xg_launch_trsm_panel32(T, k, v, v != nullptr, status, sp);
         if (k + 1 < nt) xg_launch_panel_prep(T, k, m->p64[b], m->phi[b], m->plo[b], m->passes, status, sp);
-        if (pev) cudaEventRecord(pev[5 * k + 2], sp);
+        rec(k, 2, sp);
         if (la) {
             cudaEventRecord(fs.ev_panel, sp);
             cudaStreamWaitEvent(fs.st, fs.ev_panel, 0);
         }
-        if (pev) cudaEventRecord(pev[5 * k + 3], fs.st);
+        rec(k, 3, fs.st);
         if (k + 1 < nt) {
+            xg_launch_band_gemm(m->maps[b].p64, T, k, la ? 1 : 0, status, fs.st);
+            rec(k, 4, fs.st);
+            xg_launch_offband_gemm(m->maps[b], T, k, la ? 1 : 0, m->passes, g_xg.sm_count, status, fs.st);
+            rec(k, 5, fs.st);
             if (la) {
-                xg_launch_band_gemm(m->maps[b].p64, T, k, 1, status, fs.st);
-                xg_launch_offband_gemm(m->maps[b], T, k, 1, m->passes, g_xg.sm_count, status, fs.st);
                 cudaEventRecord(fs.ev_upd, fs.st);
                 xg_launch_band_gemm(m->maps[b].p64, T, k, 2, status, fs.st);
+                rec(k, 6, fs.st);
                 xg_launch_offband_gemm(m->maps[b], T, k, 2, m->passes, g_xg.sm_count, status, fs.st);
             } else {
-                xg_launch_band_gemm(m->maps[b].p64, T, k, 0, status, fs.st);
-                xg_launch_offband_gemm(m->maps[b], T, k, 0, m->passes, g_xg.sm_count, status, fs.st);
+                rec(k, 6, fs.st);
             }
+        } else {
+            rec(k, 4, fs.st);
+            rec(k, 5, fs.st);
+            rec(k, 6, fs.st);
         }
-        if (pev) cudaEventRecord(pev[5 * k + 4], fs.st);
+        rec(k, 7, fs.st);
     }
+}
+
+/* per-step algorithmic flops of the mixed trailing update: band targets
+ * (FP64 DMMA: SYRK ts^2 (ts+1) on the diagonal tile, GEMM 2 ts^3 otherwise)
+ * and off-band targets (TF32 tensor cores, 2 ts^3 each) */
+static void xg_mixed_step_flops(int nt, int ts, int band, int k, double *band_flops, double *off_flops)
+{
+    const double t = ts;
+    double bf = 0, of = 0;
+    for (int j = k + 1; j < nt; ++j) {
+        const int rows = nt - j; /* tiles i = j .. nt-1 in column j */
+        const int nb = rows < band ? rows : band;
+        bf += t * t * (t + 1) + (nb - 1) * 2 * t * t * t;
+        if (rows > band) of += (double)(rows - band) * 2 * t * t * t;
+    }
+    *band_flops = bf;
+    *off_flops = of;
+}
+
+void xg_field_collect_profile_mixed(XgField *f)
+{
+    XgMixed *m = f->mx;
+    const int nt = m->T.nt;
+    float ms = 0;
+    auto el = [&](int a, int b) {
+        cudaEventElapsedTime(&ms, f->pev[a], f->pev[b]);
+        return ms * 1e-3;
+    };
+    cudaEventElapsedTime(&ms, f->ev[0], f->ev[1]);
+    f->prof[0] += ms * 1e-3;
+    for (int k = 0; k < nt; ++k) {
+        const int e = 8 * k;
+        f->prof[1] += el(e, e + 1);
+        f->prof[2] += el(e + 1, e + 2);
+        if (k + 1 < nt) {
+            f->prof[3] += el(e + 3, e + 7);
+            double bfl, ofl;
+            xg_mixed_step_flops(nt, m->T.ts, m->band, k, &bfl, &ofl);
+            f->prof[4] += bfl + ofl;
+            f->prof[8] += el(e + 4, e + 5) + el(e + 6, e + 7);
+            f->prof[9] += ofl;
+            f->prof[10] += el(e + 3, e + 4) + el(e + 5, e + 6);
+            f->prof[11] += bfl;
+        }
+    }
+    cudaEventElapsedTime(&ms, f->ev[0], f->ev[2]);
+    f->prof[7] += ms * 1e-3;
+    /* generation, finalize, per step POTRF + band TRSM + FP32 TRSM + panel prep
+     * + two band and two off-band trailing launches (upper bound: empty
+     * launches are skipped on the host) */
+    f->prof[5] += 2 + 8.0 * nt;
+    f->prof[6] += 1;
 }
 
 int xg_field_set_mixed(XgField *f, int band, int passes)

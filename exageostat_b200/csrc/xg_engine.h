@@ -74,9 +74,10 @@ struct XgField {
     double *gout = nullptr;      /* 4 gradient sums */
     /* optional per-kernel-class timing (exageostat_b200_set_profiling) */
     bool profiling = false;
-    cudaEvent_t *pev = nullptr; /* 4 nt + 1 events around the factorisation kernels */
-    /* gen, potrf, trsm, trailing seconds; trailing flops; launches; evals; total seconds */
-    double prof[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+    cudaEvent_t *pev = nullptr; /* 8 per step around the factorisation kernels */
+    /* gen, potrf, trsm(+panel prep), trailing seconds; trailing flops; launches; evals; total seconds;
+     * mixed only: off-band (tcgen05) seconds, off-band flops, band (DMMA) seconds, band flops */
+    double prof[12] = {0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0};
 };
 
 struct XgPredict {

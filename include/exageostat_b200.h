@@ -392,7 +392,8 @@ int exageostat_b200_set_data(MLE_data *data, const double *x, const double *y, c
  * update (the panel overlaps the trailing update, so these may add up to
  * more than the total); trailing-update algorithmic flops; kernel launches;
  * evaluations; total seconds (generation to result); tile size; tiles per
- * side; N. */
+ * side; N; and for the mixed path out[11..14] = seconds and algorithmic flops
+ * of the off-band (TF32 tensor-core) and band (FP64) trailing updates. */
 int exageostat_b200_set_profiling(MLE_data *data, int on);
 int exageostat_b200_get_profile(MLE_data *data, double *out, int n);
 
