@@ -104,7 +104,8 @@ EXPORTED_SYMBOLS = [
     "exageostat_b200_matern_pairs", "exageostat_b200_covariance_dense", "exageostat_b200_set_data",
     "exageostat_b200_set_profiling", "exageostat_b200_get_profile", "exageostat_b200_dmle_device_noalloc",
     "exageostat_b200_bobyqa", "EXAGEOSTAT_sdmle_Tile", "exageostat_b200_set_mixed",
-    "exageostat_b200_dmle_host_mixed", "exageostat_b200_mixed_factor_dense", "results",
+    "exageostat_b200_dmle_host_mixed", "exageostat_b200_mixed_factor_dense", "exageostat_b200_batch_create",
+    "exageostat_b200_batch_loglik", "exageostat_b200_batch_destroy", "results",
 ]
 
 _lib = None
@@ -161,6 +162,10 @@ def lib():
         "exageostat_b200_set_mixed": (_I, [PM, _I, _I]),
         "exageostat_b200_dmle_host_mixed": (_I, [_I, _PD, _PD, _PD, _PD, _I, _I, _I, _I, _I, _PD]),
         "exageostat_b200_mixed_factor_dense": (_I, [_I, _PD, _PD, _PD, _I, _I, _I, _I, _I, _PD]),
+        "exageostat_b200_batch_create": (_I, [_I, ctypes.POINTER(_I), _PD, _PD, _PD, _I, _I, _I,
+                                              ctypes.POINTER(_VP)]),
+        "exageostat_b200_batch_loglik": (_I, [_VP, _PD, _PD]),
+        "exageostat_b200_batch_destroy": (_I, [_VP]),
     }
     for name, (res, args) in sig.items():
         f = getattr(L, name)
@@ -366,6 +371,38 @@ class Session:
             self.L.prediction_finalize(ctypes.byref(self.data))
         if self.data.descC:
             self.L.MLE_Finalize(ctypes.byref(self.data))
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+
+class Batch:
+    """Many independent fields evaluated together (one graph launch per call)."""
+
+    def __init__(self, xs, ys, zs, kernel: int = 0, metric: int = 0, ts: int = 256):
+        self.L = lib()
+        self.n = np.array([len(a) for a in xs], dtype=np.int32)
+        self.kernel = kernel
+        self.nparams = 4 if kernel == 1 else 3
+        x, y, z = (_f64(np.concatenate(a)) for a in (xs, ys, zs))
+        h = _VP()
+        _check(self.L.exageostat_b200_batch_create(len(xs), self.n.ctypes.data_as(ctypes.POINTER(_I)), _p(x), _p(y),
+                                                   _p(z), kernel, metric, ts, ctypes.byref(h)))
+        self.h = h
+
+    def loglik(self, thetas) -> np.ndarray:
+        th = _f64(thetas).reshape(len(self.n), self.nparams)
+        out = np.empty(len(self.n))
+        _check(self.L.exageostat_b200_batch_loglik(self.h, _p(th), _p(out)))
+        return out
+
+    def close(self) -> None:
+        if self.h:
+            self.L.exageostat_b200_batch_destroy(self.h)
+            self.h = None
 
     def __enter__(self):
         return self

@@ -1,0 +1,265 @@
+/*
+ * Many independent regional fields in one graph launch.
+ *
+ * The reference evaluates one field per MLE_data; a study of many regions
+ * loops over the exact path.  Here every field of a batch shares one lower-tile
+ * store (fields packed one after the other, one TMA tensor over all of them)
+ * and the factorisation runs tile step by tile step for all fields at once:
+ * step k is one POTRF launch (one CTA per field with more than k tile rows),
+ * one TRSM launch and one trailing-update launch whose CTAs each find their
+ * field by a binary search in the step's block table.  Generation, the
+ * ~3 * max(nt) step launches and the final reduction are captured once into a
+ * CUDA graph; each evaluation uploads the fields' parameters (computed on the
+ * host exactly as for a single field) and replays the graph.  Every field has
+ * its own status word, so a field whose covariance is not positive definite
+ * reports -inf without stopping the others.
+ */
+#include <math.h>
+#include <stdlib.h>
+#include <string.h>
+
+#include <algorithm>
+#include <vector>
+
+#include "../../include/exageostat_b200.h"
+#include "xg_common.cuh"
+#include "xg_engine.h"
+#include "xg_kernels.h"
+
+struct XgBTable {
+    std::vector<int> fields;
+    std::vector<long long> start; /* nact + 1 */
+    XgBStep dev;                   /* device view (pointers into the batch's table buffer) */
+    long long blocks = 0;
+};
+
+struct XgBatch {
+    int nfields = 0, ts = 0, kernel = 0, metric = 0, maxnt = 0;
+    long long total_tiles = 0, total_vec = 0, total_part = 0;
+    std::vector<XgBField> F;
+    XgBField *F_dev = nullptr, *F_pinned = nullptr;
+    double *tiles = nullptr, *x = nullptr, *y = nullptr, *z = nullptr, *v = nullptr, *part = nullptr,
+           *out = nullptr, *h_out = nullptr;
+    int *status = nullptr, *h_status = nullptr;
+    void *table_buf = nullptr;
+    XgBTable gen;
+    std::vector<XgBTable> potrf, trsm, gemm;
+    CUtensorMap map;
+    cudaGraphExec_t graph = nullptr;
+};
+
+static void xg_batch_free(XgBatch *b)
+{
+    if (!b) return;
+    if (b->graph) cudaGraphExecDestroy(b->graph);
+    void *dev[] = {b->F_dev, b->tiles, b->x, b->y, b->z, b->v, b->part, b->out, b->status, b->table_buf};
+    for (void *p : dev)
+        if (p) cudaFree(p);
+    if (b->F_pinned) cudaFreeHost(b->F_pinned);
+    if (b->h_out) cudaFreeHost(b->h_out);
+    if (b->h_status) cudaFreeHost(b->h_status);
+    delete b;
+}
+
+/* builds the host side of a table from per-field CTA counts (0 = inactive) */
+static void xg_table_fill(XgBTable &t, const std::vector<long long> &cnt)
+{
+    t.fields.clear();
+    t.start.assign(1, 0);
+    for (size_t f = 0; f < cnt.size(); ++f)
+        if (cnt[f] > 0) {
+            t.fields.push_back((int)f);
+            t.start.push_back(t.start.back() + cnt[f]);
+        }
+    t.blocks = t.start.back();
+}
+
+extern "C" int exageostat_b200_batch_create(int nfields, const int *n, const double *x, const double *y,
+                                            const double *z, int kernel, int metric, int ts, void **handle)
+{
+    *handle = nullptr;
+    int rc = xg_context_require();
+    if (rc) return rc;
+    if (nfields <= 0 || !n || !x || !y || !z) return xg_fail(XG_ERR_BAD_ARGUMENT, "empty batch");
+    if (kernel != 0 && kernel != 1) return xg_fail(XG_ERR_BAD_ARGUMENT, "kernel %d", kernel);
+    XgBatch *b = new XgBatch();
+    b->nfields = nfields;
+    b->ts = ts > 0 ? xg_choose_ts(1 << 20, ts) : 256;
+    b->kernel = kernel;
+    b->metric = metric;
+    b->F.resize(nfields);
+    for (int f = 0; f < nfields; ++f) {
+        if (n[f] <= 0) {
+            xg_batch_free(b);
+            return xg_fail(XG_ERR_BAD_ARGUMENT, "field %d has %d locations", f, n[f]);
+        }
+        XgBField &fd = b->F[f];
+        memset(&fd, 0, sizeof fd);
+        fd.N = n[f];
+        fd.nt = (n[f] + b->ts - 1) / b->ts;
+        fd.kernel = kernel;
+        fd.tile_off = b->total_tiles;
+        fd.vec_off = b->total_vec;
+        fd.part_off = b->total_part;
+        b->total_tiles += xg_num_lower_tiles(fd.nt);
+        b->total_vec += (long long)fd.nt * b->ts;
+        b->total_part += 2LL * fd.nt;
+        if (fd.nt > b->maxnt) b->maxnt = fd.nt;
+    }
+    const size_t tile = (size_t)b->ts * b->ts;
+    cudaError_t e = cudaMalloc(&b->tiles, (size_t)b->total_tiles * tile * sizeof(double));
+    if (e == cudaSuccess) e = cudaMalloc(&b->x, b->total_vec * sizeof(double));
+    if (e == cudaSuccess) e = cudaMalloc(&b->y, b->total_vec * sizeof(double));
+    if (e == cudaSuccess) e = cudaMalloc(&b->z, b->total_vec * sizeof(double));
+    if (e == cudaSuccess) e = cudaMalloc(&b->v, b->total_vec * sizeof(double));
+    if (e == cudaSuccess) e = cudaMalloc(&b->part, b->total_part * sizeof(double));
+    if (e == cudaSuccess) e = cudaMalloc(&b->out, 2 * (size_t)nfields * sizeof(double));
+    if (e == cudaSuccess) e = cudaMalloc(&b->status, 2 * (size_t)nfields * sizeof(int));
+    if (e == cudaSuccess) e = cudaMalloc(&b->F_dev, nfields * sizeof(XgBField));
+    if (e == cudaSuccess) e = cudaMallocHost(&b->F_pinned, nfields * sizeof(XgBField));
+    if (e == cudaSuccess) e = cudaMallocHost(&b->h_out, 2 * (size_t)nfields * sizeof(double));
+    if (e == cudaSuccess) e = cudaMallocHost(&b->h_status, 2 * (size_t)nfields * sizeof(int));
+    if (e != cudaSuccess) {
+        xg_batch_free(b);
+        return xg_fail(XG_ERR_NO_MEMORY, "batch buffers (%.2f GB of tiles): %s",
+                       b->total_tiles * tile * 8.0 / 1e9, cudaGetErrorString(e));
+    }
+    /* locations and observations, zero padded per field */
+    std::vector<double> hx(b->total_vec, 0.0), hy(b->total_vec, 0.0), hz(b->total_vec, 0.0);
+    long long src = 0;
+    for (int f = 0; f < nfields; ++f) {
+        const XgBField &fd = b->F[f];
+        memcpy(&hx[fd.vec_off], x + src, fd.N * sizeof(double));
+        memcpy(&hy[fd.vec_off], y + src, fd.N * sizeof(double));
+        memcpy(&hz[fd.vec_off], z + src, fd.N * sizeof(double));
+        src += fd.N;
+    }
+    cudaMemcpy(b->x, hx.data(), b->total_vec * sizeof(double), cudaMemcpyHostToDevice);
+    cudaMemcpy(b->y, hy.data(), b->total_vec * sizeof(double), cudaMemcpyHostToDevice);
+    cudaMemcpy(b->z, hz.data(), b->total_vec * sizeof(double), cudaMemcpyHostToDevice);
+    /* launch tables */
+    const int bpt = b->ts / 128;
+    std::vector<long long> cnt(nfields);
+    for (int f = 0; f < nfields; ++f) cnt[f] = xg_num_lower_tiles(b->F[f].nt) * (b->ts / 8);
+    xg_table_fill(b->gen, cnt);
+    b->potrf.resize(b->maxnt);
+    b->trsm.resize(b->maxnt);
+    b->gemm.resize(b->maxnt);
+    for (int k = 0; k < b->maxnt; ++k) {
+        for (int f = 0; f < nfields; ++f) cnt[f] = b->F[f].nt > k ? 1 : 0;
+        xg_table_fill(b->potrf[k], cnt);
+        for (int f = 0; f < nfields; ++f) cnt[f] = (long long)std::max(0, b->F[f].nt - k - 1) * (b->ts / 32);
+        xg_table_fill(b->trsm[k], cnt);
+        for (int f = 0; f < nfields; ++f) {
+            const long long T = std::max(0, b->F[f].nt - k - 1);
+            cnt[f] = T * (T + 1) / 2 * bpt * bpt;
+        }
+        xg_table_fill(b->gemm[k], cnt);
+    }
+    /* one device buffer for every table: fields (int) then starts (long long) */
+    std::vector<XgBTable *> all;
+    all.push_back(&b->gen);
+    for (int k = 0; k < b->maxnt; ++k) {
+        all.push_back(&b->potrf[k]);
+        all.push_back(&b->trsm[k]);
+        all.push_back(&b->gemm[k]);
+    }
+    size_t bytes = 0;
+    for (XgBTable *t : all) bytes += t->start.size() * sizeof(long long) + ((t->fields.size() * sizeof(int) + 7) & ~7ULL);
+    std::vector<unsigned char> hbuf(bytes);
+    e = cudaMalloc(&b->table_buf, bytes);
+    if (e != cudaSuccess) {
+        xg_batch_free(b);
+        return xg_fail(XG_ERR_NO_MEMORY, "batch tables");
+    }
+    size_t off = 0;
+    for (XgBTable *t : all) {
+        memcpy(&hbuf[off], t->start.data(), t->start.size() * sizeof(long long));
+        t->dev.blk_start = (const long long *)((unsigned char *)b->table_buf + off);
+        off += t->start.size() * sizeof(long long);
+        memcpy(&hbuf[off], t->fields.data(), t->fields.size() * sizeof(int));
+        t->dev.fields = (const int *)((unsigned char *)b->table_buf + off);
+        off += (t->fields.size() * sizeof(int) + 7) & ~7ULL;
+        t->dev.nact = (int)t->fields.size();
+    }
+    cudaMemcpy(b->table_buf, hbuf.data(), bytes, cudaMemcpyHostToDevice);
+    /* TMA view over the whole batch store */
+    rc = xg_encode_tiles(&b->map, b->tiles, b->total_tiles, b->ts);
+    if (rc) {
+        xg_batch_free(b);
+        return rc;
+    }
+    *handle = b;
+    return XG_OK;
+}
+
+static void xg_batch_record(XgBatch *b, cudaStream_t st)
+{
+    XgTileArgs base{b->tiles, b->ts, 0};
+    cudaMemsetAsync(b->status, 0, 2 * (size_t)b->nfields * sizeof(int), st);
+    cudaMemcpyAsync(b->v, b->z, b->total_vec * sizeof(double), cudaMemcpyDeviceToDevice, st);
+    xg_launch_batch_gen(base, b->F_dev, b->gen.dev, b->gen.blocks, b->x, b->y, b->metric, st);
+    for (int k = 0; k < b->maxnt; ++k) {
+        xg_launch_batch_potrf(base, b->F_dev, b->potrf[k].dev, k, b->v, b->part, b->status, nullptr, st);
+        xg_launch_batch_trsm(base, b->F_dev, b->trsm[k].dev, b->trsm[k].blocks, k, b->v, b->status, st);
+        xg_launch_batch_gemm(b->map, base, b->F_dev, b->gemm[k].dev, b->gemm[k].blocks, k, b->status, st);
+    }
+    xg_launch_batch_finalize(b->F_dev, b->nfields, b->part, b->out, st);
+}
+
+extern "C" int exageostat_b200_batch_loglik(void *handle, const double *theta, double *loglik)
+{
+    XgBatch *b = (XgBatch *)handle;
+    if (!b || !theta || !loglik) return xg_fail(XG_ERR_BAD_ARGUMENT, "NULL argument");
+    const int np = b->kernel == 1 ? 4 : 3;
+    for (int f = 0; f < b->nfields; ++f) {
+        int rc = xg_check_theta(theta + (size_t)f * np, b->kernel);
+        if (rc) return xg_fail(rc, "field %d: %s", f, exageostat_last_error());
+        b->F[f].p = xg_params(theta + (size_t)f * np, b->kernel);
+    }
+    memcpy(b->F_pinned, b->F.data(), b->nfields * sizeof(XgBField));
+    cudaStream_t st = g_xg.stream;
+    cudaError_t e = cudaMemcpyAsync(b->F_dev, b->F_pinned, b->nfields * sizeof(XgBField), cudaMemcpyHostToDevice, st);
+    if (e != cudaSuccess) return xg_fail(XG_ERR_CUDA, "batch parameters: %s", cudaGetErrorString(e));
+    if (!b->graph) {
+        cudaGraph_t g;
+        e = cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal);
+        if (e == cudaSuccess) {
+            xg_batch_record(b, st);
+            e = cudaStreamEndCapture(st, &g);
+        }
+        if (e == cudaSuccess) {
+            e = cudaGraphInstantiate(&b->graph, g, 0);
+            cudaGraphDestroy(g);
+        }
+        if (e != cudaSuccess) return xg_fail(XG_ERR_CUDA, "batch graph capture: %s", cudaGetErrorString(e));
+    }
+    e = cudaGraphLaunch(b->graph, st);
+    if (e == cudaSuccess)
+        e = cudaMemcpyAsync(b->h_out, b->out, 2 * (size_t)b->nfields * sizeof(double), cudaMemcpyDeviceToHost, st);
+    if (e == cudaSuccess)
+        e = cudaMemcpyAsync(b->h_status, b->status, 2 * (size_t)b->nfields * sizeof(int), cudaMemcpyDeviceToHost,
+                            st);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+    if (e != cudaSuccess) return xg_fail(XG_ERR_CUDA, "batch evaluation: %s", cudaGetErrorString(e));
+    int failed = 0;
+    for (int f = 0; f < b->nfields; ++f) {
+        const int stf = b->h_status[2 * f];
+        if (stf & XG_ST_TIMEOUT) return xg_fail(XG_ERR_TIMEOUT, "field %d: a device wait timed out", f);
+        if (stf) {
+            loglik[f] = -INFINITY;
+            ++failed;
+        } else {
+            loglik[f] = b->h_out[2 * f];
+        }
+    }
+    if (failed) xg_fail(XG_ERR_NOT_SPD, "%d of %d fields are not positive definite (their loglik is -inf)", failed,
+                        b->nfields);
+    return XG_OK;
+}
+
+extern "C" int exageostat_b200_batch_destroy(void *handle)
+{
+    xg_batch_free((XgBatch *)handle);
+    return XG_OK;
+}

@@ -63,16 +63,11 @@ __device__ inline double xg_matern_value(double d, const XgMaternParams &p)
 /* One CTA fills XG_GEN_ROWS rows of one tile; threads stride the columns so
  * the row-major stores and the column-location loads are coalesced. */
 #define XG_GEN_ROWS 8
-__global__ void __launch_bounds__(256) xg_gen_matern_kernel(XgTileArgs T, const int2 *__restrict__ tile_ij,
-                                                            const double *__restrict__ xr, const double *__restrict__ yr,
-                                                            const double *__restrict__ xc, const double *__restrict__ yc,
-                                                            int n_rows, int n_cols, XgMaternParams p, int metric,
-                                                            int identity_pad)
+__device__ __forceinline__ void xg_gen_body(const XgTileArgs &T, long long t, int2 ij, int strip,
+                                            const double *__restrict__ xr, const double *__restrict__ yr,
+                                            const double *__restrict__ xc, const double *__restrict__ yc, int n_rows,
+                                            int n_cols, const XgMaternParams &p, int metric, int identity_pad)
 {
-    const int strips = T.ts / XG_GEN_ROWS;
-    const long long t = blockIdx.x / strips;
-    const int strip = blockIdx.x % strips;
-    const int2 ij = tile_ij[t];
     double *tile = T.data + t * (long long)T.ts * T.ts;
     for (int rr = 0; rr < XG_GEN_ROWS; ++rr) {
         const int r = strip * XG_GEN_ROWS + rr;
@@ -91,6 +86,35 @@ __global__ void __launch_bounds__(256) xg_gen_matern_kernel(XgTileArgs T, const 
     }
 }
 
+__global__ void __launch_bounds__(256) xg_gen_matern_kernel(XgTileArgs T, const int2 *__restrict__ tile_ij,
+                                                            const double *__restrict__ xr, const double *__restrict__ yr,
+                                                            const double *__restrict__ xc, const double *__restrict__ yc,
+                                                            int n_rows, int n_cols, XgMaternParams p, int metric,
+                                                            int identity_pad)
+{
+    const int strips = T.ts / XG_GEN_ROWS;
+    const long long t = blockIdx.x / strips;
+    xg_gen_body(T, t, tile_ij[t], (int)(blockIdx.x % strips), xr, yr, xc, yc, n_rows, n_cols, p, metric,
+                identity_pad);
+}
+
+/* batched: every field's lower tiles, CTAs resolved through the step table */
+__global__ void __launch_bounds__(256) xg_gen_matern_batch_kernel(XgTileArgs base, const XgBField *__restrict__ F,
+                                                                  XgBStep S, const double *__restrict__ x,
+                                                                  const double *__restrict__ y, int metric)
+{
+    long long local;
+    const int f = xg_batch_resolve(S, blockIdx.x, &local);
+    const XgBField &fd = F[f];
+    XgTileArgs T = base;
+    T.data = base.data + fd.tile_off * (long long)base.ts * base.ts;
+    T.nt = fd.nt;
+    const int strips = T.ts / XG_GEN_ROWS;
+    const long long t = local / strips;
+    const double *xf = x + fd.vec_off, *yf = y + fd.vec_off;
+    xg_gen_body(T, t, xg_tile_decode(t, fd.nt), (int)(local % strips), xf, yf, xf, yf, fd.N, fd.N, fd.p, metric, 1);
+}
+
 /* ========================================================================== */
 /* POTRF of a diagonal tile, fused with log-det and the z block solve         */
 /* ========================================================================== */
@@ -101,10 +125,9 @@ __global__ void __launch_bounds__(256) xg_gen_matern_kernel(XgTileArgs T, const 
 #define XG_POTRF_THREADS 512
 
 template <int NB>
-__global__ void __launch_bounds__(XG_POTRF_THREADS) xg_potrf_diag_kernel(XgTileArgs T, int k, double *__restrict__ v,
-                                                                         double *__restrict__ part_logdet,
-                                                                         double *__restrict__ part_dot, int with_rhs,
-                                                                         int *status, int *info)
+__device__ __forceinline__ void xg_potrf_body(const XgTileArgs &T, int k, double *__restrict__ v,
+                                              double *__restrict__ part_logdet, double *__restrict__ part_dot,
+                                              int with_rhs, int *status, int *info)
 {
     constexpr int LDP = NB + 4;
     extern __shared__ __align__(16) double xg_smem_d[];
@@ -292,6 +315,34 @@ __global__ void __launch_bounds__(XG_POTRF_THREADS) xg_potrf_diag_kernel(XgTileA
     }
 }
 
+template <int NB>
+__global__ void __launch_bounds__(XG_POTRF_THREADS) xg_potrf_diag_kernel(XgTileArgs T, int k, double *__restrict__ v,
+                                                                         double *__restrict__ part_logdet,
+                                                                         double *__restrict__ part_dot, int with_rhs,
+                                                                         int *status, int *info)
+{
+    xg_potrf_body<NB>(T, k, v, part_logdet, part_dot, with_rhs, status, info);
+}
+
+/* batched: one CTA per field active at step k; info records the first
+ * failing column of any field */
+template <int NB>
+__global__ void __launch_bounds__(XG_POTRF_THREADS) xg_potrf_diag_batch_kernel(XgTileArgs base,
+                                                                               const XgBField *__restrict__ F,
+                                                                               XgBStep S, int k, double *v,
+                                                                               double *part, int *status, int *info)
+{
+    long long local;
+    const int f = xg_batch_resolve(S, blockIdx.x, &local);
+    const XgBField &fd = F[f];
+    XgTileArgs T = base;
+    T.data = base.data + fd.tile_off * (long long)base.ts * base.ts;
+    T.nt = fd.nt;
+    /* per-field status words: status[2 f] (flags), status[2 f + 1] (info) */
+    xg_potrf_body<NB>(T, k, v + fd.vec_off, part + fd.part_off, part + fd.part_off + fd.nt, 1, status + 2 * f,
+                      status + 2 * f + 1);
+}
+
 /* ========================================================================== */
 /* Panel TRSM: L_ik = A_ik L_kk^-T, fused with v_i -= L_ik v_k                */
 /* ========================================================================== */
@@ -299,8 +350,8 @@ __global__ void __launch_bounds__(XG_POTRF_THREADS) xg_potrf_diag_kernel(XgTileA
 #define XG_TRSM_THREADS 512
 #define XG_TRSM_SR 32 /* rows of A_ik per CTA */
 
-__global__ void __launch_bounds__(XG_TRSM_THREADS) xg_trsm_panel_kernel(XgTileArgs T, int k, double *__restrict__ v,
-                                                                        int with_rhs, const int *status)
+__device__ __forceinline__ void xg_trsm_body(const XgTileArgs &T, int k, double *__restrict__ v, int with_rhs,
+                                             const int *status, long long bid)
 {
     const int ts = T.ts, LDS = ts + 4;
     extern __shared__ __align__(16) double xg_smem_d[];
@@ -308,8 +359,8 @@ __global__ void __launch_bounds__(XG_TRSM_THREADS) xg_trsm_panel_kernel(XgTileAr
     double *LD = S + XG_TRSM_SR * LDS;      /* [32][33] */
     if (xg_cta_should_skip(status)) return;
     const int strips = ts / XG_TRSM_SR;
-    const int i = k + 1 + blockIdx.x / strips;
-    const int strip = blockIdx.x % strips;
+    const int i = k + 1 + (int)(bid / strips);
+    const int strip = (int)(bid % strips);
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     const int g = lane >> 2, tq = lane & 3;
     double *B = T.data + xg_slot64(T, i, k) * (long long)ts * ts + (long long)strip * XG_TRSM_SR * ts;
@@ -397,6 +448,26 @@ __global__ void __launch_bounds__(XG_TRSM_THREADS) xg_trsm_panel_kernel(XgTileAr
     }
 }
 
+__global__ void __launch_bounds__(XG_TRSM_THREADS) xg_trsm_panel_kernel(XgTileArgs T, int k, double *__restrict__ v,
+                                                                        int with_rhs, const int *status)
+{
+    xg_trsm_body(T, k, v, with_rhs, status, blockIdx.x);
+}
+
+__global__ void __launch_bounds__(XG_TRSM_THREADS) xg_trsm_panel_batch_kernel(XgTileArgs base,
+                                                                              const XgBField *__restrict__ F,
+                                                                              XgBStep S, int k, double *v,
+                                                                              const int *status)
+{
+    long long local;
+    const int f = xg_batch_resolve(S, blockIdx.x, &local);
+    const XgBField &fd = F[f];
+    XgTileArgs T = base;
+    T.data = base.data + fd.tile_off * (long long)base.ts * base.ts;
+    T.nt = fd.nt;
+    xg_trsm_body(T, k, v + fd.vec_off, 1, status + 2 * f, local);
+}
+
 /* ========================================================================== */
 /* Trailing update A_ij -= L_ik L_jk^T on FP64 tensor cores (DMMA), TMA fed   */
 /* ========================================================================== */
@@ -415,8 +486,8 @@ __global__ void __launch_bounds__(XG_TRSM_THREADS) xg_trsm_panel_kernel(XgTileAr
 /* Updates the tiles (i, j), j0 <= j <= i < nt, with panel column k.  With
  * single_col the launch covers column j0 only (the lookahead split: the next
  * panel's column first, the rest of the trailing matrix in a second launch). */
-__global__ void __launch_bounds__(XG_G_THREADS, 1) xg_syrk_gemm_kernel(const __grid_constant__ CUtensorMap map, XgTileArgs T, int k,
-                                                    int j0, int single_col, int *status)
+__device__ __forceinline__ void xg_gemm_body(const CUtensorMap &map, const XgTileArgs &T, int k, int j0,
+                                             int single_col, int *status, long long bid)
 {
     extern __shared__ __align__(1024) unsigned char xg_smem_raw[];
     unsigned char *smem = (unsigned char *)(((uintptr_t)xg_smem_raw + 1023) & ~(uintptr_t)1023);
@@ -424,8 +495,8 @@ __global__ void __launch_bounds__(XG_G_THREADS, 1) xg_syrk_gemm_kernel(const __g
     uint64_t *empty = full + XG_G_STAGES;
     const int ts = T.ts;
     const int bpt = ts / XG_G_BM; /* blocks per tile side */
-    const long long pair = blockIdx.x / (bpt * bpt);
-    const int blk = blockIdx.x % (bpt * bpt);
+    const long long pair = bid / (bpt * bpt);
+    const int blk = (int)(bid % (bpt * bpt));
     const int bi = blk / bpt, bj = blk % bpt;
     int i, j;
     if (T.band) {
@@ -456,8 +527,10 @@ __global__ void __launch_bounds__(XG_G_THREADS, 1) xg_syrk_gemm_kernel(const __g
     __syncthreads();
     const int KT = ts / XG_G_BK;
     /* operands: packed tiles (i, k), (j, k), or rows of the FP64 panel copy in mixed mode */
-    const int rowA = T.band ? i * ts + bi * XG_G_BM : (int)(xg_tile_index(i, k, T.nt) * ts + bi * XG_G_BM);
-    const int rowB = T.band ? j * ts + bj * XG_G_BM : (int)(xg_tile_index(j, k, T.nt) * ts + bj * XG_G_BM);
+    const int rowA = T.band ? i * ts + bi * XG_G_BM
+                            : (int)((T.tile_off + xg_tile_index(i, k, T.nt)) * ts + bi * XG_G_BM);
+    const int rowB = T.band ? j * ts + bj * XG_G_BM
+                            : (int)((T.tile_off + xg_tile_index(j, k, T.nt)) * ts + bj * XG_G_BM);
     int issued = 0;
     if (tid == 0) {
         xg_prefetch_tensormap(&map);
@@ -562,6 +635,29 @@ __global__ void __launch_bounds__(XG_G_THREADS, 1) xg_syrk_gemm_kernel(const __g
             }
 }
 
+__global__ void __launch_bounds__(XG_G_THREADS, 1) xg_syrk_gemm_kernel(const __grid_constant__ CUtensorMap map,
+                                                                       XgTileArgs T, int k, int j0, int single_col,
+                                                                       int *status)
+{
+    xg_gemm_body(map, T, k, j0, single_col, status, blockIdx.x);
+}
+
+/* batched: the trailing update of step k of every field with nt > k + 1 */
+__global__ void __launch_bounds__(XG_G_THREADS, 1) xg_syrk_gemm_batch_kernel(const __grid_constant__ CUtensorMap map,
+                                                                             XgTileArgs base,
+                                                                             const XgBField *__restrict__ F,
+                                                                             XgBStep S, int k, int *status)
+{
+    long long local;
+    const int f = xg_batch_resolve(S, blockIdx.x, &local);
+    const XgBField &fd = F[f];
+    XgTileArgs T = base;
+    T.data = base.data + fd.tile_off * (long long)base.ts * base.ts;
+    T.nt = fd.nt;
+    T.tile_off = fd.tile_off;
+    xg_gemm_body(map, T, k, k + 1, 0, status + 2 * f, local);
+}
+
 /* ========================================================================== */
 /* Log-likelihood assembly                                                    */
 /* ========================================================================== */
@@ -585,6 +681,23 @@ __global__ void xg_finalize_kernel(const double *part_logdet, const double *part
     out[4] = (double)(*info);
 }
 
+/* batched: one thread per field */
+__global__ void xg_finalize_batch_kernel(const XgBField *__restrict__ F, int nfields, const double *part,
+                                         double *out)
+{
+    const int f = blockIdx.x * blockDim.x + threadIdx.x;
+    if (f >= nfields) return;
+    const XgBField &fd = F[f];
+    double det = 0.0, dot = 0.0;
+    for (int k = 0; k < fd.nt; ++k) {
+        det += part[fd.part_off + k];
+        dot += part[fd.part_off + fd.nt + k];
+    }
+    const double logdet = 2.0 * det;
+    out[2 * f] = -0.5 * dot - 0.5 * logdet - (double)(fd.N / 2.0) * log(2.0 * 3.141592653589793);
+    out[2 * f + 1] = logdet;
+}
+
 /* ========================================================================== */
 /* Host launchers                                                             */
 /* ========================================================================== */
@@ -605,6 +718,15 @@ cudaError_t xg_kernels_configure()
                              (int)xg_trsm_smem_bytes(XG_MAX_TS));
     if (e != cudaSuccess) return e;
     e = cudaFuncSetAttribute(xg_syrk_gemm_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             (int)xg_gemm_smem_bytes());
+    if (e != cudaSuccess) return e;
+    e = cudaFuncSetAttribute(xg_potrf_diag_batch_kernel<32>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             (int)xg_potrf_smem_bytes(512));
+    if (e != cudaSuccess) return e;
+    e = cudaFuncSetAttribute(xg_trsm_panel_batch_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             (int)xg_trsm_smem_bytes(XG_MAX_TS));
+    if (e != cudaSuccess) return e;
+    e = cudaFuncSetAttribute(xg_syrk_gemm_batch_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
                              (int)xg_gemm_smem_bytes());
     return e;
 }
@@ -666,6 +788,41 @@ void xg_launch_band_gemm(const CUtensorMap &p64map, const XgTileArgs &T, int k, 
     const long long blocks = ncol * T.band * bpt * bpt;
     xg_syrk_gemm_kernel<<<(unsigned)blocks, XG_G_THREADS, xg_gemm_smem_bytes(), st>>>(p64map, T, k, j0, part == 1,
                                                                                        status);
+}
+
+void xg_launch_batch_gen(const XgTileArgs &base, const XgBField *F, const XgBStep &S, long long blocks,
+                         const double *x, const double *y, int metric, cudaStream_t st)
+{
+    if (blocks > 0) xg_gen_matern_batch_kernel<<<(unsigned)blocks, 256, 0, st>>>(base, F, S, x, y, metric);
+}
+
+void xg_launch_batch_potrf(const XgTileArgs &base, const XgBField *F, const XgBStep &S, int k, double *v, double *part,
+                           int *status, int *info, cudaStream_t st)
+{
+    if (S.nact <= 0) return;
+    xg_potrf_diag_batch_kernel<32><<<S.nact, XG_POTRF_THREADS, xg_potrf_smem_bytes(base.ts), st>>>(
+        base, F, S, k, v, part, status, info);
+}
+
+void xg_launch_batch_trsm(const XgTileArgs &base, const XgBField *F, const XgBStep &S, long long blocks, int k,
+                          double *v, const int *status, cudaStream_t st)
+{
+    if (blocks > 0)
+        xg_trsm_panel_batch_kernel<<<(unsigned)blocks, XG_TRSM_THREADS, xg_trsm_smem_bytes(base.ts), st>>>(
+            base, F, S, k, v, status);
+}
+
+void xg_launch_batch_gemm(const CUtensorMap &map, const XgTileArgs &base, const XgBField *F, const XgBStep &S,
+                          long long blocks, int k, int *status, cudaStream_t st)
+{
+    if (blocks > 0)
+        xg_syrk_gemm_batch_kernel<<<(unsigned)blocks, XG_G_THREADS, xg_gemm_smem_bytes(), st>>>(map, base, F, S, k,
+                                                                                               status);
+}
+
+void xg_launch_batch_finalize(const XgBField *F, int nfields, const double *part, double *out, cudaStream_t st)
+{
+    xg_finalize_batch_kernel<<<(nfields + 127) / 128, 128, 0, st>>>(F, nfields, part, out);
 }
 
 void xg_launch_finalize(const double *part_logdet, const double *part_dot, int nt, int N, double *out,

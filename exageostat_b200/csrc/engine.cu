@@ -159,13 +159,18 @@ int xg_tm_alloc(XgTileMatrix &M, int N, int ts)
     if (e == cudaSuccess) e = cudaMemcpy(M.ij, hij, sizeof(int2) * M.ntiles, cudaMemcpyHostToDevice);
     free(hij);
     if (e != cudaSuccess) return xg_cuda_fail(e, "tile index table");
-    /* TMA view: a 2-D FP64 tensor [ntiles * ts rows][ts columns], boxes of
-     * 128 rows x 16 columns (128 bytes, swizzled) */
-    cuuint64_t dims[2] = {(cuuint64_t)ts, (cuuint64_t)M.ntiles * ts};
+    return xg_encode_tiles(&M.map, M.d, M.ntiles, ts);
+}
+
+/* TMA view of a lower-tile store: a 2-D FP64 tensor [ntiles * ts rows][ts
+ * columns], boxes of 128 rows x 16 columns (128 bytes, swizzled) */
+int xg_encode_tiles(CUtensorMap *map, double *base, long long ntiles, int ts)
+{
+    cuuint64_t dims[2] = {(cuuint64_t)ts, (cuuint64_t)ntiles * ts};
     cuuint64_t strides[1] = {(cuuint64_t)ts * sizeof(double)};
     cuuint32_t box[2] = {16, 128};
     cuuint32_t estr[2] = {1, 1};
-    CUresult r = g_encode(&M.map, CU_TENSOR_MAP_DATA_TYPE_FLOAT64, 2, M.d, dims, strides, box, estr,
+    CUresult r = g_encode(map, CU_TENSOR_MAP_DATA_TYPE_FLOAT64, 2, base, dims, strides, box, estr,
                           CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
                           CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
     if (r != CUDA_SUCCESS) return xg_fail(XG_ERR_CUDA, "cuTensorMapEncodeTiled failed (%d)", (int)r);

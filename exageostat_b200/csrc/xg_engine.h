@@ -96,6 +96,7 @@ int xg_context_start(int dts);
 int xg_context_require();
 int xg_choose_ts(int N, int dts);
 int xg_tm_alloc(XgTileMatrix &M, int N, int ts);
+int xg_encode_tiles(CUtensorMap *map, double *base, long long ntiles, int ts);
 void xg_tm_free(XgTileMatrix &M);
 XgMaternParams xg_params(const double *theta, int kernel);
 int xg_check_theta(const double *theta, int kernel);

@@ -23,6 +23,7 @@ struct XgTileArgs {
     int nt; /* tiles per side */
     int band = 0;
     float *data32 = nullptr;
+    long long tile_off = 0; /* first tile of this matrix inside a shared TMA tensor (batches) */
 };
 
 __host__ __device__ inline long long xg_slot64(const XgTileArgs &T, int i, int j)
@@ -57,6 +58,49 @@ struct XgMaternParams {
     int half_integer;
 };
 
+/* One field of a batch of independent fields sharing one tile store. */
+struct XgBField {
+    long long tile_off; /* first packed tile of the field in the batch store */
+    long long vec_off;  /* first entry of its vectors (x, y, z, v); a multiple of ts */
+    long long part_off; /* first entry of its partial sums (2 nt) */
+    int N, nt;
+    int kernel, pad_;
+    XgMaternParams p;   /* this evaluation's parameters */
+};
+
+/* The fields taking part in one batched launch and the CTA ranges they own. */
+struct XgBStep {
+    const int *fields;          /* nact field indices */
+    const long long *blk_start; /* nact + 1 prefix sums of CTAs */
+    int nact;
+};
+
+/* field owning CTA `bid` of a batched launch, and the CTA index within it */
+__device__ inline int xg_batch_resolve(const XgBStep &S, long long bid, long long *local)
+{
+    int lo = 0, hi = S.nact - 1;
+    while (lo < hi) {
+        const int mid = (lo + hi + 1) >> 1;
+        if (S.blk_start[mid] <= bid)
+            lo = mid;
+        else
+            hi = mid - 1;
+    }
+    *local = bid - S.blk_start[lo];
+    return S.fields[lo];
+}
+
+/* (i, j) of packed lower tile t of an nt x nt tile grid */
+__host__ __device__ inline int2 xg_tile_decode(long long t, int nt)
+{
+    int j = 0;
+    while (t >= nt - j) {
+        t -= nt - j;
+        ++j;
+    }
+    return make_int2(j + (int)t, j);
+}
+
 cudaError_t xg_kernels_configure();
 size_t xg_potrf_smem_bytes(int ts);
 size_t xg_trsm_smem_bytes(int ts);
@@ -90,6 +134,17 @@ void xg_launch_offband_gemm(const XgMixedMaps &maps, const XgTileArgs &T, int k,
                             int *status, cudaStream_t st);
 void xg_launch_finalize(const double *part_logdet, const double *part_dot, int nt, int N, double *out,
                         const int *status, const int *info, cudaStream_t st);
+
+/* batched fields (one launch per tile step covering every active field) */
+void xg_launch_batch_gen(const XgTileArgs &base, const XgBField *F, const XgBStep &S, long long blocks,
+                         const double *x, const double *y, int metric, cudaStream_t st);
+void xg_launch_batch_potrf(const XgTileArgs &base, const XgBField *F, const XgBStep &S, int k, double *v, double *part,
+                           int *status, int *info, cudaStream_t st);
+void xg_launch_batch_trsm(const XgTileArgs &base, const XgBField *F, const XgBStep &S, long long blocks, int k,
+                          double *v, const int *status, cudaStream_t st);
+void xg_launch_batch_gemm(const CUtensorMap &map, const XgTileArgs &base, const XgBField *F, const XgBStep &S,
+                          long long blocks, int k, int *status, cudaStream_t st);
+void xg_launch_batch_finalize(const XgBField *F, int nfields, const double *part, double *out, cudaStream_t st);
 
 /* solve.cu */
 void xg_launch_trmv_lower(const XgTileArgs &T, const double *e, double *z, const int *status, cudaStream_t st);

@@ -413,6 +413,21 @@ int exageostat_b200_get_profile(MLE_data *data, double *out, int n);
 int exageostat_b200_dmle_device_noalloc(int n, const double *d_x, const double *d_y, const double *d_z,
                                         const double *theta, int kernel, int metric, double *d_out, void *stream);
 
+/* ---- batches of independent fields (no counterpart in the reference) ----
+ * nfields fields with n[f] locations each; x, y, z hold the fields one after
+ * the other (sum n[f] doubles each).  kernel / metric as for
+ * exageostat_b200_dmle_host, ts = tile size (0 = 256).  The fields share one
+ * device tile store and each evaluation of all of them is one CUDA-graph
+ * launch (one launch per tile step covering every field). */
+int exageostat_b200_batch_create(int nfields, const int *n, const double *x, const double *y, const double *z,
+                                 int kernel, int metric, int ts, void **handle);
+/* theta: nfields rows of 3 (4 with the nugget) parameters; loglik receives
+ * nfields values (-INFINITY for a field whose covariance is not positive
+ * definite; the call then still returns 0 and exageostat_last_error() says
+ * how many failed). */
+int exageostat_b200_batch_loglik(void *handle, const double *theta, double *loglik);
+int exageostat_b200_batch_destroy(void *handle);
+
 /* Diagnostics used by the parity tests.  All run on the GPU. */
 int exageostat_b200_bessel_knu(int n, const double *nu, const double *x, double *out);
 int exageostat_b200_matern_pairs(int n, const double *x1, const double *y1, const double *x2, const double *y2,
