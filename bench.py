@@ -47,6 +47,11 @@ def parse():
     ap.add_argument("--cpu-seconds", type=float, default=12.0, help="target CPU time of the oracle sample")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--band", type=int, default=2, help="FP64 band width in tiles (mixed leg)")
+    ap.add_argument("--mode", choices=["evals", "bands", "mle", "batch"], default="evals",
+                    help="evals: the default bench line; bands: accuracy/time per band width; "
+                         "mle: time-to-MLE of the drivers; batch: batched regional fields")
+    ap.add_argument("--bands", default="1,2,4,8,16")
+    ap.add_argument("--fields", type=int, default=512)
     ap.add_argument("--passes", type=int, default=3, help="TF32 passes of the off-band update (1 or 3)")
     return ap.parse_args()
 
@@ -218,10 +223,122 @@ def timed_leg(sess, theta, steps, warmup, barrier):
     return lls, prof
 
 
+def mode_bands(args):
+    """|dl|/|l| and time per evaluation for each FP64 band width (mixed path)
+    against the FP64 path on the same field."""
+    os.environ.setdefault("EXAGEOSTAT_B200_SILENT", "1")
+    import exageostat_b200 as xg
+    from exageostat_b200.synthetic import dlarnv
+
+    xg.init(args.ts)
+    x, y = xg.generate_xy_loc(args.n, args.seed)
+    sess = xg.Session(x, y, dts=args.ts)
+    sess.zvg(THETA, dlarnv(args.seed, args.n))
+
+    def timed(k):
+        t0 = time.perf_counter()
+        v = [sess.loglik(THETA) for _ in range(k)]
+        return v[-1], (time.perf_counter() - t0) / k
+
+    sess.loglik(THETA)
+    ll64, t64 = timed(2)
+    rows = []
+    for band in [int(b) for b in args.bands.split(",")]:
+        sess.set_mixed(band=band, passes=args.passes)
+        sess.loglik(THETA)
+        ll, t = timed(2)
+        rows.append({"band": band, "passes": args.passes, "seconds": t, "speedup_vs_fp64": t64 / t,
+                     "loglik": ll, "rel_err_vs_fp64": abs(ll - ll64) / abs(ll64)})
+        sess.set_fp64()
+    sess.close()
+    print(json.dumps({"mode": "bands", "workload": workload(args.n), "tile": args.ts, "fp64_seconds": t64,
+                      "loglik_fp64": ll64, "rows": rows}), flush=True)
+
+
+def mode_mle(args):
+    """Time-to-MLE: derivative-free maximiser (plain FP64 and mixed) and
+    L-BFGS-B with the adjoint gradient (FP64), bounds [0.01, 5]^3, start at
+    the lower bounds (the reference driver's start) for the derivative-free
+    runs and at the box centre for L-BFGS-B."""
+    os.environ.setdefault("EXAGEOSTAT_B200_SILENT", "1")
+    import numpy as np
+
+    import exageostat_b200 as xg
+    from exageostat_b200.autograd import fit_lbfgsb
+    from exageostat_b200.synthetic import dlarnv
+
+    xg.init(args.ts)
+    theta0 = [1.0, 0.1, 0.5]
+    x, y = xg.generate_xy_loc(args.n, args.seed)
+    sess = xg.Session(x, y, dts=args.ts)
+    sess.zvg(theta0, dlarnv(args.seed, args.n))
+    lb, ub = [0.01] * 3, [5.0] * 3
+    runs = {}
+    t0 = time.perf_counter()
+    th, ll, ev = sess.fit_bobyqa(lb, ub, ftol_abs=1e-9)
+    runs["bobyqa_fp64"] = {"seconds": time.perf_counter() - t0, "evals": ev, "theta": th.tolist(), "loglik": ll}
+    sess.set_mixed(band=args.band, passes=args.passes)
+    t0 = time.perf_counter()
+    th, ll, ev = sess.fit_bobyqa(lb, ub, ftol_abs=1e-9)
+    runs["bobyqa_mixed"] = {"seconds": time.perf_counter() - t0, "evals": ev, "theta": th.tolist(), "loglik": ll,
+                            "band": args.band}
+    sess.set_fp64()
+    t0 = time.perf_counter()
+    th, ll, ev = fit_lbfgsb(sess, lb, ub, x0=[0.5, 0.5, 0.5])
+    runs["lbfgsb_grad_fp64"] = {"seconds": time.perf_counter() - t0, "evals": ev, "theta": th.tolist(),
+                                "loglik": ll}
+    ref = np.array(runs["bobyqa_fp64"]["theta"])
+    for r in runs.values():
+        r["theta_rel_diff_vs_fp64"] = float(np.max(np.abs(np.array(r["theta"]) - ref) / np.abs(ref)))
+        r["loglik_rel_diff_vs_fp64"] = abs(r["loglik"] - runs["bobyqa_fp64"]["loglik"]) / abs(
+            runs["bobyqa_fp64"]["loglik"])
+    sess.close()
+    print(json.dumps({"mode": "mle", "n": args.n, "theta0": theta0, "runs": runs}), flush=True)
+
+
+def mode_batch(args):
+    """Batched regional fields (sizes U[500, 6000], theta_i random): fields/s
+    of one batched graph launch against looping the single-field FP64 path."""
+    os.environ.setdefault("EXAGEOSTAT_B200_SILENT", "1")
+    import numpy as np
+
+    import exageostat_b200 as xg
+
+    xg.init(0)
+    rng = np.random.default_rng(args.seed)
+    xs, ys, zs, th = [], [], [], []
+    for f in range(args.fields):
+        n = int(rng.integers(500, 6001))
+        xs.append(rng.random(n))
+        ys.append(rng.random(n))
+        zs.append(rng.standard_normal(n))
+        th.append([rng.uniform(0.5, 2.0), rng.uniform(0.02, 0.3), rng.uniform(0.3, 2.5)])
+    th = np.array(th)
+    with xg.Batch(xs, ys, zs, ts=256) as b:
+        b.loglik(th)
+        t0 = time.perf_counter()
+        for _ in range(args.steps):
+            out = b.loglik(th)
+        tb = (time.perf_counter() - t0) / args.steps
+    t0 = time.perf_counter()
+    loop = [xg.dmle_host(x, y, z, t, ts=256)[0] for x, y, z, t in zip(xs[:64], ys[:64], zs[:64], th[:64])]
+    tl = (time.perf_counter() - t0) / 64 * args.fields
+    err = float(np.max(np.abs(np.array(loop) - out[:64]) / np.abs(np.array(loop))))
+    sizes = np.array([len(x) for x in xs])
+    print(json.dumps({"mode": "batch", "fields": args.fields, "sizes": [int(sizes.min()), int(sizes.max())],
+                      "flops": float(np.sum(sizes.astype(float) ** 3) / 3), "batched_seconds": tb,
+                      "fields_per_s_batched": args.fields / tb, "looped_seconds_est": tl,
+                      "fields_per_s_looped": args.fields / tl, "speedup": tl / tb,
+                      "max_rel_diff_batched_vs_looped": err}), flush=True)
+
+
 def main():
     args = parse()
     if args.impl == "reference":
         run_reference(args)
+        return
+    if args.mode != "evals":
+        {"bands": mode_bands, "mle": mode_mle, "batch": mode_batch}[args.mode](args)
         return
     import numpy as np
     import torch
