@@ -51,6 +51,7 @@ def parse():
                     help="evals: the default bench line; bands: accuracy/time per band width; "
                          "mle: time-to-MLE of the drivers; batch: batched regional fields")
     ap.add_argument("--bands", default="1,2,4,8,16")
+    ap.add_argument("--sliced-bands", default="1,2")
     ap.add_argument("--fields", type=int, default=512)
     ap.add_argument("--passes", type=int, default=3, help="TF32 passes of the off-band update (1 or 3)")
     return ap.parse_args()
@@ -243,11 +244,18 @@ def mode_bands(args):
     sess.loglik(THETA)
     ll64, t64 = timed(2)
     rows = []
-    for band in [int(b) for b in args.bands.split(",")]:
+    for band in [int(b) for b in args.bands.split(",") if b]:
         sess.set_mixed(band=band, passes=args.passes)
         sess.loglik(THETA)
         ll, t = timed(2)
-        rows.append({"band": band, "passes": args.passes, "seconds": t, "speedup_vs_fp64": t64 / t,
+        rows.append({"scheme": "fp32-offband-tf32x%d" % args.passes, "band": band, "seconds": t,
+                     "speedup_vs_fp64": t64 / t, "loglik": ll, "rel_err_vs_fp64": abs(ll - ll64) / abs(ll64)})
+        sess.set_fp64()
+    for band in [int(b) for b in args.sliced_bands.split(",") if b]:
+        sess.set_sliced(band=band)
+        sess.loglik(THETA)
+        ll, t = timed(2)
+        rows.append({"scheme": "fp64-int8-sliced", "band": band, "seconds": t, "speedup_vs_fp64": t64 / t,
                      "loglik": ll, "rel_err_vs_fp64": abs(ll - ll64) / abs(ll64)})
         sess.set_fp64()
     sess.close()

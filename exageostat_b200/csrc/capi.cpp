@@ -153,7 +153,7 @@ extern "C" void MLE_zvg(MLE_data *data, double *Nrand, double *initial_theta, in
         fprintf(stderr, "MLE_zvg: %s\n", exageostat_last_error());
         return;
     }
-    if (!xg_is_exact(data) || (data->precision != 0 && data->precision != 2)) {
+    if (!xg_is_exact(data) || (data->precision != 0 && data->precision != 2 && data->precision != 3)) {
         xg_fail(XG_ERR_UNSUPPORTED, "MLE_zvg: computation=%s precision=%d", data->computation, data->precision);
         fprintf(stderr, "%s\n", exageostat_last_error());
         return;
@@ -228,13 +228,21 @@ extern "C" int exageostat_b200_loglik(MLE_data *data, const double *theta, doubl
     int rc = xg_kernel_of(data, &kernel, &np);
     if (rc) return rc;
     if (!xg_is_exact(data)) return xg_fail(XG_ERR_UNSUPPORTED, "computation \"%s\"", data->computation);
-    if (data->precision != 0 && data->precision != 2)
-        return xg_fail(XG_ERR_UNSUPPORTED, "precision %d (0 = FP64 and 2 = banded mixed are supported)",
+    if (data->precision != 0 && data->precision != 2 && data->precision != 3)
+        return xg_fail(XG_ERR_UNSUPPORTED,
+                       "precision %d (0 = FP64, 2 = banded mixed, 3 = FP64 with INT8-sliced updates are supported)",
                        data->precision);
     const bool mixed = data->precision == 2;
-    if (mixed && grad) return xg_fail(XG_ERR_UNSUPPORTED, "the gradient is computed in FP64 only (precision 0)");
-    if (mixed && (!f->mx || f->mx->band != (data->diag_thick > 0 ? data->diag_thick : 1))) {
-        rc = xg_field_set_mixed(f, data->diag_thick > 0 ? data->diag_thick : 1, f->mx ? f->mx->passes : 3);
+    const bool sliced = data->precision == 3;
+    const int band = data->diag_thick > 0 ? data->diag_thick : 1;
+    if ((mixed || sliced) && grad)
+        return xg_fail(XG_ERR_UNSUPPORTED, "the gradient is computed in FP64 only (precision 0)");
+    if (mixed && (!f->mx || f->mx->band != band)) {
+        rc = xg_field_set_mixed(f, band, f->mx ? f->mx->passes : 3);
+        if (rc) return rc;
+    }
+    if (sliced && (!f->sl || f->sl->band != band)) {
+        rc = xg_field_set_sliced(f, band);
         if (rc) return rc;
     }
     double res[3], times[3] = {0, 0, 0};
@@ -245,9 +253,10 @@ extern "C" int exageostat_b200_loglik(MLE_data *data, const double *theta, doubl
         xg_recover(data->recovery_file, data->iter_count, np, loglik)) {
         rc = XG_OK;
     } else {
-        rc = mixed  ? xg_field_loglik_mixed(f, theta, res, times)
-             : grad ? xg_field_loglik_grad(f, theta, res, grad, times)
-                    : xg_field_loglik(f, theta, res, times);
+        rc = mixed    ? xg_field_loglik_mixed(f, theta, res, times)
+             : sliced ? xg_field_loglik_sliced(f, theta, res, times)
+             : grad   ? xg_field_loglik_grad(f, theta, res, grad, times)
+                      : xg_field_loglik(f, theta, res, times);
         if (rc == XG_OK) {
             *loglik = res[0];
             data->det = 0.5 * res[1];
@@ -324,7 +333,8 @@ extern "C" double MLE_alg(unsigned n, const double *theta, double *grad, void *v
         fprintf(stderr, "MLE_alg: computation \"%s\" is not provided by this library\n", data->computation);
         return 0;
     }
-    if (data->precision == 0 || data->precision == 2) return EXAGEOSTAT_dmle_Tile(n, theta, grad, vdata);
+    if (data->precision == 0 || data->precision == 2 || data->precision == 3)
+        return EXAGEOSTAT_dmle_Tile(n, theta, grad, vdata);
     fprintf(stderr, "MLE_alg: precision %d is not provided by this library\n", data->precision);
     return 0;
 }
@@ -359,7 +369,7 @@ extern "C" void EXAGEOSTAT_dmle_Predict_Allocate(MLE_data *data, int nZmiss, int
 
 extern "C" void prediction_init(MLE_data *data, int nZmiss, int nZobs, int ts, int p_grid, int q_grid, int mse_flag)
 {
-    if (data->precision == 0 || data->precision == 2)
+    if (data->precision == 0 || data->precision == 2 || data->precision == 3)
         EXAGEOSTAT_dmle_Predict_Allocate(data, nZmiss, nZobs, ts, p_grid, q_grid, mse_flag);
 }
 
@@ -460,6 +470,38 @@ extern "C" int exageostat_b200_dmle_host_mixed(int n, const double *x, const dou
     if (!rc) memcpy(out, res, sizeof res);
     xg_field_destroy(f);
     return rc;
+}
+
+extern "C" int exageostat_b200_set_sliced(MLE_data *data, int band)
+{
+    XgField *f = xg_field_of(data);
+    if (!f) return xg_fail(XG_ERR_NOT_INITIALIZED, "no descriptors: call EXAGEOSTAT_dmle_Call first");
+    data->diag_thick = band;
+    data->precision = 3;
+    return xg_field_set_sliced(f, band);
+}
+
+extern "C" int exageostat_b200_dmle_host_sliced(int n, const double *x, const double *y, const double *z,
+                                                const double *theta, int kernel, int metric, int ts, int band,
+                                                double *out)
+{
+    if (kernel != 0 && kernel != 1) return xg_fail(XG_ERR_BAD_ARGUMENT, "kernel %d", kernel);
+    XgField *f = nullptr;
+    int rc = xg_field_create(&f, n, ts, x, y, kernel, metric);
+    if (rc) return rc;
+    rc = xg_field_set_z(f, z);
+    if (!rc) rc = xg_field_set_sliced(f, band);
+    double res[3];
+    if (!rc) rc = xg_field_loglik_sliced(f, theta, res, nullptr);
+    if (!rc) memcpy(out, res, sizeof res);
+    xg_field_destroy(f);
+    return rc;
+}
+
+extern "C" int exageostat_b200_sliced_factor_dense(int n, const double *x, const double *y, const double *theta,
+                                                   int kernel, int metric, int ts, int band, double *out)
+{
+    return xg_sliced_factor_dense(n, x, y, theta, kernel, metric, ts, band, out);
 }
 
 extern "C" int exageostat_b200_mixed_factor_dense(int n, const double *x, const double *y, const double *theta,

@@ -499,10 +499,11 @@ __device__ __forceinline__ void xg_gemm_body(const CUtensorMap &map, const XgTil
     const int blk = (int)(bid % (bpt * bpt));
     const int bi = blk / bpt, bj = blk % bpt;
     int i, j;
-    if (T.band) {
-        /* band targets (i, j), 0 <= i - j < band, j from j0 */
-        j = j0 + (int)(pair / T.band);
-        i = j + (int)(pair % T.band);
+    const int nb = T.band ? T.band : T.band_targets;
+    if (nb) {
+        /* band targets (i, j), 0 <= i - j < nb, j from j0 */
+        j = j0 + (int)(pair / nb);
+        i = j + (int)(pair % nb);
         if (single_col && j != j0) i = T.nt; /* outside the launch */
     } else {
         int ii, jj;
@@ -785,7 +786,7 @@ void xg_launch_band_gemm(const CUtensorMap &p64map, const XgTileArgs &T, int k, 
     const long long ncol = (part == 1) ? 1 : T.nt - j0;
     if (j0 >= T.nt || ncol <= 0) return;
     const int bpt = T.ts / XG_G_BM;
-    const long long blocks = ncol * T.band * bpt * bpt;
+    const long long blocks = ncol * (T.band ? T.band : T.band_targets) * bpt * bpt;
     xg_syrk_gemm_kernel<<<(unsigned)blocks, XG_G_THREADS, xg_gemm_smem_bytes(), st>>>(p64map, T, k, j0, part == 1,
                                                                                        status);
 }

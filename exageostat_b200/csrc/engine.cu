@@ -105,6 +105,7 @@ int xg_context_start(int dts)
     cudaError_t e = xg_kernels_configure();
     if (e == cudaSuccess) e = xg_gradient_kernels_configure();
     if (e == cudaSuccess) e = xg_mixed_kernels_configure();
+    if (e == cudaSuccess) e = xg_sliced_kernels_configure();
     if (e != cudaSuccess) return xg_cuda_fail(e, "kernel attribute setup");
     g_xg.device = dev;
     g_xg.sm_count = prop.multiProcessorCount;
@@ -356,6 +357,7 @@ void xg_field_destroy(XgField *f)
     if (f->ev_upd) cudaEventDestroy(f->ev_upd);
     xg_tm_free(f->X);
     if (f->mx) xg_mixed_destroy(f->mx);
+    if (f->sl) xg_sliced_destroy(f->sl);
     if (f->gpart) cudaFree(f->gpart);
     if (f->gout) cudaFree(f->gout);
     for (int i = 0; i < 4; ++i)
@@ -576,14 +578,15 @@ int xg_field_loglik_grad(XgField *f, const double *theta, double *res, double *g
 /* ------------------------------------------------------------------------- */
 
 static int xg_encode(CUtensorMap *map, CUtensorMapDataType dt, size_t esize, void *base, cuuint64_t cols,
-                     cuuint64_t rows, cuuint32_t box_cols, cuuint32_t box_rows)
+                     cuuint64_t rows, cuuint32_t box_cols, cuuint32_t box_rows,
+                     CUtensorMapSwizzle swz = CU_TENSOR_MAP_SWIZZLE_128B)
 {
     cuuint64_t dims[2] = {cols, rows};
     cuuint64_t strides[1] = {cols * esize};
     cuuint32_t box[2] = {box_cols, box_rows};
     cuuint32_t estr[2] = {1, 1};
     CUresult r = g_encode(map, dt, 2, base, dims, strides, box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE,
-                          CU_TENSOR_MAP_SWIZZLE_128B, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+                          swz, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
                           CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
     return r == CUDA_SUCCESS ? XG_OK : xg_fail(XG_ERR_CUDA, "cuTensorMapEncodeTiled failed (%d)", (int)r);
 }
@@ -719,10 +722,12 @@ static void xg_mixed_step_flops(int nt, int ts, int band, int k, double *band_fl
     *off_flops = of;
 }
 
-void xg_field_collect_profile_mixed(XgField *f)
+/* Per-kernel-class times of a banded factorisation (mixed or sliced), from
+ * the 8 events per step; launches_per_step counts the panel and trailing
+ * launches of one step. */
+void xg_field_collect_profile_banded(XgField *f, int band, double launches_per_step)
 {
-    XgMixed *m = f->mx;
-    const int nt = m->T.nt;
+    const int nt = f->C.nt;
     float ms = 0;
     auto el = [&](int a, int b) {
         cudaEventElapsedTime(&ms, f->pev[a], f->pev[b]);
@@ -737,7 +742,7 @@ void xg_field_collect_profile_mixed(XgField *f)
         if (k + 1 < nt) {
             f->prof[3] += el(e + 3, e + 7);
             double bfl, ofl;
-            xg_mixed_step_flops(nt, m->T.ts, m->band, k, &bfl, &ofl);
+            xg_mixed_step_flops(nt, f->C.ts, band, k, &bfl, &ofl);
             f->prof[4] += bfl + ofl;
             f->prof[8] += el(e + 4, e + 5) + el(e + 6, e + 7);
             f->prof[9] += ofl;
@@ -747,11 +752,16 @@ void xg_field_collect_profile_mixed(XgField *f)
     }
     cudaEventElapsedTime(&ms, f->ev[0], f->ev[2]);
     f->prof[7] += ms * 1e-3;
-    /* generation, finalize, per step POTRF + band TRSM + FP32 TRSM + panel prep
-     * + two band and two off-band trailing launches (upper bound: empty
-     * launches are skipped on the host) */
-    f->prof[5] += 2 + 8.0 * nt;
+    /* generation and finalize, then per step (upper bound: empty launches are
+     * skipped on the host) */
+    f->prof[5] += 2 + launches_per_step * nt;
     f->prof[6] += 1;
+}
+
+void xg_field_collect_profile_mixed(XgField *f)
+{
+    /* POTRF, band TRSM, FP32 TRSM, panel prep, two band and two off-band launches */
+    xg_field_collect_profile_banded(f, f->mx->band, 8.0);
 }
 
 int xg_field_set_mixed(XgField *f, int band, int passes)
@@ -863,6 +873,224 @@ int xg_mixed_factor_dense(int n, const double *x, const double *y, const double 
                 }
                 out[(size_t)r * n + c] = val;
             }
+    xg_field_destroy(f);
+    return rc;
+}
+
+/* Copies the lower-tile store of f to a dense row-major n x n array (zeros
+ * above the diagonal), after the stream's work; reads the status word. */
+static int xg_tiles_to_dense(XgField *f, int n, double *out)
+{
+    cudaStream_t st = g_xg.stream;
+    int rc = XG_OK;
+    cudaError_t le = cudaGetLastError();
+    if (le != cudaSuccess) return xg_cuda_fail(le, "dense copy launch");
+    const int tsz = f->C.ts;
+    const size_t tile_elems = (size_t)tsz * tsz;
+    double *h = (double *)malloc(f->C.ntiles * tile_elems * sizeof(double));
+    if (!h) return xg_fail(XG_ERR_NO_MEMORY, "host copy of the tiles");
+    int sv[2] = {0, 0};
+    cudaError_t e = cudaMemcpyAsync(h, f->C.d, f->C.ntiles * tile_elems * sizeof(double), cudaMemcpyDeviceToHost, st);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(sv, f->status, sizeof sv, cudaMemcpyDeviceToHost, st);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+    if (e != cudaSuccess) rc = xg_cuda_fail(e, "tile download");
+    if (!rc && (sv[0] & XG_ST_NOT_SPD)) rc = xg_fail(XG_ERR_NOT_SPD, "not positive definite (pivot %d)", sv[1]);
+    if (!rc && sv[0]) rc = xg_fail(XG_ERR_TIMEOUT, "device status word 0x%x", sv[0]);
+    if (!rc) {
+        for (int r = 0; r < n; ++r)
+            for (int c = 0; c < n; ++c) {
+                double val = 0.0;
+                if (c <= r) {
+                    const int i = r / tsz, j = c / tsz;
+                    val = h[xg_tile_index(i, j, f->C.nt) * tile_elems + (size_t)(r % tsz) * tsz + (c % tsz)];
+                }
+                out[(size_t)r * n + c] = val;
+            }
+    }
+    free(h);
+    return rc;
+}
+
+/* ------------------------------------------------------------------------- */
+/* FP64 tiles, INT8-sliced off-band updates                                  */
+/* ------------------------------------------------------------------------- */
+
+void xg_sliced_destroy(XgSliced *s)
+{
+    if (!s) return;
+    for (int b = 0; b < 2; ++b) {
+        if (s->dig[b]) cudaFree(s->dig[b]);
+        if (s->scale[b]) cudaFree(s->scale[b]);
+    }
+    delete s;
+}
+
+int xg_field_set_sliced(XgField *f, int band)
+{
+    if (band < 1) band = 1;
+    if (band > f->C.nt) band = f->C.nt;
+    if (f->sl && f->sl->band == band) return XG_OK;
+    if (f->sl) {
+        f->sl->band = band; /* the digit buffers do not depend on the band */
+        return XG_OK;
+    }
+    const int ts = f->C.ts;
+    if (ts % 128 != 0) return xg_fail(XG_ERR_BAD_ARGUMENT, "the sliced path needs a tile size multiple of 128");
+    XgSliced *s = new XgSliced();
+    s->band = band;
+    s->plane_rows = (long long)f->C.nt * ts;
+    const size_t plane = (size_t)s->plane_rows * ts;
+    int rc = XG_OK;
+    for (int b = 0; b < 2 && !rc; ++b) {
+        if (cudaMalloc(&s->dig[b], 4 * plane) != cudaSuccess ||
+            cudaMalloc(&s->scale[b], (size_t)s->plane_rows * sizeof(double)) != cudaSuccess) {
+            rc = xg_fail(XG_ERR_NO_MEMORY, "digit planes (%.2f GB)", 8.0 * plane / 1e9);
+            break;
+        }
+        rc = xg_encode(&s->map[b], CU_TENSOR_MAP_DATA_TYPE_UINT8, 1, s->dig[b], ts, 4 * s->plane_rows, 64, 128,
+                       CU_TENSOR_MAP_SWIZZLE_64B);
+    }
+    if (rc) {
+        xg_sliced_destroy(s);
+        return rc;
+    }
+    f->sl = s;
+    return XG_OK;
+}
+
+/* The FP64 factorisation (xg_factor_lookahead) with the trailing update split
+ * by target: band targets (0 <= i - j < band) on the FP64 DMMA kernel reading
+ * the tile store, off-band targets on the INT8-sliced kernel reading the digit
+ * planes of the panel.  The panel of step k+1 (POTRF, TRSM, slicing) runs on
+ * the high-priority stream under the rest of step k's update.  Profiling
+ * events as in the banded mixed path (8 per step). */
+static void xg_factor_sliced(XgField *f, double *v, const XgFactorStreams &fs)
+{
+    XgSliced *sl = f->sl;
+    XgTileMatrix &M = f->C;
+    XgTileArgs T{M.d, M.ts, M.nt};
+    XgTileArgs Tb = T;
+    Tb.band_targets = sl->band;
+    const int nt = M.nt;
+    const long long plane = sl->plane_rows * M.ts;
+    const bool la = fs.st_hi != nullptr;
+    cudaStream_t sp = la ? fs.st_hi : fs.st;
+    cudaEvent_t *pev = fs.pev;
+    auto rec = [&](int k, int e, cudaStream_t s) {
+        if (pev) cudaEventRecord(pev[8 * k + e], s);
+    };
+    const int rhs = v != nullptr;
+    if (la) cudaEventRecord(fs.ev_upd, fs.st);
+    for (int k = 0; k < nt; ++k) {
+        const int b = k & 1;
+        if (la) cudaStreamWaitEvent(sp, fs.ev_upd, 0);
+        rec(k, 0, sp);
+        xg_launch_potrf_diag(T, k, v, f->part, f->part + nt, rhs, f->status, f->info, sp);
+        rec(k, 1, sp);
+        xg_launch_trsm_panel(T, k, v, rhs, f->status, sp);
+        if (k + 1 < nt) xg_launch_slice_panel(T, k, sl->dig[b], sl->scale[b], plane, f->status, sp);
+        rec(k, 2, sp);
+        if (la) {
+            cudaEventRecord(fs.ev_panel, sp);
+            cudaStreamWaitEvent(fs.st, fs.ev_panel, 0);
+        }
+        rec(k, 3, fs.st);
+        if (k + 1 < nt) {
+            xg_launch_band_gemm(M.map, Tb, k, la ? 1 : 0, f->status, fs.st);
+            rec(k, 4, fs.st);
+            xg_launch_sliced_gemm(sl->map[b], sl->scale[b], T, sl->band, k, la ? 1 : 0, (int)sl->plane_rows,
+                                  g_xg.sm_count, f->status, fs.st);
+            rec(k, 5, fs.st);
+            if (la) {
+                cudaEventRecord(fs.ev_upd, fs.st);
+                xg_launch_band_gemm(M.map, Tb, k, 2, f->status, fs.st);
+                rec(k, 6, fs.st);
+                xg_launch_sliced_gemm(sl->map[b], sl->scale[b], T, sl->band, k, 2, (int)sl->plane_rows,
+                                      g_xg.sm_count, f->status, fs.st);
+            } else {
+                rec(k, 6, fs.st);
+            }
+        } else {
+            rec(k, 4, fs.st);
+            rec(k, 5, fs.st);
+            rec(k, 6, fs.st);
+        }
+        rec(k, 7, fs.st);
+    }
+}
+
+int xg_field_loglik_sliced(XgField *f, const double *theta, double *res, double *times)
+{
+    int rc = xg_check_theta(theta, f->kernel);
+    if (rc) return rc;
+    if (!f->have_z) return xg_fail(XG_ERR_BAD_ARGUMENT, "no observations: call MLE_zvg or set z first");
+    if (!f->sl) {
+        rc = xg_field_set_sliced(f, 1);
+        if (rc) return rc;
+    }
+    cudaStream_t st = g_xg.stream;
+    XgTileArgs T{f->C.d, f->C.ts, f->C.nt};
+    const XgMaternParams p = xg_params(theta, f->kernel);
+    const size_t Np = (size_t)f->C.nt * f->C.ts;
+    XG_CU(cudaMemsetAsync(f->status, 0, 2 * sizeof(int), st));
+    XG_CU(cudaMemcpyAsync(f->v, f->z, Np * sizeof(double), cudaMemcpyDeviceToDevice, st));
+    XG_CU(cudaEventRecord(f->ev[0], st));
+    xg_launch_gen(T, f->C.ij, f->C.ntiles, f->x, f->y, f->x, f->y, f->N, f->N, p, f->metric, 1, st);
+    XG_CU(cudaEventRecord(f->ev[1], st));
+    XgFactorStreams fs;
+    fs.st = st;
+    fs.st_hi = g_xg.stream_hi;
+    fs.ev_panel = f->ev_panel;
+    fs.ev_upd = f->ev_upd;
+    fs.pev = f->profiling ? f->pev : nullptr;
+    xg_factor_sliced(f, f->v, fs);
+    xg_launch_finalize(f->part, f->part + f->C.nt, f->C.nt, f->N, f->out, f->status, f->info, st);
+    XG_CU(cudaEventRecord(f->ev[2], st));
+    XG_CU(cudaMemcpyAsync(f->h_out, f->out, 5 * sizeof(double), cudaMemcpyDeviceToHost, st));
+    XG_CU(cudaGetLastError());
+    XG_CU(cudaStreamSynchronize(st));
+    if (times) {
+        float a = 0, b = 0;
+        cudaEventElapsedTime(&a, f->ev[0], f->ev[1]);
+        cudaEventElapsedTime(&b, f->ev[1], f->ev[2]);
+        times[0] = a * 1e-3;
+        times[1] = b * 1e-3;
+    }
+    if (f->profiling) /* POTRF, TRSM, slicing, two band and two off-band launches */
+        xg_field_collect_profile_banded(f, f->sl->band, 7.0);
+    rc = xg_read_status(f);
+    if (rc) return rc;
+    res[0] = f->h_out[0];
+    res[1] = f->h_out[1];
+    res[2] = f->h_out[2];
+    return XG_OK;
+}
+
+/* Dense factor L (row-major n x n, zeros above the diagonal) of the sliced
+ * path, for the parity tests. */
+int xg_sliced_factor_dense(int n, const double *x, const double *y, const double *theta, int kernel, int metric,
+                           int ts, int band, double *out)
+{
+    XgField *f = nullptr;
+    int rc = xg_check_theta(theta, kernel);
+    if (rc) return rc;
+    rc = xg_field_create(&f, n, ts, x, y, kernel, metric);
+    if (!rc) rc = xg_field_set_sliced(f, band);
+    if (rc) {
+        xg_field_destroy(f);
+        return rc;
+    }
+    cudaStream_t st = g_xg.stream;
+    XgTileArgs T{f->C.d, f->C.ts, f->C.nt};
+    cudaMemsetAsync(f->status, 0, 2 * sizeof(int), st);
+    xg_launch_gen(T, f->C.ij, f->C.ntiles, f->x, f->y, f->x, f->y, n, n, xg_params(theta, kernel), metric, 1, st);
+    XgFactorStreams fs;
+    fs.st = st;
+    fs.st_hi = g_xg.stream_hi;
+    fs.ev_panel = f->ev_panel;
+    fs.ev_upd = f->ev_upd;
+    xg_factor_sliced(f, nullptr, fs);
+    rc = xg_tiles_to_dense(f, n, out);
     xg_field_destroy(f);
     return rc;
 }
@@ -986,34 +1214,7 @@ int xg_covariance_dense(int n, const double *x, const double *y, const double *t
     cudaMemsetAsync(f->status, 0, 2 * sizeof(int), st);
     xg_launch_gen(T, f->C.ij, f->C.ntiles, f->x, f->y, f->x, f->y, n, n, p, metric, 1, st);
     if (factor) xg_factor(f->C, nullptr, f->part, f->status, f->info, st);
-    {
-        cudaError_t le = cudaGetLastError();
-        if (le != cudaSuccess) {
-            xg_field_destroy(f);
-            return xg_cuda_fail(le, "covariance launch");
-        }
-    }
-    const int tsz = f->C.ts;
-    const size_t tile_elems = (size_t)tsz * tsz;
-    double *h = (double *)malloc(f->C.ntiles * tile_elems * sizeof(double));
-    int sv[2] = {0, 0};
-    cudaError_t e = cudaMemcpyAsync(h, f->C.d, f->C.ntiles * tile_elems * sizeof(double), cudaMemcpyDeviceToHost, st);
-    if (e == cudaSuccess) e = cudaMemcpyAsync(sv, f->status, sizeof sv, cudaMemcpyDeviceToHost, st);
-    if (e == cudaSuccess) e = cudaStreamSynchronize(st);
-    if (e != cudaSuccess) rc = xg_cuda_fail(e, "covariance download");
-    if (!rc && (sv[0] & XG_ST_NOT_SPD)) rc = xg_fail(XG_ERR_NOT_SPD, "not positive definite (pivot %d)", sv[1]);
-    if (!rc) {
-        for (int r = 0; r < n; ++r)
-            for (int c = 0; c < n; ++c) {
-                double val = 0.0;
-                if (c <= r) {
-                    const int i = r / tsz, j = c / tsz;
-                    val = h[xg_tile_index(i, j, f->C.nt) * tile_elems + (size_t)(r % tsz) * tsz + (c % tsz)];
-                }
-                out[(size_t)r * n + c] = val;
-            }
-    }
-    free(h);
+    rc = xg_tiles_to_dense(f, n, out);
     xg_field_destroy(f);
     return rc;
 }

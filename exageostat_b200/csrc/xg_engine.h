@@ -50,6 +50,17 @@ struct XgMixed {
     XgMixedMaps maps[2];
 };
 
+/* FP64 tiles with INT8-sliced off-band updates (sliced.cu): the FP64 tile
+ * store of the field plus double-buffered digit planes and row scales of the
+ * current panel. */
+struct XgSliced {
+    int band = 1;
+    long long plane_rows = 0;        /* rows per digit plane (nt * ts) */
+    int8_t *dig[2] = {nullptr, nullptr};
+    double *scale[2] = {nullptr, nullptr};
+    CUtensorMap map[2];
+};
+
 /* One dataset: locations, observations and the covariance / factor. */
 struct XgField {
     int N = 0;
@@ -70,6 +81,7 @@ struct XgField {
     /* gradient workspace, allocated on the first gradient request */
     XgTileMatrix X;              /* X = L^-T (lower-tile slots, X_IK at slot (K, I)) */
     XgMixed *mx = nullptr;       /* mixed-precision workspace (precision 2) */
+    XgSliced *sl = nullptr;      /* INT8-sliced workspace (precision 3) */
     double *gpart = nullptr;     /* per-CTA contraction partials */
     double *gout = nullptr;      /* 4 gradient sums */
     /* optional per-kernel-class timing (exageostat_b200_set_profiling) */
@@ -121,6 +133,11 @@ int xg_mixed_factor_dense(int n, const double *x, const double *y, const double 
 double xg_digamma(double x);
 void xg_field_collect_profile_mixed(XgField *f);
 int xg_field_get_z(XgField *f, double *z, int n);
+int xg_field_set_sliced(XgField *f, int band);
+int xg_field_loglik_sliced(XgField *f, const double *theta, double *res, double *times);
+void xg_sliced_destroy(XgSliced *s);
+int xg_sliced_factor_dense(int n, const double *x, const double *y, const double *theta, int kernel, int metric,
+                           int ts, int band, double *out);
 
 int xg_predict_create(XgPredict **out, int nmiss, int nobs, int ts);
 void xg_predict_destroy(XgPredict *q);

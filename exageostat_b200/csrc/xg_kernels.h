@@ -7,6 +7,7 @@
 #include <cuda.h>
 #include <cuda_runtime.h>
 #include <stddef.h>
+#include <stdint.h>
 
 /* Tile sizes are multiples of 128 up to XG_MAX_TS: the panel TRSM stages
  * 32 x ts doubles in shared memory. */
@@ -24,6 +25,9 @@ struct XgTileArgs {
     int band = 0;
     float *data32 = nullptr;
     long long tile_off = 0; /* first tile of this matrix inside a shared TMA tensor (batches) */
+    /* band == 0 only: restricts the DMMA trailing update to the targets
+     * 0 <= i - j < band_targets (the others go to the INT8-sliced kernel) */
+    int band_targets = 0;
 };
 
 __host__ __device__ inline long long xg_slot64(const XgTileArgs &T, int i, int j)
@@ -132,6 +136,13 @@ void xg_launch_band_gemm(const CUtensorMap &p64map, const XgTileArgs &T, int k, 
                          cudaStream_t st);
 void xg_launch_offband_gemm(const XgMixedMaps &maps, const XgTileArgs &T, int k, int part, int passes, int sm_count,
                             int *status, cudaStream_t st);
+/* sliced.cu: FP64 tiles, off-band updates on INT8 tensor cores (four digit slices) */
+cudaError_t xg_sliced_kernels_configure();
+void xg_launch_slice_panel(const XgTileArgs &T, int k, int8_t *dig, double *scale, long long plane, const int *status,
+                           cudaStream_t st);
+void xg_launch_sliced_gemm(const CUtensorMap &map, const double *scale, const XgTileArgs &T, int band, int k,
+                           int part, int plane_rows, int sm_count, int *status, cudaStream_t st);
+
 void xg_launch_finalize(const double *part_logdet, const double *part_dot, int nt, int N, double *out,
                         const int *status, const int *info, cudaStream_t st);
 

@@ -84,8 +84,8 @@ typedef struct {
 } output;
 
 /* misc/include/MLE_misc.h:184-328.  Fields this library reads: computation
- * ("exact"), kernel_fun, dm ("ed" | "gc"), precision (0 FP64, 2 mixed),
- * diag_thick (mixed band, in tiles), l1 / lobs / lmiss, verbose, log,
+ * ("exact"), kernel_fun, dm ("ed" | "gc"), precision (0 FP64, 2 mixed,
+ * 3 FP64 with INT8-sliced updates -- new), diag_thick (band, in tiles), l1 / lobs / lmiss, verbose, log,
  * pFileLog, recovery_file, checkpoint_file.  The desc* handles hold this
  * library's device objects (opaque). */
 typedef struct {
@@ -266,7 +266,8 @@ void MORSE_dmle_Call(MLE_data *data, int ncores, int gpus, int dts, int p_grid, 
 void MLE_zvg(MLE_data *data, double *Nrand, double *initial_theta, int n, int ts, int log, int p_grid, int q_grid);
 
 /* src/include/MLE.h:48-49 (src/compute/MLE.c:138-193): NLopt objective,
- * dispatching on data->precision (0: FP64, 2: banded mixed precision).
+ * dispatching on data->precision (0: FP64, 2: banded mixed precision, 3: FP64
+ * tiles with INT8-sliced off-band updates, see exageostat_b200_set_sliced).
  * Returns the log-likelihood.  New: when grad != NULL it receives d loglik /
  * d theta (the reference ignores grad).  A non-positive-definite covariance
  * returns -INFINITY (the reference exits). */
@@ -381,6 +382,19 @@ int exageostat_b200_set_mixed(MLE_data *data, int band, int passes);
 int exageostat_b200_dmle_host_mixed(int n, const double *x, const double *y, const double *z, const double *theta,
                                     int kernel, int metric, int ts, int band, int passes, double *out);
 
+/* No counterpart in the reference (precision = 3).  Every tile stays FP64;
+ * the trailing updates of tiles within `band` tiles of the diagonal run on
+ * the FP64 tensor cores, the others on the INT8 tensor cores as exact integer
+ * products of four 8-bit slices per operand with a per-row FP64 scale (~32
+ * significant bits relative to the row maximum, exact S32 accumulation).
+ * Sets data->precision = 3 and data->diag_thick = band; grad must be NULL. */
+int exageostat_b200_set_sliced(MLE_data *data, int band);
+
+/* One-shot INT8-sliced log-likelihood on host arrays (as
+ * exageostat_b200_dmle_host; ts 0 = automatic, else a multiple of 128). */
+int exageostat_b200_dmle_host_sliced(int n, const double *x, const double *y, const double *z, const double *theta,
+                                     int kernel, int metric, int ts, int band, double *out);
+
 /* Replaces the locations and/or observations (N host doubles each; NULL
  * keeps the current array) of an allocated MLE_data, e.g. for a new dataset
  * of the same size, without reallocating the device covariance. */
@@ -392,8 +406,9 @@ int exageostat_b200_set_data(MLE_data *data, const double *x, const double *y, c
  * update (the panel overlaps the trailing update, so these may add up to
  * more than the total); trailing-update algorithmic flops; kernel launches;
  * evaluations; total seconds (generation to result); tile size; tiles per
- * side; N; and for the mixed path out[11..14] = seconds and algorithmic flops
- * of the off-band (TF32 tensor-core) and band (FP64) trailing updates. */
+ * side; N; and for the banded paths (precision 2 and 3) out[11..14] = seconds
+ * and algorithmic flops of the off-band (TF32 or INT8 tensor-core) and band
+ * (FP64) trailing updates. */
 int exageostat_b200_set_profiling(MLE_data *data, int on);
 int exageostat_b200_get_profile(MLE_data *data, double *out, int n);
 
@@ -437,6 +452,11 @@ int exageostat_b200_matern_pairs(int n, const double *x1, const double *y1, cons
  * diagonal, computed with tile size ts. */
 int exageostat_b200_covariance_dense(int n, const double *x, const double *y, const double *theta, int kernel,
                                      int metric, int ts, int factor, double *out);
+/* The factor L of the INT8-sliced path (all tiles FP64), row-major n x n
+ * with zeros above the diagonal, for the parity tests. */
+int exageostat_b200_sliced_factor_dense(int n, const double *x, const double *y, const double *theta, int kernel,
+                                        int metric, int ts, int band, double *out);
+
 /* The mixed-precision factor L (band tiles FP64, off-band FP32 widened),
  * row-major n x n with zeros above the diagonal. */
 int exageostat_b200_mixed_factor_dense(int n, const double *x, const double *y, const double *theta, int kernel,
