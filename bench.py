@@ -51,9 +51,13 @@ def parse():
                     help="evals: the default bench line; bands: accuracy/time per band width; "
                          "mle: time-to-MLE of the drivers; batch: batched regional fields")
     ap.add_argument("--bands", default="1,2,4,8,16")
-    ap.add_argument("--sliced-bands", default="1,2")
+    ap.add_argument("--no-sliced-row", dest="sliced_row", action="store_false",
+                    help="bands mode: skip the INT8-sliced row")
     ap.add_argument("--fields", type=int, default=512)
     ap.add_argument("--passes", type=int, default=3, help="TF32 passes of the off-band update (1 or 3)")
+    ap.add_argument("--scheme", choices=["mixed", "sliced"], default="mixed",
+                    help="reduced-precision leg: mixed = FP32 off-band tiles on TF32 tensor cores; "
+                         "sliced = FP64 tiles with INT8-sliced off-band updates")
     return ap.parse_args()
 
 
@@ -251,11 +255,11 @@ def mode_bands(args):
         rows.append({"scheme": "fp32-offband-tf32x%d" % args.passes, "band": band, "seconds": t,
                      "speedup_vs_fp64": t64 / t, "loglik": ll, "rel_err_vs_fp64": abs(ll - ll64) / abs(ll64)})
         sess.set_fp64()
-    for band in [int(b) for b in args.sliced_bands.split(",") if b]:
-        sess.set_sliced(band=band)
+    if args.sliced_row:
+        sess.set_sliced()
         sess.loglik(THETA)
         ll, t = timed(2)
-        rows.append({"scheme": "fp64-int8-sliced", "band": band, "seconds": t, "speedup_vs_fp64": t64 / t,
+        rows.append({"scheme": "fp64-int8-sliced", "band": None, "seconds": t, "speedup_vs_fp64": t64 / t,
                      "loglik": ll, "rel_err_vs_fp64": abs(ll - ll64) / abs(ll64)})
         sess.set_fp64()
     sess.close()
@@ -398,8 +402,12 @@ def main():
     fp64_value = world * args.steps / t64
     ach64 = p64["gemm_flops"] / p64["t_gemm"] / 1e12
 
-    # ---- banded mixed-precision leg (the headline) ----
-    sess.set_mixed(band=args.band, passes=args.passes)
+    # ---- banded reduced-precision leg (the headline) ----
+    sliced = args.scheme == "sliced"
+    if sliced:
+        sess.set_sliced()
+    else:
+        sess.set_mixed(band=args.band, passes=args.passes)
     clk = ClockSampler(local)
     for _ in range(args.warmup):
         sess.loglik(THETA)
@@ -430,20 +438,28 @@ def main():
     e2e_wall = max_over_ranks(time.perf_counter() - t0)
     e2e = {"value": world * e2e_steps / e2e_wall, "unit": UNIT, "h2d_bytes_per_step": 3 * N * 8,
            "d2h_bytes_per_step": 5 * 8,
-           "path": "exageostat_b200_set_data + MLE_alg (C ABI, precision 2), wall clock"}
+           "path": "exageostat_b200_set_data + MLE_alg (C ABI, precision %d), wall clock" % (3 if sliced else 2)}
 
     passes = args.passes
     t_off = pmx["t_offband"]
-    mma_flops = pmx["offband_flops"] * passes
+    if sliced:
+        # ten 8-bit digit-pair products per FP64 product; dense INT8 runs at twice the BF16 rate
+        mult, peak, kname, unit = 10, 2.0 * bf16_peak, "xg_sliced_gemm_kernel (tcgen05 kind::i8, 10 digit " \
+            "pairs, S32 TMEM levels)", "TOP/s"
+        psrc = "dense INT8 = 2 x bf16, bf16 from %s (of measured)" % bf16_src
+    else:
+        mult, peak, kname, unit = passes, tf32_peak, "xg_offband_gemm_kernel (tcgen05 kind::tf32, %d pass%s, " \
+            "TMEM)" % (passes, "es" if passes > 1 else ""), "TFLOP/s"
+        psrc = "dense TF32 = bf16 / 2, bf16 from %s (of measured)" % bf16_src
+    mma_flops = pmx["offband_flops"] * mult
     ach_mx = mma_flops / t_off / 1e12 if t_off > 0 else 0.0
-    roofline = {"bound": "tensor", "kernel": "xg_offband_gemm_kernel (tcgen05 kind::tf32, %d pass%s, TMEM)" % (
-                    passes, "es" if passes > 1 else ""),
-                "achieved": ach_mx, "peak": tf32_peak, "unit": "TFLOP/s", "frac": ach_mx / tf32_peak,
-                "peak_source": "dense TF32 = bf16 / 2, bf16 from %s (of measured)" % bf16_src,
+    roofline = {"bound": "tensor", "kernel": kname,
+                "achieved": ach_mx, "peak": peak, "unit": unit, "frac": ach_mx / peak,
+                "peak_source": psrc,
                 "traffic": None,
-                "algorithmic_flops_per_launch": pmx["offband_flops"] * passes / max(pmx["evals"], 1) /
+                "algorithmic_ops_per_launch": pmx["offband_flops"] * mult / max(pmx["evals"], 1) /
                 max(2 * (pmx["nt"] - 1), 1),
-                "useful_fp32_tflops": pmx["offband_flops"] / t_off / 1e12 if t_off > 0 else 0.0,
+                "useful_tflops": pmx["offband_flops"] / t_off / 1e12 if t_off > 0 else 0.0,
                 "share_of_step": t_off / pmx["t_total"],
                 "phases_s_per_eval": {k: pmx[k] / pmx["evals"] for k in
                                       ("t_gen", "t_potrf", "t_trsm", "t_gemm", "t_offband", "t_band")}}
@@ -458,12 +474,14 @@ def main():
     line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": 1e3 * tmx / args.steps, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None,
-            "dtype": "f64 band + f32 off-band (tf32x%d tensor cores)" % passes, "data": "synthetic",
+            "dtype": ("f64 tiles, off-band updates as int8 digit products (4 slices, s32 accumulate)" if sliced
+                      else "f64 band + f32 off-band (tf32x%d tensor cores)" % passes), "data": "synthetic",
             "config": {"workload": workload(N), "tile": int(pmx["ts"]), "tiles_per_side": int(pmx["nt"]),
-                       "band_tiles": args.band, "tf32_passes": passes,
+                       "band_tiles": args.band, "scheme": args.scheme,
+                       "tf32_passes": None if sliced else passes,
                        "parallelism": "replicas" if world > 1 else "single-gpu",
                        "l2": "inputs larger than L2 (20-40 GB of covariance tiles per step)",
-                       "loglik_mixed": llsmx[-1], "loglik_fp64": lls64[-1], "rel_err_vs_fp64": rel_err,
+                       "loglik_reduced": llsmx[-1], "loglik_fp64": lls64[-1], "rel_err_vs_fp64": rel_err,
                        "loglik_e2e": ll_e2e, "wall_s_timed": wall},
             "fp64": fp64, "speedup_vs_fp64": value / fp64_value,
             "roofline": roofline, "e2e": e2e, "clocks": clocks,

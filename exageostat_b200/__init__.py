@@ -167,9 +167,9 @@ def lib():
                                               ctypes.POINTER(_VP)]),
         "exageostat_b200_batch_loglik": (_I, [_VP, _PD, _PD]),
         "exageostat_b200_batch_destroy": (_I, [_VP]),
-        "exageostat_b200_set_sliced": (_I, [PM, _I]),
-        "exageostat_b200_dmle_host_sliced": (_I, [_I, _PD, _PD, _PD, _PD, _I, _I, _I, _I, _PD]),
-        "exageostat_b200_sliced_factor_dense": (_I, [_I, _PD, _PD, _PD, _I, _I, _I, _I, _PD]),
+        "exageostat_b200_set_sliced": (_I, [PM]),
+        "exageostat_b200_dmle_host_sliced": (_I, [_I, _PD, _PD, _PD, _PD, _I, _I, _I, _PD]),
+        "exageostat_b200_sliced_factor_dense": (_I, [_I, _PD, _PD, _PD, _I, _I, _I, _PD]),
     }
     for name, (res, args) in sig.items():
         f = getattr(L, name)
@@ -267,21 +267,21 @@ def mixed_factor_dense(x, y, theta, kernel=0, metric=0, ts=512, band=1, passes=3
     return out
 
 
-def dmle_host_sliced(x, y, z, theta, kernel=0, metric=0, ts=0, band=1):
-    """One-shot log-likelihood with FP64 tiles and INT8-sliced off-band
+def dmle_host_sliced(x, y, z, theta, kernel=0, metric=0, ts=0):
+    """One-shot log-likelihood with FP64 tiles and INT8-sliced trailing
     updates: (loglik, logdet, dotp)."""
     x, y, z = _f64(x), _f64(y), _f64(z)
     out = np.empty(3)
     _check(lib().exageostat_b200_dmle_host_sliced(x.size, _p(x), _p(y), _p(z), _p(_f64(theta)), kernel, metric, ts,
-                                                  band, _p(out)))
+                                                  _p(out)))
     return tuple(out)
 
 
-def sliced_factor_dense(x, y, theta, kernel=0, metric=0, ts=0, band=1) -> np.ndarray:
+def sliced_factor_dense(x, y, theta, kernel=0, metric=0, ts=0) -> np.ndarray:
     x, y = _f64(x), _f64(y)
     n = x.size
     out = np.empty((n, n))
-    _check(lib().exageostat_b200_sliced_factor_dense(n, _p(x), _p(y), _p(_f64(theta)), kernel, metric, ts, band,
+    _check(lib().exageostat_b200_sliced_factor_dense(n, _p(x), _p(y), _p(_f64(theta)), kernel, metric, ts,
                                                      _p(out)))
     return out
 
@@ -376,11 +376,10 @@ class Session:
         _check(self.L.exageostat_b200_set_mixed(ctypes.byref(self.data), band, passes))
         self.data.precision = 2
 
-    def set_sliced(self, band: int = 1) -> None:
-        """Switch MLE_alg / loglik to FP64 tiles with INT8-sliced off-band
-        updates (precision 3); `band` tiles next to the diagonal stay on the
-        FP64 tensor cores."""
-        _check(self.L.exageostat_b200_set_sliced(ctypes.byref(self.data), band))
+    def set_sliced(self) -> None:
+        """Switch MLE_alg / loglik to FP64 tiles with INT8-sliced trailing
+        updates (precision 3)."""
+        _check(self.L.exageostat_b200_set_sliced(ctypes.byref(self.data)))
 
     def set_fp64(self) -> None:
         self.data.precision = 0

@@ -241,8 +241,8 @@ extern "C" int exageostat_b200_loglik(MLE_data *data, const double *theta, doubl
         rc = xg_field_set_mixed(f, band, f->mx ? f->mx->passes : 3);
         if (rc) return rc;
     }
-    if (sliced && (!f->sl || f->sl->band != band)) {
-        rc = xg_field_set_sliced(f, band);
+    if (sliced && !f->sl) {
+        rc = xg_field_set_sliced(f);
         if (rc) return rc;
     }
     double res[3], times[3] = {0, 0, 0};
@@ -472,25 +472,23 @@ extern "C" int exageostat_b200_dmle_host_mixed(int n, const double *x, const dou
     return rc;
 }
 
-extern "C" int exageostat_b200_set_sliced(MLE_data *data, int band)
+extern "C" int exageostat_b200_set_sliced(MLE_data *data)
 {
     XgField *f = xg_field_of(data);
     if (!f) return xg_fail(XG_ERR_NOT_INITIALIZED, "no descriptors: call EXAGEOSTAT_dmle_Call first");
-    data->diag_thick = band;
     data->precision = 3;
-    return xg_field_set_sliced(f, band);
+    return xg_field_set_sliced(f);
 }
 
 extern "C" int exageostat_b200_dmle_host_sliced(int n, const double *x, const double *y, const double *z,
-                                                const double *theta, int kernel, int metric, int ts, int band,
-                                                double *out)
+                                                const double *theta, int kernel, int metric, int ts, double *out)
 {
     if (kernel != 0 && kernel != 1) return xg_fail(XG_ERR_BAD_ARGUMENT, "kernel %d", kernel);
     XgField *f = nullptr;
     int rc = xg_field_create(&f, n, ts, x, y, kernel, metric);
     if (rc) return rc;
     rc = xg_field_set_z(f, z);
-    if (!rc) rc = xg_field_set_sliced(f, band);
+    if (!rc) rc = xg_field_set_sliced(f);
     double res[3];
     if (!rc) rc = xg_field_loglik_sliced(f, theta, res, nullptr);
     if (!rc) memcpy(out, res, sizeof res);
@@ -499,9 +497,9 @@ extern "C" int exageostat_b200_dmle_host_sliced(int n, const double *x, const do
 }
 
 extern "C" int exageostat_b200_sliced_factor_dense(int n, const double *x, const double *y, const double *theta,
-                                                   int kernel, int metric, int ts, int band, double *out)
+                                                   int kernel, int metric, int ts, double *out)
 {
-    return xg_sliced_factor_dense(n, x, y, theta, kernel, metric, ts, band, out);
+    return xg_sliced_factor_dense(n, x, y, theta, kernel, metric, ts, out);
 }
 
 extern "C" int exageostat_b200_mixed_factor_dense(int n, const double *x, const double *y, const double *theta,

@@ -577,6 +577,13 @@ int xg_field_loglik_grad(XgField *f, const double *theta, double *res, double *g
 /* banded mixed precision                                                    */
 /* ------------------------------------------------------------------------- */
 
+/* SMs left free by the persistent trailing-update kernels (one CTA per SM,
+ * ~197 KB of shared memory each) while the lookahead panel of the next step
+ * (POTRF, TRSM, panel conversion) runs on the high-priority stream: resident
+ * CTAs are never preempted, so without free SMs the panel would wait for the
+ * whole update. */
+#define XG_PANEL_SMS 16
+
 static int xg_encode(CUtensorMap *map, CUtensorMapDataType dt, size_t esize, void *base, cuuint64_t cols,
                      cuuint64_t rows, cuuint32_t box_cols, cuuint32_t box_rows,
                      CUtensorMapSwizzle swz = CU_TENSOR_MAP_SWIZZLE_128B)
@@ -692,7 +699,7 @@ static void xg_factor_mixed(XgMixed *m, double *v, double *part, int *status, in
                 cudaEventRecord(fs.ev_upd, fs.st);
                 xg_launch_band_gemm(m->maps[b].p64, T, k, 2, status, fs.st);
                 rec(k, 6, fs.st);
-                xg_launch_offband_gemm(m->maps[b], T, k, 2, m->passes, g_xg.sm_count, status, fs.st);
+                xg_launch_offband_gemm(m->maps[b], T, k, 2, m->passes, g_xg.sm_count - XG_PANEL_SMS, status, fs.st);
             } else {
                 rec(k, 6, fs.st);
             }
@@ -918,38 +925,37 @@ static int xg_tiles_to_dense(XgField *f, int n, double *out)
 void xg_sliced_destroy(XgSliced *s)
 {
     if (!s) return;
-    for (int b = 0; b < 2; ++b) {
-        if (s->dig[b]) cudaFree(s->dig[b]);
-        if (s->scale[b]) cudaFree(s->scale[b]);
-    }
+    if (s->dig) cudaFree(s->dig);
+    if (s->scale) cudaFree(s->scale);
+    if (s->ev_a) cudaEventDestroy(s->ev_a);
+    for (int b = 0; b < 2; ++b)
+        if (s->ev_p[b]) cudaEventDestroy(s->ev_p[b]);
     delete s;
 }
 
-int xg_field_set_sliced(XgField *f, int band)
+int xg_field_set_sliced(XgField *f)
 {
-    if (band < 1) band = 1;
-    if (band > f->C.nt) band = f->C.nt;
-    if (f->sl && f->sl->band == band) return XG_OK;
-    if (f->sl) {
-        f->sl->band = band; /* the digit buffers do not depend on the band */
-        return XG_OK;
-    }
+    if (f->sl) return XG_OK;
     const int ts = f->C.ts;
     if (ts % 128 != 0) return xg_fail(XG_ERR_BAD_ARGUMENT, "the sliced path needs a tile size multiple of 128");
     XgSliced *s = new XgSliced();
-    s->band = band;
-    s->plane_rows = (long long)f->C.nt * ts;
+    s->plane_rows = f->C.ntiles * ts;
     const size_t plane = (size_t)s->plane_rows * ts;
     int rc = XG_OK;
-    for (int b = 0; b < 2 && !rc; ++b) {
-        if (cudaMalloc(&s->dig[b], 4 * plane) != cudaSuccess ||
-            cudaMalloc(&s->scale[b], (size_t)s->plane_rows * sizeof(double)) != cudaSuccess) {
-            rc = xg_fail(XG_ERR_NO_MEMORY, "digit planes (%.2f GB)", 8.0 * plane / 1e9);
-            break;
-        }
-        rc = xg_encode(&s->map[b], CU_TENSOR_MAP_DATA_TYPE_UINT8, 1, s->dig[b], ts, 4 * s->plane_rows, 64, 128,
+    if (4 * s->plane_rows > 0x7fffffffLL)
+        rc = xg_fail(XG_ERR_BAD_ARGUMENT, "N = %d is beyond the sliced path's 2^31-row digit store", f->N);
+    if (!rc && (cudaMalloc(&s->dig, 4 * plane) != cudaSuccess ||
+                cudaMalloc(&s->scale, (size_t)s->plane_rows * sizeof(double)) != cudaSuccess))
+        rc = xg_fail(XG_ERR_NO_MEMORY, "digit planes (%.2f GB)", 4.0 * plane / 1e9);
+    /* both operands are staged in boxes of 128 rows x 64 bytes */
+    if (!rc)
+        rc = xg_encode(&s->map_a, CU_TENSOR_MAP_DATA_TYPE_UINT8, 1, s->dig, ts, 4 * s->plane_rows, 64, 128,
                        CU_TENSOR_MAP_SWIZZLE_64B);
-    }
+    if (!rc) s->map_b = s->map_a;
+    if (!rc && (cudaEventCreateWithFlags(&s->ev_a, cudaEventDisableTiming) != cudaSuccess ||
+                cudaEventCreateWithFlags(&s->ev_p[0], cudaEventDisableTiming) != cudaSuccess ||
+                cudaEventCreateWithFlags(&s->ev_p[1], cudaEventDisableTiming) != cudaSuccess))
+        rc = xg_fail(XG_ERR_CUDA, "sliced lookahead events");
     if (rc) {
         xg_sliced_destroy(s);
         return rc;
@@ -958,21 +964,25 @@ int xg_field_set_sliced(XgField *f, int band)
     return XG_OK;
 }
 
-/* The FP64 factorisation (xg_factor_lookahead) with the trailing update split
- * by target: band targets (0 <= i - j < band) on the FP64 DMMA kernel reading
- * the tile store, off-band targets on the INT8-sliced kernel reading the digit
- * planes of the panel.  The panel of step k+1 (POTRF, TRSM, slicing) runs on
- * the high-priority stream under the rest of step k's update.  Profiling
- * events as in the banded mixed path (8 per step). */
+/* Left-looking factorisation with FP64 tiles and INT8-sliced updates.  For
+ * each column j:
+ *   update  : A_ij -= sum_{k<j} L_ik L_jk^T for i >= j (xg_sliced_left_kernel)
+ *   panel   : POTRF(j, j) [+ log-det, + z block solve] -> TRSM(i, j) [+ z update]
+ *             -> slicing of the tiles (i, j), i > j, into digit planes
+ * With fs.st_hi the update of column j+1 is split: chunks k < j (needing
+ * panels already sliced) run on the main stream on all but XG_PANEL_SMS SMs
+ * while the panel chain of column j runs on the high-priority stream, and
+ * chunk k = j joins the panel chain of column j+1.  Profiling events (8 per
+ * column): panel stream before / after the last-chunk update, after POTRF,
+ * after TRSM + slicing; main stream before / after the split update. */
 static void xg_factor_sliced(XgField *f, double *v, const XgFactorStreams &fs)
 {
     XgSliced *sl = f->sl;
     XgTileMatrix &M = f->C;
     XgTileArgs T{M.d, M.ts, M.nt};
-    XgTileArgs Tb = T;
-    Tb.band_targets = sl->band;
     const int nt = M.nt;
     const long long plane = sl->plane_rows * M.ts;
+    const int pr = (int)sl->plane_rows;
     const bool la = fs.st_hi != nullptr;
     cudaStream_t sp = la ? fs.st_hi : fs.st;
     cudaEvent_t *pev = fs.pev;
@@ -980,43 +990,75 @@ static void xg_factor_sliced(XgField *f, double *v, const XgFactorStreams &fs)
         if (pev) cudaEventRecord(pev[8 * k + e], s);
     };
     const int rhs = v != nullptr;
-    if (la) cudaEventRecord(fs.ev_upd, fs.st);
-    for (int k = 0; k < nt; ++k) {
-        const int b = k & 1;
-        if (la) cudaStreamWaitEvent(sp, fs.ev_upd, 0);
-        rec(k, 0, sp);
-        xg_launch_potrf_diag(T, k, v, f->part, f->part + nt, rhs, f->status, f->info, sp);
-        rec(k, 1, sp);
-        xg_launch_trsm_panel(T, k, v, rhs, f->status, sp);
-        if (k + 1 < nt) xg_launch_slice_panel(T, k, sl->dig[b], sl->scale[b], plane, f->status, sp);
-        rec(k, 2, sp);
+    const int sms = g_xg.sm_count;
+    if (la) cudaEventRecord(sl->ev_a, fs.st); /* the generated matrix */
+    for (int j = 0; j < nt; ++j) {
+        if (la) cudaStreamWaitEvent(sp, sl->ev_a, 0); /* chunks k < j-1 of column j */
+        rec(j, 0, sp);
         if (la) {
-            cudaEventRecord(fs.ev_panel, sp);
-            cudaStreamWaitEvent(fs.st, fs.ev_panel, 0);
-        }
-        rec(k, 3, fs.st);
-        if (k + 1 < nt) {
-            xg_launch_band_gemm(M.map, Tb, k, la ? 1 : 0, f->status, fs.st);
-            rec(k, 4, fs.st);
-            xg_launch_sliced_gemm(sl->map[b], sl->scale[b], T, sl->band, k, la ? 1 : 0, (int)sl->plane_rows,
-                                  g_xg.sm_count, f->status, fs.st);
-            rec(k, 5, fs.st);
-            if (la) {
-                cudaEventRecord(fs.ev_upd, fs.st);
-                xg_launch_band_gemm(M.map, Tb, k, 2, f->status, fs.st);
-                rec(k, 6, fs.st);
-                xg_launch_sliced_gemm(sl->map[b], sl->scale[b], T, sl->band, k, 2, (int)sl->plane_rows,
-                                      g_xg.sm_count, f->status, fs.st);
-            } else {
-                rec(k, 6, fs.st);
-            }
+            if (j >= 1) xg_launch_sliced_left(sl->map_a, sl->map_b, sl->scale, T, j, j - 1, j, pr, XG_PANEL_SMS,
+                                              f->status, sp);
         } else {
-            rec(k, 4, fs.st);
-            rec(k, 5, fs.st);
-            rec(k, 6, fs.st);
+            xg_launch_sliced_left(sl->map_a, sl->map_b, sl->scale, T, j, 0, j, pr, sms, f->status, sp);
         }
-        rec(k, 7, fs.st);
+        rec(j, 1, sp);
+        xg_launch_potrf_diag(T, j, v, f->part, f->part + nt, rhs, f->status, f->info, sp);
+        rec(j, 2, sp);
+        xg_launch_trsm_panel(T, j, v, rhs, f->status, sp);
+        if (j + 1 < nt) xg_launch_slice_panel(T, j, sl->dig, sl->scale, plane, f->status, sp);
+        rec(j, 3, sp);
+        if (la) {
+            cudaEventRecord(sl->ev_p[j & 1], sp);
+            /* chunks k < j of column j+1, behind the slicing of panel j-1 */
+            if (j >= 1 && j + 1 < nt) cudaStreamWaitEvent(fs.st, sl->ev_p[(j - 1) & 1], 0);
+            rec(j, 4, fs.st);
+            if (j >= 1 && j + 1 < nt)
+                xg_launch_sliced_left(sl->map_a, sl->map_b, sl->scale, T, j + 1, 0, j, pr, sms - XG_PANEL_SMS,
+                                      f->status, fs.st);
+            rec(j, 5, fs.st);
+            cudaEventRecord(sl->ev_a, fs.st);
+        } else {
+            rec(j, 4, fs.st);
+            rec(j, 5, fs.st);
+        }
+        rec(j, 6, fs.st);
+        rec(j, 7, fs.st);
     }
+    if (la) {
+        cudaEventRecord(fs.ev_panel, sp);
+        cudaStreamWaitEvent(fs.st, fs.ev_panel, 0);
+    }
+}
+
+/* Per-kernel-class times of the sliced factorisation from its events. */
+static void xg_field_collect_profile_sliced(XgField *f)
+{
+    const int nt = f->C.nt;
+    const double t = f->C.ts;
+    float ms = 0;
+    auto el = [&](int a, int b) {
+        cudaEventElapsedTime(&ms, f->pev[a], f->pev[b]);
+        return ms * 1e-3;
+    };
+    cudaEventElapsedTime(&ms, f->ev[0], f->ev[1]);
+    f->prof[0] += ms * 1e-3;
+    for (int j = 0; j < nt; ++j) {
+        const int e = 8 * j;
+        f->prof[1] += el(e + 1, e + 2);
+        f->prof[2] += el(e + 2, e + 3);
+        const double upd = el(e, e + 1) + el(e + 4, e + 5);
+        f->prof[3] += upd;
+        f->prof[8] += upd;
+        /* column j: j chunks on nt - j - 1 off-diagonal tiles (GEMM) and the diagonal tile (SYRK) */
+        const double fl = (double)j * ((nt - j - 1) * 2.0 * t * t * t + t * t * (t + 1));
+        f->prof[4] += fl;
+        f->prof[9] += fl;
+    }
+    cudaEventElapsedTime(&ms, f->ev[0], f->ev[2]);
+    f->prof[7] += ms * 1e-3;
+    /* generation, finalize; per column two update launches, POTRF, TRSM, slicing */
+    f->prof[5] += 2 + 5.0 * nt;
+    f->prof[6] += 1;
 }
 
 int xg_field_loglik_sliced(XgField *f, const double *theta, double *res, double *times)
@@ -1025,7 +1067,7 @@ int xg_field_loglik_sliced(XgField *f, const double *theta, double *res, double 
     if (rc) return rc;
     if (!f->have_z) return xg_fail(XG_ERR_BAD_ARGUMENT, "no observations: call MLE_zvg or set z first");
     if (!f->sl) {
-        rc = xg_field_set_sliced(f, 1);
+        rc = xg_field_set_sliced(f);
         if (rc) return rc;
     }
     cudaStream_t st = g_xg.stream;
@@ -1056,8 +1098,7 @@ int xg_field_loglik_sliced(XgField *f, const double *theta, double *res, double 
         times[0] = a * 1e-3;
         times[1] = b * 1e-3;
     }
-    if (f->profiling) /* POTRF, TRSM, slicing, two band and two off-band launches */
-        xg_field_collect_profile_banded(f, f->sl->band, 7.0);
+    if (f->profiling) xg_field_collect_profile_sliced(f);
     rc = xg_read_status(f);
     if (rc) return rc;
     res[0] = f->h_out[0];
@@ -1069,13 +1110,13 @@ int xg_field_loglik_sliced(XgField *f, const double *theta, double *res, double 
 /* Dense factor L (row-major n x n, zeros above the diagonal) of the sliced
  * path, for the parity tests. */
 int xg_sliced_factor_dense(int n, const double *x, const double *y, const double *theta, int kernel, int metric,
-                           int ts, int band, double *out)
+                           int ts, double *out)
 {
     XgField *f = nullptr;
     int rc = xg_check_theta(theta, kernel);
     if (rc) return rc;
     rc = xg_field_create(&f, n, ts, x, y, kernel, metric);
-    if (!rc) rc = xg_field_set_sliced(f, band);
+    if (!rc) rc = xg_field_set_sliced(f);
     if (rc) {
         xg_field_destroy(f);
         return rc;

@@ -392,9 +392,21 @@ __global__ void __launch_bounds__(XG_OB_THREADS, 1)
     } else {
         /* ---- epilogue: warps 2-5, TMEM lanes 32 (warp % 4) .. +31 ---- */
         const int lg = warp & 3;
+        /* brings the next job's C row (256 FP32 of one row per thread) into L2
+         * while this job's accumulator is drained */
+        auto prefetch_c = [&](long long jb) {
+            if (jb >= njobs) return;
+            const XgObJob J = xg_ob_decode(jb, nt, ts, band, k, part);
+            const float *p = T32 + xg_slot32(J.i, J.j, nt, band) * (long long)ts * ts +
+                             (long long)(J.bm * XG_OB_BM + lg * 32 + lane) * ts + J.bn * XG_OB_BN;
+#pragma unroll
+            for (int l = 0; l < 8; ++l) asm volatile("prefetch.global.L2 [%0];" ::"l"(p + 32 * l));
+        };
+        prefetch_c(blockIdx.x);
         int jl = 0;
         for (long long job = blockIdx.x; job < njobs; job += gridDim.x, ++jl) {
             const int a = jl & 1;
+            prefetch_c(job + gridDim.x);
             if (!xg_mbar_wait(&acc_full[a], (uint32_t)(jl >> 1) & 1)) {
                 if (lane == 0) atomicOr(status, XG_ST_TIMEOUT);
                 break;

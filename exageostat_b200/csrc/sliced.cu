@@ -26,11 +26,25 @@
  * INT8 MMAs (= 2.5 TF32 passes) per FP64 product.  The S32 sums stay exact:
  * |level sum| <= 4 x 127^2 x ts < 2^31 for ts <= 16384.
  *
+ * Schedule (left-looking): the target tiles of column j receive the whole
+ * update A_ij -= sum_{k<j} L_ik L_jk^T in one pass, chunk by chunk over the
+ * panels k; the S32 levels restart for every chunk (each panel row has its
+ * own scale) and the scaled chunk products accumulate in FP64 registers, so
+ * every FP64 tile is read and written once per column instead of once per
+ * step (the right-looking order would move 16 bytes per trailing element
+ * per step, ~5 TB at N = 100,000).  The digit planes of every factored panel
+ * tile are kept (tile-packed, 4 bytes per element).
+ *
  * Kernels:
  *   xg_slice_panel_kernel : panel tiles (i, k), i > k -> four digit planes + row scales
- *   xg_sliced_gemm_kernel : persistent off-band update, 128 x 128 jobs, warp 0 TMA,
- *                           warp 1 MMA issue + TMEM (4 levels x 128 columns = all 512),
- *                           warps 2-9 epilogue (FP64 combine, C -= s_r s_c U)
+ *   xg_sliced_left_kernel : persistent update of the targets (i, j), i >= j, from the
+ *                           panels k0 <= k < k1; 128 x 128 jobs; warp 0 TMA, warp 1 MMA
+ *                           issue + TMEM (4 levels x 128 columns = all 512), warps 4-11
+ *                           epilogue (FP64 combine per chunk into 64 sums per thread,
+ *                           one C -= update per job); setmaxnreg moves the registers of
+ *                           warpgroup 0 to the epilogue.
+ *                           The MMA computes the transposed block so that a TMEM lane
+ *                           holds a column of C and the accesses to C are coalesced.
  */
 #include <stdint.h>
 
@@ -38,18 +52,36 @@
 #include "xg_kernels.h"
 #include "xg_tcgen05.cuh"
 
-#define XG_SL_BM 128
-#define XG_SL_BN 128
-#define XG_SL_BK 64 /* int8 per 64-byte swizzled row */
+#define XG_SL_BM 128 /* C rows per job (rows of the A operand, the MMA's N) */
+#define XG_SL_BN 128 /* C columns per job (rows of the B operand, the MMA's M) */
+#define XG_SL_BK 64  /* int8 per 64-byte swizzled row */
 #define XG_SL_SLICES 4
-#define XG_SL_LEVELS 4
-#define XG_SL_THREADS 320
+#define XG_SL_LEVELS 4 /* level sums |L_t| <= (t + 1) 127^2 ts stay exact in S32 */
+#define XG_SL_EPI_WARPS 8
+#define XG_SL_THREADS 384 /* warpgroup 0: TMA, MMA, 2 idle warps; warpgroups 1-2: epilogue */
+/* register split (setmaxnreg): launched at 168 per thread (64,512 in all);
+ * warpgroup 0 drops to 40, the epilogue warpgroups rise to 232:
+ * 128 x 40 + 256 x 232 = 64,512 */
+#define XG_SL_REG_LOW 40
+#define XG_SL_REG_HIGH 232
 #define XG_SL_STAGES 3
-#define XG_SL_BOX_BYTES (XG_SL_BM * XG_SL_BK)                           /* one digit plane, 128 rows */
-#define XG_SL_STAGE_BYTES (2 * XG_SL_SLICES * XG_SL_BOX_BYTES)          /* A and B planes: 64 KB */
+#define XG_SL_ABOX_BYTES (XG_SL_BM * XG_SL_BK)                                  /* one digit plane, 128 rows */
+#define XG_SL_BBOX_BYTES (XG_SL_BN * XG_SL_BK)                                  /* one digit plane, 128 rows */
+#define XG_SL_STAGE_BYTES (XG_SL_SLICES * (XG_SL_ABOX_BYTES + XG_SL_BBOX_BYTES)) /* 64 KB */
 #define XG_SL_SMEM (XG_SL_STAGES * XG_SL_STAGE_BYTES + 1024 + 256)
 #define XG_SL_RADIX 254.0
 #define XG_SL_TOP 127.0
+#define XG_SL_INV_RADIX3 (1.0 / (254.0 * 254.0 * 254.0))
+
+/* Exact integer -> FP64 by the magic-number method: the integer is added to
+ * the low mantissa bits of a double with a fixed exponent and the constant is
+ * subtracted (one integer add and one FP64 add, no conversion instruction). */
+/* |x| < 2^51 */
+__device__ __forceinline__ double xg_i64_to_f64(long long x)
+{
+    /* (2^52 + 2^51 + x) - (2^52 + 2^51) */
+    return __longlong_as_double(0x4338000000000000LL + x) - 6755399441055744.0;
+}
 
 /* ========================================================================== */
 /* panel slicing                                                              */
@@ -87,7 +119,7 @@ __global__ void __launch_bounds__(256) xg_slice_panel_kernel(XgTileArgs T, int k
     }
 #pragma unroll
     for (int o = 16; o; o >>= 1) m = fmax(m, __shfl_xor_sync(0xffffffffu, m, o));
-    const long long grow = (long long)i * ts + r; /* panel row index */
+    const long long grow = xg_tile_index(i, k, T.nt) * ts + r; /* tile-packed row index */
     const double c0 = m > 0.0 ? XG_SL_TOP / m : 0.0;
     if (lane == 0) scale[grow] = m / XG_SL_TOP;
 #pragma unroll
@@ -116,33 +148,6 @@ __global__ void __launch_bounds__(256) xg_slice_panel_kernel(XgTileArgs T, int k
 /* off-band trailing update: C64 -= s_r s_c sum_t 254^-t (sum_{a+b=t} D_a E_b^T) */
 /* ========================================================================== */
 
-struct XgSlJob {
-    int i, j, bm, bn;
-};
-
-/* part 1: column k+1; part 2: columns >= k+2; part 0: columns >= k+1.  Targets
- * (i, j) with i - j >= band, each split into (ts / 128)^2 jobs of 128 x 128. */
-__device__ inline XgSlJob xg_sl_decode(long long job, int ts, int band, int k, int part)
-{
-    const int bpt = ts / XG_SL_BM;
-    const long long pair = job / (bpt * bpt);
-    const int blk = (int)(job % (bpt * bpt));
-    XgSlJob J;
-    J.bm = blk / bpt;
-    J.bn = blk % bpt;
-    const int j0 = (part == 2) ? k + 2 : k + 1;
-    if (part == 1) {
-        J.j = j0;
-        J.i = j0 + band + (int)pair;
-    } else {
-        int ii, jj;
-        xg_pair_decode(pair, &ii, &jj);
-        J.j = j0 + jj;
-        J.i = j0 + band + ii;
-    }
-    return J;
-}
-
 /* digit pair p = 0..9 -> (a, b) with a + b <= 3, levels in order; the first
  * pair of each level (p = 0, 1, 3, 6) starts its accumulator */
 __device__ __forceinline__ void xg_sl_pair(int p, int &a, int &b)
@@ -154,9 +159,23 @@ __device__ __forceinline__ void xg_sl_pair(int p, int &a, int &b)
     b = lv - a;
 }
 
+/* job -> target tile i = j + job / (rb * cb) and its block of 64 rows (bm) x
+ * 128 columns (bn); blocks entirely above the diagonal of the diagonal tile
+ * are skipped */
+__device__ __forceinline__ bool xg_sl_job(long long job, int j, int ts, int &i, int &bm, int &bn)
+{
+    const int rb = ts / XG_SL_BM, cb = ts / XG_SL_BN;
+    i = j + (int)(job / (rb * cb));
+    const int blk = (int)(job % (rb * cb));
+    bm = blk / cb;
+    bn = blk % cb;
+    return !(i == j && bm * XG_SL_BM + XG_SL_BM - 1 < bn * XG_SL_BN);
+}
+
 __global__ void __launch_bounds__(XG_SL_THREADS, 1)
-    xg_sliced_gemm_kernel(const __grid_constant__ CUtensorMap map, const double *__restrict__ scale,
-                          XgTileArgs T, int band, int k, int part, long long njobs, int plane_rows, int *status)
+    xg_sliced_left_kernel(const __grid_constant__ CUtensorMap map_a, const __grid_constant__ CUtensorMap map_b,
+                          const double *__restrict__ scale, XgTileArgs T, int j, int k0, int k1, long long njobs,
+                          int plane_rows, int *status)
 {
     extern __shared__ __align__(1024) unsigned char xg_smem_raw[];
     unsigned char *smem = (unsigned char *)(((uintptr_t)xg_smem_raw + 1023) & ~(uintptr_t)1023);
@@ -167,7 +186,7 @@ __global__ void __launch_bounds__(XG_SL_THREADS, 1)
     uint64_t *drain = acc_empty + 1;
     uint32_t *tmem_slot = (uint32_t *)(drain + 1);
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-    const int ts = T.ts;
+    const int ts = T.ts, nt = T.nt;
     if (xg_cta_should_skip(status)) return;
     if (tid == 0) {
         for (int s = 0; s < XG_SL_STAGES; ++s) {
@@ -175,11 +194,11 @@ __global__ void __launch_bounds__(XG_SL_THREADS, 1)
             xg_mbar_init(&empty[s], 1);
         }
         xg_mbar_init(acc_full, 1);
-        xg_mbar_init(acc_empty, 8);
+        xg_mbar_init(acc_empty, XG_SL_EPI_WARPS);
         xg_mbar_init(drain, 1);
         xg_fence_barrier_init();
     }
-    if (warp == 1) xg_tmem_alloc(tmem_slot, 512); /* four 128 x 128 S32 level accumulators */
+    if (warp == 1) xg_tmem_alloc(tmem_slot, 512); /* four 128-lane x 128-column S32 levels */
     xg_tc_fence_before();
     __syncthreads();
     xg_tc_fence_after();
@@ -187,28 +206,36 @@ __global__ void __launch_bounds__(XG_SL_THREADS, 1)
     const int KT = ts / XG_SL_BK;
     bool ok = true;
 
+    if (warp < 4) {
+    asm volatile("setmaxnreg.dec.sync.aligned.u32 %0;" ::"n"(XG_SL_REG_LOW));
     if (warp == 0) {
         /* ---- TMA producer: per stage the four A and four B digit boxes ---- */
         if (lane == 0) {
-            xg_prefetch_tensormap(&map);
+            xg_prefetch_tensormap(&map_a);
+            xg_prefetch_tensormap(&map_b);
             long long it = 0;
             for (long long job = blockIdx.x; job < njobs && ok; job += gridDim.x) {
-                const XgSlJob J = xg_sl_decode(job, ts, band, k, part);
-                const int rowA = J.i * ts + J.bm * XG_SL_BM, rowB = J.j * ts + J.bn * XG_SL_BN;
-                for (int kb = 0; kb < KT; ++kb, ++it) {
-                    const int s = (int)(it % XG_SL_STAGES);
-                    if (it >= XG_SL_STAGES &&
-                        !xg_mbar_wait(&empty[s], (uint32_t)((it / XG_SL_STAGES) - 1) & 1)) {
-                        ok = false;
-                        break;
-                    }
-                    unsigned char *st = smem + s * XG_SL_STAGE_BYTES;
-                    xg_mbar_arrive_expect_tx(&full[s], XG_SL_STAGE_BYTES);
+                int i, bm, bn;
+                if (!xg_sl_job(job, j, ts, i, bm, bn)) continue;
+                for (int k = k0; k < k1 && ok; ++k) {
+                    const int rowA = (int)(xg_tile_index(i, k, nt) * ts) + bm * XG_SL_BM;
+                    const int rowB = (int)(xg_tile_index(j, k, nt) * ts) + bn * XG_SL_BN;
+                    for (int kb = 0; kb < KT; ++kb, ++it) {
+                        const int s = (int)(it % XG_SL_STAGES);
+                        if (it >= XG_SL_STAGES &&
+                            !xg_mbar_wait(&empty[s], (uint32_t)((it / XG_SL_STAGES) - 1) & 1)) {
+                            ok = false;
+                            break;
+                        }
+                        unsigned char *st = smem + s * XG_SL_STAGE_BYTES;
+                        xg_mbar_arrive_expect_tx(&full[s], XG_SL_STAGE_BYTES);
 #pragma unroll
-                    for (int t = 0; t < XG_SL_SLICES; ++t) {
-                        xg_tma_load_2d(st + t * XG_SL_BOX_BYTES, &map, kb * XG_SL_BK, t * plane_rows + rowA, &full[s]);
-                        xg_tma_load_2d(st + (XG_SL_SLICES + t) * XG_SL_BOX_BYTES, &map, kb * XG_SL_BK,
-                                       t * plane_rows + rowB, &full[s]);
+                        for (int t = 0; t < XG_SL_SLICES; ++t) {
+                            xg_tma_load_2d(st + t * XG_SL_ABOX_BYTES, &map_a, kb * XG_SL_BK, t * plane_rows + rowA,
+                                           &full[s]);
+                            xg_tma_load_2d(st + XG_SL_SLICES * XG_SL_ABOX_BYTES + t * XG_SL_BBOX_BYTES, &map_b,
+                                           kb * XG_SL_BK, t * plane_rows + rowB, &full[s]);
+                        }
                     }
                 }
             }
@@ -218,101 +245,160 @@ __global__ void __launch_bounds__(XG_SL_THREADS, 1)
                 xg_mbar_wait(&full[q % XG_SL_STAGES], (uint32_t)(q / XG_SL_STAGES) & 1);
         }
     } else if (warp == 1) {
-        /* ---- MMA issuer ---- */
+        /* ---- MMA issuer: one accumulation (4 levels) per (job, panel chunk) ---- */
         if (lane == 0) {
-            constexpr uint32_t idesc = xg_idesc_i8(XG_SL_BM, XG_SL_BN);
+            constexpr uint32_t idesc = xg_idesc_i8(XG_SL_BN, XG_SL_BM); /* M = 128 (C columns), N = 128 (C rows) */
             const uint32_t sbase = xg_smem_u32(smem);
-            long long it = 0;
-            int jl = 0;
-            for (long long job = blockIdx.x; job < njobs && ok; job += gridDim.x, ++jl) {
-                if (jl >= 1 && !xg_mbar_wait(acc_empty, (uint32_t)(jl - 1) & 1)) {
-                    ok = false;
-                    break;
-                }
-                xg_tc_fence_after();
-                for (int kb = 0; kb < KT; ++kb, ++it) {
-                    const int s = (int)(it % XG_SL_STAGES);
-                    if (!xg_mbar_wait(&full[s], (uint32_t)(it / XG_SL_STAGES) & 1)) {
+            long long it = 0, cc = 0;
+            for (long long job = blockIdx.x; job < njobs && ok; job += gridDim.x) {
+                int i, bm, bn;
+                if (!xg_sl_job(job, j, ts, i, bm, bn)) continue;
+                for (int k = k0; k < k1 && ok; ++k, ++cc) {
+                    if (cc >= 1 && !xg_mbar_wait(acc_empty, (uint32_t)(cc - 1) & 1)) {
                         ok = false;
                         break;
                     }
                     xg_tc_fence_after();
-                    const uint32_t sa = sbase + s * XG_SL_STAGE_BYTES;
-                    const uint32_t sb = sa + XG_SL_SLICES * XG_SL_BOX_BYTES;
-#pragma unroll
-                    for (int kk = 0; kk < XG_SL_BK / 32; ++kk) {
-                        /* K = 32 int8 = 32 bytes per MMA inside the 64-byte swizzled row */
-#pragma unroll
-                        for (int p = 0; p < 10; ++p) {
-                            int a, b;
-                            xg_sl_pair(p, a, b);
-                            const uint64_t ad = xg_umma_desc_sw64(sa + a * XG_SL_BOX_BYTES + kk * 32);
-                            const uint64_t bd = xg_umma_desc_sw64(sb + b * XG_SL_BOX_BYTES + kk * 32);
-                            const bool starts = (p == 0 || p == 1 || p == 3 || p == 6);
-                            xg_umma_i8(tmem + (uint32_t)((a + b) * XG_SL_BN), ad, bd, idesc,
-                                       (kb | kk) != 0 || !starts);
+                    const uint32_t dt = tmem;
+                    for (int kb = 0; kb < KT; ++kb, ++it) {
+                        const int s = (int)(it % XG_SL_STAGES);
+                        if (!xg_mbar_wait(&full[s], (uint32_t)(it / XG_SL_STAGES) & 1)) {
+                            ok = false;
+                            break;
                         }
+                        xg_tc_fence_after();
+                        const uint32_t sa = sbase + s * XG_SL_STAGE_BYTES;
+                        const uint32_t sb = sa + XG_SL_SLICES * XG_SL_ABOX_BYTES;
+#pragma unroll
+                        for (int kk = 0; kk < XG_SL_BK / 32; ++kk) {
+                            /* K = 32 int8 = 32 bytes per MMA inside the 64-byte swizzled row */
+#pragma unroll
+                            for (int p = 0; p < 10; ++p) {
+                                int a, b;
+                                xg_sl_pair(p, a, b);
+                                const uint64_t ad = xg_umma_desc_sw64(sa + a * XG_SL_ABOX_BYTES + kk * 32);
+                                const uint64_t bd = xg_umma_desc_sw64(sb + b * XG_SL_BBOX_BYTES + kk * 32);
+                                const bool starts = (p == 0 || p == 1 || p == 3 || p == 6);
+                                /* the transposed block E_b D_a^T: TMEM lane = column of
+                                 * C, TMEM column = row of C */
+                                xg_umma_i8(dt + (uint32_t)((a + b) * XG_SL_BM), bd, ad, idesc,
+                                           (kb | kk) != 0 || !starts);
+                            }
+                        }
+                        xg_umma_commit(&empty[s]);
                     }
-                    xg_umma_commit(&empty[s]);
+                    if (!ok) break;
+                    xg_umma_commit(acc_full);
                 }
-                if (!ok) break;
-                xg_umma_commit(acc_full);
             }
             if (!ok) atomicOr(status, XG_ST_TIMEOUT);
             xg_umma_commit(drain);
             xg_mbar_wait(drain, 0);
         }
+    }
     } else {
-        /* ---- epilogue: warps 2-9; TMEM lanes 32 (warp % 4) .. + 31, column half (warp - 2) / 4 ---- */
-        const int q = warp & 3, h = (warp - 2) >> 2;
-        const double inv = 1.0 / XG_SL_RADIX;
-        int jl = 0;
-        for (long long job = blockIdx.x; job < njobs; job += gridDim.x, ++jl) {
-            if (!xg_mbar_wait(acc_full, (uint32_t)jl & 1)) {
-                if (lane == 0) atomicOr(status, XG_ST_TIMEOUT);
-                break;
+        asm volatile("setmaxnreg.inc.sync.aligned.u32 %0;" ::"n"(XG_SL_REG_HIGH));
+        /* ---- epilogue: warps 4-11.  Thread (quarter q = warp % 4, lane l) owns
+         * C column 32 q + l of the job's block (TMEM lane 32 q + l) and the 64
+         * rows h * 64 .. + 63, h = (warp - 4) / 4 (TMEM columns of each level).
+         * Per chunk k it adds s_A(row) s_B(col) sum_t 254^-t level_t to 64 FP64
+         * sums; after the last chunk C -= sums. ---- */
+        const int q = warp & 3, h = (warp - 4) >> 2;
+        long long cc = 0;
+        for (long long job = blockIdx.x; job < njobs && ok; job += gridDim.x) {
+            int i, bm, bn;
+            if (!xg_sl_job(job, j, ts, i, bm, bn)) continue;
+            const int col = bn * XG_SL_BN + q * 32 + lane;   /* C column (row of the B operand) */
+            const int row0 = bm * XG_SL_BM + h * 64;         /* first C row (row of the A operand) */
+            double *Cc = T.data + xg_tile_index(i, j, nt) * (long long)ts * ts + (long long)row0 * ts + col;
+            {
+                /* the C block is read once, after all chunks: lane l brings rows
+                 * row0 + 2 l, + 1, this quarter's 32 columns (two 128-byte lines
+                 * each), into L2 */
+                const double *pf = Cc + (long long)(2 * lane) * ts - lane;
+                asm volatile("prefetch.global.L2 [%0];" ::"l"(pf));
+                asm volatile("prefetch.global.L2 [%0];" ::"l"(pf + 16));
+                asm volatile("prefetch.global.L2 [%0];" ::"l"(pf + ts));
+                asm volatile("prefetch.global.L2 [%0];" ::"l"(pf + ts + 16));
             }
-            xg_tc_fence_after();
             double res[64];
 #pragma unroll
-            for (int c = 0; c < 4; ++c) {
+            for (int u = 0; u < 64; ++u) res[u] = 0.0;
+            for (int k = k0; k < k1; ++k, ++cc) {
+                if (!xg_mbar_wait(acc_full, (uint32_t)cc & 1)) {
+                    if (lane == 0) atomicOr(status, XG_ST_TIMEOUT);
+                    ok = false;
+                    break;
+                }
+                xg_tc_fence_after();
+                /* s_B (this thread's column) with 254^-3 folded in: the levels are
+                 * combined as the exact integer v = L0 254^3 + L1 254^2 + L2 254 + L3
+                 * (|v| < 2^48) and converted once */
+                const double sc = scale[xg_tile_index(j, k, nt) * ts + col] * XG_SL_INV_RADIX3;
+                const double2 *sr2 =
+                    reinterpret_cast<const double2 *>(scale + xg_tile_index(i, k, nt) * ts + row0);
+                const uint32_t base = tmem + ((uint32_t)(q * 32) << 16) + (uint32_t)(h * 64);
+                /* 8 batches per chunk: (columns c * 16 .. + 15, levels 0-1 or 2-3),
+                 * software-pipelined -- the next batch's TMEM loads are issued
+                 * before the current one is processed, so every wait::ld covers
+                 * a load issued one batch earlier */
+                uint32_t A0[16], A1[16], B0[16], B1[16];
+                int hi[16];
+                xg_tmem_ld_32x32b_x16(base + 0u, A0);
+                xg_tmem_ld_32x32b_x16(base + (uint32_t)XG_SL_BM, A1);
+                xg_tmem_ld_wait();
 #pragma unroll
-                for (int t = XG_SL_LEVELS - 1; t >= 0; --t) {
-                    uint32_t r[16];
-                    xg_tmem_ld_32x32b_x16(tmem + ((uint32_t)(q * 32) << 16) +
-                                              (uint32_t)(t * XG_SL_BN + h * 64 + c * 16),
-                                          r);
-                    xg_tmem_ld_wait();
-#pragma unroll
-                    for (int u = 0; u < 16; ++u) {
-                        const double lv = (double)(int)r[u];
-                        res[c * 16 + u] = (t == XG_SL_LEVELS - 1) ? lv : fma(res[c * 16 + u], inv, lv);
+                for (int b = 0; b < 8; ++b) {
+                    const int c = b >> 1, half = b & 1;
+                    uint32_t(&C0)[16] = (b & 1) ? B0 : A0; /* current batch */
+                    uint32_t(&C1)[16] = (b & 1) ? B1 : A1;
+                    uint32_t(&N0)[16] = (b & 1) ? A0 : B0; /* next batch */
+                    uint32_t(&N1)[16] = (b & 1) ? A1 : B1;
+                    if (b < 7) {
+                        const int nc = (b + 1) >> 1, nl = 2 * ((b + 1) & 1);
+                        xg_tmem_ld_32x32b_x16(base + (uint32_t)(nl * XG_SL_BM + nc * 16), N0);
+                        xg_tmem_ld_32x32b_x16(base + (uint32_t)((nl + 1) * XG_SL_BM + nc * 16), N1);
                     }
+                    if (half == 0) {
+                        /* |L0| <= 127^2 ts, |L1| <= 2 127^2 ts: L0 254 + L1 fits int32 for ts <= 512 */
+#pragma unroll
+                        for (int w = 0; w < 16; ++w) hi[w] = (int)C0[w] * 254 + (int)C1[w];
+                    } else {
+#pragma unroll
+                        for (int u = 0; u < 16; u += 2) {
+                            const double2 s2 = sr2[(c * 16 + u) >> 1]; /* same address in every lane: a broadcast */
+#pragma unroll
+                            for (int e = 0; e < 2; ++e) {
+                                const int w = u + e;
+                                /* v = (L0 254 + L1) 254^2 + L2 254 + L3, exact in int64 (< 2^48) */
+                                const long long v =
+                                    (long long)hi[w] * 64516 + ((long long)(int)C0[w] * 254 + (int)C1[w]);
+                                const double sr = e ? s2.y : s2.x;
+                                res[c * 16 + w] = fma(sr * sc, xg_i64_to_f64(v), res[c * 16 + w]);
+                            }
+                        }
+                    }
+                    if (b < 7) xg_tmem_ld_wait();
                 }
+                /* the accumulators are free for the next chunk */
+                xg_tc_fence_before();
+                __syncwarp();
+                if (lane == 0) xg_mbar_arrive(acc_empty);
             }
-            /* the accumulators are free for the next job's MMAs */
-            xg_tc_fence_before();
-            __syncwarp();
-            if (lane == 0) xg_mbar_arrive(acc_empty);
-            const XgSlJob J = xg_sl_decode(job, ts, band, k, part);
-            const int rl = J.bm * XG_SL_BM + q * 32 + lane;
-            const double sr = scale[(long long)J.i * ts + rl];
-            const double2 *sc = reinterpret_cast<const double2 *>(scale + (long long)J.j * ts + J.bn * XG_SL_BN + h * 64);
-            double2 *C = reinterpret_cast<double2 *>(T.data + xg_tile_index(J.i, J.j, T.nt) * (long long)ts * ts +
-                                                     (long long)rl * ts + J.bn * XG_SL_BN + h * 64);
-            /* in groups of 8 column pairs: bounds how far the compiler hoists
-             * the loads (registers hold the 64 results already) */
+            if (!ok) break;
+            /* C -= U: each warp instruction touches 32 consecutive doubles of a
+             * row; 16 rows are loaded before any is stored, so 16 loads per
+             * thread are in flight (a load after a store through the same
+             * pointer would wait for it); L2-only accesses (.cg): the few KB
+             * of L1 left beside the shared-memory stages would only thrash */
 #pragma unroll
-            for (int u0 = 0; u0 < 32; u0 += 8) {
+            for (int u0 = 0; u0 < 64; u0 += 16) {
+                double cv[16];
 #pragma unroll
-                for (int u = u0; u < u0 + 8; ++u) {
-                    const double2 s2 = sc[u];
-                    double2 cv = C[u];
-                    cv.x = fma(-sr * s2.x, res[2 * u], cv.x);
-                    cv.y = fma(-sr * s2.y, res[2 * u + 1], cv.y);
-                    C[u] = cv;
-                }
-                asm volatile("" ::: "memory");
+                for (int u = 0; u < 16; ++u) cv[u] = __ldcg(Cc + (long long)u * ts);
+#pragma unroll
+                for (int u = 0; u < 16; ++u) __stcg(Cc + (long long)u * ts, cv[u] - res[u0 + u]);
+                Cc += 16LL * ts;
             }
         }
     }
@@ -330,7 +416,7 @@ __global__ void __launch_bounds__(XG_SL_THREADS, 1)
 
 cudaError_t xg_sliced_kernels_configure()
 {
-    return cudaFuncSetAttribute(xg_sliced_gemm_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, XG_SL_SMEM);
+    return cudaFuncSetAttribute(xg_sliced_left_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, XG_SL_SMEM);
 }
 
 void xg_launch_slice_panel(const XgTileArgs &T, int k, int8_t *dig, double *scale, long long plane, const int *status,
@@ -341,16 +427,14 @@ void xg_launch_slice_panel(const XgTileArgs &T, int k, int8_t *dig, double *scal
     xg_slice_panel_kernel<<<(unsigned)((rows + 7) / 8), 256, 0, st>>>(T, k, dig, scale, plane, status);
 }
 
-void xg_launch_sliced_gemm(const CUtensorMap &map, const double *scale, const XgTileArgs &T, int band, int k,
-                           int part, int plane_rows, int sm_count, int *status, cudaStream_t st)
+void xg_launch_sliced_left(const CUtensorMap &map_a, const CUtensorMap &map_b, const double *scale,
+                           const XgTileArgs &T, int j, int k0, int k1, int plane_rows, int max_ctas, int *status,
+                           cudaStream_t st)
 {
-    const int j0 = (part == 2) ? k + 2 : k + 1;
-    const long long rows = (long long)T.nt - j0 - band; /* tiles in the first target column */
-    if (rows <= 0) return;
-    const long long pairs = (part == 1) ? rows : rows * (rows + 1) / 2;
-    const long long bpt = T.ts / XG_SL_BM;
-    const long long njobs = pairs * bpt * bpt;
-    const unsigned grid = (unsigned)(njobs < sm_count ? njobs : sm_count);
-    xg_sliced_gemm_kernel<<<grid, XG_SL_THREADS, XG_SL_SMEM, st>>>(map, scale, T, band, k, part, njobs, plane_rows,
-                                                                   status);
+    if (k1 <= k0 || j >= T.nt) return;
+    const long long per_tile = (long long)(T.ts / XG_SL_BM) * (T.ts / XG_SL_BN);
+    const long long njobs = (long long)(T.nt - j) * per_tile;
+    const unsigned grid = (unsigned)(njobs < max_ctas ? njobs : max_ctas);
+    xg_sliced_left_kernel<<<grid, XG_SL_THREADS, XG_SL_SMEM, st>>>(map_a, map_b, scale, T, j, k0, k1, njobs,
+                                                                   plane_rows, status);
 }

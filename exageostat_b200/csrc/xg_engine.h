@@ -50,15 +50,15 @@ struct XgMixed {
     XgMixedMaps maps[2];
 };
 
-/* FP64 tiles with INT8-sliced off-band updates (sliced.cu): the FP64 tile
- * store of the field plus double-buffered digit planes and row scales of the
- * current panel. */
+/* FP64 tiles with INT8-sliced trailing updates (sliced.cu), left-looking:
+ * the digit planes and row scales of every factored panel tile
+ * (tile-packed, 4 bytes + 8 / ts bytes per element) and the lookahead events. */
 struct XgSliced {
-    int band = 1;
-    long long plane_rows = 0;        /* rows per digit plane (nt * ts) */
-    int8_t *dig[2] = {nullptr, nullptr};
-    double *scale[2] = {nullptr, nullptr};
-    CUtensorMap map[2];
+    long long plane_rows = 0; /* rows per digit plane (ntiles * ts) */
+    int8_t *dig = nullptr;
+    double *scale = nullptr;
+    CUtensorMap map_a, map_b; /* A and B operand views (boxes of 128 rows x 64 bytes) */
+    cudaEvent_t ev_a = nullptr, ev_p[2] = {nullptr, nullptr};
 };
 
 /* One dataset: locations, observations and the covariance / factor. */
@@ -133,11 +133,11 @@ int xg_mixed_factor_dense(int n, const double *x, const double *y, const double 
 double xg_digamma(double x);
 void xg_field_collect_profile_mixed(XgField *f);
 int xg_field_get_z(XgField *f, double *z, int n);
-int xg_field_set_sliced(XgField *f, int band);
+int xg_field_set_sliced(XgField *f);
 int xg_field_loglik_sliced(XgField *f, const double *theta, double *res, double *times);
 void xg_sliced_destroy(XgSliced *s);
 int xg_sliced_factor_dense(int n, const double *x, const double *y, const double *theta, int kernel, int metric,
-                           int ts, int band, double *out);
+                           int ts, double *out);
 
 int xg_predict_create(XgPredict **out, int nmiss, int nobs, int ts);
 void xg_predict_destroy(XgPredict *q);

@@ -136,12 +136,13 @@ void xg_launch_band_gemm(const CUtensorMap &p64map, const XgTileArgs &T, int k, 
                          cudaStream_t st);
 void xg_launch_offband_gemm(const XgMixedMaps &maps, const XgTileArgs &T, int k, int part, int passes, int sm_count,
                             int *status, cudaStream_t st);
-/* sliced.cu: FP64 tiles, off-band updates on INT8 tensor cores (four digit slices) */
+/* sliced.cu: FP64 tiles, trailing updates on INT8 tensor cores (four digit slices), left-looking */
 cudaError_t xg_sliced_kernels_configure();
 void xg_launch_slice_panel(const XgTileArgs &T, int k, int8_t *dig, double *scale, long long plane, const int *status,
                            cudaStream_t st);
-void xg_launch_sliced_gemm(const CUtensorMap &map, const double *scale, const XgTileArgs &T, int band, int k,
-                           int part, int plane_rows, int sm_count, int *status, cudaStream_t st);
+void xg_launch_sliced_left(const CUtensorMap &map_a, const CUtensorMap &map_b, const double *scale,
+                           const XgTileArgs &T, int j, int k0, int k1, int plane_rows, int max_ctas, int *status,
+                           cudaStream_t st);
 
 void xg_launch_finalize(const double *part_logdet, const double *part_dot, int nt, int N, double *out,
                         const int *status, const int *info, cudaStream_t st);

@@ -382,18 +382,20 @@ int exageostat_b200_set_mixed(MLE_data *data, int band, int passes);
 int exageostat_b200_dmle_host_mixed(int n, const double *x, const double *y, const double *z, const double *theta,
                                     int kernel, int metric, int ts, int band, int passes, double *out);
 
-/* No counterpart in the reference (precision = 3).  Every tile stays FP64;
- * the trailing updates of tiles within `band` tiles of the diagonal run on
- * the FP64 tensor cores, the others on the INT8 tensor cores as exact integer
- * products of four 8-bit slices per operand with a per-row FP64 scale (~32
- * significant bits relative to the row maximum, exact S32 accumulation).
- * Sets data->precision = 3 and data->diag_thick = band; grad must be NULL. */
-int exageostat_b200_set_sliced(MLE_data *data, int band);
+/* No counterpart in the reference (precision = 3).  Every tile stays FP64 and
+ * the diagonal POTRF, the panel TRSM, the log-det and the solve run in FP64;
+ * the trailing updates A_ij -= L_ik L_jk^T run on the INT8 tensor cores as
+ * exact integer products of four 8-bit slices per operand with an FP64 scale
+ * per row and panel (~32 significant bits relative to the row maximum, exact
+ * S32 accumulation), in left-looking order.  Sets data->precision = 3; grad
+ * must be NULL.  Needs 4 bytes of device memory per covariance element on
+ * top of the FP64 tiles (20 GB at N = 100,000). */
+int exageostat_b200_set_sliced(MLE_data *data);
 
 /* One-shot INT8-sliced log-likelihood on host arrays (as
  * exageostat_b200_dmle_host; ts 0 = automatic, else a multiple of 128). */
 int exageostat_b200_dmle_host_sliced(int n, const double *x, const double *y, const double *z, const double *theta,
-                                     int kernel, int metric, int ts, int band, double *out);
+                                     int kernel, int metric, int ts, double *out);
 
 /* Replaces the locations and/or observations (N host doubles each; NULL
  * keeps the current array) of an allocated MLE_data, e.g. for a new dataset
@@ -406,9 +408,10 @@ int exageostat_b200_set_data(MLE_data *data, const double *x, const double *y, c
  * update (the panel overlaps the trailing update, so these may add up to
  * more than the total); trailing-update algorithmic flops; kernel launches;
  * evaluations; total seconds (generation to result); tile size; tiles per
- * side; N; and for the banded paths (precision 2 and 3) out[11..14] = seconds
- * and algorithmic flops of the off-band (TF32 or INT8 tensor-core) and band
- * (FP64) trailing updates. */
+ * side; N; and for the reduced-precision paths out[11..14] = seconds and
+ * algorithmic flops of the off-band (TF32 tensor-core, precision 2; INT8
+ * tensor-core, precision 3: every target) and band (FP64, precision 2)
+ * trailing updates. */
 int exageostat_b200_set_profiling(MLE_data *data, int on);
 int exageostat_b200_get_profile(MLE_data *data, double *out, int n);
 
@@ -455,7 +458,7 @@ int exageostat_b200_covariance_dense(int n, const double *x, const double *y, co
 /* The factor L of the INT8-sliced path (all tiles FP64), row-major n x n
  * with zeros above the diagonal, for the parity tests. */
 int exageostat_b200_sliced_factor_dense(int n, const double *x, const double *y, const double *theta, int kernel,
-                                        int metric, int ts, int band, double *out);
+                                        int metric, int ts, double *out);
 
 /* The mixed-precision factor L (band tiles FP64, off-band FP32 widened),
  * row-major n x n with zeros above the diagonal. */
