@@ -5,10 +5,12 @@ One step = one evaluation of the hot path (generate Sigma(theta) -> tiled
 Cholesky with fused log-det and solve -> log-likelihood) for the N = 100,000
 univariate Matern field (317 x 317 jittered unit-square grid truncated to
 1e5 points, theta = (1.0, 0.05, 0.5), z = L e from the reference's
-generator).  Two legs are timed: plain FP64 and banded mixed precision (the
-headline value; its |dl|/|l| against the FP64 leg is in the line).  The
-covariance (20-40 GB of tiles) is far larger than L2, so no explicit L2 flush
-is needed between steps.
+generator).  Three legs are timed: plain FP64; the reduced-precision path
+that gives the headline value (default: FP64 tiles with INT8-sliced trailing
+updates on the tensor cores; its |dl|/|l| against the FP64 leg is in the
+line); and, as a reported sub-result, the reference's banded mixed-precision
+scheme (FP32 off-band tiles, TF32 tensor cores).  The covariance (20-40 GB of
+tiles) is far larger than L2, so no explicit L2 flush is needed between steps.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--n N] [--impl ours|reference]
 
@@ -29,8 +31,8 @@ import time
 ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
-METRIC = ("exact Matern log-likelihood evaluations per second, N=100000, 1 B200: banded mixed precision "
-          "(FP64 band, FP32 off-band on TF32 tensor cores) vs plain FP64")
+METRIC = ("exact Matern log-likelihood evaluations per second, N=100000, 1 B200: reduced-precision tensor-core "
+          "path (FP64 tiles, INT8-sliced trailing updates) vs plain FP64")
 UNIT = "loglik-evals/s"
 THETA = [1.0, 0.05, 0.5]
 
@@ -46,16 +48,22 @@ def parse():
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--cpu-seconds", type=float, default=12.0, help="target CPU time of the oracle sample")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-mixed-leg", action="store_true", help="skip the TF32 banded mixed-precision sub-result")
     ap.add_argument("--band", type=int, default=2, help="FP64 band width in tiles (mixed leg)")
-    ap.add_argument("--mode", choices=["evals", "bands", "mle", "batch"], default="evals",
+    ap.add_argument("--mode", choices=["evals", "bands", "mle", "batch", "grad"], default="evals",
                     help="evals: the default bench line; bands: accuracy/time per band width; "
-                         "mle: time-to-MLE of the drivers; batch: batched regional fields")
+                         "mle: time-to-MLE of the drivers; batch: batched regional fields; grad: gradient cost")
     ap.add_argument("--bands", default="1,2,4,8,16")
     ap.add_argument("--no-sliced-row", dest="sliced_row", action="store_false",
                     help="bands mode: skip the INT8-sliced row")
     ap.add_argument("--fields", type=int, default=512)
+    ap.add_argument("--theta0", default="1.0,0.1,0.5", help="mle mode: parameters of the synthetic field")
+    ap.add_argument("--drivers", default="bobyqa_fp64,bobyqa_sliced,lbfgsb_grad_fp64,lbfgsb_grad_sliced,"
+                    "lbfgsb_sliced_polish",
+                    help="mle mode: comma list of bobyqa_fp64, bobyqa_sliced, bobyqa_mixed, lbfgsb_grad_fp64, "
+                         "lbfgsb_grad_sliced, lbfgsb_sliced_polish")
     ap.add_argument("--passes", type=int, default=3, help="TF32 passes of the off-band update (1 or 3)")
-    ap.add_argument("--scheme", choices=["mixed", "sliced"], default="mixed",
+    ap.add_argument("--scheme", choices=["mixed", "sliced"], default="sliced",
                     help="reduced-precision leg: mixed = FP32 off-band tiles on TF32 tensor cores; "
                          "sliced = FP64 tiles with INT8-sliced off-band updates")
     return ap.parse_args()
@@ -268,10 +276,13 @@ def mode_bands(args):
 
 
 def mode_mle(args):
-    """Time-to-MLE: derivative-free maximiser (plain FP64 and mixed) and
-    L-BFGS-B with the adjoint gradient (FP64), bounds [0.01, 5]^3, start at
-    the lower bounds (the reference driver's start) for the derivative-free
-    runs and at the box centre for L-BFGS-B."""
+    """Time-to-MLE of the reference driver's maximiser (derivative-free, start
+    at the lower bounds, examples/examples.c:263-264, tolerance 1e-9) on the
+    plain FP64 objective and on the reduced-precision objectives, and of
+    L-BFGS-B with the adjoint gradient (FP64, or sliced with an optional FP64
+    polish from its optimum; start at the box centre); bounds [0.01, 5]^3.
+    theta-hat and loglik(theta-hat) are compared with the FP64 derivative-free
+    run."""
     os.environ.setdefault("EXAGEOSTAT_B200_SILENT", "1")
     import numpy as np
 
@@ -280,32 +291,93 @@ def mode_mle(args):
     from exageostat_b200.synthetic import dlarnv
 
     xg.init(args.ts)
-    theta0 = [1.0, 0.1, 0.5]
+    theta0 = [float(v) for v in args.theta0.split(",")]
     x, y = xg.generate_xy_loc(args.n, args.seed)
     sess = xg.Session(x, y, dts=args.ts)
     sess.zvg(theta0, dlarnv(args.seed, args.n))
     lb, ub = [0.01] * 3, [5.0] * 3
     runs = {}
-    t0 = time.perf_counter()
-    th, ll, ev = sess.fit_bobyqa(lb, ub, ftol_abs=1e-9)
-    runs["bobyqa_fp64"] = {"seconds": time.perf_counter() - t0, "evals": ev, "theta": th.tolist(), "loglik": ll}
-    sess.set_mixed(band=args.band, passes=args.passes)
-    t0 = time.perf_counter()
-    th, ll, ev = sess.fit_bobyqa(lb, ub, ftol_abs=1e-9)
-    runs["bobyqa_mixed"] = {"seconds": time.perf_counter() - t0, "evals": ev, "theta": th.tolist(), "loglik": ll,
-                            "band": args.band}
-    sess.set_fp64()
-    t0 = time.perf_counter()
-    th, ll, ev = fit_lbfgsb(sess, lb, ub, x0=[0.5, 0.5, 0.5])
-    runs["lbfgsb_grad_fp64"] = {"seconds": time.perf_counter() - t0, "evals": ev, "theta": th.tolist(),
-                                "loglik": ll}
-    ref = np.array(runs["bobyqa_fp64"]["theta"])
-    for r in runs.values():
-        r["theta_rel_diff_vs_fp64"] = float(np.max(np.abs(np.array(r["theta"]) - ref) / np.abs(ref)))
-        r["loglik_rel_diff_vs_fp64"] = abs(r["loglik"] - runs["bobyqa_fp64"]["loglik"]) / abs(
-            runs["bobyqa_fp64"]["loglik"])
+
+    def bobyqa(name, **extra):
+        t0 = time.perf_counter()
+        th, ll, ev = sess.fit_bobyqa(lb, ub, ftol_abs=1e-9)
+        runs[name] = dict({"seconds": time.perf_counter() - t0, "evals": ev, "theta": th.tolist(), "loglik": ll},
+                          **extra)
+
+    drivers = args.drivers.split(",")
+    if "bobyqa_fp64" in drivers:
+        bobyqa("bobyqa_fp64")
+    if "bobyqa_sliced" in drivers:
+        sess.set_sliced()
+        bobyqa("bobyqa_sliced")
+        sess.set_fp64()
+    if "bobyqa_mixed" in drivers:
+        sess.set_mixed(band=args.band, passes=args.passes)
+        bobyqa("bobyqa_mixed", band=args.band)
+        sess.set_fp64()
+    if "lbfgsb_grad_sliced" in drivers or "lbfgsb_sliced_polish" in drivers:
+        sess.set_sliced()
+        t0 = time.perf_counter()
+        th, ll, ev = fit_lbfgsb(sess, lb, ub, x0=[0.5, 0.5, 0.5])
+        t_sl = time.perf_counter() - t0
+        sess.set_fp64()
+        if "lbfgsb_grad_sliced" in drivers:
+            runs["lbfgsb_grad_sliced"] = {"seconds": t_sl, "evals": ev, "theta": th.tolist(), "loglik": ll}
+        if "lbfgsb_sliced_polish" in drivers:
+            # the sliced optimum refined by FP64 gradient steps
+            t0 = time.perf_counter()
+            th2, ll2, ev2 = fit_lbfgsb(sess, lb, ub, x0=th)
+            runs["lbfgsb_sliced_polish"] = {"seconds": t_sl + time.perf_counter() - t0, "evals": ev,
+                                            "evals_fp64": ev2, "theta": th2.tolist(), "loglik": ll2}
+    if "lbfgsb_grad_fp64" in drivers:
+        t0 = time.perf_counter()
+        th, ll, ev = fit_lbfgsb(sess, lb, ub, x0=[0.5, 0.5, 0.5])
+        runs["lbfgsb_grad_fp64"] = {"seconds": time.perf_counter() - t0, "evals": ev, "theta": th.tolist(),
+                                    "loglik": ll}
+    if "bobyqa_fp64" in runs:
+        ref = np.array(runs["bobyqa_fp64"]["theta"])
+        llref = runs["bobyqa_fp64"]["loglik"]
+        for name, r in runs.items():
+            r["theta_rel_diff_vs_fp64"] = float(np.max(np.abs(np.array(r["theta"]) - ref) / np.abs(ref)))
+            r["speedup_vs_bobyqa_fp64"] = runs["bobyqa_fp64"]["seconds"] / r["seconds"]
+            # the objective of every run evaluated in FP64 at its own optimum
+            r["loglik_fp64_at_theta"] = sess.loglik(r["theta"])
+            r["loglik_rel_diff_vs_fp64"] = abs(r["loglik_fp64_at_theta"] - llref) / abs(llref)
     sess.close()
     print(json.dumps({"mode": "mle", "n": args.n, "theta0": theta0, "runs": runs}), flush=True)
+
+
+def mode_grad(args):
+    """Seconds per log-likelihood + gradient evaluation, plain FP64 and
+    sliced, and the difference of the two gradients."""
+    os.environ.setdefault("EXAGEOSTAT_B200_SILENT", "1")
+    import numpy as np
+
+    import exageostat_b200 as xg
+    from exageostat_b200.synthetic import dlarnv
+
+    xg.init(args.ts)
+    x, y = xg.generate_xy_loc(args.n, args.seed)
+    sess = xg.Session(x, y, dts=args.ts)
+    sess.zvg(THETA, dlarnv(args.seed, args.n))
+    out = {"mode": "grad", "workload": workload(args.n), "tile": args.ts}
+    for name in (["fp64"] if args.n > 120000 else []) + ["fp64", "sliced"]:
+        if name == "sliced":
+            sess.set_sliced()
+        sess.loglik(THETA, grad=True)
+        t0 = time.perf_counter()
+        ll, g = sess.loglik(THETA, grad=True)
+        dt = time.perf_counter() - t0
+        t0 = time.perf_counter()
+        sess.loglik(THETA)
+        dl = time.perf_counter() - t0
+        out[name] = {"seconds_loglik_grad": dt, "seconds_loglik": dl, "ratio": dt / dl, "loglik": ll,
+                     "grad": list(np.asarray(g, dtype=float))}
+    g64, gsl = np.array(out["fp64"]["grad"]), np.array(out["sliced"]["grad"])
+    out["grad_max_rel_diff"] = float(np.max(np.abs(gsl - g64)) / max(np.max(np.abs(g64)), 1.0))
+    out["speedup_grad"] = out["fp64"]["seconds_loglik_grad"] / out["sliced"]["seconds_loglik_grad"]
+    sess.close()
+    print(json.dumps(out), flush=True)
 
 
 def mode_batch(args):
@@ -350,7 +422,7 @@ def main():
         run_reference(args)
         return
     if args.mode != "evals":
-        {"bands": mode_bands, "mle": mode_mle, "batch": mode_batch}[args.mode](args)
+        {"bands": mode_bands, "mle": mode_mle, "batch": mode_batch, "grad": mode_grad}[args.mode](args)
         return
     import numpy as np
     import torch
@@ -425,7 +497,7 @@ def main():
     value = world * args.steps / tmx
     rel_err = abs(llsmx[-1] - lls64[-1]) / abs(lls64[-1])
 
-    # ---- end to end: C ABI from pinned host buffers (mixed path) ----
+    # ---- end to end: C ABI from pinned host buffers (reduced-precision path) ----
     px = torch.from_numpy(x).pin_memory()
     py = torch.from_numpy(y).pin_memory()
     pz = torch.from_numpy(z).pin_memory()
@@ -443,26 +515,47 @@ def main():
     passes = args.passes
     t_off = pmx["t_offband"]
     if sliced:
-        # ten 8-bit digit-pair products per FP64 product; dense INT8 runs at twice the BF16 rate
-        mult, peak, kname, unit = 10, 2.0 * bf16_peak, "xg_sliced_gemm_kernel (tcgen05 kind::i8, 10 digit " \
-            "pairs, S32 TMEM levels)", "TOP/s"
+        # ten 8-bit digit-pair products per FP64 product; dense INT8 runs at twice the BF16 rate.
+        # t_offband / offband_flops: the split column updates on the main stream (nt - 2 launches per
+        # evaluation, nearly all the work); t_band / band_flops: the last-chunk updates on the panel stream
+        mult, peak, kname, unit = 10, 2.0 * bf16_peak, "xg_sliced_left_kernel (tcgen05 kind::i8, 10 digit " \
+            "pairs, S32 TMEM levels, FP64 epilogue)", "TOP/s"
         psrc = "dense INT8 = 2 x bf16, bf16 from %s (of measured)" % bf16_src
+        launches = max(pmx["nt"] - 2, 1)
     else:
         mult, peak, kname, unit = passes, tf32_peak, "xg_offband_gemm_kernel (tcgen05 kind::tf32, %d pass%s, " \
             "TMEM)" % (passes, "es" if passes > 1 else ""), "TFLOP/s"
         psrc = "dense TF32 = bf16 / 2, bf16 from %s (of measured)" % bf16_src
+        launches = max(2 * (pmx["nt"] - 1), 1)
     mma_flops = pmx["offband_flops"] * mult
     ach_mx = mma_flops / t_off / 1e12 if t_off > 0 else 0.0
     roofline = {"bound": "tensor", "kernel": kname,
                 "achieved": ach_mx, "peak": peak, "unit": unit, "frac": ach_mx / peak,
                 "peak_source": psrc,
                 "traffic": None,
-                "algorithmic_ops_per_launch": pmx["offband_flops"] * mult / max(pmx["evals"], 1) /
-                max(2 * (pmx["nt"] - 1), 1),
-                "useful_tflops": pmx["offband_flops"] / t_off / 1e12 if t_off > 0 else 0.0,
+                "algorithmic_ops_per_launch": pmx["offband_flops"] * mult / max(pmx["evals"], 1) / launches,
+                "useful_fp64_equivalent_tflops": pmx["offband_flops"] / t_off / 1e12 if t_off > 0 else 0.0,
                 "share_of_step": t_off / pmx["t_total"],
                 "phases_s_per_eval": {k: pmx[k] / pmx["evals"] for k in
                                       ("t_gen", "t_potrf", "t_trsm", "t_gemm", "t_offband", "t_band")}}
+    # the reference's banded mixed-precision scheme (FP32 off-band tiles on TF32 tensor cores), reported
+    other = None
+    if sliced and not args.no_mixed_leg:
+        sess.set_mixed(band=args.band, passes=args.passes)
+        for _ in range(2):
+            sess.loglik(THETA)
+        sess.set_profiling(True)
+        llm = [sess.loglik(THETA) for _ in range(args.steps)]
+        pm = sess.profile()
+        sess.set_profiling(False)
+        tm = max_over_ranks(pm["t_total"])
+        ach = pm["offband_flops"] * args.passes / pm["t_offband"] / 1e12 if pm["t_offband"] > 0 else 0.0
+        other = {"scheme": "FP64 band of %d tiles + FP32 off-band tiles, TF32 x%d tensor cores (psdportf.c)" % (
+                     args.band, args.passes),
+                 "value": world * args.steps / tm, "unit": UNIT, "ms_per_step": 1e3 * tm / args.steps,
+                 "rel_err_vs_fp64": abs(llm[-1] - lls64[-1]) / abs(lls64[-1]),
+                 "offband_tf32_tflops": ach, "offband_frac_of_tf32_peak": ach / tf32_peak}
+        sess.set_sliced()
     tpf = read_traffic_per_flop()
     fp64 = {"value": fp64_value, "unit": UNIT, "ms_per_step": 1e3 * t64 / args.steps, "loglik": lls64[-1],
             "roofline": {"bound": "tensor", "kernel": "xg_syrk_gemm_kernel (FP64 DMMA trailing update)",
@@ -474,7 +567,7 @@ def main():
     line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": 1e3 * tmx / args.steps, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None,
-            "dtype": ("f64 tiles, off-band updates as int8 digit products (4 slices, s32 accumulate)" if sliced
+            "dtype": ("f64 tiles, trailing updates as int8 digit products (4 slices, s32 accumulate)" if sliced
                       else "f64 band + f32 off-band (tf32x%d tensor cores)" % passes), "data": "synthetic",
             "config": {"workload": workload(N), "tile": int(pmx["ts"]), "tiles_per_side": int(pmx["nt"]),
                        "band_tiles": args.band, "scheme": args.scheme,
@@ -483,7 +576,7 @@ def main():
                        "l2": "inputs larger than L2 (20-40 GB of covariance tiles per step)",
                        "loglik_reduced": llsmx[-1], "loglik_fp64": lls64[-1], "rel_err_vs_fp64": rel_err,
                        "loglik_e2e": ll_e2e, "wall_s_timed": wall},
-            "fp64": fp64, "speedup_vs_fp64": value / fp64_value,
+            "fp64": fp64, "speedup_vs_fp64": value / fp64_value, "banded_mixed_tf32": other,
             "roofline": roofline, "e2e": e2e, "clocks": clocks,
             "gpu_launches": int(round(pmx["launches"] / max(pmx["evals"], 1) * args.steps))}
     if rank == 0 and world == 1 and not args.no_cpu_baseline:

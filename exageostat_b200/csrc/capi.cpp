@@ -235,8 +235,8 @@ extern "C" int exageostat_b200_loglik(MLE_data *data, const double *theta, doubl
     const bool mixed = data->precision == 2;
     const bool sliced = data->precision == 3;
     const int band = data->diag_thick > 0 ? data->diag_thick : 1;
-    if ((mixed || sliced) && grad)
-        return xg_fail(XG_ERR_UNSUPPORTED, "the gradient is computed in FP64 only (precision 0)");
+    if (mixed && grad)
+        return xg_fail(XG_ERR_UNSUPPORTED, "the gradient is computed with precision 0 or 3, not 2");
     if (mixed && (!f->mx || f->mx->band != band)) {
         rc = xg_field_set_mixed(f, band, f->mx ? f->mx->passes : 3);
         if (rc) return rc;
@@ -253,10 +253,11 @@ extern "C" int exageostat_b200_loglik(MLE_data *data, const double *theta, doubl
         xg_recover(data->recovery_file, data->iter_count, np, loglik)) {
         rc = XG_OK;
     } else {
-        rc = mixed    ? xg_field_loglik_mixed(f, theta, res, times)
-             : sliced ? xg_field_loglik_sliced(f, theta, res, times)
-             : grad   ? xg_field_loglik_grad(f, theta, res, grad, times)
-                      : xg_field_loglik(f, theta, res, times);
+        rc = mixed             ? xg_field_loglik_mixed(f, theta, res, times)
+             : sliced && grad  ? xg_field_loglik_grad_sliced(f, theta, res, grad, times)
+             : sliced          ? xg_field_loglik_sliced(f, theta, res, times)
+             : grad            ? xg_field_loglik_grad(f, theta, res, grad, times)
+                               : xg_field_loglik(f, theta, res, times);
         if (rc == XG_OK) {
             *loglik = res[0];
             data->det = 0.5 * res[1];

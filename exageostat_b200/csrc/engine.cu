@@ -927,6 +927,8 @@ void xg_sliced_destroy(XgSliced *s)
     if (!s) return;
     if (s->dig) cudaFree(s->dig);
     if (s->scale) cudaFree(s->scale);
+    if (s->xdig) cudaFree(s->xdig);
+    if (s->xscale) cudaFree(s->xscale);
     if (s->ev_a) cudaEventDestroy(s->ev_a);
     for (int b = 0; b < 2; ++b)
         if (s->ev_p[b]) cudaEventDestroy(s->ev_p[b]);
@@ -975,6 +977,18 @@ int xg_field_set_sliced(XgField *f)
  * chunk k = j joins the panel chain of column j+1.  Profiling events (8 per
  * column): panel stream before / after the last-chunk update, after POTRF,
  * after TRSM + slicing; main stream before / after the split update. */
+static XgSlTask factor_task(int col, int k0, int k1)
+{
+    XgSlTask S;
+    S.mode = XG_SL_FACTOR;
+    S.col = col;
+    S.k0 = k0;
+    S.k1 = k1;
+    S.sign = -1.0;
+    S.overwrite = 0;
+    return S;
+}
+
 static void xg_factor_sliced(XgField *f, double *v, const XgFactorStreams &fs)
 {
     XgSliced *sl = f->sl;
@@ -996,16 +1010,17 @@ static void xg_factor_sliced(XgField *f, double *v, const XgFactorStreams &fs)
         if (la) cudaStreamWaitEvent(sp, sl->ev_a, 0); /* chunks k < j-1 of column j */
         rec(j, 0, sp);
         if (la) {
-            if (j >= 1) xg_launch_sliced_left(sl->map_a, sl->map_b, sl->scale, T, j, j - 1, j, pr, XG_PANEL_SMS,
-                                              f->status, sp);
+            if (j >= 1) xg_launch_sliced(sl->map_a, sl->map_b, sl->scale, sl->scale, T, factor_task(j, j - 1, j), pr,
+                                         XG_PANEL_SMS, f->status, sp);
         } else {
-            xg_launch_sliced_left(sl->map_a, sl->map_b, sl->scale, T, j, 0, j, pr, sms, f->status, sp);
+            xg_launch_sliced(sl->map_a, sl->map_b, sl->scale, sl->scale, T, factor_task(j, 0, j), pr, sms, f->status,
+                             sp);
         }
         rec(j, 1, sp);
         xg_launch_potrf_diag(T, j, v, f->part, f->part + nt, rhs, f->status, f->info, sp);
         rec(j, 2, sp);
         xg_launch_trsm_panel(T, j, v, rhs, f->status, sp);
-        if (j + 1 < nt) xg_launch_slice_panel(T, j, sl->dig, sl->scale, plane, f->status, sp);
+        if (j + 1 < nt) xg_launch_slice_panel(T, j, 0, sl->dig, sl->scale, plane, f->status, sp);
         rec(j, 3, sp);
         if (la) {
             cudaEventRecord(sl->ev_p[j & 1], sp);
@@ -1013,8 +1028,8 @@ static void xg_factor_sliced(XgField *f, double *v, const XgFactorStreams &fs)
             if (j >= 1 && j + 1 < nt) cudaStreamWaitEvent(fs.st, sl->ev_p[(j - 1) & 1], 0);
             rec(j, 4, fs.st);
             if (j >= 1 && j + 1 < nt)
-                xg_launch_sliced_left(sl->map_a, sl->map_b, sl->scale, T, j + 1, 0, j, pr, sms - XG_PANEL_SMS,
-                                      f->status, fs.st);
+                xg_launch_sliced(sl->map_a, sl->map_b, sl->scale, sl->scale, T, factor_task(j + 1, 0, j), pr,
+                                 sms - XG_PANEL_SMS, f->status, fs.st);
             rec(j, 5, fs.st);
             cudaEventRecord(sl->ev_a, fs.st);
         } else {
@@ -1030,8 +1045,12 @@ static void xg_factor_sliced(XgField *f, double *v, const XgFactorStreams &fs)
     }
 }
 
-/* Per-kernel-class times of the sliced factorisation from its events. */
-static void xg_field_collect_profile_sliced(XgField *f)
+/* Per-kernel-class times of the sliced factorisation from its events:
+ * prof[8], prof[9] = seconds and algorithmic flops of the split updates on
+ * the main stream (chunks k < j-1 of column j: nearly all the work);
+ * prof[10], prof[11] = the same for the last-chunk updates on the panel
+ * stream (all chunks of a column without the lookahead). */
+static void xg_field_collect_profile_sliced(XgField *f, bool lookahead)
 {
     const int nt = f->C.nt;
     const double t = f->C.ts;
@@ -1040,19 +1059,28 @@ static void xg_field_collect_profile_sliced(XgField *f)
         cudaEventElapsedTime(&ms, f->pev[a], f->pev[b]);
         return ms * 1e-3;
     };
+    /* algorithmic flops of `chunks` panel chunks applied to column j */
+    auto col_flops = [&](int j, int chunks) {
+        return (double)chunks * ((nt - j - 1) * 2.0 * t * t * t + t * t * (t + 1));
+    };
     cudaEventElapsedTime(&ms, f->ev[0], f->ev[1]);
     f->prof[0] += ms * 1e-3;
     for (int j = 0; j < nt; ++j) {
         const int e = 8 * j;
         f->prof[1] += el(e + 1, e + 2);
         f->prof[2] += el(e + 2, e + 3);
-        const double upd = el(e, e + 1) + el(e + 4, e + 5);
-        f->prof[3] += upd;
-        f->prof[8] += upd;
-        /* column j: j chunks on nt - j - 1 off-diagonal tiles (GEMM) and the diagonal tile (SYRK) */
-        const double fl = (double)j * ((nt - j - 1) * 2.0 * t * t * t + t * t * (t + 1));
-        f->prof[4] += fl;
-        f->prof[9] += fl;
+        const double tb = el(e, e + 1), ta = el(e + 4, e + 5);
+        f->prof[3] += ta + tb;
+        f->prof[4] += col_flops(j, j);
+        if (lookahead) {
+            f->prof[10] += tb;
+            f->prof[11] += j >= 1 ? col_flops(j, 1) : 0.0;
+            f->prof[8] += ta;
+            f->prof[9] += (j >= 1 && j + 1 < nt) ? col_flops(j + 1, j) : 0.0;
+        } else {
+            f->prof[8] += tb;
+            f->prof[9] += col_flops(j, j);
+        }
     }
     cudaEventElapsedTime(&ms, f->ev[0], f->ev[2]);
     f->prof[7] += ms * 1e-3;
@@ -1098,7 +1126,7 @@ int xg_field_loglik_sliced(XgField *f, const double *theta, double *res, double 
         times[0] = a * 1e-3;
         times[1] = b * 1e-3;
     }
-    if (f->profiling) xg_field_collect_profile_sliced(f);
+    if (f->profiling) xg_field_collect_profile_sliced(f, fs.st_hi != nullptr);
     rc = xg_read_status(f);
     if (rc) return rc;
     res[0] = f->h_out[0];
@@ -1134,6 +1162,92 @@ int xg_sliced_factor_dense(int n, const double *x, const double *y, const double
     rc = xg_tiles_to_dense(f, n, out);
     xg_field_destroy(f);
     return rc;
+}
+
+/* Gradient with the sliced path: the forward factorisation as
+ * xg_field_loglik_sliced, alpha = L^-T v in FP64, the inverse factor
+ * X = L^-T column by column (INT8-sliced update from the digit planes of L and
+ * of the already finished columns of X, then the FP64 triangular solve with
+ * L_bb^T and the slicing of column b of X), S = X X^T by one sliced launch
+ * written over the factor, and the FP64 contraction with dSigma/dtheta. */
+int xg_field_loglik_grad_sliced(XgField *f, const double *theta, double *res, double *grad, double *times)
+{
+    int rc = XG_OK;
+    if (!f->sl && (rc = xg_field_set_sliced(f))) return rc;
+    XgSliced *sl = f->sl;
+    if (!f->X.d) {
+        rc = xg_tm_alloc(f->X, f->N, f->C.ts);
+        if (rc) return rc;
+        const long long blocks = xg_grad_contract_blocks(f->C.ntiles, f->C.ts);
+        if (cudaMalloc(&f->gpart, 4 * (size_t)blocks * sizeof(double)) != cudaSuccess ||
+            cudaMalloc(&f->gout, 4 * sizeof(double)) != cudaSuccess)
+            return xg_fail(XG_ERR_NO_MEMORY, "gradient workspace");
+    }
+    const int ts = f->C.ts, nt = f->C.nt;
+    const size_t plane = (size_t)sl->plane_rows * ts;
+    if (!sl->xdig) {
+        if (cudaMalloc(&sl->xdig, 4 * plane) != cudaSuccess ||
+            cudaMalloc(&sl->xscale, (size_t)sl->plane_rows * sizeof(double)) != cudaSuccess)
+            return xg_fail(XG_ERR_NO_MEMORY, "digit planes of the inverse factor (%.2f GB)", 4.0 * plane / 1e9);
+        rc = xg_encode(&sl->xmap, CU_TENSOR_MAP_DATA_TYPE_UINT8, 1, sl->xdig, ts, 4 * sl->plane_rows, 64, 128,
+                       CU_TENSOR_MAP_SWIZZLE_64B);
+        if (rc) return rc;
+    }
+    rc = xg_field_loglik_sliced(f, theta, res, times);
+    if (rc) return rc;
+    cudaStream_t st = g_xg.stream;
+    XgTileArgs T{f->C.d, ts, nt};
+    XgTileArgs TX{f->X.d, ts, nt};
+    const int pr = (int)sl->plane_rows;
+    const XgMaternParams p = xg_params(theta, f->kernel);
+    const double dlogcon = -(log(2.0) + xg_digamma(theta[2]));
+    XG_CU(cudaEventRecord(f->ev[0], st));
+    for (int k = nt - 1; k >= 0; --k) xg_launch_trsv_lower_t_step(T, k, f->v, f->status, st);
+    xg_launch_identity_x(f->X.d, nt, ts, st);
+    for (int b = 0; b < nt; ++b) {
+        if (b >= 1) {
+            XgSlTask S;
+            S.mode = XG_SL_INVERSE;
+            S.col = b;
+            S.k0 = 0;
+            S.k1 = b;
+            S.sign = -1.0;
+            S.overwrite = 0;
+            xg_launch_sliced(sl->xmap, sl->map_b, sl->xscale, sl->scale, TX, S, pr, g_xg.sm_count, f->status, st);
+        }
+        xg_launch_xtrsm(f->X.d, f->C.d, nt, ts, b, f->status, st);
+        xg_launch_slice_panel(TX, b, 1, sl->xdig, sl->xscale, (long long)plane, f->status, st);
+    }
+    XgSlTask S;
+    S.mode = XG_SL_SYRK;
+    S.col = 0;
+    S.k0 = 0;
+    S.k1 = nt;
+    S.sign = 1.0;
+    S.overwrite = 1;
+    xg_launch_sliced(sl->xmap, sl->xmap, sl->xscale, sl->xscale, T, S, pr, g_xg.sm_count, f->status, st);
+    xg_launch_grad_contract(f->C.d, f->C.ij, f->C.ntiles, nt, ts, f->x, f->y, f->v, f->N, p, f->kernel, f->metric,
+                            dlogcon, f->gpart, f->gout, st);
+    XG_CU(cudaEventRecord(f->ev[3], st));
+    double g4[4];
+    int sv[2];
+    XG_CU(cudaGetLastError());
+    XG_CU(cudaMemcpyAsync(g4, f->gout, sizeof g4, cudaMemcpyDeviceToHost, st));
+    XG_CU(cudaMemcpyAsync(sv, f->status, sizeof sv, cudaMemcpyDeviceToHost, st));
+    XG_CU(cudaStreamSynchronize(st));
+    if (sv[0]) {
+        f->h_out[3] = sv[0];
+        f->h_out[4] = sv[1];
+        return xg_read_status(f);
+    }
+    if (times) {
+        float ms = 0;
+        cudaEventElapsedTime(&ms, f->ev[0], f->ev[3]);
+        times[2] = ms * 1e-3;
+    }
+    const int np = f->kernel == 1 ? 4 : 3;
+    for (int i = 0; i < np; ++i) grad[i] = g4[i];
+    return XG_OK;
 }
 
 int xg_field_get_z(XgField *f, double *z, int n)

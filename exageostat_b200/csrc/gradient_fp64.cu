@@ -442,6 +442,18 @@ void xg_launch_inverse_factor(const CUtensorMap &mapX, const CUtensorMap &mapL, 
 }
 
 /* S = X X^T (lower tiles) into Sbuf */
+void xg_launch_identity_x(double *X, int nt, int ts, cudaStream_t st)
+{
+    cudaMemsetAsync(X, 0, (size_t)xg_num_lower_tiles(nt) * ts * ts * sizeof(double), st);
+    xg_identity_diag_kernel<<<dim3(1, nt), 256, 0, st>>>(X, nt, ts);
+}
+
+void xg_launch_xtrsm(double *X, const double *L, int nt, int ts, int K, int *status, cudaStream_t st)
+{
+    xg_xtrsm_kernel<<<(K + 1) * (ts / XG_XT_SR), XG_XT_THREADS, xg_xtrsm_smem_bytes(ts), st>>>(X, L, nt, ts, K,
+                                                                                             status);
+}
+
 void xg_launch_inverse_syrk(const CUtensorMap &mapX, double *S, int nt, int ts, int *status, cudaStream_t st)
 {
     const int bpt = ts / XG_TG_BM;

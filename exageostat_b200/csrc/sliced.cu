@@ -36,7 +36,8 @@
  * tile are kept (tile-packed, 4 bytes per element).
  *
  * Kernels:
- *   xg_slice_panel_kernel : panel tiles (i, k), i > k -> four digit planes + row scales
+ *   xg_slice_panel_kernel : panel tiles (i, k), i > k (or the slots (k, a), a <= k, of the
+ *                           inverse factor) -> four digit planes + row scales
  *   xg_sliced_left_kernel : persistent update of the targets (i, j), i >= j, from the
  *                           panels k0 <= k < k1; 128 x 128 jobs; warp 0 TMA, warp 1 MMA
  *                           issue + TMEM (4 levels x 128 columns = all 512), warps 4-11
@@ -90,18 +91,20 @@ __device__ __forceinline__ double xg_i64_to_f64(long long x)
 /* One warp per panel row: rows of tiles k+1 .. nt-1 of column k.  Lane l owns
  * elements c * 128 + 4 l .. + 3 for every 128-column chunk c, so each load
  * instruction reads 1 KB of the row and each digit store writes 128 bytes. */
-__global__ void __launch_bounds__(256) xg_slice_panel_kernel(XgTileArgs T, int k, int8_t *__restrict__ dig,
-                                                             double *__restrict__ scale, long long plane,
-                                                             const int *status)
+__global__ void __launch_bounds__(256) xg_slice_panel_kernel(XgTileArgs T, int k, int row_mode,
+                                                             int8_t *__restrict__ dig, double *__restrict__ scale,
+                                                             long long plane, const int *status)
 {
     if (*(volatile const int *)status) return;
     const int ts = T.ts;
     const int lane = threadIdx.x & 31;
     const long long row = (long long)blockIdx.x * 8 + (threadIdx.x >> 5);
-    const long long nrows = (long long)(T.nt - k - 1) * ts;
+    /* column mode: tiles (i, k), i > k; row mode: slots (k, a), a <= k */
+    const long long nrows = (long long)(row_mode ? k + 1 : T.nt - k - 1) * ts;
     if (row >= nrows) return;
-    const int i = k + 1 + (int)(row / ts), r = (int)(row % ts);
-    const double *src = T.data + (xg_tile_index(i, k, T.nt) * ts + r) * (long long)ts;
+    const int u = (int)(row / ts), r = (int)(row % ts);
+    const long long slot = row_mode ? xg_tile_index(k, u, T.nt) : xg_tile_index(k + 1 + u, k, T.nt);
+    const double *src = T.data + (slot * ts + r) * (long long)ts;
     const int nch = ts / 128; /* <= 4 */
     double v[16];
     double m = 0.0;
@@ -119,7 +122,7 @@ __global__ void __launch_bounds__(256) xg_slice_panel_kernel(XgTileArgs T, int k
     }
 #pragma unroll
     for (int o = 16; o; o >>= 1) m = fmax(m, __shfl_xor_sync(0xffffffffu, m, o));
-    const long long grow = xg_tile_index(i, k, T.nt) * ts + r; /* tile-packed row index */
+    const long long grow = slot * ts + r; /* tile-packed row index */
     const double c0 = m > 0.0 ? XG_SL_TOP / m : 0.0;
     if (lane == 0) scale[grow] = m / XG_SL_TOP;
 #pragma unroll
@@ -159,23 +162,68 @@ __device__ __forceinline__ void xg_sl_pair(int p, int &a, int &b)
     b = lv - a;
 }
 
-/* job -> target tile i = j + job / (rb * cb) and its block of 64 rows (bm) x
- * 128 columns (bn); blocks entirely above the diagonal of the diagonal tile
- * are skipped */
-__device__ __forceinline__ bool xg_sl_job(long long job, int j, int ts, int &i, int &bm, int &bn)
+/* One job: a 128 x 128 block (bm, bn) of an output tile, summed over the
+ * panel chunks k0 <= k < k1; operand tiles are packed slots of the digit
+ * stores and the output a packed slot of the FP64 store. */
+struct XgSlJob {
+    int ta, tb;       /* tile rows (A) and columns (B) index the operand slots */
+    int bm, bn, k0, k1;
+    long long c_slot;
+};
+
+/* job -> (output tile, block, chunk range) per mode (see XgSlTask); false
+ * for a block with nothing to do (entirely above the diagonal of a diagonal
+ * tile, or an empty chunk range).  Jobs are ordered longest first. */
+__device__ __forceinline__ bool xg_sl_job(const XgSlTask &S, long long job, int nt, int ts, XgSlJob &J)
 {
-    const int rb = ts / XG_SL_BM, cb = ts / XG_SL_BN;
-    i = j + (int)(job / (rb * cb));
-    const int blk = (int)(job % (rb * cb));
-    bm = blk / cb;
-    bn = blk % cb;
-    return !(i == j && bm * XG_SL_BM + XG_SL_BM - 1 < bn * XG_SL_BN);
+    const int bpt = ts / XG_SL_BM;
+    const int per = bpt * bpt;
+    const long long unit = job / per;
+    const int blk = (int)(job % per);
+    J.bm = blk / bpt;
+    J.bn = blk % bpt;
+    bool diag = false;
+    if (S.mode == XG_SL_FACTOR) { /* targets (i, j), i >= j, of column j */
+        J.ta = S.col + (int)unit;
+        J.tb = S.col;
+        J.k0 = S.k0;
+        J.k1 = S.k1;
+        J.c_slot = xg_tile_index(J.ta, J.tb, nt);
+        diag = J.ta == J.tb;
+    } else if (S.mode == XG_SL_INVERSE) { /* X(a, b), a < b = col, from chunks a <= c < b (within [k0, k1)) */
+        J.ta = (int)unit;
+        J.tb = S.col;
+        J.k0 = J.ta > S.k0 ? J.ta : S.k0;
+        J.k1 = S.col < S.k1 ? S.col : S.k1;
+        J.c_slot = xg_tile_index(J.tb, J.ta, nt);
+    } else { /* SYRK: S(a, b), a >= b, from chunks a <= c < nt */
+        int ii, jj;
+        xg_pair_decode(unit, &ii, &jj);
+        J.ta = ii;
+        J.tb = jj;
+        J.k0 = ii;
+        J.k1 = nt;
+        J.c_slot = xg_tile_index(ii, jj, nt);
+        diag = ii == jj;
+    }
+    if (diag && J.bm * XG_SL_BM + XG_SL_BM - 1 < J.bn * XG_SL_BN) return false;
+    return J.k1 > J.k0;
+}
+
+/* packed slot of the A / B operand tile of chunk k */
+__device__ __forceinline__ long long xg_sl_slot_a(const XgSlTask &S, const XgSlJob &J, int k, int nt)
+{
+    return S.mode == XG_SL_FACTOR ? xg_tile_index(J.ta, k, nt) : xg_tile_index(k, J.ta, nt); /* L(i,k) | X(a,k) */
+}
+__device__ __forceinline__ long long xg_sl_slot_b(const XgSlTask &S, const XgSlJob &J, int k, int nt)
+{
+    return S.mode == XG_SL_SYRK ? xg_tile_index(k, J.tb, nt) : xg_tile_index(J.tb, k, nt); /* X(b,k) | L(j,k) */
 }
 
 __global__ void __launch_bounds__(XG_SL_THREADS, 1)
     xg_sliced_left_kernel(const __grid_constant__ CUtensorMap map_a, const __grid_constant__ CUtensorMap map_b,
-                          const double *__restrict__ scale, XgTileArgs T, int j, int k0, int k1, long long njobs,
-                          int plane_rows, int *status)
+                          const double *__restrict__ scale_a, const double *__restrict__ scale_b, XgTileArgs T,
+                          XgSlTask S, long long njobs, int plane_rows, int *status)
 {
     extern __shared__ __align__(1024) unsigned char xg_smem_raw[];
     unsigned char *smem = (unsigned char *)(((uintptr_t)xg_smem_raw + 1023) & ~(uintptr_t)1023);
@@ -215,11 +263,11 @@ __global__ void __launch_bounds__(XG_SL_THREADS, 1)
             xg_prefetch_tensormap(&map_b);
             long long it = 0;
             for (long long job = blockIdx.x; job < njobs && ok; job += gridDim.x) {
-                int i, bm, bn;
-                if (!xg_sl_job(job, j, ts, i, bm, bn)) continue;
-                for (int k = k0; k < k1 && ok; ++k) {
-                    const int rowA = (int)(xg_tile_index(i, k, nt) * ts) + bm * XG_SL_BM;
-                    const int rowB = (int)(xg_tile_index(j, k, nt) * ts) + bn * XG_SL_BN;
+                XgSlJob J;
+                if (!xg_sl_job(S, job, nt, ts, J)) continue;
+                for (int k = J.k0; k < J.k1 && ok; ++k) {
+                    const int rowA = (int)(xg_sl_slot_a(S, J, k, nt) * ts) + J.bm * XG_SL_BM;
+                    const int rowB = (int)(xg_sl_slot_b(S, J, k, nt) * ts) + J.bn * XG_SL_BN;
                     for (int kb = 0; kb < KT; ++kb, ++it) {
                         const int s = (int)(it % XG_SL_STAGES);
                         if (it >= XG_SL_STAGES &&
@@ -251,9 +299,9 @@ __global__ void __launch_bounds__(XG_SL_THREADS, 1)
             const uint32_t sbase = xg_smem_u32(smem);
             long long it = 0, cc = 0;
             for (long long job = blockIdx.x; job < njobs && ok; job += gridDim.x) {
-                int i, bm, bn;
-                if (!xg_sl_job(job, j, ts, i, bm, bn)) continue;
-                for (int k = k0; k < k1 && ok; ++k, ++cc) {
+                XgSlJob J;
+                if (!xg_sl_job(S, job, nt, ts, J)) continue;
+                for (int k = J.k0; k < J.k1 && ok; ++k, ++cc) {
                     if (cc >= 1 && !xg_mbar_wait(acc_empty, (uint32_t)(cc - 1) & 1)) {
                         ok = false;
                         break;
@@ -306,11 +354,11 @@ __global__ void __launch_bounds__(XG_SL_THREADS, 1)
         const int q = warp & 3, h = (warp - 4) >> 2;
         long long cc = 0;
         for (long long job = blockIdx.x; job < njobs && ok; job += gridDim.x) {
-            int i, bm, bn;
-            if (!xg_sl_job(job, j, ts, i, bm, bn)) continue;
-            const int col = bn * XG_SL_BN + q * 32 + lane;   /* C column (row of the B operand) */
-            const int row0 = bm * XG_SL_BM + h * 64;         /* first C row (row of the A operand) */
-            double *Cc = T.data + xg_tile_index(i, j, nt) * (long long)ts * ts + (long long)row0 * ts + col;
+            XgSlJob J;
+            if (!xg_sl_job(S, job, nt, ts, J)) continue;
+            const int col = J.bn * XG_SL_BN + q * 32 + lane; /* C column (row of the B operand) */
+            const int row0 = J.bm * XG_SL_BM + h * 64;       /* first C row (row of the A operand) */
+            double *Cc = T.data + J.c_slot * (long long)ts * ts + (long long)row0 * ts + col;
             {
                 /* the C block is read once, after all chunks: lane l brings rows
                  * row0 + 2 l, + 1, this quarter's 32 columns (two 128-byte lines
@@ -324,7 +372,7 @@ __global__ void __launch_bounds__(XG_SL_THREADS, 1)
             double res[64];
 #pragma unroll
             for (int u = 0; u < 64; ++u) res[u] = 0.0;
-            for (int k = k0; k < k1; ++k, ++cc) {
+            for (int k = J.k0; k < J.k1; ++k, ++cc) {
                 if (!xg_mbar_wait(acc_full, (uint32_t)cc & 1)) {
                     if (lane == 0) atomicOr(status, XG_ST_TIMEOUT);
                     ok = false;
@@ -334,9 +382,9 @@ __global__ void __launch_bounds__(XG_SL_THREADS, 1)
                 /* s_B (this thread's column) with 254^-3 folded in: the levels are
                  * combined as the exact integer v = L0 254^3 + L1 254^2 + L2 254 + L3
                  * (|v| < 2^48) and converted once */
-                const double sc = scale[xg_tile_index(j, k, nt) * ts + col] * XG_SL_INV_RADIX3;
+                const double sc = scale_b[xg_sl_slot_b(S, J, k, nt) * ts + col] * (S.sign * XG_SL_INV_RADIX3);
                 const double2 *sr2 =
-                    reinterpret_cast<const double2 *>(scale + xg_tile_index(i, k, nt) * ts + row0);
+                    reinterpret_cast<const double2 *>(scale_a + xg_sl_slot_a(S, J, k, nt) * ts + row0);
                 const uint32_t base = tmem + ((uint32_t)(q * 32) << 16) + (uint32_t)(h * 64);
                 /* 8 batches per chunk: (columns c * 16 .. + 15, levels 0-1 or 2-3),
                  * software-pipelined -- the next batch's TMEM loads are issued
@@ -386,8 +434,8 @@ __global__ void __launch_bounds__(XG_SL_THREADS, 1)
                 if (lane == 0) xg_mbar_arrive(acc_empty);
             }
             if (!ok) break;
-            /* C -= U: each warp instruction touches 32 consecutive doubles of a
-             * row; 16 rows are loaded before any is stored, so 16 loads per
+            /* C += sign U (or C = sign U): each warp instruction touches 32
+             * consecutive doubles of a row; 16 rows are loaded before any is stored, so 16 loads per
              * thread are in flight (a load after a store through the same
              * pointer would wait for it); L2-only accesses (.cg): the few KB
              * of L1 left beside the shared-memory stages would only thrash */
@@ -395,9 +443,9 @@ __global__ void __launch_bounds__(XG_SL_THREADS, 1)
             for (int u0 = 0; u0 < 64; u0 += 16) {
                 double cv[16];
 #pragma unroll
-                for (int u = 0; u < 16; ++u) cv[u] = __ldcg(Cc + (long long)u * ts);
+                for (int u = 0; u < 16; ++u) cv[u] = S.overwrite ? 0.0 : __ldcg(Cc + (long long)u * ts);
 #pragma unroll
-                for (int u = 0; u < 16; ++u) __stcg(Cc + (long long)u * ts, cv[u] - res[u0 + u]);
+                for (int u = 0; u < 16; ++u) __stcg(Cc + (long long)u * ts, cv[u] + res[u0 + u]);
                 Cc += 16LL * ts;
             }
         }
@@ -419,22 +467,27 @@ cudaError_t xg_sliced_kernels_configure()
     return cudaFuncSetAttribute(xg_sliced_left_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, XG_SL_SMEM);
 }
 
-void xg_launch_slice_panel(const XgTileArgs &T, int k, int8_t *dig, double *scale, long long plane, const int *status,
-                           cudaStream_t st)
+void xg_launch_slice_panel(const XgTileArgs &T, int k, int row_mode, int8_t *dig, double *scale, long long plane,
+                           const int *status, cudaStream_t st)
 {
-    const long long rows = (long long)(T.nt - k - 1) * T.ts;
+    const long long rows = (long long)(row_mode ? k + 1 : T.nt - k - 1) * T.ts;
     if (rows <= 0) return;
-    xg_slice_panel_kernel<<<(unsigned)((rows + 7) / 8), 256, 0, st>>>(T, k, dig, scale, plane, status);
+    xg_slice_panel_kernel<<<(unsigned)((rows + 7) / 8), 256, 0, st>>>(T, k, row_mode, dig, scale, plane, status);
 }
 
-void xg_launch_sliced_left(const CUtensorMap &map_a, const CUtensorMap &map_b, const double *scale,
-                           const XgTileArgs &T, int j, int k0, int k1, int plane_rows, int max_ctas, int *status,
-                           cudaStream_t st)
+void xg_launch_sliced(const CUtensorMap &map_a, const CUtensorMap &map_b, const double *scale_a,
+                      const double *scale_b, const XgTileArgs &T, const XgSlTask &S, int plane_rows, int max_ctas,
+                      int *status, cudaStream_t st)
 {
-    if (k1 <= k0 || j >= T.nt) return;
-    const long long per_tile = (long long)(T.ts / XG_SL_BM) * (T.ts / XG_SL_BN);
-    const long long njobs = (long long)(T.nt - j) * per_tile;
+    if (S.k1 <= S.k0 || S.col >= T.nt) return;
+    const long long per = (long long)(T.ts / XG_SL_BM) * (T.ts / XG_SL_BN);
+    long long units;
+    if (S.mode == XG_SL_FACTOR) units = T.nt - S.col;
+    else if (S.mode == XG_SL_INVERSE) units = S.col;
+    else units = (long long)T.nt * (T.nt + 1) / 2;
+    const long long njobs = units * per;
+    if (njobs <= 0) return;
     const unsigned grid = (unsigned)(njobs < max_ctas ? njobs : max_ctas);
-    xg_sliced_left_kernel<<<grid, XG_SL_THREADS, XG_SL_SMEM, st>>>(map_a, map_b, scale, T, j, k0, k1, njobs,
+    xg_sliced_left_kernel<<<grid, XG_SL_THREADS, XG_SL_SMEM, st>>>(map_a, map_b, scale_a, scale_b, T, S, njobs,
                                                                    plane_rows, status);
 }

@@ -59,6 +59,10 @@ struct XgSliced {
     double *scale = nullptr;
     CUtensorMap map_a, map_b; /* A and B operand views (boxes of 128 rows x 64 bytes) */
     cudaEvent_t ev_a = nullptr, ev_p[2] = {nullptr, nullptr};
+    /* gradient: digit planes of the inverse factor X = L^-T (slot layout of X) */
+    int8_t *xdig = nullptr;
+    double *xscale = nullptr;
+    CUtensorMap xmap;
 };
 
 /* One dataset: locations, observations and the covariance / factor. */
@@ -135,6 +139,7 @@ void xg_field_collect_profile_mixed(XgField *f);
 int xg_field_get_z(XgField *f, double *z, int n);
 int xg_field_set_sliced(XgField *f);
 int xg_field_loglik_sliced(XgField *f, const double *theta, double *res, double *times);
+int xg_field_loglik_grad_sliced(XgField *f, const double *theta, double *res, double *grad, double *times);
 void xg_sliced_destroy(XgSliced *s);
 int xg_sliced_factor_dense(int n, const double *x, const double *y, const double *theta, int kernel, int metric,
                            int ts, double *out);

@@ -136,13 +136,28 @@ void xg_launch_band_gemm(const CUtensorMap &p64map, const XgTileArgs &T, int k, 
                          cudaStream_t st);
 void xg_launch_offband_gemm(const XgMixedMaps &maps, const XgTileArgs &T, int k, int part, int passes, int sm_count,
                             int *status, cudaStream_t st);
-/* sliced.cu: FP64 tiles, trailing updates on INT8 tensor cores (four digit slices), left-looking */
+/* sliced.cu: FP64 tiles, trailing updates on INT8 tensor cores (four digit slices), left-looking.
+ * One launch of xg_sliced_left_kernel computes, for each output tile, C (+)= sign sum_k A_k B_k^T
+ * over panel chunks k, with A_k, B_k read from digit stores:
+ *   XG_SL_FACTOR : column col of the Cholesky factor, chunks k0 <= k < k1: L(i,col) -= sum L(i,k) L(col,k)^T
+ *   XG_SL_INVERSE: column col of X = L^-T (X(a,b) at slot (b,a)): X(a,col) -= sum_{a<=c<col} X(a,c) L(col,c)^T
+ *   XG_SL_SYRK   : S = X X^T into the lower tiles: S(a,b) = sum_{c>=a} X(a,c) X(b,c)^T */
+#define XG_SL_FACTOR 0
+#define XG_SL_INVERSE 1
+#define XG_SL_SYRK 2
+struct XgSlTask {
+    int mode;
+    int col;       /* target column (factor, inverse) */
+    int k0, k1;    /* chunk window */
+    double sign;   /* -1: C -= sum; +1: C += sum */
+    int overwrite; /* C = sign sum (C is not read) */
+};
 cudaError_t xg_sliced_kernels_configure();
-void xg_launch_slice_panel(const XgTileArgs &T, int k, int8_t *dig, double *scale, long long plane, const int *status,
-                           cudaStream_t st);
-void xg_launch_sliced_left(const CUtensorMap &map_a, const CUtensorMap &map_b, const double *scale,
-                           const XgTileArgs &T, int j, int k0, int k1, int plane_rows, int max_ctas, int *status,
-                           cudaStream_t st);
+void xg_launch_slice_panel(const XgTileArgs &T, int k, int row_mode, int8_t *dig, double *scale, long long plane,
+                           const int *status, cudaStream_t st);
+void xg_launch_sliced(const CUtensorMap &map_a, const CUtensorMap &map_b, const double *scale_a,
+                      const double *scale_b, const XgTileArgs &T, const XgSlTask &S, int plane_rows, int max_ctas,
+                      int *status, cudaStream_t st);
 
 void xg_launch_finalize(const double *part_logdet, const double *part_dot, int nt, int N, double *out,
                         const int *status, const int *info, cudaStream_t st);
@@ -175,6 +190,9 @@ cudaError_t xg_gradient_kernels_configure();
 void xg_launch_inverse_factor(const CUtensorMap &mapX, const CUtensorMap &mapL, double *X, const double *L, int nt,
                               int ts, int *status, cudaStream_t st);
 void xg_launch_inverse_syrk(const CUtensorMap &mapX, double *S, int nt, int ts, int *status, cudaStream_t st);
+/* X = 0 with identity diagonal tiles; step K of X L^T = I: X(I, K) <- X(I, K) L_KK^-T for I <= K */
+void xg_launch_identity_x(double *X, int nt, int ts, cudaStream_t st);
+void xg_launch_xtrsm(double *X, const double *L, int nt, int ts, int K, int *status, cudaStream_t st);
 long long xg_grad_contract_blocks(long long ntiles, int ts);
 void xg_launch_grad_contract(const double *S, const int2 *tile_ij, long long ntiles, int nt, int ts, const double *x,
                              const double *y, const double *alpha, int N, const XgMaternParams &mp, int kernel,

@@ -65,3 +65,34 @@ def test_sliced_rejects_non_spd(gpu, ora):
     z = np.ones(600)
     with pytest.raises(gpu.XgError):
         gpu.dmle_host_sliced(x, y, z, [1.0, 0.1, 0.5], ts=128)
+
+
+@pytest.mark.parametrize("n,ts,theta,kernel", [
+    (1500, 128, [1.0, 0.1, 0.5], 0),
+    (2100, 256, [1.3, 0.07, 0.73], 0),
+    (1400, 128, [1.0, 0.1, 1.0, 0.01], 1),
+])
+def test_sliced_gradient_matches_fp64_adjoint(gpu, ora, n, ts, theta, kernel):
+    """Gradient with the sliced factor, inverse factor and X X^T (precision 3)
+    against the FP64 adjoint on the same field and against 4th-order finite
+    differences of the oracle: within 1e-6 of max(|grad|, 1)."""
+    x, y, z, _ = ora.synthetic_field(n, 3, theta, kernel)
+    with gpu.Session(x, y, kernel=kernel, dts=ts) as s:
+        s.set_data(z=z)
+        ll64, g64 = s.loglik(theta, grad=True)
+        s.set_sliced()
+        ll, g = s.loglik(theta, grad=True)
+        assert abs(ll - ll64) / abs(ll64) < 1e-7
+        # the sliced value after a gradient evaluation is unaffected
+        assert s.loglik(theta) == pytest.approx(ll, rel=1e-12)
+    scale = max(np.abs(g64).max(), 1.0)
+    assert np.abs(g - g64).max() / scale < 1e-6, (g, g64)
+    h = 1e-4
+    th = np.asarray(theta, dtype=float)
+    fd = np.zeros_like(th)
+    for i in range(th.size):
+        e = np.zeros_like(th)
+        e[i] = h * th[i]
+        f = lambda t: ora.dmle(x, y, z, t, kernel)[0]
+        fd[i] = (8 * (f(th + e) - f(th - e)) - (f(th + 2 * e) - f(th - 2 * e))) / (12 * e[i])
+    assert np.abs(g - fd).max() / max(np.abs(fd).max(), 1.0) < 1e-6, (g, fd)
