@@ -61,7 +61,7 @@ def parse():
     ap.add_argument("--drivers", default="bobyqa_fp64,bobyqa_sliced,lbfgsb_grad_fp64,lbfgsb_grad_sliced,"
                     "lbfgsb_sliced_polish",
                     help="mle mode: comma list of bobyqa_fp64, bobyqa_sliced, bobyqa_mixed, lbfgsb_grad_fp64, "
-                         "lbfgsb_grad_sliced, lbfgsb_sliced_polish")
+                         "lbfgsb_grad_sliced, lbfgsb_sliced_polish, bobyqa_sliced_polish, two_stage")
     ap.add_argument("--passes", type=int, default=3, help="TF32 passes of the off-band update (1 or 3)")
     ap.add_argument("--scheme", choices=["mixed", "sliced"], default="sliced",
                     help="reduced-precision leg: mixed = FP32 off-band tiles on TF32 tensor cores; "
@@ -311,6 +311,23 @@ def mode_mle(args):
         sess.set_sliced()
         bobyqa("bobyqa_sliced")
         sess.set_fp64()
+    if "bobyqa_sliced_polish" in drivers:
+        # the reference driver on the sliced objective, then FP64 gradient steps from its optimum
+        sess.set_sliced()
+        t0 = time.perf_counter()
+        th, ll, ev = sess.fit_bobyqa(lb, ub, ftol_abs=1e-9)
+        sess.set_fp64()
+        th2, ll2, ev2 = fit_lbfgsb(sess, lb, ub, x0=th)
+        runs["bobyqa_sliced_polish"] = {"seconds": time.perf_counter() - t0, "evals": ev, "evals_fp64": ev2,
+                                        "theta": th2.tolist(), "loglik": ll2, "theta_sliced": th.tolist()}
+    if "two_stage" in drivers:
+        # exageostat_b200.mle.fit_two_stage: derivative-free on the sliced objective, FP64 Newton polish
+        from exageostat_b200.mle import fit_two_stage
+
+        t0 = time.perf_counter()
+        th, ll, ev1, ev2, th1 = fit_two_stage(sess, lb, ub)
+        runs["two_stage"] = {"seconds": time.perf_counter() - t0, "evals": ev1, "grad_evals_fp64": ev2,
+                             "theta": th.tolist(), "loglik": ll, "theta_sliced": th1.tolist()}
     if "bobyqa_mixed" in drivers:
         sess.set_mixed(band=args.band, passes=args.passes)
         bobyqa("bobyqa_mixed", band=args.band)
@@ -334,17 +351,19 @@ def mode_mle(args):
         th, ll, ev = fit_lbfgsb(sess, lb, ub, x0=[0.5, 0.5, 0.5])
         runs["lbfgsb_grad_fp64"] = {"seconds": time.perf_counter() - t0, "evals": ev, "theta": th.tolist(),
                                     "loglik": ll}
-    if "bobyqa_fp64" in runs:
-        ref = np.array(runs["bobyqa_fp64"]["theta"])
-        llref = runs["bobyqa_fp64"]["loglik"]
+    refname = "bobyqa_fp64" if "bobyqa_fp64" in runs else "lbfgsb_grad_fp64" if "lbfgsb_grad_fp64" in runs else None
+    if refname:
+        ref = np.array(runs[refname]["theta"])
+        llref = runs[refname]["loglik"]
         for name, r in runs.items():
-            r["theta_rel_diff_vs_fp64"] = float(np.max(np.abs(np.array(r["theta"]) - ref) / np.abs(ref)))
-            r["speedup_vs_bobyqa_fp64"] = runs["bobyqa_fp64"]["seconds"] / r["seconds"]
+            r["theta_rel_diff_vs_ref"] = float(np.max(np.abs(np.array(r["theta"]) - ref) / np.abs(ref)))
+            r["speedup_vs_" + refname] = runs[refname]["seconds"] / r["seconds"]
             # the objective of every run evaluated in FP64 at its own optimum
             r["loglik_fp64_at_theta"] = sess.loglik(r["theta"])
-            r["loglik_rel_diff_vs_fp64"] = abs(r["loglik_fp64_at_theta"] - llref) / abs(llref)
+            r["loglik_rel_diff_vs_ref"] = abs(r["loglik_fp64_at_theta"] - llref) / abs(llref)
     sess.close()
-    print(json.dumps({"mode": "mle", "n": args.n, "theta0": theta0, "runs": runs}), flush=True)
+    print(json.dumps({"mode": "mle", "n": args.n, "theta0": theta0, "reference_run": refname, "runs": runs}),
+          flush=True)
 
 
 def mode_grad(args):
