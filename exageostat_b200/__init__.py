@@ -106,7 +106,8 @@ EXPORTED_SYMBOLS = [
     "exageostat_b200_bobyqa", "EXAGEOSTAT_sdmle_Tile", "exageostat_b200_set_mixed",
     "exageostat_b200_dmle_host_mixed", "exageostat_b200_mixed_factor_dense", "exageostat_b200_batch_create",
     "exageostat_b200_batch_loglik", "exageostat_b200_batch_destroy", "exageostat_b200_set_sliced",
-    "exageostat_b200_dmle_host_sliced", "exageostat_b200_sliced_factor_dense", "results",
+    "exageostat_b200_dmle_host_sliced", "exageostat_b200_sliced_factor_dense", "exageostat_b200_autotune",
+    "exageostat_b200_batch_autotune", "results",
 ]
 
 _lib = None
@@ -170,6 +171,9 @@ def lib():
         "exageostat_b200_set_sliced": (_I, [PM]),
         "exageostat_b200_dmle_host_sliced": (_I, [_I, _PD, _PD, _PD, _PD, _I, _I, _I, _PD]),
         "exageostat_b200_sliced_factor_dense": (_I, [_I, _PD, _PD, _PD, _I, _I, _I, _PD]),
+        "exageostat_b200_autotune": (_I, [PM, _PD, _D, ctypes.POINTER(_I), ctypes.POINTER(_I), _PD]),
+        "exageostat_b200_batch_autotune": (_I, [_I, ctypes.POINTER(_I), _PD, _PD, _PD, _I, _I, _PD,
+                                                ctypes.POINTER(_I), _PD, ctypes.POINTER(_VP)]),
     }
     for name, (res, args) in sig.items():
         f = getattr(L, name)
@@ -384,6 +388,17 @@ class Session:
     def set_fp64(self) -> None:
         self.data.precision = 0
 
+    def autotune(self, theta, tol: float = 1e-6):
+        """exageostat_b200_autotune: tile size (and band width, precision 2)
+        chosen by timing; the descriptors are rebuilt with them.  Returns
+        (ts, band, [(ts, seconds), ...])."""
+        ts, band = _I(), _I()
+        rep = np.zeros(8)
+        _check(self.L.exageostat_b200_autotune(ctypes.byref(self.data), _p(_f64(theta)), tol, ctypes.byref(ts),
+                                               ctypes.byref(band), _p(rep)))
+        pairs = [(int(rep[2 * i]), float(rep[2 * i + 1])) for i in range(4) if rep[2 * i] > 0]
+        return ts.value, band.value, pairs
+
     def set_profiling(self, on: bool = True) -> None:
         _check(self.L.exageostat_b200_set_profiling(ctypes.byref(self.data), 1 if on else 0))
 
@@ -410,15 +425,29 @@ class Session:
 class Batch:
     """Many independent fields evaluated together (one graph launch per call)."""
 
-    def __init__(self, xs, ys, zs, kernel: int = 0, metric: int = 0, ts: int = 256):
+    def __init__(self, xs, ys, zs, kernel: int = 0, metric: int = 0, ts: int = 256, autotune_theta=None):
+        """ts: tile size; with autotune_theta (one parameter row per field) the
+        tile size is chosen by exageostat_b200_batch_autotune instead
+        (self.ts, self.autotune_report)."""
         self.L = lib()
         self.n = np.array([len(a) for a in xs], dtype=np.int32)
         self.kernel = kernel
         self.nparams = 4 if kernel == 1 else 3
         x, y, z = (_f64(np.concatenate(a)) for a in (xs, ys, zs))
         h = _VP()
-        _check(self.L.exageostat_b200_batch_create(len(xs), self.n.ctypes.data_as(ctypes.POINTER(_I)), _p(x), _p(y),
-                                                   _p(z), kernel, metric, ts, ctypes.byref(h)))
+        nptr = self.n.ctypes.data_as(ctypes.POINTER(_I))
+        self.autotune_report = []
+        if autotune_theta is None:
+            _check(self.L.exageostat_b200_batch_create(len(xs), nptr, _p(x), _p(y), _p(z), kernel, metric, ts,
+                                                       ctypes.byref(h)))
+            self.ts = ts
+        else:
+            th = _f64(autotune_theta).reshape(len(self.n), self.nparams)
+            t, rep = _I(), np.zeros(8)
+            _check(self.L.exageostat_b200_batch_autotune(len(xs), nptr, _p(x), _p(y), _p(z), kernel, metric, _p(th),
+                                                         ctypes.byref(t), _p(rep), ctypes.byref(h)))
+            self.ts = t.value
+            self.autotune_report = [(int(rep[2 * i]), float(rep[2 * i + 1])) for i in range(4) if rep[2 * i] > 0]
         self.h = h
 
     def loglik(self, thetas) -> np.ndarray:

@@ -19,6 +19,7 @@
 #include <string.h>
 
 #include <algorithm>
+#include <chrono>
 #include <vector>
 
 #include "../../include/exageostat_b200.h"
@@ -263,3 +264,47 @@ extern "C" int exageostat_b200_batch_destroy(void *handle)
     xg_batch_free((XgBatch *)handle);
     return XG_OK;
 }
+
+/* Tile size of a batch chosen by timing: the batch is built with tile sizes
+ * 128, 256, 384 and 512 in turn, each timed on one evaluation at theta after
+ * the one that captures its graph, and the fastest is returned in *handle
+ * (*ts_out its tile size; report receives (ts, seconds) pairs, 4 at most). */
+extern "C" int exageostat_b200_batch_autotune(int nfields, const int *n, const double *x, const double *y,
+                                              const double *z, int kernel, int metric, const double *theta,
+                                              int *ts_out, double *report, void **handle)
+{
+    *handle = nullptr;
+    const int cands[4] = {128, 256, 384, 512};
+    void *best = nullptr;
+    double best_t = -1.0;
+    int best_ts = 0, nrep = 0;
+    std::vector<double> ll(nfields);
+    for (int c = 0; c < 4; ++c) {
+        void *h = nullptr;
+        if (exageostat_b200_batch_create(nfields, n, x, y, z, kernel, metric, cands[c], &h)) continue;
+        double sec = -1.0;
+        if (!exageostat_b200_batch_loglik(h, theta, ll.data())) {
+            const auto t0 = std::chrono::steady_clock::now();
+            if (!exageostat_b200_batch_loglik(h, theta, ll.data()))
+                sec = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+        }
+        if (sec >= 0 && report && nrep < 4) {
+            report[2 * nrep] = cands[c];
+            report[2 * nrep + 1] = sec;
+            ++nrep;
+        }
+        if (sec >= 0 && (best_t < 0 || sec < best_t)) {
+            if (best) exageostat_b200_batch_destroy(best);
+            best = h;
+            best_t = sec;
+            best_ts = cands[c];
+        } else {
+            exageostat_b200_batch_destroy(h);
+        }
+    }
+    if (!best) return xg_fail(XG_ERR_CUDA, "batch autotune: no tile size could be timed");
+    *handle = best;
+    if (ts_out) *ts_out = best_ts;
+    return XG_OK;
+}
+

@@ -503,6 +503,29 @@ extern "C" int exageostat_b200_sliced_factor_dense(int n, const double *x, const
     return xg_sliced_factor_dense(n, x, y, theta, kernel, metric, ts, out);
 }
 
+extern "C" int exageostat_b200_autotune(MLE_data *data, const double *theta, double tol, int *ts, int *band,
+                                        double *report)
+{
+    XgField *f = xg_field_of(data);
+    if (!f) return xg_fail(XG_ERR_NOT_INITIALIZED, "no descriptors: call EXAGEOSTAT_dmle_Call first");
+    if (!f->have_z) return xg_fail(XG_ERR_BAD_ARGUMENT, "no observations: call MLE_zvg or set z first");
+    if (!data->l1.x || !data->l1.y) return xg_fail(XG_ERR_BAD_ARGUMENT, "data->l1 holds no locations");
+    int kernel = 0, np = 0;
+    int rc = xg_kernel_of(data, &kernel, &np);
+    if (rc) return rc;
+    rc = xg_check_theta(theta, kernel);
+    if (rc) return rc;
+    int ts_out = 0, band_out = 0;
+    rc = xg_autotune_field(&f, data->l1.x, data->l1.y, theta, data->precision, tol > 0 ? tol : 1e-6, &ts_out,
+                           &band_out, report);
+    data->descC = data->descZ = data->descZcpy = f;
+    if (rc) return rc;
+    if (ts) *ts = ts_out;
+    if (band) *band = band_out;
+    if (data->precision == 2) data->diag_thick = band_out;
+    return XG_OK;
+}
+
 extern "C" int exageostat_b200_mixed_factor_dense(int n, const double *x, const double *y, const double *theta,
                                                   int kernel, int metric, int ts, int band, int passes, double *out)
 {

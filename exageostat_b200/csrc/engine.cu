@@ -1250,6 +1250,111 @@ int xg_field_loglik_grad_sliced(XgField *f, const double *theta, double *res, do
     return XG_OK;
 }
 
+/* ------------------------------------------------------------------------- */
+/* autotuner                                                                 */
+/* ------------------------------------------------------------------------- */
+
+/* seconds (CUDA events, generation to result) of one evaluation of f in the
+ * given precision after a warm-up one; < 0 on failure; res receives loglik */
+static double xg_time_eval(XgField *f, const double *theta, int precision, double *ll)
+{
+    double res[3], t[3] = {0, 0, 0};
+    for (int rep = 0; rep < 2; ++rep) {
+        const int rc = precision == 2   ? xg_field_loglik_mixed(f, theta, res, t)
+                       : precision == 3 ? xg_field_loglik_sliced(f, theta, res, t)
+                                        : xg_field_loglik(f, theta, res, t);
+        if (rc) return -1.0;
+    }
+    if (ll) *ll = res[0];
+    return t[0] + t[1];
+}
+
+/* Tile size (and, for precision 2, band width) chosen by timing.  Tile
+ * sizes 128, 256, 384, 512 (multiples of 256 for precision 2) up to the
+ * field size are timed on temporary fields with the same locations and
+ * observations; *pf is rebuilt with the fastest.  For precision 2 the band
+ * widths 1, 2, 4, 8 are then timed and the fastest whose |dl| / |l| against
+ * one FP64 evaluation is <= tol is kept (the most accurate if none is).
+ * report receives (ts, seconds) pairs, 4 entries at most. */
+int xg_autotune_field(XgField **pf, const double *x, const double *y, const double *theta, int precision, double tol,
+                      int *ts_out, int *band_out, double *report)
+{
+    XgField *f = *pf;
+    const int N = f->N;
+    std::vector<double> z(N);
+    int rc = xg_field_get_z(f, z.data(), N);
+    if (rc) return rc;
+    const int cands[4] = {128, 256, 384, 512};
+    int best_ts = f->C.ts, nrep = 0;
+    double best_t = -1.0;
+    for (int c = 0; c < 4; ++c) {
+        const int ts = cands[c];
+        if (precision == 2 && ts % 256) continue;
+        if (ts > 128 && ts / 2 >= N) continue; /* a single half-empty tile */
+        XgField *t = nullptr;
+        if (xg_field_create(&t, N, ts, x, y, f->kernel, f->metric)) continue;
+        double sec = -1.0;
+        if (!xg_field_set_z(t, z.data()) &&
+            (precision != 2 || !xg_field_set_mixed(t, f->mx ? f->mx->band : 1, 3)) &&
+            (precision != 3 || !xg_field_set_sliced(t)))
+            sec = xg_time_eval(t, theta, precision, nullptr);
+        xg_field_destroy(t);
+        if (sec < 0) continue;
+        if (report && nrep < 4) {
+            report[2 * nrep] = ts;
+            report[2 * nrep + 1] = sec;
+            ++nrep;
+        }
+        if (best_t < 0 || sec < best_t) {
+            best_t = sec;
+            best_ts = ts;
+        }
+    }
+    if (best_t < 0) return xg_fail(XG_ERR_CUDA, "autotune: no tile size could be timed");
+    if (best_ts != f->C.ts) {
+        XgField *g = nullptr;
+        rc = xg_field_create(&g, N, best_ts, x, y, f->kernel, f->metric);
+        if (!rc) rc = xg_field_set_z(g, z.data());
+        if (rc) {
+            if (g) xg_field_destroy(g);
+            return rc;
+        }
+        g->profiling = false;
+        xg_field_destroy(f);
+        *pf = f = g;
+    }
+    *ts_out = best_ts;
+    *band_out = 0;
+    if (precision == 2) {
+        double ll64 = 0;
+        if (xg_time_eval(f, theta, 0, &ll64) < 0) return xg_fail(XG_ERR_CUDA, "autotune: FP64 reference evaluation");
+        int best_band = 1, acc_band = 1;
+        double bt = -1.0, best_err = 1e300;
+        const int bands[4] = {1, 2, 4, 8};
+        for (int b = 0; b < 4; ++b) {
+            if (bands[b] > f->C.nt) break;
+            if (xg_field_set_mixed(f, bands[b], 3)) continue;
+            double ll = 0;
+            const double sec = xg_time_eval(f, theta, 2, &ll);
+            if (sec < 0) continue;
+            const double err = fabs(ll - ll64) / fabs(ll64);
+            if (err <= tol && (bt < 0 || sec < bt)) {
+                bt = sec;
+                best_band = bands[b];
+            }
+            if (err < best_err) {
+                best_err = err;
+                acc_band = bands[b];
+            }
+        }
+        const int band = bt >= 0 ? best_band : acc_band;
+        rc = xg_field_set_mixed(f, band, 3);
+        if (rc) return rc;
+        *band_out = band;
+    }
+    return XG_OK;
+}
+
 int xg_field_get_z(XgField *f, double *z, int n)
 {
     if (!f->have_z) return xg_fail(XG_ERR_BAD_ARGUMENT, "no observations generated yet");

@@ -137,6 +137,8 @@ int xg_mixed_factor_dense(int n, const double *x, const double *y, const double 
 double xg_digamma(double x);
 void xg_field_collect_profile_mixed(XgField *f);
 int xg_field_get_z(XgField *f, double *z, int n);
+int xg_autotune_field(XgField **pf, const double *x, const double *y, const double *theta, int precision, double tol,
+                      int *ts_out, int *band_out, double *report);
 int xg_field_set_sliced(XgField *f);
 int xg_field_loglik_sliced(XgField *f, const double *theta, double *res, double *times);
 int xg_field_loglik_grad_sliced(XgField *f, const double *theta, double *res, double *grad, double *times);

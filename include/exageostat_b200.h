@@ -397,6 +397,18 @@ int exageostat_b200_set_sliced(MLE_data *data);
 int exageostat_b200_dmle_host_sliced(int n, const double *x, const double *y, const double *z, const double *theta,
                                      int kernel, int metric, int ts, double *out);
 
+/* No counterpart in the reference.  Chooses the tile size by timing one
+ * evaluation at theta for tile sizes 128, 256, 384 and 512 (multiples of 256
+ * for precision 2) on temporary descriptors with the same locations
+ * (data->l1) and observations, and rebuilds the descriptors with the
+ * fastest (*ts).  For precision 2 it then times band widths 1, 2, 4, 8 and
+ * keeps the fastest whose |dl| / |l| against one FP64 evaluation is <= tol
+ * (0 = 1e-6; the most accurate band if none is), also written to
+ * data->diag_thick (*band; 0 for the other precisions).  report (may be NULL)
+ * receives up to 4 (tile size, seconds) pairs.  Needs the memory of two
+ * descriptor sets at once. */
+int exageostat_b200_autotune(MLE_data *data, const double *theta, double tol, int *ts, int *band, double *report);
+
 /* Replaces the locations and/or observations (N host doubles each; NULL
  * keeps the current array) of an allocated MLE_data, e.g. for a new dataset
  * of the same size, without reallocating the device covariance. */
@@ -445,6 +457,15 @@ int exageostat_b200_batch_create(int nfields, const int *n, const double *x, con
  * how many failed). */
 int exageostat_b200_batch_loglik(void *handle, const double *theta, double *loglik);
 int exageostat_b200_batch_destroy(void *handle);
+
+/* As exageostat_b200_batch_create with the tile size chosen by timing: the
+ * batch is built with tile sizes 128, 256, 384 and 512 in turn and timed on
+ * one evaluation at theta (nfields rows); the fastest is returned in *handle
+ * and its tile size in *ts.  report (may be NULL) receives up to 4
+ * (tile size, seconds) pairs. */
+int exageostat_b200_batch_autotune(int nfields, const int *n, const double *x, const double *y, const double *z,
+                                   int kernel, int metric, const double *theta, int *ts, double *report,
+                                   void **handle);
 
 /* Diagnostics used by the parity tests.  All run on the GPU. */
 int exageostat_b200_bessel_knu(int n, const double *nu, const double *x, double *out);
