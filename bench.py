@@ -50,13 +50,15 @@ def parse():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-mixed-leg", action="store_true", help="skip the TF32 banded mixed-precision sub-result")
     ap.add_argument("--band", type=int, default=2, help="FP64 band width in tiles (mixed leg)")
-    ap.add_argument("--mode", choices=["evals", "bands", "mle", "batch", "grad"], default="evals",
+    ap.add_argument("--mode", choices=["evals", "bands", "mle", "batch", "grad", "predict"], default="evals",
                     help="evals: the default bench line; bands: accuracy/time per band width; "
-                         "mle: time-to-MLE of the drivers; batch: batched regional fields; grad: gradient cost")
+                         "mle: time-to-MLE of the drivers; batch: batched regional fields; grad: gradient cost; "
+                         "predict: kriging")
     ap.add_argument("--bands", default="1,2,4,8,16")
     ap.add_argument("--no-sliced-row", dest="sliced_row", action="store_false",
                     help="bands mode: skip the INT8-sliced row")
     ap.add_argument("--fields", type=int, default=512)
+    ap.add_argument("--nmiss", type=int, default=1000, help="predict mode: held-out points")
     ap.add_argument("--theta0", default="1.0,0.1,0.5", help="mle mode: parameters of the synthetic field")
     ap.add_argument("--drivers", default="bobyqa_fp64,bobyqa_sliced,lbfgsb_grad_fp64,lbfgsb_grad_sliced,"
                     "lbfgsb_sliced_polish",
@@ -399,6 +401,50 @@ def mode_grad(args):
     print(json.dumps(out), flush=True)
 
 
+def mode_predict(args):
+    """Kriging (EXAGEOSTAT_dmle_Predict_Tile, MLE_dexact.c:688-874): a seeded
+    uniform hold-out of --nmiss points of the field, prediction from the rest
+    at theta0 through the C ABI (host arrays, copies included), wall clock;
+    the CPU oracle on a bounded sample (N_s observed points) scaled by N^3."""
+    os.environ.setdefault("EXAGEOSTAT_B200_SILENT", "1")
+    import numpy as np
+
+    import exageostat_b200 as xg
+    from exageostat_b200.synthetic import dlarnv
+
+    xg.init(args.ts)
+    theta0 = [float(v) for v in args.theta0.split(",")]
+    N, nmiss = args.n, args.nmiss
+    x, y = xg.generate_xy_loc(N, args.seed)
+    sess = xg.Session(x, y, dts=args.ts)
+    sess.zvg(theta0, dlarnv(args.seed, N))
+    z = sess.z()
+    rng = np.random.default_rng(args.seed)
+    miss = np.zeros(N, dtype=bool)
+    miss[rng.choice(N, nmiss, replace=False)] = True
+    xm, ym, zact, xo, yo, zo = x[miss], y[miss], z[miss], x[~miss], y[~miss], z[~miss]
+    sess.predict(theta0, xm, ym, xo, yo, zo, zact)  # warm-up (allocates the kriging descriptors)
+    times = []
+    for _ in range(max(1, args.steps)):
+        t0 = time.perf_counter()
+        mse, zmiss = sess.predict(theta0, xm, ym, xo, yo, zo, zact)
+        times.append(time.perf_counter() - t0)
+    sess.close()
+    out = {"mode": "predict", "n": N, "n_obs": int(N - nmiss), "n_miss": nmiss, "theta0": theta0,
+           "seconds": min(times), "mse": mse, "var_z_actual": float(np.var(zact))}
+    if not args.no_cpu_baseline:
+        import oracle
+
+        oracle.set_threads(os.cpu_count() or 1)
+        ns = min(N, 8000)
+        t0 = time.perf_counter()
+        oracle.dpredict(xm[:min(nmiss, 200)], ym[:min(nmiss, 200)], xo[:ns], yo[:ns], zo[:ns], None, theta0)
+        tc = time.perf_counter() - t0
+        out["cpu_baseline"] = {"seconds_sample": tc, "sample_n_obs": ns, "cores": os.cpu_count(), "kind": "port",
+                               "seconds_extrapolated": tc * ((N - nmiss) / ns) ** 3}
+    print(json.dumps(out), flush=True)
+
+
 def mode_batch(args):
     """Batched regional fields (sizes U[500, 6000], theta_i random): fields/s
     of one batched graph launch against looping the single-field FP64 path."""
@@ -441,7 +487,8 @@ def main():
         run_reference(args)
         return
     if args.mode != "evals":
-        {"bands": mode_bands, "mle": mode_mle, "batch": mode_batch, "grad": mode_grad}[args.mode](args)
+        {"bands": mode_bands, "mle": mode_mle, "batch": mode_batch, "grad": mode_grad,
+         "predict": mode_predict}[args.mode](args)
         return
     import numpy as np
     import torch

@@ -972,8 +972,8 @@ int xg_field_set_sliced(XgField *f)
  *   panel   : POTRF(j, j) [+ log-det, + z block solve] -> TRSM(i, j) [+ z update]
  *             -> slicing of the tiles (i, j), i > j, into digit planes
  * With fs.st_hi the update of column j+1 is split: chunks k < j (needing
- * panels already sliced) run on the main stream on all but XG_PANEL_SMS SMs
- * while the panel chain of column j runs on the high-priority stream, and
+ * panels already sliced) run on the main stream on all but xg_panel_share(j)
+ * SMs while the panel chain of column j runs on the high-priority stream, and
  * chunk k = j joins the panel chain of column j+1.  Profiling events (8 per
  * column): panel stream before / after the last-chunk update, after POTRF,
  * after TRSM + slicing; main stream before / after the split update. */
@@ -987,6 +987,20 @@ static XgSlTask factor_task(int col, int k0, int k1)
     S.sign = -1.0;
     S.overwrite = 0;
     return S;
+}
+
+/* SMs given to the panel chain of column j (last-chunk update, POTRF, TRSM,
+ * slicing) while the split update of column j+1 runs on the others.  The
+ * chain's work grows like nt - j and the split update's like j (nt - j), so
+ * per column the chain needs about 8 / (8 + j) of the machine (measured
+ * costs at tile 512: a TRSM strip of 32 rows ~63 us, a 128 x 128 job-chunk of
+ * the update ~9 us); clamped to [XG_PANEL_SMS, sms - XG_PANEL_SMS]. */
+static int xg_panel_share(int j, int sms)
+{
+    int r = (int)((long long)sms * 8 / (8 + j));
+    if (r < XG_PANEL_SMS) r = XG_PANEL_SMS;
+    if (r > sms - XG_PANEL_SMS) r = sms - XG_PANEL_SMS;
+    return r;
 }
 
 static void xg_factor_sliced(XgField *f, double *v, const XgFactorStreams &fs)
@@ -1011,7 +1025,7 @@ static void xg_factor_sliced(XgField *f, double *v, const XgFactorStreams &fs)
         rec(j, 0, sp);
         if (la) {
             if (j >= 1) xg_launch_sliced(sl->map_a, sl->map_b, sl->scale, sl->scale, T, factor_task(j, j - 1, j), pr,
-                                         XG_PANEL_SMS, f->status, sp);
+                                         xg_panel_share(j, sms), f->status, sp);
         } else {
             xg_launch_sliced(sl->map_a, sl->map_b, sl->scale, sl->scale, T, factor_task(j, 0, j), pr, sms, f->status,
                              sp);
@@ -1029,7 +1043,7 @@ static void xg_factor_sliced(XgField *f, double *v, const XgFactorStreams &fs)
             rec(j, 4, fs.st);
             if (j >= 1 && j + 1 < nt)
                 xg_launch_sliced(sl->map_a, sl->map_b, sl->scale, sl->scale, T, factor_task(j + 1, 0, j), pr,
-                                 sms - XG_PANEL_SMS, f->status, fs.st);
+                                 sms - xg_panel_share(j, sms), f->status, fs.st);
             rec(j, 5, fs.st);
             cudaEventRecord(sl->ev_a, fs.st);
         } else {
