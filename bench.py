@@ -59,6 +59,8 @@ def parse():
                     help="bands mode: skip the INT8-sliced row")
     ap.add_argument("--fields", type=int, default=512)
     ap.add_argument("--nmiss", type=int, default=1000, help="predict mode: held-out points")
+    ap.add_argument("--stage1-ftol", type=float, default=1e-3, help="mle mode, two_stage: first-stage tolerance")
+    ap.add_argument("--stage1-maxeval", type=int, default=400, help="mle mode, two_stage: first-stage cap")
     ap.add_argument("--theta0", default="1.0,0.1,0.5", help="mle mode: parameters of the synthetic field")
     ap.add_argument("--drivers", default="bobyqa_fp64,bobyqa_sliced,lbfgsb_grad_fp64,lbfgsb_grad_sliced,"
                     "lbfgsb_sliced_polish",
@@ -305,6 +307,12 @@ def mode_mle(args):
         th, ll, ev = sess.fit_bobyqa(lb, ub, ftol_abs=1e-9)
         runs[name] = dict({"seconds": time.perf_counter() - t0, "evals": ev, "theta": th.tolist(), "loglik": ll},
                           **extra)
+        progress("%s: %s" % (name, runs[name]))
+
+    t_start = time.perf_counter()
+
+    def progress(msg):
+        print("[mle %.1f s] %s" % (time.perf_counter() - t_start, msg), file=sys.stderr, flush=True)
 
     drivers = args.drivers.split(",")
     if "bobyqa_fp64" in drivers:
@@ -327,7 +335,8 @@ def mode_mle(args):
         from exageostat_b200.mle import fit_two_stage
 
         t0 = time.perf_counter()
-        th, ll, ev1, ev2, th1 = fit_two_stage(sess, lb, ub)
+        th, ll, ev1, ev2, th1 = fit_two_stage(sess, lb, ub, ftol_abs=args.stage1_ftol, maxeval=args.stage1_maxeval,
+                                              log=progress)
         runs["two_stage"] = {"seconds": time.perf_counter() - t0, "evals": ev1, "grad_evals_fp64": ev2,
                              "theta": th.tolist(), "loglik": ll, "theta_sliced": th1.tolist()}
     if "bobyqa_mixed" in drivers:

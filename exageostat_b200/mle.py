@@ -2,12 +2,13 @@
 
 `fit_two_stage` is the reduced-precision MLE: the reference driver's
 derivative-free maximiser (start at the lower bounds,
-examples/examples.c:263-264) on the INT8-sliced objective, then
-`newton_polish` in FP64 from its optimum.  The polish is a bounded Newton
+examples/examples.c:263-264) on the INT8-sliced objective to a loose
+tolerance, then `newton_polish` in FP64 from its end point.  The polish is a bounded Newton
 iteration in log-parameters with the adjoint gradient, a Hessian from
-central differences of gradients at the start and BFGS updates after; near the optimum of the flat sigma^2-beta ridge of the Matern
-likelihood it converges in a few steps where a quasi-Newton or a
-derivative-free method keeps crawling along the ridge.
+central differences of gradients at the start and BFGS updates after; near
+the optimum of the flat sigma^2-beta ridge of the Matern likelihood it
+converges in a few steps where a quasi-Newton or a derivative-free method
+keeps crawling along the ridge.
 """
 from __future__ import annotations
 
@@ -78,13 +79,20 @@ def newton_polish(loglik_grad, theta, lb, ub, max_steps=8, rel_h=1e-4, xtol=1e-6
     return th, f, evals
 
 
-def fit_two_stage(session, lb, ub, ftol_abs=1e-9, polish_steps=6):
+def fit_two_stage(session, lb, ub, ftol_abs=1e-3, maxeval=400, polish_steps=8, log=None):
     """Reduced-precision MLE: the derivative-free maximiser on the sliced
-    objective (precision 3), then the FP64 Newton polish.  Leaves the session
-    in FP64.  Returns (theta_hat, loglik, sliced evaluations, FP64 gradient
-    evaluations, theta after the first stage)."""
+    objective (precision 3) to a loose tolerance (two accepted steps in a row
+    that change loglik by less than ftol_abs, or maxeval evaluations), then
+    the FP64 Newton polish, which does the fine convergence along the ridge.
+    Leaves the session in FP64.  log(msg), when given, receives progress.
+    Returns (theta_hat, loglik, sliced evaluations, FP64 gradient evaluations,
+    theta after the first stage)."""
     session.set_sliced()
-    th1, _, ev1 = session.fit_bobyqa(lb, ub, ftol_abs=ftol_abs)
+    th1, f1, ev1 = session.fit_bobyqa(lb, ub, ftol_abs=ftol_abs, maxeval=maxeval)
+    if log:
+        log("stage 1 (sliced, derivative-free): %d evaluations, theta %s, loglik %.10g" % (ev1, list(th1), f1))
     session.set_fp64()
     th, f, ev2 = newton_polish(lambda t: session.loglik(t, grad=True), th1, lb, ub, max_steps=polish_steps)
+    if log:
+        log("stage 2 (FP64 Newton): %d gradient evaluations, theta %s, loglik %.12g" % (ev2, list(th), f))
     return th, f, ev1, ev2, th1
