@@ -24,16 +24,30 @@ def newton_polish(loglik_grad, theta, lb, ub, max_steps=8, rel_h=1e-4, xtol=1e-6
     (2 n gradient evaluations) and then carried by BFGS updates; each step is
     the Newton step d = -H^-1 g_phi when it is an ascent direction (else a
     short gradient step), projected onto the box and halved until f does not
-    decrease.  Stops when the accepted relative step is below xtol, after
-    max_steps, or when no step improves f.  Returns (theta, f, gradient
+    decrease.  A failing evaluation (an exception, or a non-finite value)
+    counts as f = -inf: it rejects a trial step, and at the start point it
+    ends the polish.  Stops when the accepted relative step is below xtol,
+    after max_steps, or when no step improves f.  Returns (theta, f, gradient
     evaluations)."""
     lb = np.asarray(lb, dtype=np.float64)
     ub = np.asarray(ub, dtype=np.float64)
     th = np.clip(np.asarray(theta, dtype=np.float64), lb, ub)
-    f, g = loglik_grad(th)
-    g = np.asarray(g, dtype=np.float64)
-    evals = 1
     n = th.size
+
+    def fg(t):
+        """f and gradient; an evaluation that fails (e.g. a covariance that is
+        not positive definite) counts as f = -inf."""
+        try:
+            fv, gv = loglik_grad(t)
+        except Exception:
+            return -np.inf, np.full(n, np.nan)
+        gv = np.asarray(gv, dtype=np.float64)
+        return (fv, gv) if np.isfinite(fv) and np.all(np.isfinite(gv)) else (-np.inf, np.full(n, np.nan))
+
+    f, g = fg(th)
+    evals = 1
+    if not np.isfinite(f):
+        return th, f, evals
     phi = np.log(th)
     gphi = g * th
     H = np.empty((n, n))
@@ -41,11 +55,13 @@ def newton_polish(loglik_grad, theta, lb, ub, max_steps=8, rel_h=1e-4, xtol=1e-6
         e = np.zeros(n)
         e[j] = rel_h
         tp, tm = np.exp(phi + e), np.exp(phi - e)
-        _, gp = loglik_grad(tp)
-        _, gm = loglik_grad(tm)
+        _, gp = fg(tp)
+        _, gm = fg(tm)
         evals += 2
-        H[:, j] = (np.asarray(gp) * tp - np.asarray(gm) * tm) / (2 * rel_h)
+        H[:, j] = (gp * tp - gm * tm) / (2 * rel_h)
     H = 0.5 * (H + H.T)
+    if not np.all(np.isfinite(H)):
+        H = -np.eye(n) * max(np.max(np.abs(gphi)), 1.0)
     for _ in range(max_steps):
         try:
             d = np.linalg.solve(H, -gphi)
@@ -58,7 +74,7 @@ def newton_polish(loglik_grad, theta, lb, ub, max_steps=8, rel_h=1e-4, xtol=1e-6
         step = 0.0
         while t >= 1.0 / 64:
             cand = np.clip(np.exp(phi + t * d), lb, ub)
-            fc, gc = loglik_grad(cand)
+            fc, gc = fg(cand)
             evals += 1
             if np.isfinite(fc) and fc >= f:
                 step = np.max(np.abs(cand - th) / th)

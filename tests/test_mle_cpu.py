@@ -34,3 +34,22 @@ def test_newton_polish_never_decreases_and_respects_bounds():
     th, f, _ = newton_polish(_ridge, start, lb, ub, max_steps=3)
     assert f >= f0
     assert np.all(th >= lb) and np.all(th <= ub)
+
+
+def test_newton_polish_treats_failing_evaluations_as_minus_infinity():
+    """A parameter region where the objective raises (as a covariance that is
+    not positive definite does) rejects steps instead of aborting."""
+    lb, ub = [0.01] * 3, [5.0] * 3
+    b0 = np.exp(-2.0)
+    opt = np.array([np.e * b0 * b0, b0, 0.5])
+
+    def guarded(th):
+        if th[2] > 0.5005:
+            raise RuntimeError("not positive definite")
+        return _ridge(th)
+
+    th, f, _ = newton_polish(guarded, opt * np.array([1.02, 1.01, 1.0]), lb, ub)
+    assert np.isfinite(f) and th[2] <= 0.5005
+    assert f >= guarded(opt * np.array([1.02, 1.01, 1.0]))[0]
+    th2, f2, ev2 = newton_polish(guarded, opt * np.array([1.0, 1.0, 1.01]), lb, ub)
+    assert f2 == -np.inf and ev2 == 1
