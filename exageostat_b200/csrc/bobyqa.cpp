@@ -20,7 +20,7 @@
  *     model is poor; a resolution rho decreasing from rhobeg to rhoend.
  *
  * It is not a transcription of NLopt's code, so its iterate sequence differs;
- * agreement with the reference is judged on the maximiser and the value.
+ * agreement with the reference is measured on the maximiser and the value.
  */
 #include <math.h>
 #include <stdio.h>

@@ -57,19 +57,6 @@ static int xg_cuda_fail(cudaError_t e, const char *what)
 
 extern "C" const char *exageostat_last_error(void) { return g_last_error.c_str(); }
 
-static bool xg_silent()
-{
-    const char *s = getenv("EXAGEOSTAT_B200_SILENT");
-    return s && *s && strcmp(s, "0") != 0;
-}
-
-static double xg_wtime()
-{
-    struct timeval tp;
-    gettimeofday(&tp, NULL);
-    return tp.tv_sec + 1e-6 * tp.tv_usec;
-}
-
 /* ------------------------------------------------------------------------- */
 /* context                                                                   */
 /* ------------------------------------------------------------------------- */

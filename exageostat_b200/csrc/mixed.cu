@@ -23,7 +23,7 @@
  * DMMA operands of band targets) and the TF32 hi / lo parts (FP32 containers,
  * the tcgen05 operands).  The reference's mixed path has signature and type
  * defects (sdpotrf.c:292 vs psdportf.c:44; codelet_exageostat_sgemm.c:95), so
- * results are judged against the FP64 path, not against it.
+ * results are compared with the FP64 path, not with it.
  */
 #include <math.h>
 #include <stdint.h>

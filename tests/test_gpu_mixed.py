@@ -1,7 +1,8 @@
 """Banded mixed precision (precision = 2) against the FP64 path and the
 oracle.  Bars: band tiles of the factor 1e-11; off-band (FP32-stored) tiles
 1e-5 of max |L|; log-likelihood |dl|/|l| <= 1e-6 with three TF32 passes
-reported and bounded by 1e-4 with one pass."""
+(the accuracy target for reduced precision), reported and bounded by 1e-4 with
+one pass."""
 import numpy as np
 import pytest
 

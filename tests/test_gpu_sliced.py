@@ -3,7 +3,7 @@ against LAPACK and the oracle.  Each update is an exact integer product of
 operands carried to ~32 bits relative to their row maximum (2^-32 ~ 2.3e-10
 per chunk product, amplified by the triangular solves), so the factor stays
 within 5e-8 of LAPACK's (relative to max |L|) and the log-likelihood within
-1e-7 relative; the north-star bar for reduced precision is 1e-6."""
+1e-7 relative; the accuracy target for reduced precision is 1e-6."""
 import numpy as np
 import pytest
 
