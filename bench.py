@@ -50,7 +50,7 @@ def parse():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-mixed-leg", action="store_true", help="skip the TF32 banded mixed-precision sub-result")
     ap.add_argument("--band", type=int, default=2, help="FP64 band width in tiles (mixed leg)")
-    ap.add_argument("--mode", choices=["evals", "bands", "mle", "batch", "grad", "predict"], default="evals",
+    ap.add_argument("--mode", choices=["evals", "bands", "mle", "batch", "grad", "predict", "assess"], default="evals",
                     help="evals: the default bench line; bands: accuracy/time per band width; "
                          "mle: time-to-MLE of the drivers; batch: batched regional fields; grad: gradient cost; "
                          "predict: kriging")
@@ -58,7 +58,9 @@ def parse():
     ap.add_argument("--no-sliced-row", dest="sliced_row", action="store_false",
                     help="bands mode: skip the INT8-sliced row")
     ap.add_argument("--fields", type=int, default=512)
-    ap.add_argument("--nmiss", type=int, default=1000, help="predict mode: held-out points")
+    ap.add_argument("--nmiss", type=int, default=1000, help="predict and assess modes: held-out points")
+    ap.add_argument("--fisher-n", type=int, default=20000, help="assess mode: locations of the Fisher matrix")
+    ap.add_argument("--assess-n", type=int, default=40000, help="assess mode: locations for MLOE / MMOM")
     ap.add_argument("--stage1-ftol", type=float, default=1e-3, help="mle mode, two_stage: first-stage tolerance")
     ap.add_argument("--stage1-maxeval", type=int, default=400, help="mle mode, two_stage: first-stage cap")
     ap.add_argument("--theta0", default="1.0,0.1,0.5", help="mle mode: parameters of the synthetic field")
@@ -454,6 +456,71 @@ def mode_predict(args):
     print(json.dumps(out), flush=True)
 
 
+def mode_assess(args):
+    """Assessment of a fit: the Fisher information (EXAGEOSTAT_Fisher_Tile,
+    MLE_dexact.c:1777-1934) of --fisher-n locations at theta0, and MLOE / MMOM
+    (EXAGEOSTAT_dmle_mloe_mmom_Tile, MLE_dexact.c:1109-1434) of kriging --nmiss
+    held-out points of --assess-n locations with a perturbed estimate, both
+    through the C ABI on host arrays (wall clock, plus the library's device
+    times).  CPU: the oracle on bounded samples, scaled by the reference
+    algorithm's operation counts."""
+    os.environ.setdefault("EXAGEOSTAT_B200_SILENT", "1")
+    import numpy as np
+
+    import exageostat_b200 as xg
+
+    xg.init(0)
+    theta0 = [float(v) for v in args.theta0.split(",")]
+    est = [theta0[0] * 0.9, theta0[1] * 1.2, theta0[2] * 1.1]
+    out = {"mode": "assess", "theta0": theta0, "estimated_theta": est}
+    # Fisher information
+    nf = args.fisher_n
+    x, y = xg.generate_xy_loc(nf, args.seed)
+    xg.fisher_host(x[:2048], y[:2048], theta0)  # warm-up (kernel load)
+    t0 = time.perf_counter()
+    F = xg.fisher_host(x, y, theta0, ts=args.ts)
+    tf = time.perf_counter() - t0
+    Np = -(-nf // 512) * 512
+    out["fisher"] = {"n": nf, "seconds": tf, "F": F.tolist(), "inverse_diag": np.diag(np.linalg.inv(F)).tolist(),
+                     "dense_gemm_tflops": 3 * 2.0 * Np ** 3 / tf / 1e12,
+                     "check_F00_vs_N_over_2sigma4": float(F[0, 0] / (nf / (2 * theta0[0] ** 2)) - 1)}
+    # MLOE / MMOM
+    n, nmiss = args.assess_n, args.nmiss
+    x, y = xg.generate_xy_loc(n, args.seed)
+    rng = np.random.default_rng(args.seed)
+    miss = np.zeros(n, dtype=bool)
+    miss[rng.choice(n, nmiss, replace=False)] = True
+    xm, ym, xo, yo = x[miss], y[miss], x[~miss], y[~miss]
+    xg.mloe_mmom_host(xm[:16], ym[:16], xo[:2048], yo[:2048], theta0, est)  # warm-up
+    t0 = time.perf_counter()
+    mloe, mmom, _, dev = xg.mloe_mmom_host(xm, ym, xo, yo, theta0, est, ts=args.ts)
+    tm = time.perf_counter() - t0
+    out["mloe_mmom"] = {"n_obs": int(n - nmiss), "n_miss": nmiss, "seconds": tm, "mloe": mloe, "mmom": mmom,
+                        "device_seconds": {"generation": dev[0], "factorisations": dev[1], "solves": dev[2],
+                                           "total": dev[3]}}
+    if not args.no_cpu_baseline:
+        import oracle
+
+        oracle.set_threads(os.cpu_count() or 1)
+        ns = min(nf, 1500)
+        t0 = time.perf_counter()
+        oracle.fisher(x[:ns], y[:ns], theta0)
+        tc = time.perf_counter() - t0
+        # the reference: N^3/3 factorisation + per (j, k) two N x N TRSMs (and
+        # per j two more) and one GEMM: 3 * 2 N^3 + 6 * (2 N^3 + 2 N^3) = 30 N^3
+        out["fisher"]["cpu_baseline"] = {"seconds_sample": tc, "sample_n": ns, "cores": os.cpu_count(),
+                                         "kind": "port", "seconds_extrapolated": tc * (nf / ns) ** 3}
+        no_s, nm_s = min(n - nmiss, 4000), min(nmiss, 100)
+        t0 = time.perf_counter()
+        oracle.mloe_mmom(xm[:nm_s], ym[:nm_s], xo[:no_s], yo[:no_s], theta0, est)
+        tc = time.perf_counter() - t0
+        cost = lambda no, nm: 2.0 * no ** 3 / 3 + 5.0 * nm * no ** 2
+        out["mloe_mmom"]["cpu_baseline"] = {
+            "seconds_sample": tc, "sample_n_obs": no_s, "sample_n_miss": nm_s, "cores": os.cpu_count(),
+            "kind": "port", "seconds_extrapolated": tc * cost(n - nmiss, nmiss) / cost(no_s, nm_s)}
+    print(json.dumps(out), flush=True)
+
+
 def mode_batch(args):
     """Batched regional fields (sizes U[500, 6000], theta_i random): fields/s
     of one batched graph launch against looping the single-field FP64 path."""
@@ -497,7 +564,7 @@ def main():
         return
     if args.mode != "evals":
         {"bands": mode_bands, "mle": mode_mle, "batch": mode_batch, "grad": mode_grad,
-         "predict": mode_predict}[args.mode](args)
+         "predict": mode_predict, "assess": mode_assess}[args.mode](args)
         return
     import numpy as np
     import torch

@@ -107,7 +107,10 @@ EXPORTED_SYMBOLS = [
     "exageostat_b200_dmle_host_mixed", "exageostat_b200_mixed_factor_dense", "exageostat_b200_batch_create",
     "exageostat_b200_batch_loglik", "exageostat_b200_batch_destroy", "exageostat_b200_set_sliced",
     "exageostat_b200_dmle_host_sliced", "exageostat_b200_sliced_factor_dense", "exageostat_b200_autotune",
-    "exageostat_b200_batch_autotune", "results",
+    "exageostat_b200_batch_autotune", "EXAGEOSTAT_Fisher_Tile", "exageostat_b200_fisher",
+    "exageostat_b200_fisher_host", "mloe_mmom_init", "EXAGEOSTAT_dmle_mloe_mmom_Allocate",
+    "EXAGEOSTAT_dmle_mloe_mmom_Tile", "EXAGEOSTAT_dmle_mloe_mmom_Tile_Async", "mloe_mmom_finalize",
+    "MLOE_MMOM_Finalize", "exageostat_b200_mloe_mmom_host", "results",
 ]
 
 _lib = None
@@ -174,6 +177,15 @@ def lib():
         "exageostat_b200_autotune": (_I, [PM, _PD, _D, ctypes.POINTER(_I), ctypes.POINTER(_I), _PD]),
         "exageostat_b200_batch_autotune": (_I, [_I, ctypes.POINTER(_I), _PD, _PD, _PD, _I, _I, _PD,
                                                 ctypes.POINTER(_I), _PD, ctypes.POINTER(_VP)]),
+        "EXAGEOSTAT_Fisher_Tile": (_PD, [PM, _I, _PD, _I, _I, _I]),
+        "exageostat_b200_fisher": (_I, [PM, _PD, _PD, _PD]),
+        "exageostat_b200_fisher_host": (_I, [_I, _PD, _PD, _PD, _I, _I, _I, _PD]),
+        "mloe_mmom_init": (None, [PM, _I, _I, _I, _I, _I]),
+        "EXAGEOSTAT_dmle_mloe_mmom_Tile": (None, [PM, _PD, _PD, _I, _I, _I]),
+        "EXAGEOSTAT_dmle_mloe_mmom_Tile_Async": (None, [PM, _PD, _PD, _I, _I, _I]),
+        "mloe_mmom_finalize": (None, [PM]),
+        "exageostat_b200_mloe_mmom_host": (_I, [_I, _PD, _PD, _I, _PD, _PD, _PD, _PD, _I, _I, _I, _PD, _PD, _PD,
+                                                _PD]),
     }
     for name, (res, args) in sig.items():
         f = getattr(L, name)
@@ -290,6 +302,31 @@ def sliced_factor_dense(x, y, theta, kernel=0, metric=0, ts=0) -> np.ndarray:
     return out
 
 
+def fisher_host(x, y, theta, kernel=0, metric=0, ts=0) -> np.ndarray:
+    """Fisher information 1/2 tr(Sigma^-1 dSigma_j Sigma^-1 dSigma_k) of the
+    locations at theta: 3 x 3 (kernel 0) or 4 x 4 with the nugget (kernel 1)."""
+    x, y = _f64(x), _f64(y)
+    np_ = 4 if kernel == 1 else 3
+    out = np.empty((np_, np_))
+    _check(lib().exageostat_b200_fisher_host(x.size, _p(x), _p(y), _p(_f64(theta)), kernel, metric, ts, _p(out)))
+    return out
+
+
+def mloe_mmom_host(x_miss, y_miss, x_obs, y_obs, truth_theta, estimated_theta, kernel=0, metric=0, ts=0):
+    """MLOE and MMOM of kriging the missing locations from the observed ones
+    with estimated_theta when truth_theta is the truth.  Returns (mloe, mmom,
+    terms, times): terms[m] = (expr1, expr2, expr3, expr4, loe, mom) of
+    missing point m, times = (generation, factorisations, solves, total) s."""
+    xm, ym, xo, yo = (_f64(a) for a in (x_miss, y_miss, x_obs, y_obs))
+    mloe, mmom = ctypes.c_double(), ctypes.c_double()
+    terms = np.empty((xm.size, 6))
+    times = np.empty(4)
+    _check(lib().exageostat_b200_mloe_mmom_host(xm.size, _p(xm), _p(ym), xo.size, _p(xo), _p(yo),
+                                                _p(_f64(truth_theta)), _p(_f64(estimated_theta)), kernel, metric, ts,
+                                                ctypes.byref(mloe), ctypes.byref(mmom), _p(terms), _p(times)))
+    return mloe.value, mmom.value, terms, times
+
+
 def dmle_host(x, y, z, theta, kernel=0, metric=0, ts=0):
     """One-shot log-likelihood on host arrays: (loglik, logdet, dotp)."""
     x, y, z = _f64(x), _f64(y), _f64(z)
@@ -369,6 +406,41 @@ class Session:
         mse = self.L.EXAGEOSTAT_dmle_Predict_Tile(ctypes.byref(d), _p(t), xm.size, xo.size, _p(zo),
                                                   None if za is None else _p(za), _p(zmiss), self.N)
         return mse, zmiss
+
+    def fisher(self, theta):
+        """exageostat_b200_fisher: (F, F^-1) for the session's kernel."""
+        np_ = 4 if self.kernel == 1 else 3
+        F, Finv = np.empty((np_, np_)), np.empty((np_, np_))
+        _check(self.L.exageostat_b200_fisher(ctypes.byref(self.data), _p(_f64(theta)), _p(F), _p(Finv)))
+        return F, Finv
+
+    def fisher_tile(self, theta) -> np.ndarray:
+        """EXAGEOSTAT_Fisher_Tile: the inverse Fisher matrix (3 x 3, from the
+        reference's 10-double column-major result)."""
+        t = _f64(theta)
+        r = self.L.EXAGEOSTAT_Fisher_Tile(ctypes.byref(self.data), self.N, _p(t), 0, 1, 1)
+        if not r:
+            raise XgError(-1, last_error())
+        out = np.array([r[i] for i in range(9)]).reshape(3, 3).T.copy()
+        ctypes.CDLL(None).free(ctypes.cast(r, ctypes.c_void_p))
+        return out
+
+    def mloe_mmom(self, truth_theta, estimated_theta, x_miss, y_miss, x_obs, y_obs, asynchronous=False):
+        """mloe_mmom_init + EXAGEOSTAT_dmle_mloe_mmom_Tile(_Async) +
+        mloe_mmom_finalize on the given locations: (data.mloe, data.mmom)."""
+        xm, ym, xo, yo = (_f64(a).copy() for a in (x_miss, y_miss, x_obs, y_obs))
+        self._keep = [xm, ym, xo, yo]
+        d = self.data
+        d.lmiss.x, d.lmiss.y = _p(xm), _p(ym)
+        d.lobs.x, d.lobs.y = _p(xo), _p(yo)
+        tt, te = _f64(truth_theta), _f64(estimated_theta)
+        self.L.mloe_mmom_init(ctypes.byref(d), xm.size, xo.size, 0, 1, 1)
+        fn = self.L.EXAGEOSTAT_dmle_mloe_mmom_Tile_Async if asynchronous else self.L.EXAGEOSTAT_dmle_mloe_mmom_Tile
+        fn(ctypes.byref(d), _p(tt), _p(te), xm.size, xo.size, self.N)
+        self.L.mloe_mmom_finalize(ctypes.byref(d))
+        if not np.isfinite(d.mloe):
+            raise XgError(-1, last_error())
+        return d.mloe, d.mmom
 
     def set_data(self, x=None, y=None, z=None) -> None:
         arrs = [None if a is None else _f64(a) for a in (x, y, z)]

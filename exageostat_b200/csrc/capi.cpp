@@ -430,6 +430,210 @@ extern "C" void prediction_finalize(MLE_data *data)
 }
 
 /* ------------------------------------------------------------------------- */
+/* assessment: Fisher information, MLOE / MMOM                               */
+/* ------------------------------------------------------------------------- */
+
+/* MLE_dexact.c:1777-1934.  The reference generates Sigma and its derivatives
+ * with univariate_matern_stationary whatever data->kernel_fun holds
+ * (:1825, :1840-1842), so kernel 0 here too. */
+extern "C" double *EXAGEOSTAT_Fisher_Tile(MLE_data *data, int N, double *initial_theta, int dts, int p_grid,
+                                          int q_grid)
+{
+    (void)dts;
+    (void)p_grid;
+    (void)q_grid;
+    XgField *f = xg_field_of(data);
+    if (!f || f->N != N) {
+        xg_fail(XG_ERR_NOT_INITIALIZED, "no descriptors for N = %d: call EXAGEOSTAT_dmle_Call first", N);
+        fprintf(stderr, "EXAGEOSTAT_Fisher_Tile: %s\n", exageostat_last_error());
+        return NULL;
+    }
+    double F[9], inv[9], t = 0.0;
+    int rc = xg_field_fisher(f, initial_theta, 0, F, &t);
+    if (!rc) rc = xg_small_spd_inverse(3, F, inv);
+    if (rc) {
+        fprintf(stderr, "EXAGEOSTAT_Fisher_Tile: %s\n", exageostat_last_error());
+        return NULL;
+    }
+    if (!xg_quiet()) {
+        printf("Fisher matrix\n");
+        for (int i = 0; i < 3; ++i) printf("%12.6e %12.6e %12.6e\n", F[i * 3], F[i * 3 + 1], F[i * 3 + 2]);
+        printf("Fisher matrix (inverse)\n");
+        for (int i = 0; i < 3; ++i) printf("%12.6e %12.6e %12.6e\n", inv[i * 3], inv[i * 3 + 1], inv[i * 3 + 2]);
+        fprintf(stderr, " ---- Time to calculate Fisher matrix: %6.4f seconds\n", t);
+    }
+    results.fisher_00 = inv[0];
+    results.fisher_11 = inv[4];
+    results.fisher_22 = inv[8];
+    results.fisher_time = t;
+    double *r = (double *)calloc(10, sizeof(double));
+    if (!r) return NULL;
+    for (int j = 0; j < 3; ++j)
+        for (int i = 0; i < 3; ++i) r[i + 3 * j] = inv[i * 3 + j];
+    return r;
+}
+
+extern "C" int exageostat_b200_fisher(MLE_data *data, const double *theta, double *fisher, double *fisher_inv)
+{
+    XgField *f = xg_field_of(data);
+    if (!f) return xg_fail(XG_ERR_NOT_INITIALIZED, "no descriptors: call EXAGEOSTAT_dmle_Call first");
+    int kernel = 0, np = 0;
+    int rc = xg_kernel_of(data, &kernel, &np);
+    if (rc) return rc;
+    double F[16], inv[16], t = 0.0;
+    rc = xg_field_fisher(f, theta, kernel, F, &t);
+    if (rc) return rc;
+    if (fisher) memcpy(fisher, F, np * np * sizeof(double));
+    if (fisher_inv) {
+        rc = xg_small_spd_inverse(np, F, inv);
+        if (rc) return rc;
+        memcpy(fisher_inv, inv, np * np * sizeof(double));
+    }
+    results.fisher_time = t;
+    return XG_OK;
+}
+
+/* MLE_dexact.c:1002-1107: the descriptor handles all point at one workspace;
+ * the reference exits on an unknown kernel_fun (:1055-1059), this prints the error. */
+extern "C" void EXAGEOSTAT_dmle_mloe_mmom_Allocate(MLE_data *data, int nZmiss, int nZobs, int dts, int p_grid,
+                                                   int q_grid)
+{
+    (void)p_grid;
+    (void)q_grid;
+    if (nZmiss <= 0) {
+        fprintf(stderr, " Number of missing values should be positive value\n");
+        return;
+    }
+    int kernel = 0, np = 0;
+    if (xg_kernel_of(data, &kernel, &np)) {
+        fprintf(stderr, "EXAGEOSTAT_dmle_mloe_mmom_Allocate: %s\n", exageostat_last_error());
+        return;
+    }
+    if (data->desck_t) mloe_mmom_finalize(data);
+    XgAssess *q = nullptr;
+    if (xg_assess_create(&q, nZmiss, nZobs, dts > 0 ? dts : g_xg.dts)) {
+        fprintf(stderr, "EXAGEOSTAT_dmle_mloe_mmom_Allocate: %s\n", exageostat_last_error());
+        return;
+    }
+    data->mloe = 0;
+    data->mmom = 0;
+    data->desck_t = data->desck_a = data->desck_atmp = data->desck_ttmp = q;
+    data->descK_t = data->descK_a = q;
+    data->descexpr1 = data->descexpr2 = data->descexpr3 = data->descexpr4 = q;
+    data->descmloe = &data->mloe;
+    data->descmmom = &data->mmom;
+}
+
+extern "C" void mloe_mmom_init(MLE_data *data, int nZmiss, int nZobs, int ts, int p_grid, int q_grid)
+{
+    EXAGEOSTAT_dmle_mloe_mmom_Allocate(data, nZmiss, nZobs, ts, p_grid, q_grid);
+}
+
+extern "C" void mloe_mmom_finalize(MLE_data *data)
+{
+    XgAssess *q = (XgAssess *)data->desck_t;
+    if (q) xg_assess_destroy(q);
+    data->desck_t = data->desck_a = data->desck_atmp = data->desck_ttmp = NULL;
+    data->descK_t = data->descK_a = NULL;
+    data->descexpr1 = data->descexpr2 = data->descexpr3 = data->descexpr4 = NULL;
+    data->descmloe = data->descmmom = NULL;
+}
+
+extern "C" void MLOE_MMOM_Finalize(MLE_data *data) { mloe_mmom_finalize(data); }
+
+/* flop count the reference reports (MLE_dexact.c:1265-1359, 1395): two
+ * factorisations and, per missing point, four vector TRSMs and four
+ * vector-vector products */
+static double xg_mloe_mmom_flops(int nmiss, int nobs)
+{
+    const double n = nobs;
+    return 2.0 * (n * n * n / 3.0 + n * n / 2.0 + n / 6.0) + (double)nmiss * (4.0 * n * n + 4.0 * 2.0 * n);
+}
+
+static void xg_mloe_mmom(MLE_data *data, double *truth_theta, double *estimated_theta, int nZmiss, int nZobs,
+                         const char *mode)
+{
+    int kernel = 0, np = 0;
+    if (xg_kernel_of(data, &kernel, &np)) {
+        fprintf(stderr, "EXAGEOSTAT_dmle_mloe_mmom_Tile: %s\n", exageostat_last_error());
+        return;
+    }
+    XgAssess *q = (XgAssess *)data->desck_t;
+    if (!q || q->nmiss != nZmiss || q->nobs != nZobs) {
+        EXAGEOSTAT_dmle_mloe_mmom_Allocate(data, nZmiss, nZobs, 0, 1, 1);
+        q = (XgAssess *)data->desck_t;
+        if (!q) return;
+    }
+    double mloe = 0, mmom = 0, times[4] = {0, 0, 0, 0};
+    int rc = xg_assess_run(q, truth_theta, estimated_theta, kernel, xg_metric_of(data), data->lmiss.x, data->lmiss.y,
+                           data->lobs.x, data->lobs.y, &mloe, &mmom, NULL, times);
+    if (rc) {
+        fprintf(stderr, "EXAGEOSTAT_dmle_mloe_mmom_Tile: %s\n", exageostat_last_error());
+        data->mloe = data->mmom = NAN;
+        return;
+    }
+    data->mloe = mloe;
+    data->mmom = mmom;
+    results.mloe = mloe;
+    results.mmom = mmom;
+    results.mloe_exec = (char *)mode;
+    results.total_mloe_mmom_time = times[3];
+    results.matrix_gen_mloe_mmom_time = times[0];
+    results.cho_fact_mloe_mmom_time = times[1];
+    results.loop_mloe_mmom_time = times[2];
+    results.total_mloe_mmom_flops = xg_mloe_mmom_flops(nZmiss, nZobs) / 1e9 / (times[1] + times[2]);
+    if (!xg_quiet()) {
+        printf("\nnZmiss = %d\n", nZmiss);
+        printf(" ----(MLOE-MMOM) Gflop/s: %6.2f\n", results.total_mloe_mmom_flops);
+        printf("\nMMLOE = %f", mloe);
+        printf("\nMMOM = %f\n\n\n", mmom);
+        fprintf(stderr, " ---- mloe_mmom Time: %6.2f seconds\n\n", times[3]);
+    }
+}
+
+extern "C" void EXAGEOSTAT_dmle_mloe_mmom_Tile(MLE_data *data, double *truth_theta, double *estimated_theta,
+                                               int nZmiss, int nZobs, int n)
+{
+    (void)n;
+    xg_mloe_mmom(data, truth_theta, estimated_theta, nZmiss, nZobs, "sync");
+}
+
+extern "C" void EXAGEOSTAT_dmle_mloe_mmom_Tile_Async(MLE_data *data, double *truth_theta, double *estimated_theta,
+                                                     int nZmiss, int nZobs, int n)
+{
+    (void)n;
+    xg_mloe_mmom(data, truth_theta, estimated_theta, nZmiss, nZobs, "async");
+}
+
+extern "C" int exageostat_b200_fisher_host(int n, const double *x, const double *y, const double *theta, int kernel,
+                                           int metric, int ts, double *fisher)
+{
+    if (kernel != 0 && kernel != 1) return xg_fail(XG_ERR_BAD_ARGUMENT, "kernel %d", kernel);
+    XgField *f = nullptr;
+    int rc = xg_field_create(&f, n, ts, x, y, kernel, metric);
+    if (rc) return rc;
+    double t = 0.0;
+    rc = xg_field_fisher(f, theta, kernel, fisher, &t);
+    xg_field_destroy(f);
+    return rc;
+}
+
+extern "C" int exageostat_b200_mloe_mmom_host(int nmiss, const double *xmiss, const double *ymiss, int nobs,
+                                              const double *xobs, const double *yobs, const double *truth_theta,
+                                              const double *estimated_theta, int kernel, int metric, int ts,
+                                              double *mloe, double *mmom, double *terms, double *times)
+{
+    if (kernel != 0 && kernel != 1) return xg_fail(XG_ERR_BAD_ARGUMENT, "kernel %d", kernel);
+    XgAssess *q = nullptr;
+    int rc = xg_assess_create(&q, nmiss, nobs, ts);
+    if (rc) return rc;
+    rc = xg_assess_run(q, truth_theta, estimated_theta, kernel, metric, xmiss, ymiss, xobs, yobs, mloe, mmom, terms,
+                       times);
+    xg_assess_destroy(q);
+    return rc;
+}
+
+/* ------------------------------------------------------------------------- */
 /* one-shot and diagnostic entry points                                      */
 /* ------------------------------------------------------------------------- */
 

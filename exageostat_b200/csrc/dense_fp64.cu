@@ -28,37 +28,11 @@
 #include "kbessel.cuh"
 #include "xg_common.cuh"
 #include "xg_kernels.h"
+#include "xg_matern.cuh"
 
 /* ========================================================================== */
 /* Matern tile generation                                                     */
 /* ========================================================================== */
-
-__device__ inline double xg_deg2rad(double d) { return d * (XG_PI / 180.0); }
-
-/* Distance between (x1, y1) [row location] and (x2, y2) [column location].
- * Euclidean: sqrt(pow(x2 - x1, 2) + pow(y2 - y1, 2)) as core_zcmg.c:84, with
- * explicit round-to-nearest products and sum so no FMA contraction changes
- * the rounding.  Great circle (dm = "gc"): haversine in km on (lat, lon) in
- * degrees, as distanceEarth (core_zcmg.c:51-60). */
-__device__ inline double xg_distance(double x1, double y1, double x2, double y2, int metric)
-{
-    if (metric == 1) {
-        const double lat1 = xg_deg2rad(x1), lon1 = xg_deg2rad(y1);
-        const double lat2 = xg_deg2rad(x2), lon2 = xg_deg2rad(y2);
-        const double u = sin((lat2 - lat1) / 2), v = sin((lon2 - lon1) / 2);
-        return 2.0 * 6371.0 * asin(sqrt(u * u + cos(lat1) * cos(lat2) * v * v));
-    }
-    const double dx = x2 - x1, dy = y2 - y1;
-    return sqrt(__dadd_rn(__dmul_rn(dx, dx), __dmul_rn(dy, dy)));
-}
-
-__device__ inline double xg_matern_value(double d, const XgMaternParams &p)
-{
-    const double r = d / p.beta;
-    if (r == 0.0) return p.sigma2 + p.nugget;
-    if (p.half_integer >= 0) return xg_matern_half_integer(r, p.sigma2, p.half_integer);
-    return xg_matern_general(r, p.nu, p.con);
-}
 
 /* One CTA fills XG_GEN_ROWS rows of one tile; threads stride the columns so
  * the row-major stores and the column-location loads are coalesced. */

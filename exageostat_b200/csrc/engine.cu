@@ -513,19 +513,33 @@ double xg_digamma(double x)
     return r + log(x) - 0.5 / x - series;
 }
 
-/* log-likelihood and its gradient (see gradient_fp64.cu for the steps);
- * grad has 3 entries (4 for the nugget kernel) */
-int xg_field_loglik_grad(XgField *f, const double *theta, double *res, double *grad, double *times)
+/* The gradient's inverse-factor store and contraction partials, each
+ * allocated on first use (the Fisher path allocates only the store). */
+static int xg_grad_workspace(XgField *f)
 {
     if (!f->X.d) {
         int rc = xg_tm_alloc(f->X, f->N, f->C.ts);
         if (rc) return rc;
-        const long long blocks = xg_grad_contract_blocks(f->C.ntiles, f->C.ts);
-        if (cudaMalloc(&f->gpart, 4 * (size_t)blocks * sizeof(double)) != cudaSuccess ||
-            cudaMalloc(&f->gout, 4 * sizeof(double)) != cudaSuccess)
-            return xg_fail(XG_ERR_NO_MEMORY, "gradient workspace");
     }
-    int rc = xg_field_loglik(f, theta, res, times);
+    const long long blocks = xg_grad_contract_blocks(f->C.ntiles, f->C.ts);
+    if (!f->gpart && cudaMalloc(&f->gpart, 4 * (size_t)blocks * sizeof(double)) != cudaSuccess) {
+        f->gpart = nullptr;
+        return xg_fail(XG_ERR_NO_MEMORY, "gradient workspace");
+    }
+    if (!f->gout && cudaMalloc(&f->gout, 4 * sizeof(double)) != cudaSuccess) {
+        f->gout = nullptr;
+        return xg_fail(XG_ERR_NO_MEMORY, "gradient workspace");
+    }
+    return XG_OK;
+}
+
+/* log-likelihood and its gradient (see gradient_fp64.cu for the steps);
+ * grad has 3 entries (4 for the nugget kernel) */
+int xg_field_loglik_grad(XgField *f, const double *theta, double *res, double *grad, double *times)
+{
+    int rc = xg_grad_workspace(f);
+    if (rc) return rc;
+    rc = xg_field_loglik(f, theta, res, times);
     if (rc) return rc;
     cudaStream_t st = g_xg.stream;
     XgTileArgs T{f->C.d, f->C.ts, f->C.nt};
@@ -1176,14 +1190,7 @@ int xg_field_loglik_grad_sliced(XgField *f, const double *theta, double *res, do
     int rc = XG_OK;
     if (!f->sl && (rc = xg_field_set_sliced(f))) return rc;
     XgSliced *sl = f->sl;
-    if (!f->X.d) {
-        rc = xg_tm_alloc(f->X, f->N, f->C.ts);
-        if (rc) return rc;
-        const long long blocks = xg_grad_contract_blocks(f->C.ntiles, f->C.ts);
-        if (cudaMalloc(&f->gpart, 4 * (size_t)blocks * sizeof(double)) != cudaSuccess ||
-            cudaMalloc(&f->gout, 4 * sizeof(double)) != cudaSuccess)
-            return xg_fail(XG_ERR_NO_MEMORY, "gradient workspace");
-    }
+    if ((rc = xg_grad_workspace(f))) return rc;
     const int ts = f->C.ts, nt = f->C.nt;
     const size_t plane = (size_t)sl->plane_rows * ts;
     if (!sl->xdig) {

@@ -28,6 +28,7 @@
 #include "kbessel.cuh"
 #include "xg_common.cuh"
 #include "xg_kernels.h"
+#include "xg_matern.cuh"
 
 /* ========================================================================== */
 /* Generalised tile GEMM: C (+)= -/+ sum_q A_q B_q^T over 128 x 128 blocks    */
@@ -39,9 +40,14 @@
 #define XG_TG_THREADS 256
 #define XG_TG_STAGE_BYTES (2 * XG_TG_BM * XG_TG_BK * 8)
 
-/* modes */
+/* modes.  "R layout": an mt x nt grid of tiles whose tile (R, K) sits at
+ * slot K * mt + R (right-hand sides stored transposed, one row per
+ * right-hand side). */
 #define XG_TG_XUPDATE 1 /* step K of X L^T = I: slot(K', I) of X -= X_slot(K, I) L_slot(K', K)^T */
 #define XG_TG_SYRKX 2   /* S_IJ = sum_{K >= I} X_slot(K, I) X_slot(K, J)^T, written to C storage */
+#define XG_TG_RFWD 3    /* step K of Y L^T = B (R layout): B(R, K') -= Y(R, K) L_slot(K', K)^T, K' > K */
+#define XG_TG_RTRI 4    /* C(R, I) = sum_{K >= I} A(R, K) B_slot(K, I)^T (R layout, B lower-tile packed) */
+#define XG_TG_DENSE 5   /* full nt x nt tiles (slot A nt + B): C(A, B) = sum_K A(A, K) B(B, K)^T */
 
 struct XgTileGemmJob {
     int c_slot;  /* packed slot of the output tile */
@@ -53,11 +59,34 @@ struct XgTileGemmJob {
     bool skip;
 };
 
-__device__ inline XgTileGemmJob xg_tg_decode(int mode, long long job, int nt, int K)
+__device__ inline XgTileGemmJob xg_tg_decode(int mode, long long job, int nt, int K, int mt)
 {
     XgTileGemmJob j;
     j.skip = false;
-    if (mode == XG_TG_XUPDATE) {
+    if (mode == XG_TG_RFWD) {
+        const int R = (int)(job % mt), Kp = K + 1 + (int)(job / mt);
+        j.c_slot = Kp * mt + R;
+        j.a_slot0 = K * mt + R;
+        j.b_slot0 = (int)xg_tile_index(Kp, K, nt);
+        j.ntiles_k = 1;
+        j.k_step_a = j.k_step_b = 0;
+    } else if (mode == XG_TG_RTRI) {
+        const int R = (int)(job % mt), I = (int)(job / mt);
+        j.c_slot = I * mt + R;
+        j.a_slot0 = I * mt + R;
+        j.k_step_a = mt;
+        /* slot(K, I) for K = I.. nt-1 are consecutive in the packed column I */
+        j.b_slot0 = (int)xg_tile_index(I, I, nt);
+        j.k_step_b = 1;
+        j.ntiles_k = nt - I;
+    } else if (mode == XG_TG_DENSE) {
+        const int A = (int)(job / nt), B = (int)(job % nt);
+        j.c_slot = A * nt + B;
+        j.a_slot0 = A * nt;
+        j.b_slot0 = B * nt;
+        j.k_step_a = j.k_step_b = 1;
+        j.ntiles_k = nt;
+    } else if (mode == XG_TG_XUPDATE) {
         const int width = K + 1; /* I in [0, K] */
         const int I = (int)(job % width), Kp = K + 1 + (int)(job / width);
         j.c_slot = (int)xg_tile_index(Kp, I, nt);
@@ -81,7 +110,7 @@ __device__ inline XgTileGemmJob xg_tg_decode(int mode, long long job, int nt, in
 
 __global__ void __launch_bounds__(XG_TG_THREADS, 1)
     xg_tile_gemm_kernel(const __grid_constant__ CUtensorMap mapA, const __grid_constant__ CUtensorMap mapB,
-                        double *__restrict__ Cbase, int nt, int ts, int mode, int K, int *status)
+                        double *__restrict__ Cbase, int nt, int ts, int mode, int K, int mt, int *status)
 {
     extern __shared__ __align__(1024) unsigned char xg_smem_raw[];
     unsigned char *smem = (unsigned char *)(((uintptr_t)xg_smem_raw + 1023) & ~(uintptr_t)1023);
@@ -91,7 +120,7 @@ __global__ void __launch_bounds__(XG_TG_THREADS, 1)
     const long long job = blockIdx.x / (bpt * bpt);
     const int blk = blockIdx.x % (bpt * bpt);
     const int bi = blk / bpt, bj = blk % bpt;
-    const XgTileGemmJob J = xg_tg_decode(mode, job, nt, K);
+    const XgTileGemmJob J = xg_tg_decode(mode, job, nt, K, mt);
     /* S output is symmetric: skip the strictly upper 128-blocks of diagonal tiles */
     bool diag_upper = false;
     if (mode == XG_TG_SYRKX) {
@@ -130,7 +159,7 @@ __global__ void __launch_bounds__(XG_TG_THREADS, 1)
     const int g = lane >> 2, tq = lane & 3;
     double *C = Cbase + (long long)J.c_slot * ts * ts + (long long)(bi * XG_TG_BM) * ts + bj * XG_TG_BM;
     double acc[4][4][4];
-    const bool subtract = (mode == XG_TG_XUPDATE);
+    const bool subtract = (mode == XG_TG_XUPDATE || mode == XG_TG_RFWD);
 #pragma unroll
     for (int mi = 0; mi < 4; ++mi)
 #pragma unroll
@@ -221,8 +250,10 @@ __global__ void __launch_bounds__(XG_TG_THREADS, 1)
 #define XG_XT_THREADS 512
 #define XG_XT_SR 32
 
+/* mt == 0: the tiles X_IK, I <= K, at slot (K, I) (inverse factor);
+ * mt  > 0: the tiles (R, K), R < mt, of an R-layout matrix (right-hand sides) */
 __global__ void __launch_bounds__(XG_XT_THREADS) xg_xtrsm_kernel(double *__restrict__ X, const double *__restrict__ Lt,
-                                                                 int nt, int ts, int K, const int *status)
+                                                                 int nt, int ts, int K, int mt, const int *status)
 {
     const int LDS = ts + 4;
     extern __shared__ __align__(16) double xg_smem_d[];
@@ -233,7 +264,8 @@ __global__ void __launch_bounds__(XG_XT_THREADS) xg_xtrsm_kernel(double *__restr
     const int I = blockIdx.x / strips, strip = blockIdx.x % strips; /* I in [0, K] */
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     const int g = lane >> 2, tq = lane & 3;
-    double *B = X + xg_tile_index(K, I, nt) * (long long)ts * ts + (long long)strip * XG_XT_SR * ts;
+    const long long bslot = mt > 0 ? (long long)K * mt + I : xg_tile_index(K, I, nt);
+    double *B = X + bslot * (long long)ts * ts + (long long)strip * XG_XT_SR * ts;
     const double *L = Lt + xg_tile_index(K, K, nt) * (long long)ts * ts;
     for (int idx = tid; idx < XG_XT_SR * ts; idx += blockDim.x) {
         const int r = idx / ts, c = idx - r * ts;
@@ -324,18 +356,6 @@ struct XgGradParams {
     int metric;
 };
 
-__device__ inline double xg_gdist(double x1, double y1, double x2, double y2, int metric)
-{
-    if (metric == 1) {
-        const double d2r = XG_PI / 180.0;
-        const double lat1 = x1 * d2r, lon1 = y1 * d2r, lat2 = x2 * d2r, lon2 = y2 * d2r;
-        const double u = sin((lat2 - lat1) / 2), v = sin((lon2 - lon1) / 2);
-        return 2.0 * 6371.0 * asin(sqrt(u * u + cos(lat1) * cos(lat2) * v * v));
-    }
-    const double dx = x2 - x1, dy = y2 - y1;
-    return sqrt(__dadd_rn(__dmul_rn(dx, dx), __dmul_rn(dy, dy)));
-}
-
 #define XG_GC_ROWS 8
 /* one CTA: XG_GC_ROWS rows of one lower tile of S; partial sums of the four
  * parameters' contractions go to part[4 * blockIdx.x + p] */
@@ -362,7 +382,7 @@ __global__ void __launch_bounds__(256) xg_grad_contract_kernel(const double *__r
             const int Cc = ij.y * ts + c;
             if (Cc >= N || Cc > R) continue;
             const double w = (Cc == R ? 0.5 : 1.0) * (ar * alpha[Cc] - tile[(long long)r * ts + c]);
-            const double d = xg_gdist(xr, yr, x[Cc], y[Cc], p.metric);
+            const double d = xg_distance(xr, yr, x[Cc], y[Cc], p.metric);
             const double rd = d / p.beta;
             if (rd == 0.0) {
                 acc[0] += w;                     /* dSigma/dsigma2 = 1 on the zero-distance branch */
@@ -432,12 +452,12 @@ void xg_launch_inverse_factor(const CUtensorMap &mapX, const CUtensorMap &mapL, 
     xg_identity_diag_kernel<<<dim3(1, nt), 256, 0, st>>>(X, nt, ts);
     const int bpt = ts / XG_TG_BM;
     for (int K = 0; K < nt; ++K) {
-        xg_xtrsm_kernel<<<(K + 1) * (ts / XG_XT_SR), XG_XT_THREADS, xg_xtrsm_smem_bytes(ts), st>>>(X, L, nt, ts, K,
+        xg_xtrsm_kernel<<<(K + 1) * (ts / XG_XT_SR), XG_XT_THREADS, xg_xtrsm_smem_bytes(ts), st>>>(X, L, nt, ts, K, 0,
                                                                                                  status);
         const long long jobs = (long long)(K + 1) * (nt - K - 1);
         if (jobs > 0)
             xg_tile_gemm_kernel<<<(unsigned)(jobs * bpt * bpt), XG_TG_THREADS, xg_tile_gemm_smem_bytes(), st>>>(
-                mapX, mapL, X, nt, ts, XG_TG_XUPDATE, K, status);
+                mapX, mapL, X, nt, ts, XG_TG_XUPDATE, K, 0, status);
     }
 }
 
@@ -450,7 +470,7 @@ void xg_launch_identity_x(double *X, int nt, int ts, cudaStream_t st)
 
 void xg_launch_xtrsm(double *X, const double *L, int nt, int ts, int K, int *status, cudaStream_t st)
 {
-    xg_xtrsm_kernel<<<(K + 1) * (ts / XG_XT_SR), XG_XT_THREADS, xg_xtrsm_smem_bytes(ts), st>>>(X, L, nt, ts, K,
+    xg_xtrsm_kernel<<<(K + 1) * (ts / XG_XT_SR), XG_XT_THREADS, xg_xtrsm_smem_bytes(ts), st>>>(X, L, nt, ts, K, 0,
                                                                                              status);
 }
 
@@ -459,7 +479,7 @@ void xg_launch_inverse_syrk(const CUtensorMap &mapX, double *S, int nt, int ts, 
     const int bpt = ts / XG_TG_BM;
     const long long jobs = xg_num_lower_tiles(nt);
     xg_tile_gemm_kernel<<<(unsigned)(jobs * bpt * bpt), XG_TG_THREADS, xg_tile_gemm_smem_bytes(), st>>>(
-        mapX, mapX, S, nt, ts, XG_TG_SYRKX, 0, status);
+        mapX, mapX, S, nt, ts, XG_TG_SYRKX, 0, 0, status);
 }
 
 long long xg_grad_contract_blocks(long long ntiles, int ts) { return ntiles * (ts / XG_GC_ROWS); }
@@ -480,4 +500,43 @@ void xg_launch_grad_contract(const double *S, const int2 *tile_ij, long long nti
     const long long blocks = xg_grad_contract_blocks(ntiles, ts);
     xg_grad_contract_kernel<<<(unsigned)blocks, 256, 0, st>>>(S, tile_ij, nt, ts, x, y, alpha, N, p, part);
     xg_grad_reduce_kernel<<<1, dim3(32, 4), 0, st>>>(part, blocks, out);
+}
+
+/* Y L^T = B for an R-layout right-hand side B (mt tile rows) and the lower
+ * tile factor L, right-looking like the inverse factor: B is overwritten with
+ * Y, the transpose of L^-1 B^T. */
+void xg_launch_rhs_forward_solve(const CUtensorMap &mapR, double *R, int mt, const CUtensorMap &mapL, const double *L,
+                                 int nt, int ts, int *status, cudaStream_t st)
+{
+    const int bpt = ts / XG_TG_BM;
+    for (int K = 0; K < nt; ++K) {
+        xg_xtrsm_kernel<<<mt * (ts / XG_XT_SR), XG_XT_THREADS, xg_xtrsm_smem_bytes(ts), st>>>(R, L, nt, ts, K, mt,
+                                                                                            status);
+        const long long jobs = (long long)mt * (nt - K - 1);
+        if (jobs > 0)
+            xg_tile_gemm_kernel<<<(unsigned)(jobs * bpt * bpt), XG_TG_THREADS, xg_tile_gemm_smem_bytes(), st>>>(
+                mapR, mapL, R, nt, ts, XG_TG_RFWD, K, mt, status);
+    }
+}
+
+/* C(R, I) = sum_{K >= I} A(R, K) B_slot(K, I)^T: A and C R-layout (C != A),
+ * B lower-tile packed.  With B = X (X_IK at slot (K, I)) this is C = A X^T;
+ * with B holding the transposed tiles of a factor L, C = A L. */
+void xg_launch_rhs_tri_product(const CUtensorMap &mapA, const CUtensorMap &mapB, double *C, int mt, int nt, int ts,
+                               int *status, cudaStream_t st)
+{
+    const int bpt = ts / XG_TG_BM;
+    const long long jobs = (long long)mt * nt;
+    xg_tile_gemm_kernel<<<(unsigned)(jobs * bpt * bpt), XG_TG_THREADS, xg_tile_gemm_smem_bytes(), st>>>(
+        mapA, mapB, C, nt, ts, XG_TG_RTRI, 0, mt, status);
+}
+
+/* C = A B^T on full nt x nt tile grids (tile (A, B) at slot A nt + B) */
+void xg_launch_dense_gemm_nt(const CUtensorMap &mapA, const CUtensorMap &mapB, double *C, int nt, int ts, int *status,
+                             cudaStream_t st)
+{
+    const int bpt = ts / XG_TG_BM;
+    const long long jobs = (long long)nt * nt;
+    xg_tile_gemm_kernel<<<(unsigned)(jobs * bpt * bpt), XG_TG_THREADS, xg_tile_gemm_smem_bytes(), st>>>(
+        mapA, mapB, C, nt, ts, XG_TG_DENSE, 0, 0, status);
 }

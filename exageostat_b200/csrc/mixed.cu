@@ -31,31 +31,12 @@
 #include "kbessel.cuh"
 #include "xg_common.cuh"
 #include "xg_kernels.h"
+#include "xg_matern.cuh"
 #include "xg_tcgen05.cuh"
 
 /* ========================================================================== */
 /* generation into the band (FP64) / off-band (FP32) stores                   */
 /* ========================================================================== */
-
-__device__ inline double xg_mx_distance(double x1, double y1, double x2, double y2, int metric)
-{
-    if (metric == 1) {
-        const double d2r = XG_PI / 180.0;
-        const double lat1 = x1 * d2r, lon1 = y1 * d2r, lat2 = x2 * d2r, lon2 = y2 * d2r;
-        const double u = sin((lat2 - lat1) / 2), v = sin((lon2 - lon1) / 2);
-        return 2.0 * 6371.0 * asin(sqrt(u * u + cos(lat1) * cos(lat2) * v * v));
-    }
-    const double dx = x2 - x1, dy = y2 - y1;
-    return sqrt(__dadd_rn(__dmul_rn(dx, dx), __dmul_rn(dy, dy)));
-}
-
-__device__ inline double xg_mx_matern(double d, const XgMaternParams &p)
-{
-    const double r = d / p.beta;
-    if (r == 0.0) return p.sigma2 + p.nugget;
-    if (p.half_integer >= 0) return xg_matern_half_integer(r, p.sigma2, p.half_integer);
-    return xg_matern_general(r, p.nu, p.con);
-}
 
 #define XG_MG_ROWS 8
 __global__ void __launch_bounds__(256) xg_gen_mixed_kernel(XgTileArgs T, const int2 *__restrict__ tile_ij,
@@ -79,7 +60,7 @@ __global__ void __launch_bounds__(256) xg_gen_mixed_kernel(XgTileArgs T, const i
             const int C = ij.y * ts + c;
             double val;
             if (row_ok && C < n)
-                val = xg_mx_matern(xg_mx_distance(x1, y1, x[C], y[C], metric), p);
+                val = xg_matern_value(xg_distance(x1, y1, x[C], y[C], metric), p);
             else
                 val = (R == C) ? 1.0 : 0.0;
             if (band)

@@ -14,26 +14,7 @@
 #include "kbessel.cuh"
 #include "xg_common.cuh"
 #include "xg_kernels.h"
-
-__device__ inline double xg_distance2(double x1, double y1, double x2, double y2, int metric)
-{
-    if (metric == 1) {
-        const double d2r = XG_PI / 180.0;
-        const double lat1 = x1 * d2r, lon1 = y1 * d2r, lat2 = x2 * d2r, lon2 = y2 * d2r;
-        const double u = sin((lat2 - lat1) / 2), v = sin((lon2 - lon1) / 2);
-        return 2.0 * 6371.0 * asin(sqrt(u * u + cos(lat1) * cos(lat2) * v * v));
-    }
-    const double dx = x2 - x1, dy = y2 - y1;
-    return sqrt(__dadd_rn(__dmul_rn(dx, dx), __dmul_rn(dy, dy)));
-}
-
-__device__ inline double xg_matern_at(double d, const XgMaternParams &p)
-{
-    const double r = d / p.beta;
-    if (r == 0.0) return p.sigma2 + p.nugget;
-    if (p.half_integer >= 0) return xg_matern_half_integer(r, p.sigma2, p.half_integer);
-    return xg_matern_general(r, p.nu, p.con);
-}
+#include "xg_matern.cuh"
 
 /* ---- z = L e : 32 rows of tile-row i per CTA, 8 warps x 4 rows ---- */
 __global__ void __launch_bounds__(256) xg_trmv_lower_kernel(XgTileArgs T, const double *__restrict__ e,
@@ -146,7 +127,7 @@ __global__ void __launch_bounds__(256) xg_predict_cross_kernel(const double *__r
     const double x1 = xm[m], y1 = ym[m];
     double s = 0.0;
     for (int o = threadIdx.x; o < nobs; o += blockDim.x)
-        s += xg_matern_at(xg_distance2(x1, y1, xo[o], yo[o], metric), p) * alpha[o];
+        s += xg_matern_value(xg_distance(x1, y1, xo[o], yo[o], metric), p) * alpha[o];
     for (int off = 16; off > 0; off >>= 1) s += __shfl_xor_sync(0xffffffffu, s, off);
     if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = s;
     __syncthreads();
@@ -193,7 +174,7 @@ __global__ void xg_matern_pairs_kernel(const double *x1, const double *y1, const
                                        XgMaternParams p, int metric, double *out)
 {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i < n) out[i] = xg_matern_at(xg_distance2(x1[i], y1[i], x2[i], y2[i], metric), p);
+    if (i < n) out[i] = xg_matern_value(xg_distance(x1[i], y1[i], x2[i], y2[i], metric), p);
 }
 
 void xg_launch_matern_pairs(const double *x1, const double *y1, const double *x2, const double *y2, int n,

@@ -152,6 +152,29 @@ int xg_predict_run(XgPredict *q, const double *theta, int kernel, int metric, co
                    const double *xo, const double *yo, const double *zobs, const double *zactual, double *zmiss,
                    double *mse);
 
+/* MLOE / MMOM workspace (assess.cu): the two observed-set factors, the
+ * inverse factor, and five R-layout right-hand-side stores (one row per
+ * missing point): k_a -> A, k_t -> U, k_t -> T, W, V. */
+struct XgAssess {
+    int nmiss = 0, nobs = 0, ts = 0, nt = 0, mt = 0;
+    XgTileMatrix Ca, Ct, X;
+    double *R[5] = {nullptr, nullptr, nullptr, nullptr, nullptr};
+    CUtensorMap mR[5];
+    double *xo = nullptr, *yo = nullptr, *xm = nullptr, *ym = nullptr;
+    double *terms = nullptr, *part = nullptr;
+    int *status = nullptr;
+    cudaEvent_t ev[4] = {nullptr, nullptr, nullptr, nullptr};
+    cudaEvent_t ev_panel = nullptr, ev_upd = nullptr;
+};
+
+int xg_field_fisher(XgField *f, const double *theta, int kernel, double *F, double *seconds);
+int xg_small_spd_inverse(int n, const double *A, double *inv);
+int xg_assess_create(XgAssess **out, int nmiss, int nobs, int ts);
+void xg_assess_destroy(XgAssess *q);
+int xg_assess_run(XgAssess *q, const double *truth, const double *est, int kernel, int metric, const double *xm,
+                  const double *ym, const double *xo, const double *yo, double *mloe, double *mmom, double *terms,
+                  double *times);
+
 int xg_covariance_dense(int n, const double *x, const double *y, const double *theta, int kernel, int metric, int ts,
                         int factor, double *out);
 int xg_matern_pairs_host(int n, const double *x1, const double *y1, const double *x2, const double *y2,

@@ -193,9 +193,28 @@ void xg_launch_inverse_syrk(const CUtensorMap &mapX, double *S, int nt, int ts, 
 /* X = 0 with identity diagonal tiles; step K of X L^T = I: X(I, K) <- X(I, K) L_KK^-T for I <= K */
 void xg_launch_identity_x(double *X, int nt, int ts, cudaStream_t st);
 void xg_launch_xtrsm(double *X, const double *L, int nt, int ts, int K, int *status, cudaStream_t st);
+void xg_launch_rhs_forward_solve(const CUtensorMap &mapR, double *R, int mt, const CUtensorMap &mapL, const double *L,
+                                 int nt, int ts, int *status, cudaStream_t st);
+void xg_launch_rhs_tri_product(const CUtensorMap &mapA, const CUtensorMap &mapB, double *C, int mt, int nt, int ts,
+                               int *status, cudaStream_t st);
+void xg_launch_dense_gemm_nt(const CUtensorMap &mapA, const CUtensorMap &mapB, double *C, int nt, int ts, int *status,
+                             cudaStream_t st);
 long long xg_grad_contract_blocks(long long ntiles, int ts);
 void xg_launch_grad_contract(const double *S, const int2 *tile_ij, long long ntiles, int nt, int ts, const double *x,
                              const double *y, const double *alpha, int N, const XgMaternParams &mp, int kernel,
                              int metric, double dlogcon, double *part, double *out, cudaStream_t st);
+
+/* assess.cu (Fisher information, MLOE / MMOM) */
+void xg_launch_cross_gen_r(double *D, int mt, int nt, int ts, const double *xm, const double *ym, int nmiss,
+                           const double *xo, const double *yo, int nobs, const XgMaternParams &p, int metric,
+                           cudaStream_t st);
+void xg_launch_tile_transpose(double *D, long long ntiles, int ts, cudaStream_t st);
+void xg_launch_mloe_terms(const double *A, const double *U, const double *T, const double *V, int mt, int nt, int ts,
+                          int nmiss, double sigma2_t, double sigma2_a, double *terms, cudaStream_t st);
+void xg_launch_sym_full(const double *S, double *F, int nt, int ts, cudaStream_t st);
+void xg_launch_dsigma_full(double *D, int nt, int ts, const double *x, const double *y, int N,
+                           const XgMaternParams &p, double dlogcon, int metric, int which, cudaStream_t st);
+void xg_launch_fisher_trace(const double *const g[4], int np, int nt, int ts, int N, double *part, int nctas,
+                            cudaStream_t st);
 
 #endif

@@ -307,6 +307,44 @@ double MORSE_dmle_Predict_Tile(MLE_data *data, double *theta, int nZmiss, int nZ
 void prediction_finalize(MLE_data *data);
 void MLE_Finalize(MLE_data *data);
 
+/* ---- assessment of a fitted model ---- */
+
+/* exageostat_exact/src/include/MLE_exact.h:78-79 (MLE_dexact.c:1777-1934).
+ * Fisher information of the N locations behind data (after
+ * EXAGEOSTAT_dmle_Call) for univariate_matern_stationary at initial_theta:
+ * F_jk = 1/2 tr(Sigma^-1 dSigma_j Sigma^-1 dSigma_k), j, k over (sigma^2,
+ * beta, nu).  Returns a malloc'd array of 10 doubles, the first 9 the
+ * column-major inverse of F (the last 0), as the reference; sets
+ * results.fisher_00/_11/_22 (diagonal of the inverse) and fisher_time.
+ * NULL on an error (non-positive-definite Sigma or F; see exageostat_last_error). */
+double *EXAGEOSTAT_Fisher_Tile(MLE_data *data, int N, double *initial_theta, int dts, int p_grid, int q_grid);
+
+/* src/include/MLE.h:71-72 (src/compute/MLE.c:309-320 -> MLE_dexact.c:1002-1107):
+ * allocates the MLOE / MMOM workspace for nZmiss missing and nZobs observed
+ * locations and sets data->mloe = data->mmom = 0. */
+void mloe_mmom_init(MLE_data *data, int nZmiss, int nZobs, int ts, int p_grid, int q_grid);
+void EXAGEOSTAT_dmle_mloe_mmom_Allocate(MLE_data *data, int nZmiss, int nZobs, int dts, int p_grid, int q_grid);
+
+/* exageostat_exact/src/include/MLE_exact.h:72-76 (MLE_dexact.c:1109-1434 and
+ * :1437-1774).  Mean loss of efficiency and mean misspecification of the
+ * mean square error of kriging the locations data->lmiss from data->lobs
+ * with estimated_theta when truth_theta is the truth:
+ *   MLOE = mean_m (E_t[err_a^2] / E_t[err_t^2] - 1),
+ *   MMOM = mean_m (E_a[err_a^2] / E_t[err_a^2] - 1).
+ * Results in data->mloe, data->mmom, results.mloe / mmom and the
+ * results.*_mloe_mmom_* times.  Each call computes both afresh (the reference
+ * adds to the previous values of data->mloe / mmom).  The two entry points
+ * are one computation (all missing points in one batch of tile solves). */
+void EXAGEOSTAT_dmle_mloe_mmom_Tile(MLE_data *data, double *truth_theta, double *estimated_theta, int nZmiss,
+                                    int nZobs, int n);
+void EXAGEOSTAT_dmle_mloe_mmom_Tile_Async(MLE_data *data, double *truth_theta, double *estimated_theta, int nZmiss,
+                                          int nZobs, int n);
+
+/* src/compute/MLE.c:323-337; src/include/MLE.h:74 declares it as
+ * MLOE_MMOM_Finalize, which is exported too. */
+void mloe_mmom_finalize(MLE_data *data);
+void MLOE_MMOM_Finalize(MLE_data *data);
+
 /* ---- host-side synthetic data helpers (misc/include/MLE_misc.h) ---- */
 
 /* misc/compute/MLE_misc.c:763-792: srand(seed), jittered ceil(sqrt(n))^2
@@ -442,6 +480,25 @@ int exageostat_b200_get_profile(MLE_data *data, double *out, int n);
  * on the GPU race and must be serialised by the caller. */
 int exageostat_b200_dmle_device_noalloc(int n, const double *d_x, const double *d_y, const double *d_z,
                                         const double *theta, int kernel, int metric, double *d_out, void *stream);
+
+/* Status-returning Fisher information for data's kernel (3 x 3, or 4 x 4
+ * with the nugget tau^2 last): fisher and fisher_inv (either may be NULL)
+ * receive the row-major matrix and its inverse. */
+int exageostat_b200_fisher(MLE_data *data, const double *theta, double *fisher, double *fisher_inv);
+
+/* One-shot forms on host arrays.  fisher_host: n locations, fisher np x np.
+ * mloe_mmom_host: terms (NULL or 6 doubles per missing point) receives, per
+ * point, expr1 = k_t' K_a^-1 k_a, expr2 = E_t[err_a^2], expr3 = E_t[err_t^2],
+ * expr4 = E_a[err_a^2], loe, mom (the reference's descexpr1..4 after its
+ * geadd steps, MLE_dexact.c:1371-1375, and the per-point terms of
+ * codelet_zmloe_mmom.c:48-60); times (NULL or 4) generation, factorisation,
+ * solves and total seconds. */
+int exageostat_b200_fisher_host(int n, const double *x, const double *y, const double *theta, int kernel, int metric,
+                                int ts, double *fisher);
+int exageostat_b200_mloe_mmom_host(int nmiss, const double *xmiss, const double *ymiss, int nobs, const double *xobs,
+                                   const double *yobs, const double *truth_theta, const double *estimated_theta,
+                                   int kernel, int metric, int ts, double *mloe, double *mmom, double *terms,
+                                   double *times);
 
 /* ---- batches of independent fields (no counterpart in the reference) ----
  * nfields fields with n[f] locations each; x, y, z hold the fields one after

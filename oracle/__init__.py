@@ -45,6 +45,7 @@ def lib():
         L.ora_locations_obs_zsort_inplace.argtypes = [_I, _PD, _PD, _PD]
         L.ora_core_dcmg.argtypes = [_PD, _I, _I, _I, _I, _PD, _PD, _PD, _PD, _PD, _I]
         L.ora_gen_lower_dense.argtypes = [_PD, _I, _PD, _PD, _PD, _I]
+        L.ora_dcmg_deriv.argtypes = [_PD, _I, _I, _I, _I, _PD, _PD, _PD, _PD, _PD, _I]
         L.ora_dlarnv.argtypes = [_I, _I, _PD]
         L.ora_dzvg.argtypes = [_I, _PD, _PD, _PD, _I, _PD, _PD]
         L.ora_dmle.argtypes = [_I, _PD, _PD, _PD, _PD, _I, _PD, _PD, _PD, _PD]
@@ -116,6 +117,104 @@ def covariance_lower(x, y, theta, kernel=0) -> np.ndarray:
     C = np.zeros((N, N))  # column-major buffer; transposed on return
     lib().ora_gen_lower_dense(_p(C), N, _p(x), _p(y), _p(th), int(kernel))
     return C.T.copy()
+
+
+def dcmg_deriv(m, n, m0, n0, x1, y1, x2, y2, theta, which) -> np.ndarray:
+    """dSigma/dtheta_which (0 sigma^2, 1 beta, 2 nu) of the Matern part, an
+    (m, n) block (core_dcmg_matern_dsigma_square / _dbeta / _dnu,
+    exageostat_exact/cpu_core/compute/core_zcmg.c:315-488)."""
+    A = np.empty((n, m))
+    x1, y1, x2, y2, th = _f64(x1), _f64(y1), _f64(x2), _f64(y2), _f64(theta)
+    lib().ora_dcmg_deriv(_p(A), m, n, m0, n0, _p(x1), _p(y1), _p(x2), _p(y2), _p(th), int(which))
+    return A.T.copy()
+
+
+def covariance_full(x, y, theta, kernel=0) -> np.ndarray:
+    C = covariance_lower(x, y, theta, kernel)
+    return C + np.tril(C, -1).T
+
+
+def _spd_inverse_as_reference(A):
+    """LAPACKE_dpotrf('L') then two dtrsm on the identity
+    (exageostat_exact/src/compute/MLE_dexact.c:1893-1916)."""
+    from scipy.linalg import solve_triangular
+
+    L = np.linalg.cholesky(A)
+    Y = solve_triangular(L, np.eye(A.shape[0]), lower=True)
+    return solve_triangular(L, Y, lower=True, trans="T")
+
+
+def fisher(x, y, theta, kernel=0):
+    """EXAGEOSTAT_Fisher_Tile (exageostat_exact/src/compute/MLE_dexact.c:1777-1934):
+    C = Sigma(theta) factored; for j <= k: CJ = L^-T L^-1 dSigma_j, CK likewise
+    (two dtrsm each, :1846-1847, :1866-1867), A[k + 3 j] = 1/2 trace(CJ CK) (:1870-1879);
+    then the inverse of A.  kernel 1 adds tau^2 (dSigma = I) as a fourth
+    parameter, which the reference does not have.  Returns (F, F^-1), both
+    symmetric np x np."""
+    from scipy.linalg import solve_triangular
+
+    x, y = _f64(x), _f64(y)
+    N = x.size
+    C = covariance_full(x, y, theta, kernel)
+    L = np.linalg.cholesky(C)
+    D = [dcmg_deriv(N, N, 0, 0, x, y, x, y, theta, j) for j in range(3)]
+    if kernel == 1:
+        D.append(np.eye(N))
+    M = []
+    for Dj in D:
+        T = solve_triangular(L, Dj, lower=True)
+        M.append(solve_triangular(L, T, lower=True, trans="T"))
+    n = len(D)
+    F = np.empty((n, n))
+    for j in range(n):
+        for k in range(j, n):
+            F[j, k] = F[k, j] = 0.5 * np.sum(M[j] * M[k].T)
+    return F, _spd_inverse_as_reference(F)
+
+
+def mloe_mmom(x_miss, y_miss, x_obs, y_obs, truth_theta, estimated_theta, kernel=0):
+    """EXAGEOSTAT_dmle_mloe_mmom_Tile (exageostat_exact/src/compute/MLE_dexact.c:1109-1434)
+    restated with the missing points as columns: K_a, K_t (:1239-1245) and
+    their factors (:1252, :1261); per point k_t, k_a (:1283-1286), the four
+    triangular solves (:1302-1326), expr1 = k_t^T k_a, expr4 = k_a^T k_a,
+    expr3 = k_t^T k_t on the solved vectors (:1334-1350), k_a <- L_t^T k_a and
+    expr2 = k_a^T k_a (:1357-1362), the geadd steps (:1371-1375) and the
+    accumulation of CORE_dmloe_mmom_starpu
+    (exageostat_exact/runtime/starpu/codelets/codelet_zmloe_mmom.c:42-60).
+    Returns (mloe, mmom, terms) with terms[m] = (k_t^T K_a^-1 k_a, expr2,
+    expr3, expr4, loe, mom)."""
+    from scipy.linalg import solve_triangular
+
+    xm, ym, xo, yo = (_f64(a) for a in (x_miss, y_miss, x_obs, y_obs))
+    nobs, nmiss = xo.size, xm.size
+    La = np.linalg.cholesky(covariance_full(xo, yo, estimated_theta, kernel))
+    Lt = np.linalg.cholesky(covariance_full(xo, yo, truth_theta, kernel))
+    kt = core_dcmg(nobs, nmiss, 0, 0, xo, yo, xm, ym, truth_theta, kernel)
+    ka = core_dcmg(nobs, nmiss, 0, 0, xo, yo, xm, ym, estimated_theta, kernel)
+    kttmp, katmp = kt.copy(), ka.copy()
+    ka = solve_triangular(La, ka, lower=True)
+    kt = solve_triangular(Lt, kt, lower=True)
+    ka = solve_triangular(La, ka, lower=True, trans="T")
+    kt = solve_triangular(Lt, kt, lower=True, trans="T")
+    e1 = np.sum(kttmp * ka, axis=0)
+    e4 = np.sum(katmp * ka, axis=0)
+    e3 = np.sum(kttmp * kt, axis=0)
+    ka = Lt.T @ ka
+    e2 = np.sum(ka * ka, axis=0)
+    t0, a0 = float(truth_theta[0]), float(estimated_theta[0])
+    expr1 = t0 - 2.0 * e1
+    expr2 = expr1 + e2
+    expr3 = t0 - e3
+    expr4 = a0 - e4
+    terms = np.empty((nmiss, 6))
+    mloe = mmom = 0.0
+    for p in range(nmiss):
+        loe = -1.0 if expr3[p] == 0.0 else expr2[p] / expr3[p] - 1.0
+        mom = -1.0 if expr2[p] == 0.0 else expr4[p] / expr2[p] - 1.0
+        mloe += loe
+        mmom += mom
+        terms[p] = (e1[p], expr2[p], expr3[p], expr4[p], loe, mom)
+    return mloe / nmiss, mmom / nmiss, terms
 
 
 def dlarnv(seed: int, n: int) -> np.ndarray:

@@ -17,6 +17,8 @@
  *   - core_dmdet           exageostat_exact/cpu_core/compute/core_zmdet.c:50-59
  *   - EXAGEOSTAT_MLE_dzvg_Tile (Z = L e)   exageostat_exact/src/compute/MLE_dexact.c:25-148
  *   - EXAGEOSTAT_dmle_Tile (log-likelihood) exageostat_exact/src/compute/MLE_dexact.c:231-489
+ *   - core_dcmg_matern_dsigma_square / _dbeta / _dnu and psi
+ *                          exageostat_exact/cpu_core/compute/core_zcmg.c:189-235, 315-488
  *   - EXAGEOSTAT_dmle_Predict_Tile + CORE_dmse_starpu
  *                          exageostat_exact/src/compute/MLE_dexact.c:688-874,
  *                          exageostat_exact/runtime/starpu/codelets/codelet_zmse.c:22-38
@@ -427,6 +429,70 @@ void ora_core_dcmg(double *A, int m, int n, int m0, int n0, const double *x1, co
     for (int j = 0; j < n; ++j)
         for (int i = 0; i < m; ++i)
             A[i + (size_t)j * m] = ora_matern_elem(x1[m0 + i], y1[m0 + i], x2[n0 + j], y2[n0 + j], theta, con, kernel);
+}
+
+/* ========================================================================== */
+/* Covariance derivatives: core_dcmg_matern_dsigma_square / _dbeta / _dnu      */
+/* ========================================================================== */
+
+/* psi (digamma) as the reference's series (core_zcmg.c:199-211): upward
+ * recurrence to x >= 7, then the asymptotic expansion of psi(t + 1/2) at
+ * t = x - 1/2 (absolute error below 1e-10). */
+static double ora_psi(double x)
+{
+    double result = 0.0;
+    for (; x < 7; ++x) result -= 1 / x;
+    x -= 1.0 / 2.0;
+    const double xx = 1.0 / x, xx2 = xx * xx, xx4 = xx2 * xx2;
+    return result + log(x) + (1. / 24.) * xx2 - (7.0 / 960.0) * xx4 + (31.0 / 8064.0) * xx4 * xx2 -
+           (127.0 / 30720.0) * xx4 * xx4;
+}
+
+/* dK_nu(x)/dnu.  The reference takes a forward difference with h = 1e-9
+ * (dbessel_nu, core_zcmg.c:228-235), good to ~1e-7 relative; the oracle takes
+ * the 4th-order central difference with h = 2e-4 (truncation ~h^4 log(2/x)^5
+ * and rounding ~eps / h, both near 1e-12 relative for x >= 1e-4).  K_nu is
+ * even in nu, so orders below zero are taken at |nu|. */
+static double ora_dknu_dnu(double nu, double x)
+{
+    const double h = 2e-4;
+    const double kp1 = ora_bessel_knu(nu + h, x), km1 = ora_bessel_knu(fabs(nu - h), x);
+    const double kp2 = ora_bessel_knu(nu + 2 * h, x), km2 = ora_bessel_knu(fabs(nu - 2 * h), x);
+    return (8.0 * (kp1 - km1) - (kp2 - km2)) / (12.0 * h);
+}
+
+/* Derivative `which` (0 sigma^2, 1 beta, 2 nu) of one Matern element,
+ * core_zcmg.c:315-342 (dsigma_square), 453-488 (dbeta, with dbessel_input
+ * :189-191), 380-416 (dnu); zero distance gives 1, 0, 0. */
+static double ora_dmatern_elem(double x1, double y1, double x2, double y2, const double *theta, int which)
+{
+    const double expr = sqrt(pow(x2 - x1, 2) + pow(y2 - y1, 2)) / theta[1];
+    if (expr == 0) return which == 0 ? 1.0 : 0.0;
+    const double nu = theta[2], beta = theta[1], sigma2 = theta[0];
+    const double con = 1.0 / (pow(2, (nu - 1)) * tgamma(nu));
+    const double knu = ora_bessel_knu(nu, expr);
+    if (which == 0) return con * pow(expr, nu) * knu;
+    if (which == 1) {
+        const double dk = nu / expr * knu - ora_bessel_knu(nu + 1, expr);
+        const double beta_expr = -nu / beta * pow(expr, nu) * knu - pow(expr, nu) * dk * expr / beta;
+        return sigma2 * con * beta_expr;
+    }
+    const double g = tgamma(nu);
+    const double nu_expr =
+        -2 * log(2.0) * pow(2, -nu) * 1 / g * pow(expr, nu) * knu +
+        pow(2, 1 - nu) * (-1 / g * ora_psi(nu) * pow(expr, nu) * knu +
+                          1 / g * (pow(expr, nu) * log(expr) * knu + pow(expr, nu) * ora_dknu_dnu(nu, expr)));
+    return sigma2 * nu_expr;
+}
+
+/* A (column-major, lda = m) = dSigma/dtheta_which (l1[m0:m0+m], l2[n0:n0+n]). */
+void ora_dcmg_deriv(double *A, int m, int n, int m0, int n0, const double *x1, const double *y1, const double *x2,
+                    const double *y2, const double *theta, int which)
+{
+#pragma omp parallel for schedule(static)
+    for (int j = 0; j < n; ++j)
+        for (int i = 0; i < m; ++i)
+            A[i + (size_t)j * m] = ora_dmatern_elem(x1[m0 + i], y1[m0 + i], x2[n0 + j], y2[n0 + j], theta, which);
 }
 
 /* Lower triangle (with the diagonal) of the N x N covariance, column-major.

@@ -1,0 +1,93 @@
+"""Assessment oracle (Fisher information, MLOE / MMOM) pinned on CPU, and the
+device element derivatives compiled for the host against it (no GPU).
+
+Pins (the reference has no tests for these routines):
+  * dSigma/dtheta element kernels == central differences of the covariance
+    generator, itself pinned to mpmath through K_nu;
+  * F_{sigma^2 sigma^2} = N / (2 sigma^4) exactly for the Matern kernel
+    (dSigma/dsigma^2 = Sigma / sigma^2);
+  * MLOE = MMOM = 0 when the estimate equals the truth; with only the variance
+    scaled by c, the kriging weights are unchanged, so MLOE = 0 and MMOM = c - 1.
+"""
+import os
+import subprocess
+
+import numpy as np
+import pytest
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+
+
+@pytest.mark.parametrize("theta", [[1.3, 0.1, 0.7], [0.8, 0.05, 1.5], [1.0, 0.2, 0.5]])
+def test_oracle_derivatives_match_covariance_differences(ora, theta):
+    n = 150
+    x, y = ora.generate_xy_loc(n, 1)
+    for j in range(3):
+        D = ora.dcmg_deriv(n, n, 0, 0, x, y, x, y, theta, j)
+        h = 1e-5 * theta[j]
+        tp, tm = list(theta), list(theta)
+        tp[j] += h
+        tm[j] -= h
+        fd = (ora.covariance_full(x, y, tp) - ora.covariance_full(x, y, tm)) / (2 * h)
+        assert np.abs(D - fd).max() / np.abs(D).max() < 1e-8, j
+
+
+def test_oracle_fisher_identities(ora):
+    n = 250
+    x, y = ora.generate_xy_loc(n, 2)
+    theta = [1.3, 0.1, 0.7]
+    F, Finv = ora.fisher(x, y, theta)
+    assert F[0, 0] == pytest.approx(n / (2 * theta[0] ** 2), rel=1e-12)
+    assert np.allclose(F, F.T)
+    assert np.allclose(Finv @ F, np.eye(3), atol=1e-10)
+    F4, F4inv = ora.fisher(x, y, [1.3, 0.1, 0.7, 0.05], kernel=1)
+    assert F4.shape == (4, 4) and np.all(np.linalg.eigvalsh(F4) > 0)
+    assert np.allclose(F4inv @ F4, np.eye(4), atol=1e-9)
+
+
+def test_oracle_mloe_mmom_identities(ora):
+    x, y = ora.generate_xy_loc(300, 4)
+    xo, yo, xm, ym = x[:240], y[:240], x[240:], y[240:]
+    theta = [1.3, 0.1, 0.7]
+    mloe, mmom, terms = ora.mloe_mmom(xm, ym, xo, yo, theta, theta)
+    assert abs(mloe) < 1e-12 and abs(mmom) < 1e-12
+    c = 2.5
+    mloe, mmom, _ = ora.mloe_mmom(xm, ym, xo, yo, theta, [c * theta[0], theta[1], theta[2]])
+    assert abs(mloe) < 1e-12 and mmom == pytest.approx(c - 1, abs=1e-12)
+    mloe, mmom, terms = ora.mloe_mmom(xm, ym, xo, yo, theta, [1.0, 0.05, 0.5])
+    assert mloe > 0 and terms.shape == (60, 6)
+    assert np.all(terms[:, 2] > 0) and np.all(terms[:, 1] >= terms[:, 2] * (1 - 1e-12))
+
+
+def test_device_element_derivatives_match_oracle(ora, tmp_path):
+    """xg_matern_grad (kbessel.cuh, host/device code) compiled with g++ against
+    the oracle's restatement of the reference derivative kernels."""
+    from scipy.special import digamma
+
+    src = tmp_path / "dm.cpp"
+    src.write_text('#include <cstdio>\n#include <cmath>\n#include "kbessel.cuh"\n'
+                   'int main(){double r,nu,s2,b,dl;while(scanf("%lf %lf %lf %lf %lf",&r,&nu,&s2,&b,&dl)==5){'
+                   'double con=s2/(pow(2.0,nu-1)*tgamma(nu));double m,ds,db,dn;'
+                   'xg_matern_grad(r,nu,con,s2,b,dl,&m,&ds,&db,&dn);printf("%.17g %.17g %.17g\\n",ds,db,dn);}}\n')
+    exe = tmp_path / "dm"
+    subprocess.run(["g++", "-O2", "-I", os.path.join(ROOT, "exageostat_b200", "csrc"), str(src), "-o", str(exe)],
+                   check=True)
+    rows, ref = [], []
+    for nu in (0.3, 0.5, 0.73, 1.0, 1.5, 2.5, 4.0):
+        for beta in (0.05, 0.1, 0.3):
+            th = [1.3, beta, nu]
+            d = np.geomspace(1e-4, 3.0, 25)
+            x1, y1 = np.zeros(1), np.zeros(1)
+            for j in range(3):
+                ref.append(ora.dcmg_deriv(1, d.size, 0, 0, x1, y1, d, np.zeros(d.size), th, j)[0])
+            dl = -(np.log(2.0) + digamma(nu))
+            rows += ["%r %r %r %r %r" % (float(dd / beta), nu, th[0], beta, float(dl)) for dd in d]
+    out = subprocess.run([str(exe)], input="\n".join(rows), capture_output=True, text=True, check=True).stdout
+    got = np.array(out.split(), dtype=float).reshape(-1, 3)
+    want = np.concatenate([np.stack(ref[i:i + 3], axis=1) for i in range(0, len(ref), 3)])
+    scale = np.abs(want).max(axis=0)
+    err = np.abs(got - want).max(axis=0) / scale
+    # the oracle's nu derivative (the reference's psi series, a central
+    # difference of K_nu) is good to ~7e-10 of the largest entry; the device
+    # function agrees with mpmath to ~1e-13
+    assert np.all(err < 2e-9), err
