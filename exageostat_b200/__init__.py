@@ -110,7 +110,8 @@ EXPORTED_SYMBOLS = [
     "exageostat_b200_batch_autotune", "EXAGEOSTAT_Fisher_Tile", "exageostat_b200_fisher",
     "exageostat_b200_fisher_host", "mloe_mmom_init", "EXAGEOSTAT_dmle_mloe_mmom_Allocate",
     "EXAGEOSTAT_dmle_mloe_mmom_Tile", "EXAGEOSTAT_dmle_mloe_mmom_Tile_Async", "mloe_mmom_finalize",
-    "MLOE_MMOM_Finalize", "exageostat_b200_mloe_mmom_host", "results",
+    "MLOE_MMOM_Finalize", "exageostat_b200_mloe_mmom_host", "countlines", "readLocsFile", "readLocsFile3d",
+    "readObsFile", "readTimeFile", "results",
 ]
 
 _lib = None
@@ -178,6 +179,11 @@ def lib():
         "exageostat_b200_batch_autotune": (_I, [_I, ctypes.POINTER(_I), _PD, _PD, _PD, _I, _I, _PD,
                                                 ctypes.POINTER(_I), _PD, ctypes.POINTER(_VP)]),
         "EXAGEOSTAT_Fisher_Tile": (_PD, [PM, _I, _PD, _I, _I, _I]),
+        "countlines": (_I, [_CP]),
+        "readLocsFile": (ctypes.POINTER(Location), [_CP, _I]),
+        "readLocsFile3d": (ctypes.POINTER(Location), [_CP, _I]),
+        "readObsFile": (_PD, [_CP, _I]),
+        "readTimeFile": (_PD, [_CP, _I]),
         "exageostat_b200_fisher": (_I, [PM, _PD, _PD, _PD]),
         "exageostat_b200_fisher_host": (_I, [_I, _PD, _PD, _PD, _I, _I, _I, _PD]),
         "mloe_mmom_init": (None, [PM, _I, _I, _I, _I, _I]),
@@ -300,6 +306,57 @@ def sliced_factor_dense(x, y, theta, kernel=0, metric=0, ts=0) -> np.ndarray:
     _check(lib().exageostat_b200_sliced_factor_dense(n, _p(x), _p(y), _p(_f64(theta)), kernel, metric, ts,
                                                      _p(out)))
     return out
+
+
+def _take_malloced(p, n) -> np.ndarray:
+    """Copies n doubles from a library-malloc'd array and frees it."""
+    out = np.ctypeslib.as_array(p, shape=(n,)).copy()
+    _libc().free(ctypes.cast(p, ctypes.c_void_p))
+    return out
+
+
+_libc_handle = None
+
+
+def _libc():
+    global _libc_handle
+    if _libc_handle is None:
+        _libc_handle = ctypes.CDLL(None)
+        _libc_handle.free.argtypes = [ctypes.c_void_p]
+        _libc_handle.free.restype = None
+    return _libc_handle
+
+
+def countlines(path: str) -> int:
+    """countlines (misc/compute/MLE_misc.c:965-985): '\n' characters in the file."""
+    return int(lib().countlines(os.fsencode(path)))
+
+
+def read_locs_file(path: str, n: int | None = None, dims: int = 2):
+    """readLocsFile / readLocsFile3d (misc/compute/flat_file.c:23-111): n rows
+    (default countlines(path)) of "x,y" (dims 2) or "x,y,z" (dims 3); returns
+    (x, y) or (x, y, z)."""
+    n = countlines(path) if n is None else int(n)
+    fn = lib().readLocsFile3d if dims == 3 else lib().readLocsFile
+    p = fn(os.fsencode(path), n)
+    if not p:
+        raise XgError(XG_ERR_BAD_ARGUMENT, "cannot read %d locations from %s" % (n, path))
+    loc = p.contents
+    cols = [_take_malloced(loc.x, n), _take_malloced(loc.y, n)]
+    if dims == 3:
+        cols.append(_take_malloced(loc.z, n))
+    _libc().free(ctypes.cast(p, ctypes.c_void_p))
+    return tuple(cols)
+
+
+def read_obs_file(path: str, n: int | None = None, time: bool = False) -> np.ndarray:
+    """readObsFile / readTimeFile (misc/compute/flat_file.c:115-171): n values,
+    one per line (default countlines(path))."""
+    n = countlines(path) if n is None else int(n)
+    p = (lib().readTimeFile if time else lib().readObsFile)(os.fsencode(path), n)
+    if not p:
+        raise XgError(XG_ERR_BAD_ARGUMENT, "cannot read %d values from %s" % (n, path))
+    return _take_malloced(p, n)
 
 
 def fisher_host(x, y, theta, kernel=0, metric=0, ts=0) -> np.ndarray:

@@ -3,8 +3,11 @@
  * (misc/compute/MLE_misc.c).  They consume the libc rand() stream in the
  * reference's order, so a driver that calls GenerateXYLoc(N, seed) and later
  * pick_random_points() sees the same locations and the same hold-out split.
+ * Also the real-data flat-file readers of the reference's CSV drivers
+ * (misc/compute/flat_file.c, countlines in misc/compute/MLE_misc.c).
  */
 #include <math.h>
+#include <stdio.h>
 #include <stdint.h>
 #include <stdlib.h>
 #include <string.h>
@@ -184,3 +187,125 @@ extern "C" void pick_random_points(MLE_data *data, double *Zobs, double *Zactual
     locations_obs_zsort_inplace(nZobs, &data->lobs, Zobs);
     locations_obs_zsort_inplace(nZmiss, &data->lmiss, Zactual);
 }
+
+/* ------------------------------------------------------------------------- */
+/* real-data flat files (misc/compute/flat_file.c, misc/compute/MLE_misc.c)  */
+/* ------------------------------------------------------------------------- */
+
+/* MLE_misc.c:965-985: the number of '\n' characters in the file (so a last
+ * line without a newline is not counted), 0 if it cannot be opened. */
+extern "C" int countlines(char *filename)
+{
+    FILE *fp = fopen(filename, "r");
+    if (!fp) {
+        fprintf(stderr, "cannot open locations file\n");
+        return 0;
+    }
+    int lines = 0, ch;
+    while ((ch = fgetc(fp)) != EOF)
+        if (ch == '\n') ++lines;
+    fclose(fp);
+    return lines;
+}
+
+/* Reads n rows of nf comma-separated numbers (the field values the
+ * reference's strtok + atof loop takes, flat_file.c:38-45) into cols[0..nf).
+ * Blank lines are skipped.  Unlike the reference, which writes past the n
+ * entries it allocated when the file is longer and dereferences NULL on a
+ * short line, reading stops after n rows and a short, missing or malformed
+ * row is an error.  Returns 0, or -1 with a message. */
+static int xg_read_rows(const char *path, int n, int nf, double **cols, const char *who)
+{
+    FILE *fp = fopen(path, "r");
+    if (!fp) {
+        fprintf(stderr, "%s: cannot open %s\n", who, path);
+        return -1;
+    }
+    char *line = nullptr;
+    size_t cap = 0;
+    int row = 0, lineno = 0, rc = 0;
+    while (row < n && getline(&line, &cap, fp) != -1) {
+        ++lineno;
+        const char *p = line;
+        while (*p == ' ' || *p == '\t' || *p == '\r' || *p == '\n') ++p;
+        if (!*p) continue;
+        for (int f = 0; f < nf; ++f) {
+            char *end = nullptr;
+            const double v = strtod(p, &end);
+            if (end == p) {
+                fprintf(stderr, "%s: %s line %d: expected %d comma-separated numbers\n", who, path, lineno, nf);
+                rc = -1;
+                break;
+            }
+            cols[f][row] = v;
+            p = end;
+            if (f + 1 < nf) {
+                while (*p == ' ' || *p == '\t') ++p;
+                if (*p != ',') {
+                    fprintf(stderr, "%s: %s line %d: expected %d comma-separated numbers\n", who, path, lineno, nf);
+                    rc = -1;
+                    break;
+                }
+                ++p;
+            }
+        }
+        if (rc) break;
+        ++row;
+    }
+    free(line);
+    fclose(fp);
+    if (!rc && row < n) {
+        fprintf(stderr, "%s: %s holds %d rows, %d requested\n", who, path, row, n);
+        rc = -1;
+    }
+    return rc;
+}
+
+static location *xg_read_locations(char *path, int n, int dims, const char *who)
+{
+    if (n <= 0) {
+        fprintf(stderr, "%s: n = %d\n", who, n);
+        return nullptr;
+    }
+    location *l = (location *)calloc(1, sizeof(location));
+    double *cols[3] = {nullptr, nullptr, nullptr};
+    for (int f = 0; f < dims && l; ++f) cols[f] = (double *)malloc((size_t)n * sizeof(double));
+    bool ok = l != nullptr;
+    for (int f = 0; f < dims; ++f) ok = ok && cols[f] != nullptr;
+    if (ok && xg_read_rows(path, n, dims, cols, who) == 0) {
+        l->x = cols[0];
+        l->y = cols[1];
+        l->z = cols[2];
+        return l;
+    }
+    for (int f = 0; f < dims; ++f) free(cols[f]);
+    free(l);
+    return nullptr;
+}
+
+/* flat_file.c:23-64: n two-column rows "x,y" -> a malloc'd location (z = NULL). */
+extern "C" location *readLocsFile(char *locs_file, int n) { return xg_read_locations(locs_file, n, 2, "readLocsFile"); }
+
+/* flat_file.c:68-111: n rows "x,y,z". */
+extern "C" location *readLocsFile3d(char *locs_file, int n)
+{
+    return xg_read_locations(locs_file, n, 3, "readLocsFile3d");
+}
+
+static double *xg_read_column(char *path, int n, const char *who)
+{
+    if (n <= 0) {
+        fprintf(stderr, "%s: n = %d\n", who, n);
+        return nullptr;
+    }
+    double *v = (double *)malloc((size_t)n * sizeof(double));
+    if (v && xg_read_rows(path, n, 1, &v, who) == 0) return v;
+    free(v);
+    return nullptr;
+}
+
+/* flat_file.c:115-142: one value per line. */
+extern "C" double *readObsFile(char *obsfile, int n) { return xg_read_column(obsfile, n, "readObsFile"); }
+
+/* flat_file.c:146-171: one time value per line (space-time data). */
+extern "C" double *readTimeFile(char *timefile, int n) { return xg_read_column(timefile, n, "readTimeFile"); }

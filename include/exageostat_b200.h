@@ -363,6 +363,19 @@ int locations_obs_zsort_inplace(int n, location *locations, double *z);
  * at offset nZmiss, as in the reference. */
 void pick_random_points(MLE_data *data, double *Zobs, double *Zactual, int nZmiss, int nZobs, int N);
 
+/* ---- real-data flat files (misc/include/flat_file.h:25-31, MLE_misc.h:382) ----
+ * countlines: the number of '\n' characters of the file (0 if it cannot be
+ * opened).  The readers take n rows of comma-separated numbers ("x,y",
+ * "x,y,z", or one value per line) into malloc'd arrays the caller frees;
+ * blank lines are skipped.  They return NULL with a message on a missing
+ * file, a short or malformed row, or fewer than n rows (the reference
+ * writes past its arrays on a longer file and crashes on a short row). */
+int countlines(char *filename);
+location *readLocsFile(char *locs_file, int n);
+location *readLocsFile3d(char *locs_file, int n);
+double *readObsFile(char *obsfile, int n);
+double *readTimeFile(char *timefile, int n);
+
 /* ---- MLE driver ---- */
 
 /* Bound-constrained derivative-free maximiser standing in for NLopt's
