@@ -25,8 +25,8 @@
  *   tile solves (an "R layout" matrix: one row per missing point, tile (R, K)
  *   at slot K mt + R), so the work runs on the FP64 tensor cores:
  *     A = L_a^-1 k_a,  U = L_a^-1 k_t,  T = L_t^-1 k_t      (forward solves)
- *     W = L_a^-T A = K_a^-1 k_a                               (A times the inverse factor)
- *     V = L_t^T W                                            (triangular product)
+ *     W = L_a^-T A = K_a^-1 k_a        (backward solve on L_a's tiles transposed in place)
+ *     V = L_t^T W                      (triangular product with L_t's tiles transposed in place)
  *   and per missing point (one reduction kernel)
  *     expr1 = U.A,  expr2 = sigma_t^2 - 2 expr1 + V.V,
  *     expr3 = sigma_t^2 - T.T,  expr4 = sigma_a^2 - A.A,
@@ -472,7 +472,6 @@ void xg_assess_destroy(XgAssess *q)
     if (!q) return;
     xg_tm_free(q->Ca);
     xg_tm_free(q->Ct);
-    xg_tm_free(q->X);
     for (int i = 0; i < 5; ++i) cudaFree(q->R[i]);
     cudaFree(q->xo);
     cudaFree(q->yo);
@@ -510,7 +509,6 @@ int xg_assess_create(XgAssess **out, int nmiss, int nobs, int ts)
     q->ts = xg_choose_ts(nobs, ts);
     rc = xg_tm_alloc(q->Ca, nobs, q->ts);
     if (!rc) rc = xg_tm_alloc(q->Ct, nobs, q->ts);
-    if (!rc) rc = xg_tm_alloc(q->X, nobs, q->ts);
     q->nt = q->Ca.nt;
     q->mt = (nmiss + q->ts - 1) / q->ts;
     const long long rtiles = (long long)q->mt * q->nt;
@@ -582,8 +580,10 @@ int xg_assess_run(XgAssess *q, const double *truth, const double *est, int kerne
     xg_launch_rhs_forward_solve(q->mR[0], RA, mt, q->Ca.map, q->Ca.d, nt, ts, q->status, st); /* A = L_a^-1 k_a */
     xg_launch_rhs_forward_solve(q->mR[1], RU, mt, q->Ca.map, q->Ca.d, nt, ts, q->status, st); /* U = L_a^-1 k_t */
     xg_launch_rhs_forward_solve(q->mR[2], RT, mt, q->Ct.map, q->Ct.d, nt, ts, q->status, st); /* T = L_t^-1 k_t */
-    xg_launch_inverse_factor(q->X.map, q->Ca.map, q->X.d, q->Ca.d, nt, ts, q->status, st);    /* X = L_a^-T */
-    xg_launch_rhs_tri_product(q->mR[0], q->X.map, RW, mt, nt, ts, q->status, st);               /* W = X A */
+    /* W = L_a^-T A: the factor's tiles transposed in place, then the backward solve */
+    XG_ACU(cudaMemcpyAsync(RW, RA, rbytes, cudaMemcpyDeviceToDevice, st));
+    xg_launch_tile_transpose(q->Ca.d, q->Ca.ntiles, ts, st);
+    xg_launch_rhs_backward_solve(q->mR[3], RW, mt, q->Ca.map, q->Ca.d, nt, ts, q->status, st);
     xg_launch_tile_transpose(q->Ct.d, q->Ct.ntiles, ts, st);
     xg_launch_rhs_tri_product(q->mR[3], q->Ct.map, RV, mt, nt, ts, q->status, st); /* V = L_t^T W */
     xg_launch_mloe_terms(RA, RU, RT, RV, mt, nt, ts, nmiss, truth[0], est[0], q->terms, st);

@@ -48,6 +48,8 @@
 #define XG_TG_RFWD 3    /* step K of Y L^T = B (R layout): B(R, K') -= Y(R, K) L_slot(K', K)^T, K' > K */
 #define XG_TG_RTRI 4    /* C(R, I) = sum_{K >= I} A(R, K) B_slot(K, I)^T (R layout, B lower-tile packed) */
 #define XG_TG_DENSE 5   /* full nt x nt tiles (slot A nt + B): C(A, B) = sum_K A(A, K) B(B, K)^T */
+#define XG_TG_RBWD 6    /* step K of Z L = B (R layout), B holding L's tiles transposed in place:
+                           B(R, K') -= Z(R, K) B_slot(K, K')^T, K' < K */
 
 struct XgTileGemmJob {
     int c_slot;  /* packed slot of the output tile */
@@ -79,6 +81,13 @@ __device__ inline XgTileGemmJob xg_tg_decode(int mode, long long job, int nt, in
         j.b_slot0 = (int)xg_tile_index(I, I, nt);
         j.k_step_b = 1;
         j.ntiles_k = nt - I;
+    } else if (mode == XG_TG_RBWD) {
+        const int R = (int)(job % mt), Kp = (int)(job / mt);
+        j.c_slot = Kp * mt + R;
+        j.a_slot0 = K * mt + R;
+        j.b_slot0 = (int)xg_tile_index(K, Kp, nt);
+        j.ntiles_k = 1;
+        j.k_step_a = j.k_step_b = 0;
     } else if (mode == XG_TG_DENSE) {
         const int A = (int)(job / nt), B = (int)(job % nt);
         j.c_slot = A * nt + B;
@@ -159,7 +168,7 @@ __global__ void __launch_bounds__(XG_TG_THREADS, 1)
     const int g = lane >> 2, tq = lane & 3;
     double *C = Cbase + (long long)J.c_slot * ts * ts + (long long)(bi * XG_TG_BM) * ts + bj * XG_TG_BM;
     double acc[4][4][4];
-    const bool subtract = (mode == XG_TG_XUPDATE || mode == XG_TG_RFWD);
+    const bool subtract = (mode == XG_TG_XUPDATE || mode == XG_TG_RFWD || mode == XG_TG_RBWD);
 #pragma unroll
     for (int mi = 0; mi < 4; ++mi)
 #pragma unroll
@@ -251,7 +260,11 @@ __global__ void __launch_bounds__(XG_TG_THREADS, 1)
 #define XG_XT_SR 32
 
 /* mt == 0: the tiles X_IK, I <= K, at slot (K, I) (inverse factor);
- * mt  > 0: the tiles (R, K), R < mt, of an R-layout matrix (right-hand sides) */
+ * mt  > 0: the tiles (R, K), R < mt, of an R-layout matrix (right-hand sides).
+ * UPPER: the diagonal tile holds U = L_KK^T (a factor transposed in place)
+ * and the solve is B <- B U^-T = B L_KK^-1, by 32-column blocks from the
+ * right (backward substitution). */
+template <bool UPPER>
 __global__ void __launch_bounds__(XG_XT_THREADS) xg_xtrsm_kernel(double *__restrict__ X, const double *__restrict__ Lt,
                                                                  int nt, int ts, int K, int mt, const int *status)
 {
@@ -271,7 +284,8 @@ __global__ void __launch_bounds__(XG_XT_THREADS) xg_xtrsm_kernel(double *__restr
         const int r = idx / ts, c = idx - r * ts;
         S[r * LDS + c] = B[(long long)r * ts + c];
     }
-    for (int cb = 0; cb < ts; cb += 32) {
+    for (int blk = 0; blk < ts / 32; ++blk) {
+        const int cb = UPPER ? ts - 32 * (blk + 1) : 32 * blk;
         for (int idx = tid; idx < 32 * 32; idx += blockDim.x) {
             const int r = idx >> 5, c = idx & 31;
             LD[r * 33 + c] = L[(long long)(cb + r) * ts + cb + c];
@@ -281,20 +295,32 @@ __global__ void __launch_bounds__(XG_XT_THREADS) xg_xtrsm_kernel(double *__restr
             double row[32];
 #pragma unroll
             for (int j = 0; j < 32; ++j) row[j] = S[lane * LDS + cb + j];
+            if (UPPER) {
 #pragma unroll
-            for (int j = 0; j < 32; ++j) {
-                double s = row[j];
+                for (int j = 31; j >= 0; --j) {
+                    double s = row[j];
 #pragma unroll
-                for (int q = 0; q < j; ++q) s -= row[q] * LD[j * 33 + q];
-                row[j] = s / LD[j * 33 + j];
+                    for (int q = j + 1; q < 32; ++q) s -= row[q] * LD[j * 33 + q];
+                    row[j] = s / LD[j * 33 + j];
+                }
+            } else {
+#pragma unroll
+                for (int j = 0; j < 32; ++j) {
+                    double s = row[j];
+#pragma unroll
+                    for (int q = 0; q < j; ++q) s -= row[q] * LD[j * 33 + q];
+                    row[j] = s / LD[j * 33 + j];
+                }
             }
 #pragma unroll
             for (int j = 0; j < 32; ++j) S[lane * LDS + cb + j] = row[j];
         }
         __syncthreads();
-        const int ngrp = (ts - cb - 32) / 32;
+        /* the solved block's contribution to the columns still to solve:
+         * right of it (lower) or left of it (upper) */
+        const int ngrp = UPPER ? cb / 32 : (ts - cb - 32) / 32;
         for (int grp = warp; grp < ngrp; grp += XG_XT_THREADS / 32) {
-            const int c0 = cb + 32 + grp * 32;
+            const int c0 = UPPER ? grp * 32 : cb + 32 + grp * 32;
             double acc[2][4][4];
 #pragma unroll
             for (int mi = 0; mi < 2; ++mi)
@@ -439,7 +465,10 @@ cudaError_t xg_gradient_kernels_configure()
     cudaError_t e = cudaFuncSetAttribute(xg_tile_gemm_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                          (int)xg_tile_gemm_smem_bytes());
     if (e != cudaSuccess) return e;
-    return cudaFuncSetAttribute(xg_xtrsm_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+    e = cudaFuncSetAttribute(xg_xtrsm_kernel<false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             (int)xg_xtrsm_smem_bytes(XG_MAX_TS));
+    if (e != cudaSuccess) return e;
+    return cudaFuncSetAttribute(xg_xtrsm_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                 (int)xg_xtrsm_smem_bytes(XG_MAX_TS));
 }
 
@@ -452,7 +481,7 @@ void xg_launch_inverse_factor(const CUtensorMap &mapX, const CUtensorMap &mapL, 
     xg_identity_diag_kernel<<<dim3(1, nt), 256, 0, st>>>(X, nt, ts);
     const int bpt = ts / XG_TG_BM;
     for (int K = 0; K < nt; ++K) {
-        xg_xtrsm_kernel<<<(K + 1) * (ts / XG_XT_SR), XG_XT_THREADS, xg_xtrsm_smem_bytes(ts), st>>>(X, L, nt, ts, K, 0,
+        xg_xtrsm_kernel<false><<<(K + 1) * (ts / XG_XT_SR), XG_XT_THREADS, xg_xtrsm_smem_bytes(ts), st>>>(X, L, nt, ts, K, 0,
                                                                                                  status);
         const long long jobs = (long long)(K + 1) * (nt - K - 1);
         if (jobs > 0)
@@ -470,7 +499,7 @@ void xg_launch_identity_x(double *X, int nt, int ts, cudaStream_t st)
 
 void xg_launch_xtrsm(double *X, const double *L, int nt, int ts, int K, int *status, cudaStream_t st)
 {
-    xg_xtrsm_kernel<<<(K + 1) * (ts / XG_XT_SR), XG_XT_THREADS, xg_xtrsm_smem_bytes(ts), st>>>(X, L, nt, ts, K, 0,
+    xg_xtrsm_kernel<false><<<(K + 1) * (ts / XG_XT_SR), XG_XT_THREADS, xg_xtrsm_smem_bytes(ts), st>>>(X, L, nt, ts, K, 0,
                                                                                              status);
 }
 
@@ -510,12 +539,29 @@ void xg_launch_rhs_forward_solve(const CUtensorMap &mapR, double *R, int mt, con
 {
     const int bpt = ts / XG_TG_BM;
     for (int K = 0; K < nt; ++K) {
-        xg_xtrsm_kernel<<<mt * (ts / XG_XT_SR), XG_XT_THREADS, xg_xtrsm_smem_bytes(ts), st>>>(R, L, nt, ts, K, mt,
+        xg_xtrsm_kernel<false><<<mt * (ts / XG_XT_SR), XG_XT_THREADS, xg_xtrsm_smem_bytes(ts), st>>>(R, L, nt, ts, K, mt,
                                                                                             status);
         const long long jobs = (long long)mt * (nt - K - 1);
         if (jobs > 0)
             xg_tile_gemm_kernel<<<(unsigned)(jobs * bpt * bpt), XG_TG_THREADS, xg_tile_gemm_smem_bytes(), st>>>(
                 mapR, mapL, R, nt, ts, XG_TG_RFWD, K, mt, status);
+    }
+}
+
+/* Z L = B for an R-layout right-hand side B and a factor whose tiles were
+ * transposed in place (LT: slot (i, j) holds L_ij^T), left-looking from the
+ * last tile column: B is overwritten with Z, the transpose of L^-T B^T. */
+void xg_launch_rhs_backward_solve(const CUtensorMap &mapR, double *R, int mt, const CUtensorMap &mapLT,
+                                  const double *LT, int nt, int ts, int *status, cudaStream_t st)
+{
+    const int bpt = ts / XG_TG_BM;
+    for (int K = nt - 1; K >= 0; --K) {
+        xg_xtrsm_kernel<true><<<mt * (ts / XG_XT_SR), XG_XT_THREADS, xg_xtrsm_smem_bytes(ts), st>>>(R, LT, nt, ts, K,
+                                                                                                 mt, status);
+        const long long jobs = (long long)mt * K;
+        if (jobs > 0)
+            xg_tile_gemm_kernel<<<(unsigned)(jobs * bpt * bpt), XG_TG_THREADS, xg_tile_gemm_smem_bytes(), st>>>(
+                mapR, mapLT, R, nt, ts, XG_TG_RBWD, K, mt, status);
     }
 }
 

@@ -152,12 +152,12 @@ int xg_predict_run(XgPredict *q, const double *theta, int kernel, int metric, co
                    const double *xo, const double *yo, const double *zobs, const double *zactual, double *zmiss,
                    double *mse);
 
-/* MLOE / MMOM workspace (assess.cu): the two observed-set factors, the
- * inverse factor, and five R-layout right-hand-side stores (one row per
- * missing point): k_a -> A, k_t -> U, k_t -> T, W, V. */
+/* MLOE / MMOM workspace (assess.cu): the two observed-set factors and five
+ * R-layout right-hand-side stores (one row per missing point): k_a -> A,
+ * k_t -> U, k_t -> T, W, V. */
 struct XgAssess {
     int nmiss = 0, nobs = 0, ts = 0, nt = 0, mt = 0;
-    XgTileMatrix Ca, Ct, X;
+    XgTileMatrix Ca, Ct;
     double *R[5] = {nullptr, nullptr, nullptr, nullptr, nullptr};
     CUtensorMap mR[5];
     double *xo = nullptr, *yo = nullptr, *xm = nullptr, *ym = nullptr;

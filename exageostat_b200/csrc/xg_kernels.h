@@ -195,6 +195,8 @@ void xg_launch_identity_x(double *X, int nt, int ts, cudaStream_t st);
 void xg_launch_xtrsm(double *X, const double *L, int nt, int ts, int K, int *status, cudaStream_t st);
 void xg_launch_rhs_forward_solve(const CUtensorMap &mapR, double *R, int mt, const CUtensorMap &mapL, const double *L,
                                  int nt, int ts, int *status, cudaStream_t st);
+void xg_launch_rhs_backward_solve(const CUtensorMap &mapR, double *R, int mt, const CUtensorMap &mapLT,
+                                  const double *LT, int nt, int ts, int *status, cudaStream_t st);
 void xg_launch_rhs_tri_product(const CUtensorMap &mapA, const CUtensorMap &mapB, double *C, int mt, int nt, int ts,
                                int *status, cudaStream_t st);
 void xg_launch_dense_gemm_nt(const CUtensorMap &mapA, const CUtensorMap &mapB, double *C, int nt, int ts, int *status,
