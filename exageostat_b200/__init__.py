@@ -242,7 +242,14 @@ def finalize() -> None:
     lib().exageostat_finalize()
 
 
-KERNELS = {0: b"univariate_matern_stationary", 1: b"univariate_matern_nuggets_stationary"}
+KERNELS = {0: b"univariate_matern_stationary", 1: b"univariate_matern_nuggets_stationary",
+           2: b"bivariate_matern_parsimonious"}
+NPARAMS = {0: 3, 1: 4, 2: 6}
+
+
+def _dim(x, kernel) -> int:
+    """Matrix dimension: the locations, times 2 for the bivariate kernel."""
+    return x.size * (2 if kernel == 2 else 1)
 
 
 def bessel_knu(nu, x) -> np.ndarray:
@@ -264,7 +271,7 @@ def matern_pairs(x1, y1, x2, y2, theta, kernel=0, metric=0) -> np.ndarray:
 
 def covariance_dense(x, y, theta, kernel=0, metric=0, ts=0, factor=False) -> np.ndarray:
     x, y = _f64(x), _f64(y)
-    n = x.size
+    n = _dim(x, kernel)
     out = np.empty((n, n))
     _check(lib().exageostat_b200_covariance_dense(n, _p(x), _p(y), _p(_f64(theta)), kernel, metric, ts,
                                                   1 if factor else 0, _p(out)))
@@ -294,14 +301,14 @@ def dmle_host_sliced(x, y, z, theta, kernel=0, metric=0, ts=0):
     updates: (loglik, logdet, dotp)."""
     x, y, z = _f64(x), _f64(y), _f64(z)
     out = np.empty(3)
-    _check(lib().exageostat_b200_dmle_host_sliced(x.size, _p(x), _p(y), _p(z), _p(_f64(theta)), kernel, metric, ts,
+    _check(lib().exageostat_b200_dmle_host_sliced(z.size, _p(x), _p(y), _p(z), _p(_f64(theta)), kernel, metric, ts,
                                                   _p(out)))
     return tuple(out)
 
 
 def sliced_factor_dense(x, y, theta, kernel=0, metric=0, ts=0) -> np.ndarray:
     x, y = _f64(x), _f64(y)
-    n = x.size
+    n = _dim(x, kernel)
     out = np.empty((n, n))
     _check(lib().exageostat_b200_sliced_factor_dense(n, _p(x), _p(y), _p(_f64(theta)), kernel, metric, ts,
                                                      _p(out)))
@@ -388,7 +395,7 @@ def dmle_host(x, y, z, theta, kernel=0, metric=0, ts=0):
     """One-shot log-likelihood on host arrays: (loglik, logdet, dotp)."""
     x, y, z = _f64(x), _f64(y), _f64(z)
     out = np.empty(3)
-    _check(lib().exageostat_b200_dmle_host(x.size, _p(x), _p(y), _p(z), _p(_f64(theta)), kernel, metric, ts,
+    _check(lib().exageostat_b200_dmle_host(z.size, _p(x), _p(y), _p(z), _p(_f64(theta)), kernel, metric, ts,
                                            _p(out)))
     return tuple(out)
 
@@ -401,9 +408,9 @@ class Session:
                  diag_thick: int = 1):
         self.L = lib()
         self.x, self.y = _f64(x).copy(), _f64(y).copy()
-        self.N = self.x.size
+        self.N = _dim(self.x, kernel)
         self.kernel = kernel
-        self.nparams = 4 if kernel == 1 else 3
+        self.nparams = NPARAMS[kernel]
         d = MLEData()
         d.computation = b"exact"
         d.kernel_fun = KERNELS[kernel]

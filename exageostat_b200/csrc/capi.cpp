@@ -39,8 +39,15 @@ static int xg_kernel_of(const MLE_data *data, int *kernel, int *nparams)
         *nparams = 4;
         return XG_OK;
     }
-    return xg_fail(XG_ERR_UNSUPPORTED, "kernel_fun \"%s\" is not supported (univariate_matern_stationary and "
-                                       "univariate_matern_nuggets_stationary are)", k);
+    if (strcmp(k, "bivariate_matern_parsimonious") == 0) {
+        /* N is 2 x the number of locations in data->l1 (synthetic_dmle_test.c:67-69, 134, 153) */
+        *kernel = 2;
+        *nparams = 6;
+        return XG_OK;
+    }
+    return xg_fail(XG_ERR_UNSUPPORTED, "kernel_fun \"%s\" is not supported (univariate_matern_stationary, "
+                                       "univariate_matern_nuggets_stationary and bivariate_matern_parsimonious are)",
+                   k);
 }
 
 static int xg_metric_of(const MLE_data *data)
@@ -237,6 +244,8 @@ extern "C" int exageostat_b200_loglik(MLE_data *data, const double *theta, doubl
     const int band = data->diag_thick > 0 ? data->diag_thick : 1;
     if (mixed && grad)
         return xg_fail(XG_ERR_UNSUPPORTED, "the gradient is computed with precision 0 or 3, not 2");
+    if (kernel == 2 && (mixed || grad))
+        return xg_fail(XG_ERR_UNSUPPORTED, "bivariate_matern_parsimonious: precision 0 or 3 without a gradient");
     if (mixed && (!f->mx || f->mx->band != band)) {
         rc = xg_field_set_mixed(f, band, f->mx ? f->mx->passes : 3);
         if (rc) return rc;
@@ -388,6 +397,11 @@ extern "C" double EXAGEOSTAT_dmle_Predict_Tile(MLE_data *data, double *theta, in
         fprintf(stderr, "EXAGEOSTAT_dmle_Predict_Tile: %s\n", exageostat_last_error());
         return -1;
     }
+    if (kernel == 2) {
+        xg_fail(XG_ERR_UNSUPPORTED, "kriging with bivariate_matern_parsimonious");
+        fprintf(stderr, "EXAGEOSTAT_dmle_Predict_Tile: %s\n", exageostat_last_error());
+        return -1;
+    }
     XgPredict *q = (XgPredict *)data->descC22;
     if (!q || q->nmiss != nZmiss || q->nobs != nZobs) {
         if (q) prediction_finalize(data);
@@ -443,6 +457,11 @@ extern "C" double *EXAGEOSTAT_Fisher_Tile(MLE_data *data, int N, double *initial
     (void)p_grid;
     (void)q_grid;
     XgField *f = xg_field_of(data);
+    if (f && f->kernel == 2) {
+        xg_fail(XG_ERR_UNSUPPORTED, "the Fisher matrix of a bivariate field");
+        fprintf(stderr, "EXAGEOSTAT_Fisher_Tile: %s\n", exageostat_last_error());
+        return NULL;
+    }
     if (!f || f->N != N) {
         xg_fail(XG_ERR_NOT_INITIALIZED, "no descriptors for N = %d: call EXAGEOSTAT_dmle_Call first", N);
         fprintf(stderr, "EXAGEOSTAT_Fisher_Tile: %s\n", exageostat_last_error());
@@ -505,7 +524,8 @@ extern "C" void EXAGEOSTAT_dmle_mloe_mmom_Allocate(MLE_data *data, int nZmiss, i
         return;
     }
     int kernel = 0, np = 0;
-    if (xg_kernel_of(data, &kernel, &np)) {
+    if (xg_kernel_of(data, &kernel, &np) ||
+        (kernel == 2 && xg_fail(XG_ERR_UNSUPPORTED, "MLOE / MMOM with bivariate_matern_parsimonious"))) {
         fprintf(stderr, "EXAGEOSTAT_dmle_mloe_mmom_Allocate: %s\n", exageostat_last_error());
         return;
     }
@@ -554,8 +574,10 @@ static void xg_mloe_mmom(MLE_data *data, double *truth_theta, double *estimated_
                          const char *mode)
 {
     int kernel = 0, np = 0;
-    if (xg_kernel_of(data, &kernel, &np)) {
+    if (xg_kernel_of(data, &kernel, &np) ||
+        (kernel == 2 && xg_fail(XG_ERR_UNSUPPORTED, "MLOE / MMOM with bivariate_matern_parsimonious"))) {
         fprintf(stderr, "EXAGEOSTAT_dmle_mloe_mmom_Tile: %s\n", exageostat_last_error());
+        data->mloe = data->mmom = NAN;
         return;
     }
     XgAssess *q = (XgAssess *)data->desck_t;
@@ -640,7 +662,7 @@ extern "C" int exageostat_b200_mloe_mmom_host(int nmiss, const double *xmiss, co
 extern "C" int exageostat_b200_dmle_host(int n, const double *x, const double *y, const double *z,
                                          const double *theta, int kernel, int metric, int ts, double *out)
 {
-    if (kernel != 0 && kernel != 1) return xg_fail(XG_ERR_BAD_ARGUMENT, "kernel %d", kernel);
+    if (kernel < 0 || kernel > 2) return xg_fail(XG_ERR_BAD_ARGUMENT, "kernel %d", kernel);
     XgField *f = nullptr;
     int rc = xg_field_create(&f, n, ts, x, y, kernel, metric);
     if (rc) return rc;
@@ -688,7 +710,7 @@ extern "C" int exageostat_b200_set_sliced(MLE_data *data)
 extern "C" int exageostat_b200_dmle_host_sliced(int n, const double *x, const double *y, const double *z,
                                                 const double *theta, int kernel, int metric, int ts, double *out)
 {
-    if (kernel != 0 && kernel != 1) return xg_fail(XG_ERR_BAD_ARGUMENT, "kernel %d", kernel);
+    if (kernel < 0 || kernel > 2) return xg_fail(XG_ERR_BAD_ARGUMENT, "kernel %d", kernel);
     XgField *f = nullptr;
     int rc = xg_field_create(&f, n, ts, x, y, kernel, metric);
     if (rc) return rc;

@@ -43,18 +43,22 @@ __device__ __forceinline__ void xg_gen_body(const XgTileArgs &T, long long t, in
                                             int n_cols, const XgMaternParams &p, int metric, int identity_pad)
 {
     double *tile = T.data + t * (long long)T.ts * T.ts;
+    /* bivariate: matrix index 2 l + v -> location l, variable v */
+    const int sh = p.bivariate ? 1 : 0;
     for (int rr = 0; rr < XG_GEN_ROWS; ++rr) {
         const int r = strip * XG_GEN_ROWS + rr;
         const int R = ij.x * T.ts + r;
         const bool row_ok = R < n_rows;
-        const double x1 = row_ok ? xr[R] : 0.0, y1 = row_ok ? yr[R] : 0.0;
+        const double x1 = row_ok ? xr[R >> sh] : 0.0, y1 = row_ok ? yr[R >> sh] : 0.0;
         for (int c = threadIdx.x; c < T.ts; c += blockDim.x) {
             const int C = ij.y * T.ts + c;
             double val;
-            if (row_ok && C < n_cols)
-                val = xg_matern_value(xg_distance(x1, y1, xc[C], yc[C], metric), p);
-            else
+            if (row_ok && C < n_cols) {
+                const double d = xg_distance(x1, y1, xc[C >> sh], yc[C >> sh], metric);
+                val = sh ? xg_matern_value_biv(d, p, R & 1, C & 1) : xg_matern_value(d, p);
+            } else {
                 val = (identity_pad && R == C) ? 1.0 : 0.0;
+            }
             tile[(long long)r * T.ts + c] = val;
         }
     }

@@ -176,6 +176,35 @@ void xg_tm_free(XgTileMatrix &M)
 XgMaternParams xg_params(const double *theta, int kernel)
 {
     XgMaternParams p;
+    p.bivariate = 0;
+    p.sigma2b = p.nu2 = p.con2 = p.nu12 = p.con12 = p.cross0 = 0.0;
+    if (kernel == 2) {
+        /* theta = (sigma_1^2, sigma_2^2, beta, nu_1, nu_2, rho): the constants of
+         * core_dcmg_bivariate_parsimonious (core_zcmg.c:1637-1651), in its order */
+        p.bivariate = 1;
+        p.sigma2 = theta[0];
+        p.sigma2b = theta[1];
+        p.beta = theta[2];
+        p.nu = theta[3];
+        p.nu2 = theta[4];
+        p.nugget = 0.0;
+        p.half_integer = -1;
+        double con1 = pow(2, (theta[3] - 1)) * tgamma(theta[3]);
+        con1 = 1.0 / con1;
+        p.con = theta[0] * con1;
+        double con2 = pow(2, (theta[4] - 1)) * tgamma(theta[4]);
+        con2 = 1.0 / con2;
+        p.con2 = theta[1] * con2;
+        p.nu12 = 0.5 * (theta[3] + theta[4]);
+        const double rho = theta[5] * sqrt((tgamma(theta[3] + 1) * tgamma(theta[4] + 1)) /
+                                           (tgamma(theta[3]) * tgamma(theta[4]))) *
+                           tgamma(p.nu12) / tgamma(p.nu12 + 1);
+        double con12 = pow(2, (p.nu12 - 1)) * tgamma(p.nu12);
+        con12 = 1.0 / con12;
+        p.con12 = rho * sqrt(theta[0] * theta[1]) * con12;
+        p.cross0 = rho * sqrt(theta[0] * theta[1]);
+        return p;
+    }
     p.sigma2 = theta[0];
     p.beta = theta[1];
     p.nu = theta[2];
@@ -190,6 +219,15 @@ XgMaternParams xg_params(const double *theta, int kernel)
 
 int xg_check_theta(const double *theta, int kernel)
 {
+    if (kernel == 2) {
+        for (int i = 0; i < 6; ++i)
+            if (!isfinite(theta[i])) return xg_fail(XG_ERR_BAD_ARGUMENT, "theta[%d] is not finite", i);
+        for (int i = 0; i < 5; ++i)
+            if (!(theta[i] > 0)) return xg_fail(XG_ERR_BAD_ARGUMENT, "theta[%d] = %g must be positive", i, theta[i]);
+        if (theta[3] > 25.0 || theta[4] > 25.0)
+            return xg_fail(XG_ERR_BAD_ARGUMENT, "smoothness above the supported maximum 25");
+        return XG_OK;
+    }
     const int np = kernel == 1 ? 4 : 3;
     for (int i = 0; i < np; ++i)
         if (!isfinite(theta[i])) return xg_fail(XG_ERR_BAD_ARGUMENT, "theta[%d] is not finite", i);
@@ -307,8 +345,9 @@ static void xg_field_collect_profile(XgField *f)
 int xg_field_set_data(XgField *f, const double *x, const double *y, const double *z)
 {
     cudaStream_t st = g_xg.stream;
-    if (x) XG_CU(cudaMemcpyAsync(f->x, x, f->N * sizeof(double), cudaMemcpyHostToDevice, st));
-    if (y) XG_CU(cudaMemcpyAsync(f->y, y, f->N * sizeof(double), cudaMemcpyHostToDevice, st));
+    const int nloc = f->kernel == 2 ? f->N / 2 : f->N; /* bivariate: two variables per location */
+    if (x) XG_CU(cudaMemcpyAsync(f->x, x, nloc * sizeof(double), cudaMemcpyHostToDevice, st));
+    if (y) XG_CU(cudaMemcpyAsync(f->y, y, nloc * sizeof(double), cudaMemcpyHostToDevice, st));
     if (z) XG_CU(cudaMemcpyAsync(f->z, z, f->N * sizeof(double), cudaMemcpyHostToDevice, st));
     XG_CU(cudaStreamSynchronize(st));
     if (z) f->have_z = true;
@@ -359,6 +398,10 @@ int xg_field_create(XgField **out, int N, int ts, const double *x, const double 
     if (rc) return rc;
     if (N <= 0) return xg_fail(XG_ERR_BAD_ARGUMENT, "N = %d must be positive", N);
     if (!x || !y) return xg_fail(XG_ERR_BAD_ARGUMENT, "locations are NULL");
+    if (kernel == 2 && (N & 1))
+        return xg_fail(XG_ERR_BAD_ARGUMENT, "bivariate kernel: N = %d must be 2 x the number of locations", N);
+    /* bivariate: N / 2 locations, two variables each */
+    const int nloc = kernel == 2 ? N / 2 : N;
     XgField *f = new XgField();
     f->N = N;
     f->kernel = kernel;
@@ -380,9 +423,9 @@ int xg_field_create(XgField **out, int N, int ts, const double *x, const double 
     if (!rc && (cudaEventCreateWithFlags(&f->ev_panel, cudaEventDisableTiming) != cudaSuccess ||
                 cudaEventCreateWithFlags(&f->ev_upd, cudaEventDisableTiming) != cudaSuccess))
         rc = xg_fail(XG_ERR_CUDA, "lookahead events");
-    if (!rc && cudaMemcpy(f->x, x, N * sizeof(double), cudaMemcpyHostToDevice) != cudaSuccess)
+    if (!rc && cudaMemcpy(f->x, x, nloc * sizeof(double), cudaMemcpyHostToDevice) != cudaSuccess)
         rc = xg_fail(XG_ERR_CUDA, "upload x");
-    if (!rc && cudaMemcpy(f->y, y, N * sizeof(double), cudaMemcpyHostToDevice) != cudaSuccess)
+    if (!rc && cudaMemcpy(f->y, y, nloc * sizeof(double), cudaMemcpyHostToDevice) != cudaSuccess)
         rc = xg_fail(XG_ERR_CUDA, "upload y");
     if (rc) {
         xg_field_destroy(f);
@@ -1288,6 +1331,8 @@ int xg_autotune_field(XgField **pf, const double *x, const double *y, const doub
                       int *ts_out, int *band_out, double *report)
 {
     XgField *f = *pf;
+    if (precision == 2 && f->kernel == 2)
+        return xg_fail(XG_ERR_UNSUPPORTED, "banded mixed precision with bivariate_matern_parsimonious");
     const int N = f->N;
     std::vector<double> z(N);
     int rc = xg_field_get_z(f, z.data(), N);

@@ -60,6 +60,12 @@ struct XgMaternParams {
     double nugget; /* tau^2, added on the zero-distance branch only */
     double con;
     int half_integer;
+    /* bivariate parsimonious Matern (kernel 2): rows and columns interleave
+     * the two variables of each location (index 2 l + v); sigma2, nu, con
+     * above are variable 0's, these variable 1's and the cross block's
+     * (core_zcmg.c:1628-1651) */
+    int bivariate;
+    double sigma2b, nu2, con2, nu12, con12, cross0;
 };
 
 /* One field of a batch of independent fields sharing one tile store. */

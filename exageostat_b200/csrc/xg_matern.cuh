@@ -11,7 +11,8 @@
 #include "kbessel.cuh"
 #include "xg_kernels.h"
 
-__device__ inline double xg_deg2rad(double d) { return d * (XG_PI / 180.0); }
+/* deg * PI / 180 in the reference's order of operations (core_zcmg.c:30-32) */
+__device__ inline double xg_deg2rad(double d) { return d * XG_PI / 180.0; }
 
 /* Distance between (x1, y1) [row location] and (x2, y2) [column location].
  * Euclidean: sqrt(pow(x2 - x1, 2) + pow(y2 - y1, 2)) as core_zcmg.c:84, with
@@ -38,6 +39,19 @@ __device__ inline double xg_matern_value(double d, const XgMaternParams &p)
     if (r == 0.0) return p.sigma2 + p.nugget;
     if (p.half_integer >= 0) return xg_matern_half_integer(r, p.sigma2, p.half_integer);
     return xg_matern_general(r, p.nu, p.con);
+}
+
+/* Bivariate parsimonious Matern element between variable a of one location
+ * and variable b of another (core_dcmg_bivariate_parsimonious,
+ * core_zcmg.c:1628-1726): Matern(sigma_a^2, beta, nu_a) on the diagonal
+ * blocks, rho sqrt(sigma_1^2 sigma_2^2) Matern(1, beta, nu12) across, and the
+ * values at d / beta == 0 exactly as the reference. */
+__device__ inline double xg_matern_value_biv(double d, const XgMaternParams &p, int a, int b)
+{
+    const double r = d / p.beta;
+    if (a != b) return r == 0.0 ? p.cross0 : xg_matern_general(r, p.nu12, p.con12);
+    if (a == 0) return r == 0.0 ? p.sigma2 : xg_matern_general(r, p.nu, p.con);
+    return r == 0.0 ? p.sigma2b : xg_matern_general(r, p.nu2, p.con2);
 }
 
 #endif

@@ -46,6 +46,7 @@ def lib():
         L.ora_core_dcmg.argtypes = [_PD, _I, _I, _I, _I, _PD, _PD, _PD, _PD, _PD, _I]
         L.ora_gen_lower_dense.argtypes = [_PD, _I, _PD, _PD, _PD, _I]
         L.ora_dcmg_deriv.argtypes = [_PD, _I, _I, _I, _I, _PD, _PD, _PD, _PD, _PD, _I]
+        L.ora_set_metric.argtypes = [_I]
         L.ora_dlarnv.argtypes = [_I, _I, _PD]
         L.ora_dzvg.argtypes = [_I, _PD, _PD, _PD, _I, _PD, _PD]
         L.ora_dmle.argtypes = [_I, _PD, _PD, _PD, _PD, _I, _PD, _PD, _PD, _PD]
@@ -102,35 +103,40 @@ def pick_random_points(x, y, z, n_miss: int, seed: int | None = None, skip: int 
     return dict(x_miss=xm, y_miss=ym, z_actual=za, x_obs=xo, y_obs=yo, z_obs=zo)
 
 
-def core_dcmg(m, n, m0, n0, x1, y1, x2, y2, theta, kernel=0) -> np.ndarray:
-    """Column-major m x n tile, returned as an (m, n) array."""
+def core_dcmg(m, n, m0, n0, x1, y1, x2, y2, theta, kernel=0, metric=0) -> np.ndarray:
+    """Column-major m x n tile, returned as an (m, n) array (metric 1: great
+    circle on (lat, lon) in degrees, km)."""
+    lib().ora_set_metric(int(metric))
     A = np.empty((n, m))  # column-major storage == C-order (n, m)
     x1, y1, x2, y2, th = _f64(x1), _f64(y1), _f64(x2), _f64(y2), _f64(theta)
     lib().ora_core_dcmg(_p(A), m, n, m0, n0, _p(x1), _p(y1), _p(x2), _p(y2), _p(th), int(kernel))
     return A.T.copy()
 
 
-def covariance_lower(x, y, theta, kernel=0) -> np.ndarray:
-    """Lower triangle of Sigma(theta) (upper part left as zeros)."""
+def covariance_lower(x, y, theta, kernel=0, metric=0) -> np.ndarray:
+    """Lower triangle of Sigma(theta) (upper part left as zeros); for the
+    bivariate kernel 2 the matrix is 2 n x 2 n (index 2 l + v)."""
+    lib().ora_set_metric(int(metric))
     x, y, th = _f64(x), _f64(y), _f64(theta)
-    N = x.size
+    N = x.size * (2 if kernel == 2 else 1)
     C = np.zeros((N, N))  # column-major buffer; transposed on return
     lib().ora_gen_lower_dense(_p(C), N, _p(x), _p(y), _p(th), int(kernel))
     return C.T.copy()
 
 
-def dcmg_deriv(m, n, m0, n0, x1, y1, x2, y2, theta, which) -> np.ndarray:
+def dcmg_deriv(m, n, m0, n0, x1, y1, x2, y2, theta, which, metric=0) -> np.ndarray:
     """dSigma/dtheta_which (0 sigma^2, 1 beta, 2 nu) of the Matern part, an
     (m, n) block (core_dcmg_matern_dsigma_square / _dbeta / _dnu,
     exageostat_exact/cpu_core/compute/core_zcmg.c:315-488)."""
     A = np.empty((n, m))
     x1, y1, x2, y2, th = _f64(x1), _f64(y1), _f64(x2), _f64(y2), _f64(theta)
+    lib().ora_set_metric(int(metric))
     lib().ora_dcmg_deriv(_p(A), m, n, m0, n0, _p(x1), _p(y1), _p(x2), _p(y2), _p(th), int(which))
     return A.T.copy()
 
 
-def covariance_full(x, y, theta, kernel=0) -> np.ndarray:
-    C = covariance_lower(x, y, theta, kernel)
+def covariance_full(x, y, theta, kernel=0, metric=0) -> np.ndarray:
+    C = covariance_lower(x, y, theta, kernel, metric)
     return C + np.tril(C, -1).T
 
 
@@ -144,7 +150,7 @@ def _spd_inverse_as_reference(A):
     return solve_triangular(L, Y, lower=True, trans="T")
 
 
-def fisher(x, y, theta, kernel=0):
+def fisher(x, y, theta, kernel=0, metric=0):
     """EXAGEOSTAT_Fisher_Tile (exageostat_exact/src/compute/MLE_dexact.c:1777-1934):
     C = Sigma(theta) factored; for j <= k: CJ = L^-T L^-1 dSigma_j, CK likewise
     (two dtrsm each, :1846-1847, :1866-1867), A[k + 3 j] = 1/2 trace(CJ CK) (:1870-1879);
@@ -155,9 +161,9 @@ def fisher(x, y, theta, kernel=0):
 
     x, y = _f64(x), _f64(y)
     N = x.size
-    C = covariance_full(x, y, theta, kernel)
+    C = covariance_full(x, y, theta, kernel, metric)
     L = np.linalg.cholesky(C)
-    D = [dcmg_deriv(N, N, 0, 0, x, y, x, y, theta, j) for j in range(3)]
+    D = [dcmg_deriv(N, N, 0, 0, x, y, x, y, theta, j, metric) for j in range(3)]
     if kernel == 1:
         D.append(np.eye(N))
     M = []
@@ -172,7 +178,7 @@ def fisher(x, y, theta, kernel=0):
     return F, _spd_inverse_as_reference(F)
 
 
-def mloe_mmom(x_miss, y_miss, x_obs, y_obs, truth_theta, estimated_theta, kernel=0):
+def mloe_mmom(x_miss, y_miss, x_obs, y_obs, truth_theta, estimated_theta, kernel=0, metric=0):
     """EXAGEOSTAT_dmle_mloe_mmom_Tile (exageostat_exact/src/compute/MLE_dexact.c:1109-1434)
     restated with the missing points as columns: K_a, K_t (:1239-1245) and
     their factors (:1252, :1261); per point k_t, k_a (:1283-1286), the four
@@ -187,10 +193,10 @@ def mloe_mmom(x_miss, y_miss, x_obs, y_obs, truth_theta, estimated_theta, kernel
 
     xm, ym, xo, yo = (_f64(a) for a in (x_miss, y_miss, x_obs, y_obs))
     nobs, nmiss = xo.size, xm.size
-    La = np.linalg.cholesky(covariance_full(xo, yo, estimated_theta, kernel))
-    Lt = np.linalg.cholesky(covariance_full(xo, yo, truth_theta, kernel))
-    kt = core_dcmg(nobs, nmiss, 0, 0, xo, yo, xm, ym, truth_theta, kernel)
-    ka = core_dcmg(nobs, nmiss, 0, 0, xo, yo, xm, ym, estimated_theta, kernel)
+    La = np.linalg.cholesky(covariance_full(xo, yo, estimated_theta, kernel, metric))
+    Lt = np.linalg.cholesky(covariance_full(xo, yo, truth_theta, kernel, metric))
+    kt = core_dcmg(nobs, nmiss, 0, 0, xo, yo, xm, ym, truth_theta, kernel, metric)
+    ka = core_dcmg(nobs, nmiss, 0, 0, xo, yo, xm, ym, estimated_theta, kernel, metric)
     kttmp, katmp = kt.copy(), ka.copy()
     ka = solve_triangular(La, ka, lower=True)
     kt = solve_triangular(Lt, kt, lower=True)
@@ -225,29 +231,32 @@ def dlarnv(seed: int, n: int) -> np.ndarray:
     return out
 
 
-def dzvg(x, y, theta, nrand, kernel=0) -> np.ndarray:
+def dzvg(x, y, theta, nrand, kernel=0, metric=0) -> np.ndarray:
+    lib().ora_set_metric(int(metric))
     x, y, th, e = _f64(x), _f64(y), _f64(theta), _f64(nrand)
-    z = np.empty(x.size)
-    info = lib().ora_dzvg(x.size, _p(x), _p(y), _p(th), int(kernel), _p(e), _p(z))
+    z = np.empty(e.size)  # 2 x the locations for the bivariate kernel
+    info = lib().ora_dzvg(e.size, _p(x), _p(y), _p(th), int(kernel), _p(e), _p(z))
     if info != 0:
         raise RuntimeError("oracle dzvg: dpotrf info=%d" % info)
     return z
 
 
-def dmle(x, y, z, theta, kernel=0):
+def dmle(x, y, z, theta, kernel=0, metric=0):
     """Returns (loglik, logdet, dotp, (t_gen, t_chol, t_solve))."""
+    lib().ora_set_metric(int(metric))
     x, y, z, th = _f64(x), _f64(y), _f64(z), _f64(theta)
     ll, ld, dp = _D(), _D(), _D()
     times = np.zeros(3)
-    info = lib().ora_dmle(x.size, _p(x), _p(y), _p(z), _p(th), int(kernel), ctypes.byref(ll), ctypes.byref(ld),
+    info = lib().ora_dmle(z.size, _p(x), _p(y), _p(z), _p(th), int(kernel), ctypes.byref(ll), ctypes.byref(ld),
                           ctypes.byref(dp), _p(times))
     if info != 0:
         raise RuntimeError("oracle dmle: dpotrf info=%d" % info)
     return ll.value, ld.value, dp.value, tuple(times)
 
 
-def dpredict(x_miss, y_miss, x_obs, y_obs, z_obs, z_actual, theta, kernel=0):
+def dpredict(x_miss, y_miss, x_obs, y_obs, z_obs, z_actual, theta, kernel=0, metric=0):
     """Returns (mse, zmiss)."""
+    lib().ora_set_metric(int(metric))
     xm, ym, xo, yo, zo, th = (_f64(a) for a in (x_miss, y_miss, x_obs, y_obs, z_obs, theta))
     za = None if z_actual is None else _f64(z_actual)
     zmiss = np.empty(xm.size)
@@ -256,11 +265,12 @@ def dpredict(x_miss, y_miss, x_obs, y_obs, z_obs, z_actual, theta, kernel=0):
     return float(mse), zmiss
 
 
-def synthetic_field(N: int, seed: int, theta, kernel=0):
+def synthetic_field(N: int, seed: int, theta, kernel=0, metric=0, locations=None):
     """The reference's synthetic workflow (synthetic_dmle_test.c:103-147,278):
     e = dlarnv(3, {seed,seed,seed,1}), locations = GenerateXYLoc(N, seed),
     z = L(theta) e."""
     e = dlarnv(seed, N)
-    x, y = generate_xy_loc(N, seed)
-    z = dzvg(x, y, theta, e, kernel)
+    nloc = N // 2 if kernel == 2 else N  # N = p x locations (synthetic_dmle_test.c:134, 153)
+    x, y = generate_xy_loc(nloc, seed) if locations is None else (_f64(locations[0]), _f64(locations[1]))
+    z = dzvg(x, y, theta, e, kernel, metric)
     return x, y, z, e

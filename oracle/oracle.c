@@ -17,6 +17,8 @@
  *   - core_dmdet           exageostat_exact/cpu_core/compute/core_zmdet.c:50-59
  *   - EXAGEOSTAT_MLE_dzvg_Tile (Z = L e)   exageostat_exact/src/compute/MLE_dexact.c:25-148
  *   - EXAGEOSTAT_dmle_Tile (log-likelihood) exageostat_exact/src/compute/MLE_dexact.c:231-489
+ *   - core_dcmg_bivariate_parsimonious
+ *                          exageostat_exact/cpu_core/compute/core_zcmg.c:1628-1726
  *   - core_dcmg_matern_dsigma_square / _dbeta / _dnu and psi
  *                          exageostat_exact/cpu_core/compute/core_zcmg.c:189-235, 315-488
  *   - EXAGEOSTAT_dmle_Predict_Tile + CORE_dmse_starpu
@@ -402,13 +404,34 @@ void ora_pick_random_points(int N, const double *x, const double *y, const doubl
 /* Covariance generation: core_dcmg / core_dcmg_nuggets                       */
 /* ========================================================================== */
 
+/* Distance metric of the generators: 0 Euclidean (core_zcmg.c:84), 1 great
+ * circle (distanceEarth, core_zcmg.c:51-60: haversine in km on (lat, lon) in
+ * degrees, deg2rad :30-32, earthRadiusKm MLE_misc.h:68).  Set with
+ * ora_set_metric; not thread-safe, like the reference's own globals. */
+static int ora_metric = 0;
+
+void ora_set_metric(int metric) { ora_metric = metric; }
+
+static double ora_deg2rad(double deg) { return (deg * 3.141592653589793 / 180); }
+
+static inline double ora_distance(double x1, double y1, double x2, double y2)
+{
+    if (ora_metric == 1) {
+        const double lat1r = ora_deg2rad(x1), lon1r = ora_deg2rad(y1);
+        const double lat2r = ora_deg2rad(x2), lon2r = ora_deg2rad(y2);
+        const double u = sin((lat2r - lat1r) / 2), v = sin((lon2r - lon1r) / 2);
+        return 2.0 * 6371.0 * asin(sqrt(u * u + cos(lat1r) * cos(lat2r) * v * v));
+    }
+    return sqrt(pow(x2 - x1, 2) + pow(y2 - y1, 2));
+}
+
 /* One Matern element (core_zcmg.c:975-990): distance with pow(.,2) and sqrt,
  * an exact compare with zero, then con * expr^nu * K_nu(expr). kernel 1 adds
  * the nugget theta[3] on the zero-distance branch (core_zcmg_nuggets.c:131). */
 static inline double ora_matern_elem(double x1, double y1, double x2, double y2, const double *theta, double con,
                                      int kernel)
 {
-    double expr = sqrt(pow(x2 - x1, 2) + pow(y2 - y1, 2)) / theta[1];
+    double expr = ora_distance(x1, y1, x2, y2) / theta[1];
     if (expr == 0) return kernel == 1 ? theta[0] + theta[3] : theta[0];
     return con * pow(expr, theta[2]) * ora_bessel_knu(theta[2], expr);
 }
@@ -420,10 +443,64 @@ static double ora_matern_con(const double *theta)
     return theta[0] * con;
 }
 
-/* core_dcmg: A (column-major, lda = m) = Sigma(l1[m0:m0+m], l2[n0:n0+n]). */
+/* Bivariate parsimonious Matern (kernel 2, theta = (sigma_1^2, sigma_2^2,
+ * beta, nu_1, nu_2, rho)): the constants of core_dcmg_bivariate_parsimonious
+ * (core_zcmg.c:1637-1651) in its order, c[] = con1, con2, con12, rho, nu12. */
+static void ora_biv_consts(const double *theta, double *c)
+{
+    double con1 = pow(2, (theta[3] - 1)) * tgamma(theta[3]);
+    con1 = 1.0 / con1;
+    con1 = theta[0] * con1;
+    double con2 = pow(2, (theta[4] - 1)) * tgamma(theta[4]);
+    con2 = 1.0 / con2;
+    con2 = theta[1] * con2;
+    const double nu12 = 0.5 * (theta[3] + theta[4]);
+    const double rho = theta[5] * sqrt((tgamma(theta[3] + 1) * tgamma(theta[4] + 1)) /
+                                       (tgamma(theta[3]) * tgamma(theta[4]))) *
+                       tgamma(nu12) / tgamma(nu12 + 1);
+    double con12 = pow(2, (nu12 - 1)) * tgamma(nu12);
+    con12 = 1.0 / con12;
+    con12 = rho * sqrt(theta[0] * theta[1]) * con12;
+    c[0] = con1;
+    c[1] = con2;
+    c[2] = con12;
+    c[3] = rho;
+    c[4] = nu12;
+}
+
+/* Element between variable a of (x1, y1) and variable b of (x2, y2)
+ * (core_zcmg.c:1656-1671: the 2 x 2 block of one location pair). */
+static inline double ora_biv_elem(double x1, double y1, double x2, double y2, int a, int b, const double *theta,
+                                  const double *c)
+{
+    const double expr = ora_distance(x1, y1, x2, y2) / theta[2];
+    if (expr == 0) {
+        if (a != b) return c[3] * sqrt(theta[0] * theta[1]);
+        return a == 0 ? theta[0] : theta[1];
+    }
+    if (a != b) return c[2] * pow(expr, c[4]) * ora_bessel_knu(c[4], expr);
+    if (a == 0) return c[0] * pow(expr, theta[3]) * ora_bessel_knu(theta[3], expr);
+    return c[1] * pow(expr, theta[4]) * ora_bessel_knu(theta[4], expr);
+}
+
+/* core_dcmg: A (column-major, lda = m) = Sigma(l1[m0:m0+m], l2[n0:n0+n]).
+ * Bivariate (kernel 2): rows and columns are matrix indices 2 l + v (location
+ * l, variable v), as the reference's i0 = m0 / 2 loop (core_zcmg.c:1652-1673). */
 void ora_core_dcmg(double *A, int m, int n, int m0, int n0, const double *x1, const double *y1, const double *x2,
                    const double *y2, const double *theta, int kernel)
 {
+    if (kernel == 2) {
+        double c[5];
+        ora_biv_consts(theta, c);
+#pragma omp parallel for schedule(static)
+        for (int j = 0; j < n; ++j)
+            for (int i = 0; i < m; ++i) {
+                const int gi = m0 + i, gj = n0 + j;
+                A[i + (size_t)j * m] = ora_biv_elem(x1[gi / 2], y1[gi / 2], x2[gj / 2], y2[gj / 2], gi % 2, gj % 2,
+                                                    theta, c);
+            }
+        return;
+    }
     const double con = ora_matern_con(theta);
 #pragma omp parallel for schedule(static)
     for (int j = 0; j < n; ++j)
@@ -466,7 +543,7 @@ static double ora_dknu_dnu(double nu, double x)
  * :189-191), 380-416 (dnu); zero distance gives 1, 0, 0. */
 static double ora_dmatern_elem(double x1, double y1, double x2, double y2, const double *theta, int which)
 {
-    const double expr = sqrt(pow(x2 - x1, 2) + pow(y2 - y1, 2)) / theta[1];
+    const double expr = ora_distance(x1, y1, x2, y2) / theta[1];
     if (expr == 0) return which == 0 ? 1.0 : 0.0;
     const double nu = theta[2], beta = theta[1], sigma2 = theta[0];
     const double con = 1.0 / (pow(2, (nu - 1)) * tgamma(nu));
@@ -500,6 +577,15 @@ void ora_dcmg_deriv(double *A, int m, int n, int m0, int n0, const double *x1, c
  * (codelet_zcmg.c:316-342); LAPACK dpotrf reads only the lower triangle. */
 static void ora_gen_lower(double *C, int N, const double *x, const double *y, const double *theta, int kernel)
 {
+    if (kernel == 2) {
+        double c[5];
+        ora_biv_consts(theta, c);
+#pragma omp parallel for schedule(dynamic, 16)
+        for (int j = 0; j < N; ++j)
+            for (int i = j; i < N; ++i)
+                C[i + (size_t)j * N] = ora_biv_elem(x[i / 2], y[i / 2], x[j / 2], y[j / 2], i % 2, j % 2, theta, c);
+        return;
+    }
     const double con = ora_matern_con(theta);
 #pragma omp parallel for schedule(dynamic, 16)
     for (int j = 0; j < N; ++j)
