@@ -486,7 +486,7 @@ class Session:
         if not r:
             raise XgError(-1, last_error())
         out = np.array([r[i] for i in range(9)]).reshape(3, 3).T.copy()
-        ctypes.CDLL(None).free(ctypes.cast(r, ctypes.c_void_p))
+        _libc().free(ctypes.cast(r, ctypes.c_void_p))
         return out
 
     def mloe_mmom(self, truth_theta, estimated_theta, x_miss, y_miss, x_obs, y_obs, asynchronous=False):
