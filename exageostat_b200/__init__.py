@@ -111,7 +111,7 @@ EXPORTED_SYMBOLS = [
     "exageostat_b200_fisher_host", "mloe_mmom_init", "EXAGEOSTAT_dmle_mloe_mmom_Allocate",
     "EXAGEOSTAT_dmle_mloe_mmom_Tile", "EXAGEOSTAT_dmle_mloe_mmom_Tile_Async", "mloe_mmom_finalize",
     "MLOE_MMOM_Finalize", "exageostat_b200_mloe_mmom_host", "countlines", "readLocsFile", "readLocsFile3d",
-    "readObsFile", "readTimeFile", "results",
+    "readObsFile", "readTimeFile", "shuffle2", "pick_random_points2", "results",
 ]
 
 _lib = None
@@ -149,6 +149,7 @@ def lib():
         "uniform_distribution": (_D, [_D, _D]),
         "locations_obs_zsort_inplace": (_I, [_I, ctypes.POINTER(Location), _PD]),
         "pick_random_points": (None, [PM, _PD, _PD, _I, _I, _I]),
+        "pick_random_points2": (None, [PM, _PD, _PD, _I, _I, _I]),
         "exageostat_b200_loglik": (_I, [PM, _PD, _PD, _PD]),
         "exageostat_last_error": (_CP, []),
         "exageostat_b200_abi_version": (_I, []),
@@ -465,9 +466,10 @@ class Session:
         d = self.data
         d.lmiss.x, d.lmiss.y = _p(xm), _p(ym)
         d.lobs.x, d.lobs.y = _p(xo), _p(yo)
-        zmiss = np.empty(xm.size)
+        nm, no = _dim(xm, self.kernel), _dim(xo, self.kernel)  # rows: 2 per location when bivariate
+        zmiss = np.empty(nm)
         t = _f64(theta)
-        mse = self.L.EXAGEOSTAT_dmle_Predict_Tile(ctypes.byref(d), _p(t), xm.size, xo.size, _p(zo),
+        mse = self.L.EXAGEOSTAT_dmle_Predict_Tile(ctypes.byref(d), _p(t), nm, no, _p(zo),
                                                   None if za is None else _p(za), _p(zmiss), self.N)
         return mse, zmiss
 

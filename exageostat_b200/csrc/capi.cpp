@@ -363,6 +363,12 @@ extern "C" void EXAGEOSTAT_dmle_Predict_Allocate(MLE_data *data, int nZmiss, int
         return;
     }
     if (data->descC22) prediction_finalize(data);
+    int kernel = 0, np = 0;
+    if (xg_kernel_of(data, &kernel, &np) == XG_OK && kernel == 2) {
+        /* the bivariate matrices have two rows per location (MLE_dexact.c:640-653) */
+        nZobs *= 2;
+        nZmiss *= 2;
+    }
     XgPredict *q = nullptr;
     if (xg_predict_create(&q, nZmiss, nZobs, dts > 0 ? dts : g_xg.dts)) {
         fprintf(stderr, "EXAGEOSTAT_dmle_Predict_Allocate: %s\n", exageostat_last_error());
@@ -397,15 +403,12 @@ extern "C" double EXAGEOSTAT_dmle_Predict_Tile(MLE_data *data, double *theta, in
         fprintf(stderr, "EXAGEOSTAT_dmle_Predict_Tile: %s\n", exageostat_last_error());
         return -1;
     }
-    if (kernel == 2) {
-        xg_fail(XG_ERR_UNSUPPORTED, "kriging with bivariate_matern_parsimonious");
-        fprintf(stderr, "EXAGEOSTAT_dmle_Predict_Tile: %s\n", exageostat_last_error());
-        return -1;
-    }
     XgPredict *q = (XgPredict *)data->descC22;
     if (!q || q->nmiss != nZmiss || q->nobs != nZobs) {
         if (q) prediction_finalize(data);
-        EXAGEOSTAT_dmle_Predict_Allocate(data, nZmiss, nZobs, 0, 1, 1, Zactual != NULL);
+        /* nZmiss / nZobs count matrix rows here; the allocation takes locations */
+        const int p = kernel == 2 ? 2 : 1;
+        EXAGEOSTAT_dmle_Predict_Allocate(data, nZmiss / p, nZobs / p, 0, 1, 1, Zactual != NULL);
         q = (XgPredict *)data->descC22;
         if (!q) return -1;
     }
@@ -416,8 +419,9 @@ extern "C" double EXAGEOSTAT_dmle_Predict_Tile(MLE_data *data, double *theta, in
     }
     double mse = -1;
     const double t0 = 0;
+    double parts[2] = {-1, -1};
     int rc = xg_predict_run(q, theta, kernel, xg_metric_of(data), data->lmiss.x, data->lmiss.y, data->lobs.x,
-                            data->lobs.y, Zobs, Zactual, Zmiss, &mse);
+                            data->lobs.y, Zobs, Zactual, Zmiss, &mse, parts);
     (void)t0;
     if (rc) {
         fprintf(stderr, "EXAGEOSTAT_dmle_Predict_Tile: %s\n", exageostat_last_error());
@@ -426,6 +430,12 @@ extern "C" double EXAGEOSTAT_dmle_Predict_Tile(MLE_data *data, double *theta, in
     }
     data->mserror = mse;
     results.mse_pred = mse;
+    if (kernel == 2) { /* per-variable errors of the bivariate field (MLE_dexact.c:838-847, 859-860) */
+        data->mserror1 = parts[0];
+        data->mserror2 = parts[1];
+        results.mse_pred1 = parts[0];
+        results.mse_pred2 = parts[1];
+    }
     return mse;
 }
 

@@ -1467,22 +1467,27 @@ int xg_predict_create(XgPredict **out, int nmiss, int nobs, int ts)
 
 int xg_predict_run(XgPredict *q, const double *theta, int kernel, int metric, const double *xm, const double *ym,
                    const double *xo, const double *yo, const double *zobs, const double *zactual, double *zmiss,
-                   double *mse)
+                   double *mse, double *mse_parts)
 {
     int rc = xg_check_theta(theta, kernel);
     if (rc) return rc;
+    if (kernel == 2 && ((q->nmiss | q->nobs) & 1))
+        return xg_fail(XG_ERR_BAD_ARGUMENT, "bivariate kriging: nZmiss = %d and nZobs = %d must be even (2 x locations)",
+                       q->nmiss, q->nobs);
     cudaStream_t st = g_xg.stream;
     const int nmiss = q->nmiss, nobs = q->nobs;
+    /* bivariate: nmiss and nobs count matrix rows, two per location */
+    const int lmiss = kernel == 2 ? nmiss / 2 : nmiss, lobs = kernel == 2 ? nobs / 2 : nobs;
     XgTileArgs T{q->C22.d, q->C22.ts, q->C22.nt};
     const XgMaternParams p = xg_params(theta, kernel);
     const size_t Np = (size_t)q->C22.nt * q->C22.ts;
     XG_CU(cudaMemsetAsync(q->status, 0, 2 * sizeof(int), st));
     XG_CU(cudaMemsetAsync(q->v, 0, Np * sizeof(double), st));
-    XG_CU(cudaMemcpyAsync(q->xo, xo, nobs * sizeof(double), cudaMemcpyHostToDevice, st));
-    XG_CU(cudaMemcpyAsync(q->yo, yo, nobs * sizeof(double), cudaMemcpyHostToDevice, st));
+    XG_CU(cudaMemcpyAsync(q->xo, xo, lobs * sizeof(double), cudaMemcpyHostToDevice, st));
+    XG_CU(cudaMemcpyAsync(q->yo, yo, lobs * sizeof(double), cudaMemcpyHostToDevice, st));
     XG_CU(cudaMemcpyAsync(q->v, zobs, nobs * sizeof(double), cudaMemcpyHostToDevice, st));
-    XG_CU(cudaMemcpyAsync(q->xm, xm, nmiss * sizeof(double), cudaMemcpyHostToDevice, st));
-    XG_CU(cudaMemcpyAsync(q->ym, ym, nmiss * sizeof(double), cudaMemcpyHostToDevice, st));
+    XG_CU(cudaMemcpyAsync(q->xm, xm, lmiss * sizeof(double), cudaMemcpyHostToDevice, st));
+    XG_CU(cudaMemcpyAsync(q->ym, ym, lmiss * sizeof(double), cudaMemcpyHostToDevice, st));
     if (zactual) XG_CU(cudaMemcpyAsync(q->zact, zactual, nmiss * sizeof(double), cudaMemcpyHostToDevice, st));
     /* C22 = Sigma(obs, obs); POSV: L L^T alpha = zobs */
     xg_launch_gen(T, q->C22.ij, q->C22.ntiles, q->xo, q->yo, q->xo, q->yo, nobs, nobs, p, metric, 1, st);
@@ -1500,12 +1505,16 @@ int xg_predict_run(XgPredict *q, const double *theta, int kernel, int metric, co
     int sv[2];
     XG_CU(cudaMemcpyAsync(sv, q->status, sizeof sv, cudaMemcpyDeviceToHost, st));
     XG_CU(cudaMemcpyAsync(zmiss, q->zmiss, nmiss * sizeof(double), cudaMemcpyDeviceToHost, st));
-    double m = -1;
-    if (zactual) XG_CU(cudaMemcpyAsync(&m, q->out, sizeof(double), cudaMemcpyDeviceToHost, st));
+    double m[3] = {-1, -1, -1};
+    if (zactual) XG_CU(cudaMemcpyAsync(m, q->out, sizeof m, cudaMemcpyDeviceToHost, st));
     XG_CU(cudaStreamSynchronize(st));
     if (sv[0] & XG_ST_NOT_SPD) return xg_fail(XG_ERR_NOT_SPD, "C22 is not positive definite (pivot %d)", sv[1]);
     if (sv[0]) return xg_fail(XG_ERR_TIMEOUT, "device status word 0x%x", sv[0]);
-    *mse = zactual ? m : -1.0;
+    *mse = zactual ? m[0] : -1.0;
+    if (mse_parts) {
+        mse_parts[0] = zactual ? m[1] : -1.0;
+        mse_parts[1] = zactual ? m[2] : -1.0;
+    }
     return XG_OK;
 }
 

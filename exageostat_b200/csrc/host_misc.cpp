@@ -188,6 +188,57 @@ extern "C" void pick_random_points(MLE_data *data, double *Zobs, double *Zactual
     locations_obs_zsort_inplace(nZmiss, &data->lmiss, Zactual);
 }
 
+/* MLE_misc.c:1261-1285: shuffle of the two variables of a bivariate field
+ * and their locations with one draw per step, as shuffle does. */
+extern "C" void shuffle2(double *array, double *array2, location *locations, size_t n)
+{
+    if (n <= 1) return;
+    for (size_t i = 0; i < n - 1; ++i) {
+        const size_t j = i + (size_t)rand() / (RAND_MAX / (n - i) + 1);
+        std::swap(array[i], array[j]);
+        std::swap(array2[i], array2[j]);
+        std::swap(locations->x[i], locations->x[j]);
+        std::swap(locations->y[i], locations->y[j]);
+    }
+}
+
+/* MLE_misc.c:1744-1810: the bivariate hold-out.  N is the matrix dimension (2
+ * x locations); nZmiss and nZobs count locations.  z is split into its two
+ * variables, locations and both variables are shuffled together, and the
+ * first nZmiss locations are missing; Zactual and Zobs interleave the two
+ * variables again.  No Morton re-sort (the reference has it commented out). */
+extern "C" void pick_random_points2(MLE_data *data, double *Zobs, double *Zactual, int nZmiss, int nZobs, int N)
+{
+    const int nloc = N / 2;
+    std::vector<double> Z((size_t)N), Z1((size_t)nloc), Z2((size_t)nloc);
+    location l;
+    l.x = (double *)malloc(sizeof(double) * (size_t)nloc);
+    l.y = (double *)malloc(sizeof(double) * (size_t)nloc);
+    l.z = NULL;
+    MLE_get_zobs(data, Z.data(), N);
+    for (int i = 0; i < nloc; ++i) {
+        Z1[i] = Z[2 * (size_t)i];
+        Z2[i] = Z[2 * (size_t)i + 1];
+        l.x[i] = data->l1.x[i];
+        l.y[i] = data->l1.y[i];
+    }
+    shuffle2(Z1.data(), Z2.data(), &l, (size_t)nloc);
+    for (int i = 0; i < nZmiss; ++i) {
+        Zactual[2 * i] = Z1[i];
+        Zactual[2 * i + 1] = Z2[i];
+    }
+    for (int i = 0; i < nZobs; ++i) {
+        Zobs[2 * i] = Z1[nZmiss + i];
+        Zobs[2 * i + 1] = Z2[nZmiss + i];
+    }
+    data->lmiss.x = l.x;
+    data->lmiss.y = l.y;
+    data->lmiss.z = NULL;
+    data->lobs.x = &l.x[nZmiss];
+    data->lobs.y = &l.y[nZmiss];
+    data->lobs.z = NULL;
+}
+
 /* ------------------------------------------------------------------------- */
 /* real-data flat files (misc/compute/flat_file.c, misc/compute/MLE_misc.c)  */
 /* ------------------------------------------------------------------------- */

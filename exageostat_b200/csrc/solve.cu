@@ -124,10 +124,17 @@ __global__ void __launch_bounds__(256) xg_predict_cross_kernel(const double *__r
 {
     __shared__ double red[8];
     const int m = blockIdx.x;
-    const double x1 = xm[m], y1 = ym[m];
     double s = 0.0;
-    for (int o = threadIdx.x; o < nobs; o += blockDim.x)
-        s += xg_matern_value(xg_distance(x1, y1, xo[o], yo[o], metric), p) * alpha[o];
+    if (p.bivariate) {
+        /* rows and columns interleave the two variables: index 2 l + v */
+        const double x1 = xm[m >> 1], y1 = ym[m >> 1];
+        for (int o = threadIdx.x; o < nobs; o += blockDim.x)
+            s += xg_matern_value_biv(xg_distance(x1, y1, xo[o >> 1], yo[o >> 1], metric), p, m & 1, o & 1) * alpha[o];
+    } else {
+        const double x1 = xm[m], y1 = ym[m];
+        for (int o = threadIdx.x; o < nobs; o += blockDim.x)
+            s += xg_matern_value(xg_distance(x1, y1, xo[o], yo[o], metric), p) * alpha[o];
+    }
     for (int off = 16; off > 0; off >>= 1) s += __shfl_xor_sync(0xffffffffu, s, off);
     if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = s;
     __syncthreads();
@@ -148,19 +155,36 @@ void xg_launch_predict_cross(const double *xm, const double *ym, int nmiss, cons
 
 __global__ void xg_mse_kernel(const double *__restrict__ za, const double *__restrict__ zm, int n, double *out)
 {
-    __shared__ double red[32];
+    /* out[0] = the MSE; out[1], out[2] = the MSEs of the even and odd entries
+     * (the two variables of a bivariate field, CORE_dmse_bivariate_starpu,
+     * codelet_zmse_bivariate.c:22-51, averaged over n / 2 as MLE_dexact.c:845-847).
+     * blockDim is even, so each thread sees entries of one parity only. */
+    __shared__ double red[2][32];
     double s = 0.0;
     for (int i = threadIdx.x; i < n; i += blockDim.x) {
         const double d = za[i] - zm[i];
         s += d * d;
     }
-    for (int off = 16; off > 0; off >>= 1) s += __shfl_xor_sync(0xffffffffu, s, off);
-    if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = s;
+    double se = (threadIdx.x & 1) ? 0.0 : s, so = (threadIdx.x & 1) ? s : 0.0;
+    for (int off = 16; off > 0; off >>= 1) {
+        se += __shfl_xor_sync(0xffffffffu, se, off);
+        so += __shfl_xor_sync(0xffffffffu, so, off);
+    }
+    if ((threadIdx.x & 31) == 0) {
+        red[0][threadIdx.x >> 5] = se;
+        red[1][threadIdx.x >> 5] = so;
+    }
     __syncthreads();
     if (threadIdx.x == 0) {
-        double t = 0.0;
-        for (int w = 0; w < (int)(blockDim.x >> 5); ++w) t += red[w];
-        out[0] = t / n;
+        double te = 0.0, to = 0.0;
+        for (int w = 0; w < (int)(blockDim.x >> 5); ++w) {
+            te += red[0][w];
+            to += red[1][w];
+        }
+        out[0] = (te + to) / n;
+        const int half = n / 2;
+        out[1] = half > 0 ? te / half : 0.0;
+        out[2] = half > 0 ? to / half : 0.0;
     }
 }
 

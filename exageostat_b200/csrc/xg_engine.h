@@ -150,7 +150,7 @@ int xg_predict_create(XgPredict **out, int nmiss, int nobs, int ts);
 void xg_predict_destroy(XgPredict *q);
 int xg_predict_run(XgPredict *q, const double *theta, int kernel, int metric, const double *xm, const double *ym,
                    const double *xo, const double *yo, const double *zobs, const double *zactual, double *zmiss,
-                   double *mse);
+                   double *mse, double *mse_parts);
 
 /* MLOE / MMOM workspace (assess.cu): the two observed-set factors and five
  * R-layout right-hand-side stores (one row per missing point): k_a -> A,

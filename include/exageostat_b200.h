@@ -288,7 +288,11 @@ double MORSE_dmle_Tile(unsigned n, const double *theta, double *grad, void *data
  * (n doubles) to host memory. */
 void MLE_get_zobs(MLE_data *data, double *z, int n);
 
-/* src/include/MLE.h:59-61 (src/compute/MLE.c:284-306 -> MLE_dexact.c:613-685). */
+/* src/include/MLE.h:59-61 (src/compute/MLE.c:284-306 -> MLE_dexact.c:613-685).
+ * nZmiss, nZobs count locations; the bivariate kernel doubles them into
+ * matrix rows (MLE_dexact.c:640-653), and EXAGEOSTAT_dmle_Predict_Tile then
+ * takes the row counts (2 nZmiss, 2 nZobs), sets data->mserror1 / mserror2
+ * and results.mse_pred1 / _pred2 to the per-variable errors. */
 void prediction_init(MLE_data *data, int nZmiss, int nZobs, int ts, int p_grid, int q_grid, int mse_flag);
 void EXAGEOSTAT_dmle_Predict_Allocate(MLE_data *data, int nZmiss, int nZobs, int dts, int p_grid, int q_grid,
                                       int mse_flag);
@@ -362,6 +366,11 @@ int locations_obs_zsort_inplace(int n, location *locations, double *z);
  * data->lmiss.x / .y are malloc'd N-arrays and data->lobs points into them
  * at offset nZmiss, as in the reference. */
 void pick_random_points(MLE_data *data, double *Zobs, double *Zactual, int nZmiss, int nZobs, int N);
+/* misc/compute/MLE_misc.c:1261-1285, 1744-1810 (MLE_misc.h:442): the
+ * bivariate forms.  N = 2 x locations; nZmiss, nZobs count locations; Zobs
+ * and Zactual receive 2 nZobs and 2 nZmiss interleaved values. */
+void shuffle2(double *array, double *array2, location *locations, size_t n);
+void pick_random_points2(MLE_data *data, double *Zobs, double *Zactual, int nZmiss, int nZobs, int N);
 
 /* ---- real-data flat files (misc/include/flat_file.h:25-31, MLE_misc.h:382) ----
  * countlines: the number of '\n' characters of the file (0 if it cannot be

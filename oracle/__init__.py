@@ -43,6 +43,7 @@ def lib():
         L.ora_rand_replay.argtypes = [_I, ctypes.c_long]
         L.ora_pick_random_points.argtypes = [_I, _PD, _PD, _PD, _I, _PD, _PD, _PD, _PD, _PD, _PD]
         L.ora_locations_obs_zsort_inplace.argtypes = [_I, _PD, _PD, _PD]
+        L.ora_pick_random_points2.argtypes = [_I, _PD, _PD, _PD, _I, _PD, _PD, _PD, _PD, _PD, _PD]
         L.ora_core_dcmg.argtypes = [_PD, _I, _I, _I, _I, _PD, _PD, _PD, _PD, _PD, _I]
         L.ora_gen_lower_dense.argtypes = [_PD, _I, _PD, _PD, _PD, _I]
         L.ora_dcmg_deriv.argtypes = [_PD, _I, _I, _I, _I, _PD, _PD, _PD, _PD, _PD, _I]
@@ -99,6 +100,20 @@ def pick_random_points(x, y, z, n_miss: int, seed: int | None = None, skip: int 
     n_obs = N - n_miss
     out = [np.empty(n_miss), np.empty(n_miss), np.empty(n_miss), np.empty(n_obs), np.empty(n_obs), np.empty(n_obs)]
     lib().ora_pick_random_points(N, _p(x), _p(y), _p(z), int(n_miss), *[_p(a) for a in out])
+    xm, ym, za, xo, yo, zo = out
+    return dict(x_miss=xm, y_miss=ym, z_actual=za, x_obs=xo, y_obs=yo, z_obs=zo)
+
+
+def pick_random_points2(x, y, z, n_miss: int):
+    """Bivariate hold-out (pick_random_points2): x, y hold the locations, z
+    the interleaved values (2 per location); the libc stream is used as it
+    stands (replay it first with rand_replay)."""
+    x, y, z = _f64(x), _f64(y), _f64(z)
+    nloc = x.size
+    n_obs = nloc - n_miss
+    out = [np.empty(n_miss), np.empty(n_miss), np.empty(2 * n_miss), np.empty(n_obs), np.empty(n_obs),
+           np.empty(2 * n_obs)]
+    lib().ora_pick_random_points2(nloc, _p(x), _p(y), _p(z), int(n_miss), *[_p(a) for a in out])
     xm, ym, za, xo, yo, zo = out
     return dict(x_miss=xm, y_miss=ym, z_actual=za, x_obs=xo, y_obs=yo, z_obs=zo)
 
@@ -259,8 +274,9 @@ def dpredict(x_miss, y_miss, x_obs, y_obs, z_obs, z_actual, theta, kernel=0, met
     lib().ora_set_metric(int(metric))
     xm, ym, xo, yo, zo, th = (_f64(a) for a in (x_miss, y_miss, x_obs, y_obs, z_obs, theta))
     za = None if z_actual is None else _f64(z_actual)
-    zmiss = np.empty(xm.size)
-    mse = lib().ora_dpredict(xm.size, xo.size, _p(xm), _p(ym), _p(xo), _p(yo), _p(zo),
+    nm = xm.size * (2 if kernel == 2 else 1)  # matrix rows: two per location for the bivariate kernel
+    zmiss = np.empty(nm)
+    mse = lib().ora_dpredict(nm, zo.size, _p(xm), _p(ym), _p(xo), _p(yo), _p(zo),
                              None if za is None else _p(za), _p(th), int(kernel), _p(zmiss))
     return float(mse), zmiss
 

@@ -9,7 +9,8 @@
  * What it restates (paths are inside the reference project):
  *   - GenerateXYLoc / uniform_distribution / zsort_locations and the Morton
  *     helpers              misc/compute/MLE_misc.c:225-319, 753-792
- *   - shuffle, pick_random_points, locations_obs_zsort_inplace + radix sort
+ *   - shuffle, shuffle2, pick_random_points, pick_random_points2,
+ *     locations_obs_zsort_inplace + radix sort
  *                          misc/compute/MLE_misc.c:405-534, 1238-1259, 1700-1741
  *   - core_dcmg (Matern) and core_dcmg_nuggets
  *                          exageostat_exact/cpu_core/compute/core_zcmg.c:71-92, 963-994
@@ -398,6 +399,51 @@ void ora_pick_random_points(int N, const double *x, const double *y, const doubl
     free(ly);
     free(lx);
     free(Z);
+}
+
+/* pick_random_points2 + shuffle2 (MLE_misc.c:1261-1285, 1744-1810): the
+ * bivariate hold-out over nloc locations, z interleaved (2 nloc values); the
+ * first nZmiss shuffled locations are missing, outputs interleaved again. */
+void ora_pick_random_points2(int nloc, const double *x, const double *y, const double *z, int nZmiss,
+                             double *xmiss, double *ymiss, double *zactual, double *xobs, double *yobs, double *zobs)
+{
+    double *Z1 = (double *)malloc(sizeof(double) * (size_t)nloc);
+    double *Z2 = (double *)malloc(sizeof(double) * (size_t)nloc);
+    double *lx = (double *)malloc(sizeof(double) * (size_t)nloc);
+    double *ly = (double *)malloc(sizeof(double) * (size_t)nloc);
+    for (int i = 0; i < nloc; ++i) {
+        Z1[i] = z[2 * (size_t)i];
+        Z2[i] = z[2 * (size_t)i + 1];
+        lx[i] = x[i];
+        ly[i] = y[i];
+    }
+    size_t n = (size_t)nloc;
+    if (n > 1) {
+        for (size_t i = 0; i < n - 1; ++i) {
+            size_t j = i + (size_t)rand() / (RAND_MAX / (n - i) + 1);
+            double t = Z1[j]; Z1[j] = Z1[i]; Z1[i] = t;
+            t = Z2[j]; Z2[j] = Z2[i]; Z2[i] = t;
+            t = lx[j]; lx[j] = lx[i]; lx[i] = t;
+            t = ly[j]; ly[j] = ly[i]; ly[i] = t;
+        }
+    }
+    const int nZobs = nloc - nZmiss;
+    for (int i = 0; i < nZmiss; ++i) {
+        zactual[2 * i] = Z1[i];
+        zactual[2 * i + 1] = Z2[i];
+        xmiss[i] = lx[i];
+        ymiss[i] = ly[i];
+    }
+    for (int i = 0; i < nZobs; ++i) {
+        zobs[2 * i] = Z1[nZmiss + i];
+        zobs[2 * i + 1] = Z2[nZmiss + i];
+        xobs[i] = lx[nZmiss + i];
+        yobs[i] = ly[nZmiss + i];
+    }
+    free(ly);
+    free(lx);
+    free(Z2);
+    free(Z1);
 }
 
 /* ========================================================================== */

@@ -69,3 +69,43 @@ def test_bivariate_short_mle(gpu, ora):
         assert np.isfinite(f) and ev > 10
         assert f >= s.mle_alg([1.0, 1.0, 0.2, 0.6, 0.6, 0.0])
         assert f == pytest.approx(ora.dmle(x, y, z, th, kernel=2)[0], rel=1e-10)
+
+
+def test_bivariate_holdout_and_kriging(gpu, ora):
+    """pick_random_points2 (bit-exact against the oracle with the same libc
+    draws) and kriging of both variables through EXAGEOSTAT_dmle_Predict_Tile
+    with the row counts 2 nZmiss, 2 nZobs (1e-9), with the per-variable
+    errors in data.mserror1 / mserror2 and results.mse_pred1 / _pred2."""
+    import ctypes
+
+    libc = ctypes.CDLL(None)
+    theta = [1.0, 2.0, 0.1, 0.5, 1.2, 0.4]
+    nloc, nmiss = 600, 50
+    x, y, z_ref, e = ora.synthetic_field(2 * nloc, 8, theta, kernel=2)
+    P = ctypes.POINTER(ctypes.c_double)
+    with gpu.Session(x, y, kernel=2, dts=128) as s:
+        s.zvg(theta, e)
+        z = s.z()
+        zobs, zact = np.empty(2 * (nloc - nmiss)), np.empty(2 * nmiss)
+        libc.srand(11)
+        s.L.pick_random_points2(ctypes.byref(s.data), zobs.ctypes.data_as(P), zact.ctypes.data_as(P), nmiss,
+                                nloc - nmiss, 2 * nloc)
+        xm = np.ctypeslib.as_array(s.data.lmiss.x, (nmiss,)).copy()
+        ym = np.ctypeslib.as_array(s.data.lmiss.y, (nmiss,)).copy()
+        xo = np.ctypeslib.as_array(s.data.lobs.x, (nloc - nmiss,)).copy()
+        yo = np.ctypeslib.as_array(s.data.lobs.y, (nloc - nmiss,)).copy()
+        libc.srand(11)
+        ref = ora.pick_random_points2(x, y, z, nmiss)
+        for a, b in ((xm, "x_miss"), (ym, "y_miss"), (xo, "x_obs"), (yo, "y_obs"), (zobs, "z_obs"),
+                     (zact, "z_actual")):
+            assert np.array_equal(a, ref[b]), b
+        mse, zmiss = s.predict(theta, xm, ym, xo, yo, zobs, zact)
+        res = gpu.Output.in_dll(gpu.lib(), "results")
+        m1, m2 = s.data.mserror1, s.data.mserror2
+        assert (res.mse_pred1, res.mse_pred2) == (m1, m2)
+    mse_ref, zm_ref = ora.dpredict(xm, ym, xo, yo, zobs, zact, theta, kernel=2)
+    assert zmiss.size == 2 * nmiss
+    assert np.allclose(zmiss, zm_ref, rtol=1e-9, atol=1e-12)
+    assert mse == pytest.approx(mse_ref, rel=1e-9)
+    assert m1 == pytest.approx(np.mean((zact[0::2] - zm_ref[0::2]) ** 2), rel=1e-9)
+    assert m2 == pytest.approx(np.mean((zact[1::2] - zm_ref[1::2]) ** 2), rel=1e-9)
