@@ -78,3 +78,33 @@ def test_sliced_great_circle(gpu, ora):
     ref = ora.dmle(lat, lon, z, theta, metric=1)[0]
     got = gpu.dmle_host_sliced(lat, lon, z, theta, metric=1, ts=128)[0]
     assert abs(got - ref) / abs(ref) < 1e-7
+
+
+def test_batch_and_mixed_great_circle(gpu, ora):
+    """Batched regional fields and the banded TF32 path with great-circle
+    distance (per-field bar relative to the scale of the loglik terms, as in
+    the Euclidean batch tests; mixed 1e-6)."""
+    import math
+
+    rng = np.random.default_rng(9)
+    xs, ys, zs, th = [], [], [], []
+    for f in range(8):
+        n = int(rng.integers(300, 1200))
+        lat0, lon0 = rng.uniform(-40, 40), rng.uniform(-120, 120)
+        x, y = lat0 + 5 * rng.random(n), lon0 + 5 * rng.random(n)
+        theta = [rng.uniform(0.5, 2.0), rng.uniform(30.0, 80.0), rng.uniform(0.3, 1.0)]
+        zs.append(ora.dzvg(x, y, theta, rng.standard_normal(n), metric=1))
+        xs.append(x), ys.append(y), th.append(theta)
+    th = np.array(th)
+    with gpu.Batch(xs, ys, zs, metric=1, ts=256) as b:
+        got = b.loglik(th)
+    for i in range(8):
+        l, ld, dp, _ = ora.dmle(xs[i], ys[i], zs[i], th[i], metric=1)
+        scale = 0.5 * abs(dp) + 0.5 * abs(ld) + 0.5 * len(xs[i]) * math.log(2 * math.pi)
+        assert abs(got[i] - l) / scale < 1e-10
+    theta = [1.0, 100.0, 0.5]
+    lat, lon = _latlon(1300, 10)
+    _, _, z, _ = ora.synthetic_field(1300, 10, theta, metric=1, locations=(lat, lon))
+    ref = ora.dmle(lat, lon, z, theta, metric=1)[0]
+    got = gpu.dmle_host_mixed(lat, lon, z, theta, metric=1, ts=256, band=1, passes=3)[0]
+    assert abs(got - ref) / abs(ref) < 1e-6
