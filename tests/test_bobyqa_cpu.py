@@ -1,6 +1,5 @@
 """The library's bound-constrained derivative-free maximiser (host code, no GPU)."""
 import numpy as np
-import pytest
 
 
 def test_maximises_concave_quadratic_in_the_interior(xg):

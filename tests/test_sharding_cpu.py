@@ -4,7 +4,6 @@ import os
 import socket
 
 import numpy as np
-import pytest
 
 
 def test_lpt_partition_balances_cubic_costs():
