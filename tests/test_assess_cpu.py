@@ -91,3 +91,35 @@ def test_device_element_derivatives_match_oracle(ora, tmp_path):
     # difference of K_nu) is good to ~7e-10 of the largest entry; the device
     # function agrees with mpmath to ~1e-13
     assert np.all(err < 2e-9), err
+
+
+def _golden():
+    import json
+
+    with open(os.path.join(ROOT, "tests", "golden", "assess_mpmath.json")) as f:
+        return json.load(f)
+
+
+def test_oracle_fisher_matches_mpmath(ora):
+    """tests/golden/assess_mpmath.json (tests/golden/gen_assess_mpmath.py):
+    30-digit Fisher matrices of small fields; the oracle's locations are the
+    golden ones bit for bit and its F agrees to 1e-8 of sqrt(F_jj F_kk) (its
+    nu derivative uses the reference's psi series and a difference quotient)."""
+    for c in _golden()["fisher"]:
+        x, y = ora.generate_xy_loc(c["n"], c["seed"])
+        assert np.array_equal(x, c["x"]) and np.array_equal(y, c["y"])
+        F, _ = ora.fisher(x, y, c["theta"], c["kernel"])
+        G = np.array([[float(v) for v in row] for row in c["F"]])
+        scale = np.sqrt(np.outer(np.diag(G), np.diag(G)))
+        assert (np.abs(F - G) / scale).max() < 1e-8, (c["name"], F, G)
+
+
+def test_oracle_mloe_mmom_matches_mpmath(ora):
+    for c in _golden()["mloe_mmom"]:
+        x, y = ora.generate_xy_loc(c["n"], c["seed"])
+        k = c["nmiss"]
+        mloe, mmom, terms = ora.mloe_mmom(x[:k], y[:k], x[k:], y[k:], c["truth"], c["est"], c["kernel"])
+        G = np.array([[float(v) for v in r] for r in c["terms"]])
+        assert np.abs(terms[:, :4] - G[:, :4]).max() < 1e-12 * c["truth"][0], c["name"]
+        assert np.abs(terms[:, 4:] - G[:, 4:]).max() < 1e-10, c["name"]
+        assert mloe == pytest.approx(float(c["mloe"]), abs=1e-11) and mmom == pytest.approx(float(c["mmom"]), abs=1e-11)
