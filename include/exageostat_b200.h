@@ -8,6 +8,9 @@
  * the reference project.  Differences from the reference are listed per
  * function; the main one is that no function calls exit(): failures are
  * reported through return values, data fields and exageostat_last_error().
+ * Beyond the likelihood path: kriging, the Fisher information, MLOE / MMOM,
+ * the flat-file readers, great-circle distance (dm = "gc") and the
+ * bivariate parsimonious Matern kernel.
  *
  * Everything runs on one CUDA device (the current device at
  * exageostat_init).  All pointers in these signatures are HOST pointers.
