@@ -549,13 +549,14 @@ int exageostat_b200_batch_autotune(int nfields, const int *n, const double *x, c
                                    int kernel, int metric, const double *theta, int *ts, double *report,
                                    void **handle);
 
-/* Diagnostics used by the parity tests.  All run on the GPU. */
+/* ---- diagnostics used by the parity tests (no counterpart in the reference; all run on the GPU) ---- */
 int exageostat_b200_bessel_knu(int n, const double *nu, const double *x, double *out);
 int exageostat_b200_matern_pairs(int n, const double *x1, const double *y1, const double *x2, const double *y2,
                                  const double *theta, int kernel, int metric, double *out);
 /* Dense lower-triangular Sigma (factor = 0) or its Cholesky factor L
- * (factor = 1) for n locations, row-major n x n with zeros above the
- * diagonal, computed with tile size ts. */
+ * (factor = 1) of dimension n (the locations, or 2 x the locations for the
+ * bivariate kernel), row-major n x n with zeros above the diagonal, computed
+ * with tile size ts. */
 int exageostat_b200_covariance_dense(int n, const double *x, const double *y, const double *theta, int kernel,
                                      int metric, int ts, int factor, double *out);
 /* The factor L of the INT8-sliced path (all tiles FP64), row-major n x n
