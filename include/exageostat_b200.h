@@ -254,7 +254,9 @@ void exageostat_finalize(void);
 
 /* exageostat_exact/src/include/MLE_exact.h:60-62 (MLE_dexact.c:1938-2017).
  * Allocates the device covariance (lower tiles of size dts), z and the
- * solve buffers for N locations and uploads data->l1.x / l1.y.  Handles are
+ * solve buffers for N locations and uploads data->l1.x / l1.y (for
+ * bivariate_matern_parsimonious N is twice the number of locations, as the
+ * reference driver sets it, synthetic_dmle_test.c:134).  Handles are
  * stored in data->descC / descZ / descZcpy.  On failure data->descC stays
  * NULL and exageostat_last_error() says why.  MORSE_dmle_Call is the
  * MORSE-era name of the same function. */
