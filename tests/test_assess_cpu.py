@@ -123,3 +123,41 @@ def test_oracle_mloe_mmom_matches_mpmath(ora):
         assert np.abs(terms[:, :4] - G[:, :4]).max() < 1e-12 * c["truth"][0], c["name"]
         assert np.abs(terms[:, 4:] - G[:, 4:]).max() < 1e-10, c["name"]
         assert mloe == pytest.approx(float(c["mloe"]), abs=1e-11) and mmom == pytest.approx(float(c["mmom"]), abs=1e-11)
+
+
+def test_device_formulations_equal_the_reference_sequences(ora):
+    """The GPU computes MLOE / MMOM as A = L_a^-1 k_a, U = L_a^-1 k_t,
+    T = L_t^-1 k_t, W = L_a^-T A, V = L_t^T W with expr1 = U.A,
+    expr2 = s_t - 2 expr1 + V.V, expr3 = s_t - T.T, expr4 = s_a - A.A, and the
+    Fisher matrix as tr(G_j G_k) with G_j = Sigma^-1 dSigma_j; restated here in
+    numpy, both equal the oracle's restatement of the reference's own sequence
+    (per-point TRSM/TRMM/GEMM, MLE_dexact.c:1300-1375; CJ CK products,
+    :1846-1879) to rounding."""
+    from scipy.linalg import solve_triangular
+
+    x, y = ora.generate_xy_loc(400, 11)
+    xo, yo, xm, ym = x[:340], y[:340], x[340:], y[340:]
+    truth, est = [1.3, 0.1, 0.7], [1.0, 0.08, 0.9]
+    La = np.linalg.cholesky(ora.covariance_full(xo, yo, est))
+    Lt = np.linalg.cholesky(ora.covariance_full(xo, yo, truth))
+    ka = ora.core_dcmg(340, 60, 0, 0, xo, yo, xm, ym, est)
+    kt = ora.core_dcmg(340, 60, 0, 0, xo, yo, xm, ym, truth)
+    A = solve_triangular(La, ka, lower=True)
+    U = solve_triangular(La, kt, lower=True)
+    T = solve_triangular(Lt, kt, lower=True)
+    W = solve_triangular(La, A, lower=True, trans="T")
+    V = Lt.T @ W
+    e1 = np.sum(U * A, axis=0)
+    e2 = (truth[0] - 2 * e1) + np.sum(V * V, axis=0)
+    e3 = truth[0] - np.sum(T * T, axis=0)
+    e4 = est[0] - np.sum(A * A, axis=0)
+    _, _, ref = ora.mloe_mmom(xm, ym, xo, yo, truth, est)
+    assert np.abs(np.stack([e1, e2, e3, e4], axis=1) - ref[:, :4]).max() < 1e-13
+    # Fisher: traces of S dSigma_j S dSigma_k
+    n = 200
+    theta = [1.3, 0.1, 0.7]
+    S = np.linalg.inv(ora.covariance_full(x[:n], y[:n], theta))
+    G = [S @ ora.dcmg_deriv(n, n, 0, 0, x[:n], y[:n], x[:n], y[:n], theta, j) for j in range(3)]
+    F = np.array([[0.5 * np.sum(G[j] * G[k].T) for k in range(3)] for j in range(3)])
+    Fo, _ = ora.fisher(x[:n], y[:n], theta)
+    assert np.abs(F - Fo).max() / np.abs(Fo).max() < 1e-10
