@@ -53,7 +53,7 @@ def parse():
     ap.add_argument("--mode", choices=["evals", "bands", "mle", "batch", "grad", "predict", "assess"], default="evals",
                     help="evals: the default bench line; bands: accuracy/time per band width; "
                          "mle: time-to-MLE of the drivers; batch: batched regional fields; grad: gradient cost; "
-                         "predict: kriging")
+                         "predict: kriging; assess: Fisher information and MLOE / MMOM")
     ap.add_argument("--bands", default="1,2,4,8,16")
     ap.add_argument("--no-sliced-row", dest="sliced_row", action="store_false",
                     help="bands mode: skip the INT8-sliced row")
