@@ -590,6 +590,12 @@ static void xg_mloe_mmom(MLE_data *data, double *truth_theta, double *estimated_
         data->mloe = data->mmom = NAN;
         return;
     }
+    if (!data->lmiss.x || !data->lmiss.y || !data->lobs.x || !data->lobs.y) {
+        xg_fail(XG_ERR_BAD_ARGUMENT, "data->lobs / data->lmiss hold no locations (pick_random_points sets them)");
+        fprintf(stderr, "EXAGEOSTAT_dmle_mloe_mmom_Tile: %s\n", exageostat_last_error());
+        data->mloe = data->mmom = NAN;
+        return;
+    }
     XgAssess *q = (XgAssess *)data->desck_t;
     if (!q || q->nmiss != nZmiss || q->nobs != nZobs) {
         EXAGEOSTAT_dmle_mloe_mmom_Allocate(data, nZmiss, nZobs, 0, 1, 1);
