@@ -14,6 +14,13 @@
  *
  * Everything runs on one CUDA device (the current device at
  * exageostat_init).  All pointers in these signatures are HOST pointers.
+ *
+ * Threads: one MLE_data (or batch handle) is used by one host thread at a
+ * time.  Calls for different MLE_data may come from different threads; they
+ * share the library's CUDA stream and so run one after the other on the
+ * device.  The first exageostat_b200_batch_loglik of a batch records its
+ * launch sequence into a CUDA graph on that stream: make no other library
+ * call from another thread while it runs.
  */
 #ifndef EXAGEOSTAT_B200_H
 #define EXAGEOSTAT_B200_H
