@@ -3,20 +3,26 @@
  *
  * Some callers cannot call cudaMalloc: code running inside another
  * framework's memory pool or allocator (which owns every device allocation
- * and may forbid or interpose foreign ones), code that has to keep working
- * while the device heap is exhausted, and code recorded into CUDA graphs by
- * a host that does not allow allocation calls on its thread.  For them
+ * and may forbid or interpose foreign ones), and code that has to keep
+ * working while the device heap is exhausted.  For them
  * exageostat_b200_dmle_device_noalloc() evaluates the exact Matern
  * log-likelihood for up to XG_NOALLOC_MAX_N locations using only caller
  * buffers (device x, y, z and result) plus one file-scope device array,
  * xg_noalloc_scratch, that the library carries for every GPU that loads it
  * (about 18 MB) until the process exits.
  *
+ * The call is synchronous: it enqueues its work on the caller's stream, then
+ * reads the device status word back and waits for the stream before it
+ * returns.  d_out is written only when the evaluation succeeded; on any
+ * error its contents are left as they were.
+ *
  * The scratch array is shared by all calls on a device and keeps the
  * previous call's contents; every buffer inside it that must start at zero
- * (solve-vector padding, status word) is cleared by each call.  Calls whose
- * work overlaps on the GPU (other streams, other host threads) race on the
- * array: serialise them.
+ * (solve-vector padding, status word) is cleared by each call, and the tile
+ * table is rebuilt.  Calls whose work overlaps on the GPU (other streams,
+ * other host threads) race on the array: serialise them.  The scratch
+ * address is cached per device ordinal, so only the primary context of each
+ * device (the runtime API's default) is supported.
  */
 #include <stdint.h>
 #include <string.h>
@@ -76,6 +82,17 @@ static double *xg_noalloc_setup(int *rc)
     }
     std::lock_guard<std::mutex> lk(g_noalloc_mu);
     if (g_noalloc_ptr[dev]) return g_noalloc_ptr[dev];
+    int major = 0;
+    e = cudaDeviceGetAttribute(&major, cudaDevAttrComputeCapabilityMajor, dev);
+    if (e != cudaSuccess) {
+        *rc = xg_fail(XG_ERR_CUDA, "cudaDeviceGetAttribute: %s", cudaGetErrorString(e));
+        return nullptr;
+    }
+    if (major != 10) {
+        *rc = xg_fail(XG_ERR_UNSUPPORTED, "device %d is sm_%dx; the library is built for sm_100a (B200) only", dev,
+                      major);
+        return nullptr;
+    }
     void *ptr = nullptr;
     e = cudaGetSymbolAddress(&ptr, xg_noalloc_scratch);
     if (e != cudaSuccess || !ptr) {
@@ -112,6 +129,8 @@ extern "C" int exageostat_b200_dmle_device_noalloc(int n, const double *d_x, con
     if (!d_x || !d_y || !d_z || !d_out || !theta)
         return xg_fail(XG_ERR_BAD_ARGUMENT, "a buffer argument is NULL");
     if (kernel != 0 && kernel != 1) return xg_fail(XG_ERR_BAD_ARGUMENT, "kernel %d", kernel);
+    if (metric != 0 && metric != 1)
+        return xg_fail(XG_ERR_BAD_ARGUMENT, "metric %d (0 Euclidean, 1 great circle)", metric);
     int rc = xg_check_theta(theta, kernel);
     if (rc) return rc;
     rc = XG_OK;
@@ -152,12 +171,15 @@ extern "C" int exageostat_b200_dmle_device_noalloc(int n, const double *d_x, con
     xg_launch_finalize(part, part + M.nt, M.nt, n, out, status, status + 1, st);
     e = cudaGetLastError();
     if (e != cudaSuccess) return xg_fail(XG_ERR_CUDA, "launch: %s", cudaGetErrorString(e));
-    e = cudaMemcpyAsync(d_out, out, 3 * sizeof(double), cudaMemcpyDeviceToDevice, st);
     int sv[2] = {0, 0};
-    if (e == cudaSuccess) e = cudaMemcpyAsync(sv, status, sizeof sv, cudaMemcpyDeviceToHost, st);
+    e = cudaMemcpyAsync(sv, status, sizeof sv, cudaMemcpyDeviceToHost, st);
     if (e == cudaSuccess) e = cudaStreamSynchronize(st);
     if (e != cudaSuccess) return xg_fail(XG_ERR_CUDA, "no-allocation evaluation: %s", cudaGetErrorString(e));
     if (sv[0] & XG_ST_NOT_SPD) return xg_fail(XG_ERR_NOT_SPD, "the covariance is not positive definite (pivot %d)", sv[1]);
     if (sv[0]) return xg_fail(XG_ERR_TIMEOUT, "device status word 0x%x", sv[0]);
+    /* the result reaches the caller's buffer only once the status is clean */
+    e = cudaMemcpyAsync(d_out, out, 3 * sizeof(double), cudaMemcpyDeviceToDevice, st);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+    if (e != cudaSuccess) return xg_fail(XG_ERR_CUDA, "no-allocation result copy: %s", cudaGetErrorString(e));
     return XG_OK;
 }

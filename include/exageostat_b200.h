@@ -505,13 +505,18 @@ int exageostat_b200_get_profile(MLE_data *data, double *out, int n);
  * device heap exhausted).  Inputs and the result are DEVICE pointers owned by
  * the caller: d_x, d_y, d_z (n doubles each) and d_out (3 doubles: loglik,
  * logdet, z^T Sigma^-1 z); theta (3 or 4 values) is a host pointer; stream is
- * a cudaStream_t (NULL = default stream); the call returns after the stream
- * work completes.  The library works in one static device array of about
- * 18 MB that every GPU loading the library holds until exit, so n is at most
- * 2048 (larger n returns XG_ERR_BAD_ARGUMENT).  The first call on a device
- * looks up that array's device address and sets up the kernels: make it
- * before any stream capture.  All calls share the array; calls that overlap
- * on the GPU race and must be serialised by the caller. */
+ * a cudaStream_t (NULL = default stream); metric is 0 (Euclidean) or 1
+ * (great circle), anything else is XG_ERR_BAD_ARGUMENT.  The call is
+ * synchronous: it waits for its stream work and reads the status back before
+ * it returns.  d_out is written only on success; when the call returns an
+ * error, d_out keeps its previous contents.  The library works in one static
+ * device array of about 18 MB that every GPU loading the library holds until
+ * exit, so n is at most 2048 (larger n returns XG_ERR_BAD_ARGUMENT).  The
+ * first call on a device checks that it is an sm_100 GPU, looks up that
+ * array's device address and sets up the kernels: make it before any stream
+ * capture.  The address is cached per device ordinal, so only each device's
+ * primary context is supported.  All calls share the array; calls that
+ * overlap on the GPU race and must be serialised by the caller. */
 int exageostat_b200_dmle_device_noalloc(int n, const double *d_x, const double *d_y, const double *d_z,
                                         const double *theta, int kernel, int metric, double *d_out, void *stream);
 
@@ -559,6 +564,12 @@ int exageostat_b200_batch_autotune(int nfields, const int *n, const double *x, c
                                    void **handle);
 
 /* ---- diagnostics used by the parity tests (no counterpart in the reference; all run on the GPU) ---- */
+/* Runs the bounded-wait path of the kernels on purpose: one thread waits on
+ * a shared-memory barrier that nothing arrives on, gives up after limit_us
+ * microseconds (1 to 1e6), records the timeout bit of a status word and
+ * returns.  Returns XG_ERR_TIMEOUT (the expected result) and the measured
+ * wait in *waited_us (may be NULL); the CUDA context stays usable. */
+int exageostat_b200_diag_wait_timeout(double limit_us, double *waited_us);
 int exageostat_b200_bessel_knu(int n, const double *nu, const double *x, double *out);
 int exageostat_b200_matern_pairs(int n, const double *x1, const double *y1, const double *x2, const double *y2,
                                  const double *theta, int kernel, int metric, double *out);
