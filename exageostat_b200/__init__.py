@@ -163,6 +163,7 @@ def lib():
         "exageostat_b200_set_data": (_I, [PM, _PD, _PD, _PD]),
         "exageostat_b200_set_profiling": (_I, [PM, _I]),
         "exageostat_b200_get_profile": (_I, [PM, _PD, _I]),
+        "exageostat_b200_diag_wait_timeout": (_I, [_D, _PD]),
         "exageostat_b200_dmle_device_noalloc": (_I, [_I, _PD, _PD, _PD, _PD, _I, _I, _PD, _VP]),
         "exageostat_b200_bobyqa": (_I, [_I, _PD, _PD, _PD, _D, _D, _D, _I, _VP, _VP, _PD]),
         "EXAGEOSTAT_sdmle_Tile": (_D, [ctypes.c_uint, _PD, _PD, _VP]),
@@ -212,6 +213,14 @@ def _f64(a) -> np.ndarray:
 
 def last_error() -> str:
     return lib().exageostat_last_error().decode()
+
+
+def diag_wait_timeout(limit_us: float):
+    """Runs a kernel whose bounded wait must run out: returns (rc, waited
+    microseconds); rc is XG_ERR_TIMEOUT when the wait gave up as designed."""
+    w = _D(0.0)
+    rc = lib().exageostat_b200_diag_wait_timeout(float(limit_us), ctypes.byref(w))
+    return rc, w.value
 
 
 def _check(rc: int):

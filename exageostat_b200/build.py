@@ -20,7 +20,7 @@ CSRC = os.path.join(HERE, "csrc")
 BUILD = os.path.join(HERE, "_build")
 LIBDIR = os.path.join(HERE, "lib")
 LIB = os.path.join(LIBDIR, "libexageostat_b200.so")
-SOURCES = ["dense_fp64.cu", "solve.cu", "engine.cu", "capi.cpp", "host_misc.cpp", "noalloc.cu", "bobyqa.cpp", "gradient_fp64.cu", "mixed.cu", "batch.cu", "sliced.cu", "assess.cu"]
+SOURCES = ["dense_fp64.cu", "solve.cu", "engine.cu", "capi.cpp", "host_misc.cpp", "noalloc.cu", "bobyqa.cpp", "gradient_fp64.cu", "mixed.cu", "batch.cu", "sliced.cu", "assess.cu", "diag.cu"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
 FLAGS = ARCH + ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC,-O2,-Wall", "-I", os.path.join(ROOT, "include"),
