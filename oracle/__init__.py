@@ -290,3 +290,39 @@ def synthetic_field(N: int, seed: int, theta, kernel=0, metric=0, locations=None
     x, y = generate_xy_loc(nloc, seed) if locations is None else (_f64(locations[0]), _f64(locations[1]))
     z = dzvg(x, y, theta, e, kernel, metric)
     return x, y, z, e
+
+
+def maximise(x, y, z, lb, ub, starts, kernel=0, metric=0):
+    """Maximiser of the oracle log-likelihood on the box [lb, ub] (lb > 0):
+    scipy's L-BFGS-B in log-parameters with a 4th-order central-difference
+    gradient (h = 1e-5 in log theta), from each start; the best is returned
+    as (theta_hat, loglik).  The reference's own driver is derivative-free
+    (NLopt BOBYQA, synthetic_dmle_test.c:140-142), which is not available
+    here, so the oracle's maximiser is defined by this independent method."""
+    from scipy.optimize import minimize
+
+    x, y, z = _f64(x), _f64(y), _f64(z)
+    lb, ub = _f64(lb), _f64(ub)
+    n = lb.size
+
+    def negll(phi):
+        try:
+            return -dmle(x, y, z, np.exp(phi), kernel, metric)[0]
+        except RuntimeError:
+            return 1e30
+
+    def grad(phi, h=1e-5):
+        g = np.zeros(n)
+        for k in range(n):
+            e = np.zeros(n)
+            e[k] = h
+            g[k] = (8 * (negll(phi + e) - negll(phi - e)) - (negll(phi + 2 * e) - negll(phi - 2 * e))) / (12 * h)
+        return g
+
+    best = None
+    for start in starts:
+        r = minimize(negll, np.log(_f64(start)), jac=grad, method="L-BFGS-B",
+                     bounds=list(zip(np.log(lb), np.log(ub))), options=dict(ftol=1e-15, gtol=1e-9, maxiter=500))
+        if best is None or r.fun < best.fun:
+            best = r
+    return np.exp(best.x), -best.fun

@@ -34,9 +34,16 @@
  *     normalisation (I. J. Thompson & A. R. Barnett, J. Comput. Phys. 64
  *     (1986) 490-509) for x >= 2, then forward recurrence in the order.
  *     Checked against mpmath besselk (tests/golden/kv_mpmath.json).
- *   - LAPACK dpotrf / dtrsv / dtrmv / dposv / dgemv / dlarnv: called from the
- *     OpenBLAS 0.3.30 (ILP64, "scipy_" symbol prefix) bundled with numpy,
- *     exactly as the reference calls MKL/Chameleon for the same operations.
+ *   - The Cholesky factorisation is the tile algorithm of the reference's
+ *     CHAMELEON_dpotrf_Tile (MLE_dexact.c:372; its step structure is the one
+ *     chameleon_psdpotrf spells out with an infinite band, psdportf.c:85-186):
+ *     per block column k, POTRF of the diagonal block, TRSM of the blocks
+ *     below it and the SYRK/GEMM update of the trailing matrix, with the
+ *     block operations (dpotrf, dtrsm, dsyrk, dgemm) called from the OpenBLAS
+ *     0.3.30 (ILP64, "scipy_" symbol prefix) bundled with numpy.  OpenBLAS's
+ *     own one-call dpotrf is not used: it segfaults at N = 40 000 here.
+ *   - dtrsv / dtrmv / dgemv / dlarnv: called from the same OpenBLAS, as the
+ *     reference calls MKL/Chameleon for the same operations.
  *
  * Parity of the reference's GSL values themselves is unpinned (GSL is absent
  * here); this oracle is pinned to mpmath for K_nu and to the reference's own
@@ -73,6 +80,51 @@ extern void scipy_cblas_dgemv64_(int order, int trans, blasint64 m, blasint64 n,
                                  blasint64 incy);
 extern double scipy_cblas_ddot64_(blasint64 n, const double *x, blasint64 incx, const double *y, blasint64 incy);
 extern void scipy_openblas_set_num_threads64_(int n);
+extern void scipy_cblas_dtrsm64_(int order, int side, int uplo, int trans, int diag, blasint64 m, blasint64 n,
+                                 double alpha, const double *a, blasint64 lda, double *b, blasint64 ldb);
+extern void scipy_cblas_dsyrk64_(int order, int uplo, int trans, blasint64 n, blasint64 k, double alpha,
+                                 const double *a, blasint64 lda, double beta, double *c, blasint64 ldc);
+extern void scipy_cblas_dgemm64_(int order, int transa, int transb, blasint64 m, blasint64 n, blasint64 k,
+                                 double alpha, const double *a, blasint64 lda, const double *b, blasint64 ldb,
+                                 double beta, double *c, blasint64 ldc);
+enum { ORA_RIGHT = 142 };
+
+/* Block size of the tile Cholesky (the reference's default dense tile size is
+ * of this order; the factor does not depend on it beyond rounding). */
+#define ORA_NB 512
+
+/* Lower Cholesky factor in place of the column-major N x N array C (leading
+ * dimension N), by block columns of ORA_NB (the tile algorithm):
+ *   C_kk = chol(C_kk); C_ik = C_ik C_kk^-T (i > k);
+ *   C_jj -= C_jk C_jk^T, C_ij -= C_ik C_jk^T (i > j > k).
+ * Returns 0, or the 1-based column of the first non-positive pivot. */
+static blasint64 ora_potrf_tiles(blasint64 N, double *C)
+{
+    for (blasint64 k = 0; k < N; k += ORA_NB) {
+        const blasint64 kb = N - k < ORA_NB ? N - k : ORA_NB;
+        double *Ckk = C + k + k * N;
+        blasint64 info = scipy_LAPACKE_dpotrf64_(ORA_COL_MAJOR, 'L', kb, Ckk, N);
+        if (info != 0) return info > 0 ? k + info : info;
+        const blasint64 m = N - k - kb;
+        if (m == 0) break;
+        double *Cik = Ckk + kb;
+        scipy_cblas_dtrsm64_(ORA_COL_MAJOR, ORA_RIGHT, ORA_LOWER, ORA_TRANS, ORA_NONUNIT, m, kb, 1.0, Ckk, N, Cik,
+                             N);
+        /* trailing update block column by block column: SYRK on the diagonal
+         * block, GEMM on the blocks below it (one dsyrk over the whole
+         * trailing matrix segfaults inside OpenBLAS at N = 40 000) */
+        for (blasint64 j = k + kb; j < N; j += ORA_NB) {
+            const blasint64 jb = N - j < ORA_NB ? N - j : ORA_NB;
+            const double *Cjk = C + j + k * N;
+            scipy_cblas_dsyrk64_(ORA_COL_MAJOR, ORA_LOWER, ORA_NOTRANS, jb, kb, -1.0, Cjk, N, 1.0, C + j + j * N, N);
+            const blasint64 mb = N - j - jb;
+            if (mb > 0)
+                scipy_cblas_dgemm64_(ORA_COL_MAJOR, ORA_NOTRANS, ORA_TRANS, mb, jb, kb, -1.0, Cjk + jb, N, Cjk, N,
+                                     1.0, C + (j + jb) + j * N, N);
+        }
+    }
+    return 0;
+}
 
 #define ORA_PI 3.141592653589793 /* MLE_misc.h:64 */
 
@@ -656,7 +708,7 @@ int ora_dzvg(int N, const double *x, const double *y, const double *theta, int k
     double *C = (double *)malloc(sizeof(double) * (size_t)N * N);
     if (!C) return -100;
     ora_gen_lower(C, N, x, y, theta, kernel);
-    blasint64 info = scipy_LAPACKE_dpotrf64_(ORA_COL_MAJOR, 'L', N, C, N);
+    blasint64 info = ora_potrf_tiles(N, C);
     if (info != 0) {
         free(C);
         return (int)info;
@@ -683,7 +735,7 @@ int ora_dmle(int N, const double *x, const double *y, const double *z, const dou
     }
     ora_gen_lower(C, N, x, y, theta, kernel);
     double t1 = ora_now();
-    blasint64 info = scipy_LAPACKE_dpotrf64_(ORA_COL_MAJOR, 'L', N, C, N);
+    blasint64 info = ora_potrf_tiles(N, C);
     double t2 = ora_now();
     if (info != 0) {
         free(C);
@@ -733,7 +785,12 @@ double ora_dpredict(int nmiss, int nobs, const double *xmiss, const double *ymis
     ora_gen_lower(C22, nobs, xobs, yobs, theta, kernel);
     ora_core_dcmg(C12, nmiss, nobs, 0, 0, xmiss, ymiss, xobs, yobs, theta, kernel);
     memcpy(alpha, zobs, sizeof(double) * (size_t)nobs);
-    blasint64 info = scipy_LAPACKE_dposv64_(ORA_COL_MAJOR, 'L', nobs, 1, C22, nobs, alpha, nobs);
+    /* dposv: the tile Cholesky, then L y = b and L^T alpha = y */
+    blasint64 info = ora_potrf_tiles(nobs, C22);
+    if (info == 0) {
+        scipy_cblas_dtrsv64_(ORA_COL_MAJOR, ORA_LOWER, ORA_NOTRANS, ORA_NONUNIT, nobs, C22, nobs, alpha, 1);
+        scipy_cblas_dtrsv64_(ORA_COL_MAJOR, ORA_LOWER, ORA_TRANS, ORA_NONUNIT, nobs, C22, nobs, alpha, 1);
+    }
     double mse = -1;
     if (info != 0) {
         mse = -2;

@@ -1,0 +1,2 @@
+/* Empty stand-in for <nlopt.h>: the reference functions compiled into oracle/_ref
+ * use none of its declarations (see oracle/ref_shim/prelude.h). */

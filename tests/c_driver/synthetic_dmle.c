@@ -4,11 +4,15 @@
  * only: synthetic field, derivative-free MLE from the lower bounds, kriging
  * of held-out points, the Fisher matrix and MLOE / MMOM.  It shows that a C
  * caller of the reference API compiles and links against the library
- * unchanged.  The N(0,1) draws come from a Box-Muller transform of rand()
- * (the reference draws them with LAPACKE_dlarnv, which is not part of this
- * library).  Prints one line "key=value ..." and exits 0 on success.
+ * unchanged.  The reference draws the N(0,1) vector with LAPACKE_dlarnv,
+ * which is not part of this library: with a fifth argument the driver reads
+ * that vector from a file (one value per line, readObsFile), as a caller
+ * holding the reference's draws would; without it the draws come from a
+ * Box-Muller transform of rand().  Prints one line "key=value ..." (the
+ * log-likelihood at theta0, checksums of z and of the predictions, theta-hat,
+ * the MSE, ...) and exits 0 on success.
  *
- *   synthetic_dmle N dts nZmiss seed
+ *   synthetic_dmle N dts nZmiss seed [nrand_file]
  */
 #include <math.h>
 #include <stdio.h>
@@ -45,12 +49,30 @@ int main(int argc, char **argv)
     exageostat_init(&ncores, &gpus, &dts, &lts);
     location *l = GenerateXYLoc(N, seed);
     data.l1 = *l;
-    double *Nrand = malloc(N * sizeof(double));
-    normals(Nrand, N);
+    double *Nrand;
+    if (argc > 5) {
+        Nrand = readObsFile(argv[5], N);
+        if (!Nrand) {
+            fprintf(stderr, "reading %s: %s\n", argv[5], exageostat_last_error());
+            return 1;
+        }
+    } else {
+        Nrand = malloc(N * sizeof(double));
+        normals(Nrand, N);
+    }
 
     EXAGEOSTAT_dmle_Call(&data, ncores, gpus, dts, 1, 1, N, nZobs, nZmiss);
     double theta0[3] = {1.0, 0.1, 0.5};
     MLE_zvg(&data, Nrand, theta0, N, dts, 0, 1, 1);
+    double *z = malloc(N * sizeof(double));
+    MLE_get_zobs(&data, z, N);
+    double zsum = 0, zsq = 0;
+    for (int i = 0; i < N; ++i) {
+        zsum += z[i];
+        zsq += z[i] * z[i];
+    }
+    free(z);
+    const double loglik0 = MLE_alg(3, theta0, NULL, &data);
 
     double lb[3] = {0.01, 0.01, 0.01}, ub[3] = {5, 5, 5}, x[3] = {0.01, 0.01, 0.01}, fmax = 0;
     const int evals = exageostat_b200_bobyqa(3, x, lb, ub, 0.0, 0.0, 1e-9, 0, MLE_alg, &data, &fmax);
@@ -65,6 +87,8 @@ int main(int argc, char **argv)
     pick_random_points(&data, Zobs, Zact, nZmiss, nZobs, N);
     const double mse = EXAGEOSTAT_dmle_Predict_Tile(&data, x, nZmiss, nZobs, Zobs, Zact, Zmiss, N);
     prediction_finalize(&data);
+    double pred_sum = 0;
+    for (int i = 0; i < nZmiss; ++i) pred_sum += Zmiss[i];
 
     double *finv = EXAGEOSTAT_Fisher_Tile(&data, N, x, dts, 1, 1);
     if (!finv) {
@@ -76,8 +100,10 @@ int main(int argc, char **argv)
     EXAGEOSTAT_dmle_mloe_mmom_Tile(&data, theta0, x, nZmiss, nZobs, N);
     mloe_mmom_finalize(&data);
 
-    printf("evals=%d loglik=%.12f theta=%.8f,%.8f,%.8f mse=%.8f fisher_inv_diag=%.6e,%.6e,%.6e mloe=%.8f mmom=%.8f\n",
-           evals, fmax, x[0], x[1], x[2], mse, finv[0], finv[4], finv[8], data.mloe, data.mmom);
+    printf("evals=%d loglik0=%.17g zsum=%.17g zsq=%.17g loglik=%.17g theta=%.17g,%.17g,%.17g mse=%.17g "
+           "pred_sum=%.17g fisher_inv_diag=%.6e,%.6e,%.6e mloe=%.8f mmom=%.8f\n",
+           evals, loglik0, zsum, zsq, fmax, x[0], x[1], x[2], mse, pred_sum, finv[0], finv[4], finv[8], data.mloe,
+           data.mmom);
     const int ok = mse >= 0 && isfinite(data.mloe) && isfinite(data.mmom) && finv[0] > 0 && finv[4] > 0 &&
                    finv[8] > 0 && results.fisher_00 == finv[0] && results.mloe == data.mloe;
     free(finv);

@@ -1,0 +1,147 @@
+"""Oracle parity at the sizes of the benchmark configurations.
+
+C1  N = 1 600, tile 320: theta-hat of the derivative-free MLE (start at the
+    lower bounds, bounds [0.01, 5]^3, ftol 1e-9; synthetic_dmle_test.c:140-142,
+    283-285) against the maximiser of the oracle's log-likelihood found by
+    scipy's L-BFGS-B, within 1e-3 relative.
+C2  N = 40 000 (200 x 200 jittered grid, seed 0), theta0 = (1, 0.1, 1.5): l at
+    theta0 (closed-form nu = 3/2 on the GPU, the general Bessel path in the
+    oracle) and at nu = 0.73 (general path on both), tile 512 and autotuned,
+    1e-10 relative; kriging of 1 000 held-out points from the other 39 000
+    (pick_random_points, synthetic_dmle_test.c:404-494), predictions and MSE
+    1e-9 relative.
+C4  N = 20 000, nugget, theta = (1, 0.1, 1.0, 0.01): the adjoint gradient
+    against the oracle's central differences with h = 1e-6 theta_k.
+C5  regional fields at the far corner of the batch workload's parameter box
+    (beta near 0.3, nu near 2.5) against the oracle, with a bar scaled by the
+    rounding noise of FP64 Cholesky on those fields.
+
+These are the slowest GPU tests: the oracle runs the C2 and C4 fields on the
+host's cores (about a minute each on 16 threads)."""
+import math
+
+import numpy as np
+import pytest
+
+pytestmark = [pytest.mark.gpu, pytest.mark.slow]
+
+LL_RTOL = 1e-10
+
+
+@pytest.fixture(scope="module")
+def c2_field(gpu):
+    from exageostat_b200.synthetic import dlarnv
+
+    N, seed, theta0 = 40000, 0, [1.0, 0.1, 1.5]
+    x, y = gpu.generate_xy_loc(N, seed)
+    e = dlarnv(seed, N)
+    with gpu.Session(x, y, dts=512) as s:
+        s.zvg(theta0, e)
+        z = s.z()
+    return x, y, z, theta0
+
+
+def test_c2_loglik_matches_oracle(gpu, ora, c2_field):
+    x, y, z, theta0 = c2_field
+    thetas = [theta0, [1.0, 0.1, 0.73]]
+    refs = [ora.dmle(x, y, z, th)[0] for th in thetas]
+    with gpu.Session(x, y, dts=512) as s:
+        s.set_data(z=z)
+        for th, ref in zip(thetas, refs):
+            assert s.mle_alg(th) == pytest.approx(ref, rel=LL_RTOL), (th, ref)
+        ts, _, _ = s.autotune(theta0)
+        assert ts % 128 == 0
+        for th, ref in zip(thetas, refs):
+            assert s.mle_alg(th) == pytest.approx(ref, rel=LL_RTOL), (ts, th, ref)
+
+
+def test_c2_kriging_matches_oracle(gpu, ora, c2_field):
+    x, y, z, theta0 = c2_field
+    split = ora.pick_random_points(x, y, z, 1000, seed=0)
+    assert split["x_obs"].size == 39000
+    mref, zref = ora.dpredict(split["x_miss"], split["y_miss"], split["x_obs"], split["y_obs"], split["z_obs"],
+                              split["z_actual"], theta0)
+    with gpu.Session(x, y, dts=512) as s:
+        s.set_data(z=z)
+        mse, zm = s.predict(theta0, split["x_miss"], split["y_miss"], split["x_obs"], split["y_obs"],
+                            split["z_obs"], split["z_actual"])
+    assert np.linalg.norm(zm - zref) / np.linalg.norm(zref) < 1e-9
+    assert mse == pytest.approx(mref, rel=1e-9)
+
+
+def test_c4_gradient_matches_oracle_central_differences(gpu, ora):
+    """Central differences of the oracle with h_k = 1e-6 theta_k carry
+    rounding noise of about |dl| / (2 h_k), where dl is the change of the
+    oracle's rounding error between the two evaluations; the bar adds that
+    noise (measured as the asymmetry between forward and backward
+    differences) to 1e-6 of max |grad|."""
+    from exageostat_b200.synthetic import dlarnv
+
+    N, seed, theta = 20000, 0, np.array([1.0, 0.1, 1.0, 0.01])
+    x, y = gpu.generate_xy_loc(N, seed)
+    e = dlarnv(seed, N)
+    with gpu.Session(x, y, kernel=1, dts=512) as s:
+        s.zvg(theta, e)
+        z = s.z()
+        ll, g = s.loglik(theta, grad=True)
+    l0 = ora.dmle(x, y, z, theta, 1)[0]
+    assert ll == pytest.approx(l0, rel=LL_RTOL)
+    fd = np.zeros(4)
+    noise = np.zeros(4)
+    for k in range(4):
+        h = 1e-6 * theta[k]
+        ep = np.zeros(4)
+        ep[k] = h
+        lp = ora.dmle(x, y, z, theta + ep, 1)[0]
+        lm = ora.dmle(x, y, z, theta - ep, 1)[0]
+        fd[k] = (lp - lm) / (2 * h)
+        # second difference: curvature (h^2 l'') plus rounding; its size bounds
+        # the rounding part of the central difference
+        noise[k] = abs(lp - 2 * l0 + lm) / (2 * h)
+    scale = np.abs(fd).max()
+    bar = 1e-6 * scale + noise
+    assert np.all(np.abs(g - fd) <= bar), (g, fd, bar)
+
+
+def test_c1_theta_hat_matches_oracle_maximiser(gpu, ora):
+    x, y, z, _ = ora.synthetic_field(1600, 0, [1.0, 0.1, 0.5])
+    lb, ub = np.full(3, 0.01), np.full(3, 5.0)
+    with gpu.Session(x, y, dts=320) as s:
+        s.set_data(z=z)
+        th_gpu, ll_gpu, _ = s.fit_bobyqa(lb, ub, ftol_abs=1e-9)
+    th_ora, ll_ora = ora.maximise(x, y, z, lb, ub, [[0.5, 0.5, 0.5], [1.0, 0.1, 0.5]])
+    assert ll_ora == pytest.approx(ll_gpu, abs=1e-6)
+    assert np.all(np.abs(th_gpu - th_ora) <= 1e-3 * np.abs(th_ora)), (th_gpu, th_ora)
+
+
+def test_c5_corner_fields_match_oracle(gpu, ora):
+    """Fields at the corner beta in [0.25, 0.3], nu in [2, 2.5] with uniform
+    locations are the worst-conditioned of the batch workload.  Two correct
+    FP64 factorisations of them differ by far more than 1e-10 of l, so the
+    bar is ten times the disagreement between the oracle and an independent
+    LAPACK factorisation of the same matrix (numpy's), plus 1e-10 of the
+    scale of the terms of l."""
+    rng = np.random.default_rng(21)
+    xs, ys, zs, th = [], [], [], []
+    for _ in range(6):
+        n = int(rng.integers(500, 2200))
+        x, y = rng.random(n), rng.random(n)
+        theta = [rng.uniform(0.5, 2.0), rng.uniform(0.25, 0.3), rng.uniform(2.0, 2.5)]
+        z = ora.dzvg(x, y, theta, rng.standard_normal(n))
+        xs.append(x), ys.append(y), zs.append(z), th.append(theta)
+    th = np.array(th)
+    with gpu.Batch(xs, ys, zs, ts=256) as b:
+        got = b.loglik(th)
+    for f in range(len(xs)):
+        n = xs[f].size
+        ll, ld, dp, _ = ora.dmle(xs[f], ys[f], zs[f], th[f])
+        C = ora.covariance_lower(xs[f], ys[f], th[f])
+        L = np.linalg.cholesky(np.tril(C) + np.tril(C, -1).T)
+        v = np.linalg.solve(L, zs[f])
+        ll_np = -0.5 * (v @ v) - np.log(np.diag(L)).sum() - 0.5 * n * math.log(2 * math.pi)
+        scale = 0.5 * abs(dp) + 0.5 * abs(ld) + 0.5 * n * math.log(2 * math.pi)
+        bar = 1e-10 * scale + 10 * abs(ll - ll_np)
+        assert abs(got[f] - ll) <= bar, (f, n, th[f], got[f], ll, ll_np)
+        # the single-field path agrees with the batch to the same bar
+        single = gpu.dmle_host(xs[f], ys[f], zs[f], th[f], ts=256)[0]
+        assert abs(single - got[f]) <= 1e-13 * scale
