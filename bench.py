@@ -46,7 +46,6 @@ def parse():
     ap.add_argument("--ts", type=int, default=512)
     ap.add_argument("--seed", type=int, default=0)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
-    ap.add_argument("--cpu-seconds", type=float, default=12.0, help="target CPU time of the oracle sample")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-mixed-leg", action="store_true", help="skip the TF32 banded mixed-precision sub-result")
     ap.add_argument("--band", type=int, default=2, help="FP64 band width in tiles (mixed leg)")
@@ -67,7 +66,11 @@ def parse():
     ap.add_argument("--drivers", default="bobyqa_fp64,bobyqa_sliced,lbfgsb_grad_fp64,lbfgsb_grad_sliced,"
                     "lbfgsb_sliced_polish",
                     help="mle mode: comma list of bobyqa_fp64, bobyqa_sliced, bobyqa_mixed, lbfgsb_grad_fp64, "
-                         "lbfgsb_grad_sliced, lbfgsb_sliced_polish, bobyqa_sliced_polish, two_stage")
+                         "lbfgsb_grad_sliced, lbfgsb_sliced_polish, bobyqa_sliced_polish, two_stage, tr_fp64, "
+                         "tr_sliced, tr_sliced_polish")
+    ap.add_argument("--tr-gtol", type=float, default=1e-2, help="mle mode: trust-region stop, max |dl/dlog theta|")
+    ap.add_argument("--tr-gtol-fp64", type=float, default=1e-3, help="mle mode: the same for the FP64 run")
+    ap.add_argument("--polish-iter", type=int, default=2, help="mle mode, tr_sliced_polish: FP64 steps")
     ap.add_argument("--passes", type=int, default=3, help="TF32 passes of the off-band update (1 or 3)")
     ap.add_argument("--scheme", choices=["mixed", "sliced"], default="sliced",
                     help="reduced-precision leg: mixed = FP32 off-band tiles on TF32 tensor cores; "
@@ -137,52 +140,74 @@ class ClockSampler:
 
 
 # ------------------------------------------------------- CPU (oracle) leg ----
-def cpu_sample(n_target, seconds):
-    """Time the oracle (the C restatement of the reference CPU path, all host
-    threads) on a bounded sample: one full evaluation at N_s, grown until it
-    takes a few seconds, then scaled to N_target by N^2 (generation, solve)
-    and N^3 (Cholesky)."""
+C2_N = 40000  # the 200 x 200 grid of the plain-FP64 GPU configuration
+
+
+def cpu_eval(n, seed=0, theta=THETA):
+    """One full oracle log-likelihood evaluation (the C restatement of the
+    reference CPU path: generation, tile Cholesky, log-det, solve) of the
+    GenerateXYLoc(n, seed) field on all host threads; z ~ N(0,1).  Returns
+    (seconds, (generation, factorisation, solve) seconds)."""
+    import numpy as np
+
     import oracle
 
     oracle.build()
-    threads = os.cpu_count() or 1
-    oracle.set_threads(threads)
-    n = 4000
-    while True:
-        x, y = oracle.generate_xy_loc(n, 0)
-        import numpy as np
+    oracle.set_threads(os.cpu_count() or 1)
+    x, y = oracle.generate_xy_loc(n, seed)
+    z = np.random.default_rng(seed).standard_normal(n)
+    t0 = time.perf_counter()
+    _, _, _, phases = oracle.dmle(x, y, z, theta)
+    return time.perf_counter() - t0, phases
 
-        z = np.random.default_rng(0).standard_normal(n)
-        t0 = time.perf_counter()
-        _, _, _, (tg, tc, tsv) = oracle.dmle(x, y, z, THETA)
-        wall = time.perf_counter() - t0
-        if wall * 8 > seconds or n >= 32000:
-            break
-        n *= 2
+
+def scaled_to(n_target, n, phases):
+    """Seconds of one evaluation at n_target from the phases measured at n:
+    generation and solve scale by N^2, the Cholesky by N^3."""
     s = n_target / n
-    t_full = tg * s * s + tc * s ** 3 + tsv * s * s
+    tg, tc, tsv = phases
+    return tg * s * s + tc * s ** 3 + tsv * s * s
+
+
+def cpu_baseline_from(n_target, n, wall, phases, label):
+    threads = os.cpu_count() or 1
+    t_full = scaled_to(n_target, n, phases)
     return {"value": 1.0 / t_full, "unit": UNIT, "cores": threads, "kind": "port",
-            "sample": "oracle loglik at N=%d (gen %.3fs, chol %.3fs, solve %.3fs) on %d threads, scaled to N=%d "
-                      "by N^2 (gen, solve) and N^3 (chol)" % (n, tg, tc, tsv, threads, n_target),
-            "seconds_per_eval_extrapolated": t_full, "sample_n": n}
+            "sample": "%s: one full oracle evaluation at N=%d measured (%.2f s: gen %.2f, chol %.2f, solve %.2f) on "
+                      "%d threads, extrapolated to N=%d by N^2 (gen, solve) and N^3 (chol)" % (
+                          label, n, wall, phases[0], phases[1], phases[2], threads, n_target),
+            "measured_n": n, "measured_seconds_per_eval": wall, "extrapolated": n_target != n,
+            "seconds_per_eval_extrapolated": t_full}
 
 
 def run_reference(args):
+    """The reference arm: the oracle port of the reference CPU path on all
+    host threads.  A full evaluation at N = 1e5 needs an 80 GB dense array and
+    ~10 minutes of CPU per step, so every timed step is one full evaluation of
+    the C2-sized field (N = 40 000, the same generator and theta) and the
+    value is extrapolated from it to N = 1e5 (N^3 factorisation, N^2 rest),
+    labelled as such.  Warm-up steps evaluate a small field."""
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
         return
-    samples = []
-    for i in range(args.warmup + args.steps):
-        cb = cpu_sample(args.n, args.cpu_seconds)
-        if i >= args.warmup:
-            samples.append(cb)
-    value = statistics.median(c["value"] for c in samples)
-    cb = dict(samples[-1])
-    cb["value"] = value
+    n_s = min(args.n, C2_N)
+    for _ in range(args.warmup):
+        cpu_eval(2000, args.seed)
+    walls, phases = [], []
+    for _ in range(args.steps):
+        w, ph = cpu_eval(n_s, args.seed)
+        walls.append(w)
+        phases.append(ph)
+    med = sorted(range(len(walls)), key=lambda i: walls[i])[len(walls) // 2]
+    cb = cpu_baseline_from(args.n, n_s, walls[med], phases[med], "reference arm step")
+    value = cb["value"]
     line = {"impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 / value, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-            "config": {"workload": workload(args.n), "sample": cb["sample"]},
+            "config": {"workload": workload(args.n), "sample": cb["sample"],
+                       "measured_seconds_per_step": walls, "measured_n": n_s,
+                       "value_is": "extrapolated from the measured N=%d evaluations" % n_s if n_s != args.n
+                       else "measured"},
             "cpu_baseline": cb, "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0,
                                         "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
@@ -207,16 +232,6 @@ def measured_dgemm_tflops(torch):
     del a, b, c
     torch.cuda.empty_cache()
     return best
-
-
-def read_traffic_per_flop():
-    p = os.path.join(ROOT, "profiles", "xg_syrk_gemm_kernel.md")
-    if not os.path.exists(p):
-        return None
-    for ln in open(p):
-        if ln.startswith("dram_bytes_per_flop:"):
-            return float(ln.split(":")[1])
-    return None
 
 
 def peak_bf16_tflops():
@@ -359,12 +374,35 @@ def mode_mle(args):
             th2, ll2, ev2 = fit_lbfgsb(sess, lb, ub, x0=th)
             runs["lbfgsb_sliced_polish"] = {"seconds": t_sl + time.perf_counter() - t0, "evals": ev,
                                             "evals_fp64": ev2, "theta": th2.tolist(), "loglik": ll2}
+    if "tr_sliced" in drivers or "tr_sliced_polish" in drivers:
+        # mixed-precision adjoint-gradient MLE (exageostat_b200.mle.fit_mixed), from the lower bounds
+        from exageostat_b200.mle import fit_mixed
+
+        for name in ("tr_sliced", "tr_sliced_polish"):
+            if name not in drivers:
+                continue
+            t0 = time.perf_counter()
+            th, ll, ev1, ev2, th1 = fit_mixed(sess, lb, ub, gtol=args.tr_gtol,
+                                              polish_iter=args.polish_iter if name == "tr_sliced_polish" else 0,
+                                              log=progress)
+            runs[name] = {"seconds": time.perf_counter() - t0, "evals": ev1, "grad_evals_fp64": ev2,
+                          "theta": th.tolist(), "loglik": ll, "theta_sliced": th1.tolist()}
+            progress("%s: %s" % (name, runs[name]))
+    if "tr_fp64" in drivers:
+        # the same trust-region driver on the plain FP64 objective and gradient, from the lower bounds
+        from exageostat_b200.mle import fit_trust_region
+
+        t0 = time.perf_counter()
+        th, ll, ev, _ = fit_trust_region(lambda t: sess.loglik(t, grad=True), lb, lb, ub, gtol=args.tr_gtol_fp64,
+                                         log=progress)
+        runs["tr_fp64"] = {"seconds": time.perf_counter() - t0, "evals": ev, "theta": th.tolist(), "loglik": ll}
+        progress("tr_fp64: %s" % runs["tr_fp64"])
     if "lbfgsb_grad_fp64" in drivers:
         t0 = time.perf_counter()
         th, ll, ev = fit_lbfgsb(sess, lb, ub, x0=[0.5, 0.5, 0.5])
         runs["lbfgsb_grad_fp64"] = {"seconds": time.perf_counter() - t0, "evals": ev, "theta": th.tolist(),
                                     "loglik": ll}
-    refname = "bobyqa_fp64" if "bobyqa_fp64" in runs else "lbfgsb_grad_fp64" if "lbfgsb_grad_fp64" in runs else None
+    refname = next((r for r in ("bobyqa_fp64", "tr_fp64", "lbfgsb_grad_fp64") if r in runs), None)
     if refname:
         ref = np.array(runs[refname]["theta"])
         llref = runs[refname]["loglik"]
@@ -557,6 +595,63 @@ def mode_batch(args):
                       "max_rel_diff_batched_vs_looped": err}), flush=True)
 
 
+def c2_pair(xg, seed, ts):
+    """Measured at the C2 size (N = 40 000, 200 x 200 grid, the headline's
+    theta): evaluations per second of the GPU's plain FP64 and INT8-sliced
+    paths (CUDA events, 3 timed after 2 warm-up) and of the CPU oracle (one
+    full evaluation, all host threads) on the same z, with the log-likelihoods
+    of all three."""
+    from exageostat_b200.synthetic import dlarnv
+
+    n = C2_N
+    x, y = xg.generate_xy_loc(n, seed)
+    sess = xg.Session(x, y, dts=ts)
+    sess.zvg(THETA, dlarnv(seed, n))
+    z = sess.z()
+    out = {"n": n, "theta": THETA, "tile": ts}
+    for name in ("fp64", "sliced"):
+        if name == "sliced":
+            sess.set_sliced()
+        for _ in range(2):
+            sess.loglik(THETA)
+        sess.set_profiling(True)
+        lls = [sess.loglik(THETA) for _ in range(3)]
+        p = sess.profile()
+        sess.set_profiling(False)
+        out["gpu_" + name] = {"evals_per_s": p["evals"] / p["t_total"], "loglik": lls[-1]}
+    sess.close()
+    import oracle
+
+    oracle.build()
+    oracle.set_threads(os.cpu_count() or 1)
+    t0 = time.perf_counter()
+    ll, _, _, phases = oracle.dmle(x, y, z, THETA)
+    wall = time.perf_counter() - t0
+    out["cpu_seconds_per_eval"] = wall
+    out["cpu_phases"] = list(phases)
+    out["cpu_cores"] = os.cpu_count()
+    out["cpu_evals_per_s"] = 1.0 / wall
+    out["cpu_loglik"] = ll
+    out["gpu_fp64_rel_diff_vs_cpu"] = abs(out["gpu_fp64"]["loglik"] - ll) / abs(ll)
+    out["gpu_sliced_rel_diff_vs_cpu"] = abs(out["gpu_sliced"]["loglik"] - ll) / abs(ll)
+    out["speedup_fp64_vs_cpu"] = out["gpu_fp64"]["evals_per_s"] * wall
+    out["speedup_sliced_vs_cpu"] = out["gpu_sliced"]["evals_per_s"] * wall
+    return out
+
+
+def ncu_traffic(kernel):
+    """DRAM bytes per algorithmic operation of `kernel` from an ncu capture
+    (profiles/ncu_traffic.json, written from the capture's raw CSV by
+    profiles' recipe; holds the command that made it), or None."""
+    p = os.path.join(ROOT, "profiles", "ncu_traffic.json")
+    try:
+        with open(p) as f:
+            d = json.load(f)[kernel]
+        return float(d["dram_bytes_per_op"]), d
+    except (OSError, KeyError, ValueError, TypeError):
+        return None, None
+
+
 def main():
     args = parse()
     if args.impl == "reference":
@@ -660,22 +755,28 @@ def main():
         # ten 8-bit digit-pair products per FP64 product; dense INT8 runs at twice the BF16 rate.
         # t_offband / offband_flops: the split column updates on the main stream (nt - 2 launches per
         # evaluation, nearly all the work); t_band / band_flops: the last-chunk updates on the panel stream
-        mult, peak, kname, unit = 10, 2.0 * bf16_peak, "xg_sliced_left_kernel (tcgen05 kind::i8, 10 digit " \
+        mult, peak, kname, unit = 10, 2.0 * bf16_sust, "xg_sliced_left_kernel (tcgen05 kind::i8, 10 digit " \
             "pairs, S32 TMEM levels, FP64 epilogue)", "TOP/s"
-        psrc = "dense INT8 = 2 x bf16, bf16 from %s (of measured)" % bf16_src
+        psrc = "dense INT8 = 2 x sustained bf16 (the kernel runs inside a seconds-long step), bf16 from %s " \
+            "(of measured); burst: %.1f TOP/s" % (bf16_src, 2.0 * bf16_peak)
         launches = max(pmx["nt"] - 2, 1)
     else:
-        mult, peak, kname, unit = passes, tf32_peak, "xg_offband_gemm_kernel (tcgen05 kind::tf32, %d pass%s, " \
-            "TMEM)" % (passes, "es" if passes > 1 else ""), "TFLOP/s"
-        psrc = "dense TF32 = bf16 / 2, bf16 from %s (of measured)" % bf16_src
+        mult, peak, kname, unit = passes, bf16_sust / 2.0, "xg_offband_gemm_kernel (tcgen05 kind::tf32, %d " \
+            "pass%s, TMEM)" % (passes, "es" if passes > 1 else ""), "TFLOP/s"
+        psrc = "dense TF32 = sustained bf16 / 2, bf16 from %s (of measured)" % bf16_src
         launches = max(2 * (pmx["nt"] - 1), 1)
     mma_flops = pmx["offband_flops"] * mult
     ach_mx = mma_flops / t_off / 1e12 if t_off > 0 else 0.0
+    ops_per_launch = pmx["offband_flops"] * mult / max(pmx["evals"], 1) / launches
+    bpo, tsrc = ncu_traffic("xg_sliced_left_kernel" if sliced else "xg_offband_gemm_kernel")
     roofline = {"bound": "tensor", "kernel": kname,
                 "achieved": ach_mx, "peak": peak, "unit": unit, "frac": ach_mx / peak,
                 "peak_source": psrc,
-                "traffic": None,
-                "algorithmic_ops_per_launch": pmx["offband_flops"] * mult / max(pmx["evals"], 1) / launches,
+                "traffic": bpo * ops_per_launch if bpo else None,
+                "traffic_source": ("dram__bytes_read.sum + dram__bytes_write.sum per algorithmic op from the ncu "
+                                   "capture in profiles/ncu_traffic.json (%s), times this launch's ops" %
+                                   tsrc.get("case", "")) if bpo else None,
+                "algorithmic_ops_per_launch": ops_per_launch,
                 "useful_fp64_equivalent_tflops": pmx["offband_flops"] / t_off / 1e12 if t_off > 0 else 0.0,
                 "share_of_step": t_off / pmx["t_total"],
                 "phases_s_per_eval": {k: pmx[k] / pmx["evals"] for k in
@@ -698,13 +799,15 @@ def main():
                  "rel_err_vs_fp64": abs(llm[-1] - lls64[-1]) / abs(lls64[-1]),
                  "offband_tf32_tflops": ach, "offband_frac_of_tf32_peak": ach / tf32_peak}
         sess.set_sliced()
-    tpf = read_traffic_per_flop()
+    tpf, tsrc64 = ncu_traffic("xg_syrk_gemm_kernel")
     fp64 = {"value": fp64_value, "unit": UNIT, "ms_per_step": 1e3 * t64 / args.steps, "loglik": lls64[-1],
             "roofline": {"bound": "tensor", "kernel": "xg_syrk_gemm_kernel (FP64 DMMA trailing update)",
                          "achieved": ach64, "peak": fp64_peak, "unit": "TFLOP/s", "frac": ach64 / fp64_peak,
                          "peak_source": "cuBLAS DGEMM 8192^3 measured in this process (of measured)",
                          "traffic": (tpf * p64["gemm_flops"] / p64["evals"] / max(2 * (p64["nt"] - 1) - 1, 1))
                          if tpf else None,
+                         "traffic_source": ("ncu capture in profiles/ncu_traffic.json (%s), scaled by flops" %
+                                            tsrc64.get("case", "")) if tpf else None,
                          "share_of_step": p64["t_gemm"] / p64["t_total"]}}
     line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": 1e3 * tmx / args.steps, "higher_is_better": True,
@@ -721,9 +824,14 @@ def main():
             "fp64": fp64, "speedup_vs_fp64": value / fp64_value, "banded_mixed_tf32": other,
             "roofline": roofline, "e2e": e2e, "clocks": clocks,
             "gpu_launches": int(round(pmx["launches"] / max(pmx["evals"], 1) * args.steps))}
-    if rank == 0 and world == 1 and not args.no_cpu_baseline:
-        line["cpu_baseline"] = cpu_sample(N, args.cpu_seconds)
     sess.close()
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        pair = c2_pair(xg, args.seed, args.ts)
+        line["c2_measured"] = pair
+        line["cpu_baseline"] = cpu_baseline_from(N, pair["n"], pair["cpu_seconds_per_eval"], pair["cpu_phases"],
+                                                 "C2 pair")
+        # the same baseline's speed-up over the extrapolated CPU time at this N, for reading beside the C2 pair
+        line["cpu_baseline"]["gpu_speedup_extrapolated"] = value / line["cpu_baseline"]["value"]
     if rank == 0:
         print(json.dumps(line), flush=True)
     if dist is not None:

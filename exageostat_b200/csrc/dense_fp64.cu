@@ -322,6 +322,34 @@ __global__ void __launch_bounds__(XG_POTRF_THREADS) xg_potrf_diag_batch_kernel(X
 }
 
 /* ========================================================================== */
+/* Inverses of the 32 x 32 diagonal blocks of L_kk (for the panel TRSM)       */
+/* ========================================================================== */
+
+/* One warp per diagonal block b: lane c forms column c of the inverse by
+ * forward substitution, z_i = (delta_ic - sum_{q<i} L_iq z_q) / L_ii, and
+ * writes T.dinv[(32 b + i) * 32 + c] = z_i (lower triangular). */
+__global__ void __launch_bounds__(32) xg_diag_inv_kernel(XgTileArgs T, int k, const int *status)
+{
+    if (*(volatile const int *)status) return;
+    __shared__ double LB[32][33];
+    const int ts = T.ts, b = blockIdx.x, lane = threadIdx.x;
+    const double *L = T.data + xg_slot64(T, k, k) * (long long)ts * ts + (long long)(b * 32) * ts + b * 32;
+    for (int r = 0; r < 32; ++r) LB[r][lane] = L[(long long)r * ts + lane];
+    __syncwarp();
+    double z[32];
+#pragma unroll
+    for (int i = 0; i < 32; ++i) {
+        double s = (i == lane) ? 1.0 : 0.0;
+#pragma unroll
+        for (int q = 0; q < i; ++q) s -= LB[i][q] * z[q];
+        z[i] = s / LB[i][i];
+    }
+    double *D = T.dinv + (long long)(b * 32) * 32;
+#pragma unroll
+    for (int i = 0; i < 32; ++i) D[i * 32 + lane] = z[i];
+}
+
+/* ========================================================================== */
 /* Panel TRSM: L_ik = A_ik L_kk^-T, fused with v_i -= L_ik v_k                */
 /* ========================================================================== */
 
@@ -348,12 +376,51 @@ __device__ __forceinline__ void xg_trsm_body(const XgTileArgs &T, int k, double 
         S[r * LDS + c] = B[(long long)r * ts + c];
     }
     for (int cb = 0; cb < ts; cb += 32) {
-        for (int idx = tid; idx < 32 * 32; idx += blockDim.x) {
-            const int r = idx >> 5, c = idx & 31;
-            LD[r * 33 + c] = L[(long long)(cb + r) * ts + cb + c];
+        if (T.dinv) {
+            /* the inverse D of this 32 x 32 diagonal block (xg_diag_inv_kernel) */
+            for (int idx = tid; idx < 32 * 32; idx += blockDim.x) {
+                const int r = idx >> 5, c = idx & 31;
+                LD[r * 33 + c] = T.dinv[(cb + r) * 32 + c];
+            }
+        } else {
+            for (int idx = tid; idx < 32 * 32; idx += blockDim.x) {
+                const int r = idx >> 5, c = idx & 31;
+                LD[r * 33 + c] = L[(long long)(cb + r) * ts + cb + c];
+            }
         }
         __syncthreads();
-        if (warp == 0) { /* lane = row of the strip */
+        if (T.dinv) {
+            /* S[:, cb:cb+32] <- S[:, cb:cb+32] D^T on DMMA: warp w < 4 computes
+             * the 32 x 8 column block w (both 16-row halves); the results are
+             * written after every warp has read its operands */
+            double acc[2][4];
+#pragma unroll
+            for (int mi = 0; mi < 2; ++mi)
+#pragma unroll
+                for (int e = 0; e < 4; ++e) acc[mi][e] = 0.0;
+            if (warp < 4) {
+#pragma unroll
+                for (int p0 = 0; p0 < 32; p0 += 4) {
+                    const double b0 = LD[(warp * 8 + g) * 33 + p0 + tq];
+#pragma unroll
+                    for (int mi = 0; mi < 2; ++mi)
+                        xg_dmma_16x8x4(acc[mi][0], acc[mi][1], acc[mi][2], acc[mi][3],
+                                       S[(mi * 16 + g) * LDS + cb + p0 + tq], S[(mi * 16 + g + 8) * LDS + cb + p0 + tq],
+                                       b0);
+                }
+            }
+            __syncthreads();
+            if (warp < 4) {
+#pragma unroll
+                for (int mi = 0; mi < 2; ++mi)
+#pragma unroll
+                    for (int h = 0; h < 2; ++h) {
+                        double *ps = S + (mi * 16 + g + 8 * h) * LDS + cb + warp * 8 + 2 * tq;
+                        ps[0] = acc[mi][2 * h];
+                        ps[1] = acc[mi][2 * h + 1];
+                    }
+            }
+        } else if (warp == 0) { /* lane = row of the strip */
             double row[32];
 #pragma unroll
             for (int j = 0; j < 32; ++j) row[j] = S[lane * LDS + cb + j];
@@ -729,6 +796,12 @@ void xg_launch_potrf_diag(const XgTileArgs &T, int k, double *v, double *part_lo
     else
         xg_potrf_diag_kernel<32><<<1, XG_POTRF_THREADS, smem, st>>>(T, k, v, part_logdet, part_dot, with_rhs, status,
                                                                      info);
+}
+
+void xg_launch_diag_inv(const XgTileArgs &T, int k, const int *status, cudaStream_t st)
+{
+    if (!T.dinv) return;
+    xg_diag_inv_kernel<<<T.ts / 32, 32, 0, st>>>(T, k, status);
 }
 
 void xg_launch_trsm_panel(const XgTileArgs &T, int k, double *v, int with_rhs, const int *status, cudaStream_t st,

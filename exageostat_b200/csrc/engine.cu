@@ -147,6 +147,11 @@ int xg_tm_alloc(XgTileMatrix &M, int N, int ts)
     if (e == cudaSuccess) e = cudaMemcpy(M.ij, hij, sizeof(int2) * M.ntiles, cudaMemcpyHostToDevice);
     free(hij);
     if (e != cudaSuccess) return xg_cuda_fail(e, "tile index table");
+    e = cudaMalloc(&M.dinv, sizeof(double) * (size_t)ts * 32);
+    if (e != cudaSuccess) {
+        M.dinv = nullptr;
+        return xg_cuda_fail(e, "diagonal-block inverses");
+    }
     return xg_encode_tiles(&M.map, M.d, M.ntiles, ts);
 }
 
@@ -169,8 +174,10 @@ void xg_tm_free(XgTileMatrix &M)
 {
     if (M.d) cudaFree(M.d);
     if (M.ij) cudaFree(M.ij);
+    if (M.dinv) cudaFree(M.dinv);
     M.d = nullptr;
     M.ij = nullptr;
+    M.dinv = nullptr;
 }
 
 XgMaternParams xg_params(const double *theta, int kernel)
@@ -252,6 +259,7 @@ int xg_check_theta(const double *theta, int kernel)
 void xg_factor_lookahead(XgTileMatrix &M, double *v, double *part, int *status, int *info, const XgFactorStreams &fs)
 {
     XgTileArgs T{M.d, M.ts, M.nt};
+    T.dinv = M.dinv;
     const bool la = fs.st_hi != nullptr;
     cudaStream_t sp = la ? fs.st_hi : fs.st; /* panel stream */
     cudaEvent_t *pev = fs.pev;
@@ -264,6 +272,7 @@ void xg_factor_lookahead(XgTileMatrix &M, double *v, double *part, int *status, 
         if (pev) cudaEventRecord(pev[5 * k], sp);
         xg_launch_potrf_diag(T, k, v, part, part + M.nt, rhs, status, info, sp);
         if (pev) cudaEventRecord(pev[5 * k + 1], sp);
+        xg_launch_diag_inv(T, k, status, sp);
         xg_launch_trsm_panel(T, k, v, rhs, status, sp);
         if (pev) cudaEventRecord(pev[5 * k + 2], sp);
         if (la) {
@@ -1052,6 +1061,7 @@ static void xg_factor_sliced(XgField *f, double *v, const XgFactorStreams &fs)
     XgSliced *sl = f->sl;
     XgTileMatrix &M = f->C;
     XgTileArgs T{M.d, M.ts, M.nt};
+    T.dinv = M.dinv;
     const int nt = M.nt;
     const long long plane = sl->plane_rows * M.ts;
     const int pr = (int)sl->plane_rows;
@@ -1077,6 +1087,7 @@ static void xg_factor_sliced(XgField *f, double *v, const XgFactorStreams &fs)
         rec(j, 1, sp);
         xg_launch_potrf_diag(T, j, v, f->part, f->part + nt, rhs, f->status, f->info, sp);
         rec(j, 2, sp);
+        xg_launch_diag_inv(T, j, f->status, sp);
         xg_launch_trsm_panel(T, j, v, rhs, f->status, sp);
         if (j + 1 < nt) xg_launch_slice_panel(T, j, 0, sl->dig, sl->scale, plane, f->status, sp);
         rec(j, 3, sp);

@@ -69,7 +69,9 @@
 #define XG_SL_ABOX_BYTES (XG_SL_BM * XG_SL_BK)                                  /* one digit plane, 128 rows */
 #define XG_SL_BBOX_BYTES (XG_SL_BN * XG_SL_BK)                                  /* one digit plane, 128 rows */
 #define XG_SL_STAGE_BYTES (XG_SL_SLICES * (XG_SL_ABOX_BYTES + XG_SL_BBOX_BYTES)) /* 64 KB */
-#define XG_SL_SMEM (XG_SL_STAGES * XG_SL_STAGE_BYTES + 1024 + 256)
+/* per panel chunk, the 128 A-row and 128 B-row scales, double-buffered */
+#define XG_SL_SCALE_BYTES (2 * 2 * 128 * 8)
+#define XG_SL_SMEM (XG_SL_STAGES * XG_SL_STAGE_BYTES + XG_SL_SCALE_BYTES + 1024 + 256)
 #define XG_SL_RADIX 254.0
 #define XG_SL_TOP 127.0
 #define XG_SL_INV_RADIX3 (1.0 / (254.0 * 254.0 * 254.0))
@@ -227,12 +229,15 @@ __global__ void __launch_bounds__(XG_SL_THREADS, 1)
 {
     extern __shared__ __align__(1024) unsigned char xg_smem_raw[];
     unsigned char *smem = (unsigned char *)(((uintptr_t)xg_smem_raw + 1023) & ~(uintptr_t)1023);
-    uint64_t *full = (uint64_t *)(smem + XG_SL_STAGES * XG_SL_STAGE_BYTES);
+    double *sscale = (double *)(smem + XG_SL_STAGES * XG_SL_STAGE_BYTES); /* [2][A 128 | B 128] */
+    uint64_t *full = (uint64_t *)(smem + XG_SL_STAGES * XG_SL_STAGE_BYTES + XG_SL_SCALE_BYTES);
     uint64_t *empty = full + XG_SL_STAGES;
     uint64_t *acc_full = empty + XG_SL_STAGES;
     uint64_t *acc_empty = acc_full + 1;
     uint64_t *drain = acc_empty + 1;
-    uint32_t *tmem_slot = (uint32_t *)(drain + 1);
+    uint64_t *sfull = drain + 1;  /* [2] the chunk's row scales have landed */
+    uint64_t *sempty = sfull + 2; /* [2] the epilogue is done with them */
+    uint32_t *tmem_slot = (uint32_t *)(sempty + 2);
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     const int ts = T.ts, nt = T.nt;
     if (xg_cta_should_skip(status)) return;
@@ -244,6 +249,10 @@ __global__ void __launch_bounds__(XG_SL_THREADS, 1)
         xg_mbar_init(acc_full, 1);
         xg_mbar_init(acc_empty, XG_SL_EPI_WARPS);
         xg_mbar_init(drain, 1);
+        for (int b = 0; b < 2; ++b) {
+            xg_mbar_init(&sfull[b], 1);
+            xg_mbar_init(&sempty[b], XG_SL_EPI_WARPS);
+        }
         xg_fence_barrier_init();
     }
     if (warp == 1) xg_tmem_alloc(tmem_slot, 512); /* four 128-lane x 128-column S32 levels */
@@ -257,17 +266,32 @@ __global__ void __launch_bounds__(XG_SL_THREADS, 1)
     if (warp < 4) {
     asm volatile("setmaxnreg.dec.sync.aligned.u32 %0;" ::"n"(XG_SL_REG_LOW));
     if (warp == 0) {
-        /* ---- TMA producer: per stage the four A and four B digit boxes ---- */
+        /* ---- TMA producer: per panel chunk the 128 + 128 row scales of the
+         * job's A and B blocks (one bulk copy each, into a double buffer the
+         * epilogue reads), then per stage the four A and four B digit boxes ---- */
         if (lane == 0) {
             xg_prefetch_tensormap(&map_a);
             xg_prefetch_tensormap(&map_b);
-            long long it = 0;
+            long long it = 0, cs = 0;
             for (long long job = blockIdx.x; job < njobs && ok; job += gridDim.x) {
                 XgSlJob J;
                 if (!xg_sl_job(S, job, nt, ts, J)) continue;
-                for (int k = J.k0; k < J.k1 && ok; ++k) {
-                    const int rowA = (int)(xg_sl_slot_a(S, J, k, nt) * ts) + J.bm * XG_SL_BM;
-                    const int rowB = (int)(xg_sl_slot_b(S, J, k, nt) * ts) + J.bn * XG_SL_BN;
+                for (int k = J.k0; k < J.k1 && ok; ++k, ++cs) {
+                    const long long slot_a = xg_sl_slot_a(S, J, k, nt), slot_b = xg_sl_slot_b(S, J, k, nt);
+                    const int rowA = (int)(slot_a * ts) + J.bm * XG_SL_BM;
+                    const int rowB = (int)(slot_b * ts) + J.bn * XG_SL_BN;
+                    {
+                        const int sb = (int)(cs & 1);
+                        if (cs >= 2 && !xg_mbar_wait(&sempty[sb], (uint32_t)((cs >> 1) - 1) & 1)) {
+                            ok = false;
+                            break;
+                        }
+                        xg_mbar_arrive_expect_tx(&sfull[sb], 2 * XG_SL_BM * 8);
+                        xg_bulk_load(sscale + sb * 256, scale_a + slot_a * ts + J.bm * XG_SL_BM, XG_SL_BM * 8,
+                                     &sfull[sb]);
+                        xg_bulk_load(sscale + sb * 256 + 128, scale_b + slot_b * ts + J.bn * XG_SL_BN, XG_SL_BN * 8,
+                                     &sfull[sb]);
+                    }
                     for (int kb = 0; kb < KT; ++kb, ++it) {
                         const int s = (int)(it % XG_SL_STAGES);
                         if (it >= XG_SL_STAGES &&
@@ -288,9 +312,11 @@ __global__ void __launch_bounds__(XG_SL_THREADS, 1)
                 }
             }
             if (!ok) atomicOr(status, XG_ST_TIMEOUT);
+            /* copies still in flight land before the CTA may exit */
             const long long first = it > XG_SL_STAGES ? it - XG_SL_STAGES : 0;
             for (long long q = first; q < it; ++q)
                 xg_mbar_wait(&full[q % XG_SL_STAGES], (uint32_t)(q / XG_SL_STAGES) & 1);
+            for (long long q = cs > 2 ? cs - 2 : 0; q < cs; ++q) xg_mbar_wait(&sfull[q & 1], (uint32_t)(q >> 1) & 1);
         }
     } else if (warp == 1) {
         /* ---- MMA issuer: one accumulation (4 levels) per (job, panel chunk) ---- */
@@ -373,7 +399,8 @@ __global__ void __launch_bounds__(XG_SL_THREADS, 1)
 #pragma unroll
             for (int u = 0; u < 64; ++u) res[u] = 0.0;
             for (int k = J.k0; k < J.k1; ++k, ++cc) {
-                if (!xg_mbar_wait(acc_full, (uint32_t)cc & 1)) {
+                const int sb = (int)(cc & 1);
+                if (!xg_mbar_wait(&sfull[sb], (uint32_t)(cc >> 1) & 1) || !xg_mbar_wait(acc_full, (uint32_t)cc & 1)) {
                     if (lane == 0) atomicOr(status, XG_ST_TIMEOUT);
                     ok = false;
                     break;
@@ -381,10 +408,10 @@ __global__ void __launch_bounds__(XG_SL_THREADS, 1)
                 xg_tc_fence_after();
                 /* s_B (this thread's column) with 254^-3 folded in: the levels are
                  * combined as the exact integer v = L0 254^3 + L1 254^2 + L2 254 + L3
-                 * (|v| < 2^48) and converted once */
-                const double sc = scale_b[xg_sl_slot_b(S, J, k, nt) * ts + col] * (S.sign * XG_SL_INV_RADIX3);
-                const double2 *sr2 =
-                    reinterpret_cast<const double2 *>(scale_a + xg_sl_slot_a(S, J, k, nt) * ts + row0);
+                 * (|v| < 2^48) and converted once.  The row scales come from the
+                 * shared-memory copy the producer staged for this chunk. */
+                const double sc = sscale[sb * 256 + 128 + q * 32 + lane] * (S.sign * XG_SL_INV_RADIX3);
+                const double2 *sr2 = reinterpret_cast<const double2 *>(sscale + sb * 256 + h * 64);
                 const uint32_t base = tmem + ((uint32_t)(q * 32) << 16) + (uint32_t)(h * 64);
                 /* 8 batches per chunk: (columns c * 16 .. + 15, levels 0-1 or 2-3),
                  * software-pipelined -- the next batch's TMEM loads are issued
@@ -427,11 +454,18 @@ __global__ void __launch_bounds__(XG_SL_THREADS, 1)
                         }
                     }
                     if (b < 7) xg_tmem_ld_wait();
+                    if (b == 6) {
+                        /* every TMEM load of this chunk is complete: the
+                         * accumulators are free for the next chunk while the
+                         * last batch is combined */
+                        xg_tc_fence_before();
+                        __syncwarp();
+                        if (lane == 0) xg_mbar_arrive(acc_empty);
+                    }
                 }
-                /* the accumulators are free for the next chunk */
-                xg_tc_fence_before();
+                /* this chunk's scale buffer may be refilled */
                 __syncwarp();
-                if (lane == 0) xg_mbar_arrive(acc_empty);
+                if (lane == 0) xg_mbar_arrive(&sempty[sb]);
             }
             if (!ok) break;
             /* C += sign U (or C = sign U): each warp instruction touches 32

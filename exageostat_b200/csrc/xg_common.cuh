@@ -115,6 +115,16 @@ __device__ inline void xg_tma_load_2d(void *smem_dst, const CUtensorMap *map, in
         : "memory");
 }
 
+/* ---- untiled bulk copy, global -> this CTA's shared memory, completing on an
+ * mbarrier (both addresses 16-byte aligned, bytes a multiple of 16) ---- */
+__device__ inline void xg_bulk_load(void *smem_dst, const void *gsrc, uint32_t bytes, uint64_t *bar)
+{
+    asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
+                     xg_smem_u32(smem_dst)),
+                 "l"(gsrc), "r"(bytes), "r"(xg_smem_u32(bar))
+                 : "memory");
+}
+
 __device__ inline void xg_prefetch_tensormap(const CUtensorMap *map)
 {
     asm volatile("prefetch.tensormap [%0];" ::"l"(map) : "memory");

@@ -38,6 +38,7 @@ struct XgTileMatrix {
     double *d = nullptr;
     int2 *ij = nullptr; /* (i, j) of every packed tile */
     CUtensorMap map;    /* TMA view for the trailing-update kernel */
+    double *dinv = nullptr; /* ts x 32: inverted 32 x 32 diagonal blocks of the current panel */
 };
 
 /* Banded mixed-precision workspace (mixed.cu): compact FP64 band tiles,
