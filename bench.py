@@ -194,7 +194,10 @@ def run_reference(args):
     for _ in range(args.warmup):
         cpu_eval(2000, args.seed)
     walls, phases = [], []
-    for _ in range(args.steps):
+    # each step is a full N = 40 000 evaluation (about 30-60 s on 16 host
+    # cores); at most three are run so the arm ends within a few minutes
+    steps_run = min(args.steps, 3)
+    for _ in range(steps_run):
         w, ph = cpu_eval(n_s, args.seed)
         walls.append(w)
         phases.append(ph)
@@ -205,7 +208,7 @@ def run_reference(args):
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 / value, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
             "config": {"workload": workload(args.n), "sample": cb["sample"],
-                       "measured_seconds_per_step": walls, "measured_n": n_s,
+                       "measured_seconds_per_step": walls, "measured_n": n_s, "steps_run": steps_run,
                        "value_is": "extrapolated from the measured N=%d evaluations" % n_s if n_s != args.n
                        else "measured"},
             "cpu_baseline": cb, "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0,
