@@ -67,10 +67,7 @@ def parse():
                     "lbfgsb_sliced_polish",
                     help="mle mode: comma list of bobyqa_fp64, bobyqa_sliced, bobyqa_mixed, lbfgsb_grad_fp64, "
                          "lbfgsb_grad_sliced, lbfgsb_sliced_polish, bobyqa_sliced_polish, two_stage, tr_fp64, "
-                         "tr_sliced, tr_sliced_polish")
-    ap.add_argument("--tr-gtol", type=float, default=1e-2, help="mle mode: trust-region stop, max |dl/dlog theta|")
-    ap.add_argument("--tr-gtol-fp64", type=float, default=1e-3, help="mle mode: the same for the FP64 run")
-    ap.add_argument("--polish-iter", type=int, default=2, help="mle mode, tr_sliced_polish: FP64 steps")
+                         "tr_sliced")
     ap.add_argument("--passes", type=int, default=3, help="TF32 passes of the off-band update (1 or 3)")
     ap.add_argument("--scheme", choices=["mixed", "sliced"], default="sliced",
                     help="reduced-precision leg: mixed = FP32 off-band tiles on TF32 tensor cores; "
@@ -377,28 +374,24 @@ def mode_mle(args):
             th2, ll2, ev2 = fit_lbfgsb(sess, lb, ub, x0=th)
             runs["lbfgsb_sliced_polish"] = {"seconds": t_sl + time.perf_counter() - t0, "evals": ev,
                                             "evals_fp64": ev2, "theta": th2.tolist(), "loglik": ll2}
-    if "tr_sliced" in drivers or "tr_sliced_polish" in drivers:
-        # mixed-precision adjoint-gradient MLE (exageostat_b200.mle.fit_mixed), from the lower bounds
+    if "tr_sliced" in drivers:
+        # mixed-precision adjoint-gradient MLE (exageostat_b200.mle.fit_mixed): start point, trust region on the
+        # sliced objective and gradient, ridge search with sliced values
         from exageostat_b200.mle import fit_mixed
 
-        for name in ("tr_sliced", "tr_sliced_polish"):
-            if name not in drivers:
-                continue
-            t0 = time.perf_counter()
-            th, ll, ev1, ev2, th1 = fit_mixed(sess, lb, ub, gtol=args.tr_gtol,
-                                              polish_iter=args.polish_iter if name == "tr_sliced_polish" else 0,
-                                              log=progress)
-            runs[name] = {"seconds": time.perf_counter() - t0, "evals": ev1, "grad_evals_fp64": ev2,
-                          "theta": th.tolist(), "loglik": ll, "theta_sliced": th1.tolist()}
-            progress("%s: %s" % (name, runs[name]))
+        t0 = time.perf_counter()
+        th, ll, ev1, ev2, th1 = fit_mixed(sess, lb, ub, log=progress)
+        runs["tr_sliced"] = {"seconds": time.perf_counter() - t0, "grad_evals": ev1, "loglik_evals": ev2,
+                             "theta": th.tolist(), "loglik": ll, "theta_gradient_stage": th1.tolist()}
+        progress("tr_sliced: %s" % runs["tr_sliced"])
     if "tr_fp64" in drivers:
-        # the same trust-region driver on the plain FP64 objective and gradient, from the lower bounds
-        from exageostat_b200.mle import fit_trust_region
+        # the same driver in plain FP64 (exageostat_b200.mle.fit_fp64)
+        from exageostat_b200.mle import fit_fp64
 
         t0 = time.perf_counter()
-        th, ll, ev, _ = fit_trust_region(lambda t: sess.loglik(t, grad=True), lb, lb, ub, gtol=args.tr_gtol_fp64,
-                                         log=progress)
-        runs["tr_fp64"] = {"seconds": time.perf_counter() - t0, "evals": ev, "theta": th.tolist(), "loglik": ll}
+        th, ll, ev, ne = fit_fp64(sess, lb, ub, log=progress)
+        runs["tr_fp64"] = {"seconds": time.perf_counter() - t0, "grad_evals": ev, "loglik_evals": ne,
+                           "theta": th.tolist(), "loglik": ll}
         progress("tr_fp64: %s" % runs["tr_fp64"])
     if "lbfgsb_grad_fp64" in drivers:
         t0 = time.perf_counter()
@@ -563,22 +556,32 @@ def mode_assess(args):
 
 
 def mode_batch(args):
-    """Batched regional fields (sizes U[500, 6000], theta_i random): fields/s
-    of one batched graph launch against looping the single-field FP64 path."""
+    """Batched regional fields (the batch workload: sizes U[500, 6000],
+    locations uniform in each region's unit square, sigma^2 ~ U(0.5, 2), beta ~
+    U(0.02, 0.3), nu ~ U(0.3, 2.5), z_i = L_i e_i from the library's MLE_zvg):
+    seconds per evaluation of every field's loglik (one persistent launch
+    under a CUDA graph), and of loglik + gradient, against looping the
+    single-field FP64 path over every field (measured, wall clock)."""
     os.environ.setdefault("EXAGEOSTAT_B200_SILENT", "1")
     import numpy as np
+    import torch
 
     import exageostat_b200 as xg
 
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    if world > 1:
+        return mode_batch_sharded(args)
     xg.init(0)
     rng = np.random.default_rng(args.seed)
     xs, ys, zs, th = [], [], [], []
     for f in range(args.fields):
         n = int(rng.integers(500, 6001))
-        xs.append(rng.random(n))
-        ys.append(rng.random(n))
-        zs.append(rng.standard_normal(n))
-        th.append([rng.uniform(0.5, 2.0), rng.uniform(0.02, 0.3), rng.uniform(0.3, 2.5)])
+        x, y = rng.random(n), rng.random(n)
+        t = [rng.uniform(0.5, 2.0), rng.uniform(0.02, 0.3), rng.uniform(0.3, 2.5)]
+        with xg.Session(x, y, dts=256) as s:
+            s.zvg(t, rng.standard_normal(n))
+            z = s.z()
+        xs.append(x), ys.append(y), zs.append(z), th.append(t)
     th = np.array(th)
     with xg.Batch(xs, ys, zs, ts=256) as b:
         b.loglik(th)
@@ -586,15 +589,23 @@ def mode_batch(args):
         for _ in range(args.steps):
             out = b.loglik(th)
         tb = (time.perf_counter() - t0) / args.steps
+        b.loglik(th, grad=True)
+        t0 = time.perf_counter()
+        _, gb = b.loglik(th, grad=True)
+        tbg = time.perf_counter() - t0
     t0 = time.perf_counter()
-    loop = [xg.dmle_host(x, y, z, t, ts=256)[0] for x, y, z, t in zip(xs[:64], ys[:64], zs[:64], th[:64])]
-    tl = (time.perf_counter() - t0) / 64 * args.fields
-    err = float(np.max(np.abs(np.array(loop) - out[:64]) / np.abs(np.array(loop))))
+    loop = np.array([xg.dmle_host(x, y, z, t, ts=256)[0] for x, y, z, t in zip(xs, ys, zs, th)])
+    tl = time.perf_counter() - t0
+    ok = np.isfinite(loop) & np.isfinite(out)
+    err = float(np.max(np.abs(loop[ok] - out[ok]) / np.abs(loop[ok])))
     sizes = np.array([len(x) for x in xs])
     print(json.dumps({"mode": "batch", "fields": args.fields, "sizes": [int(sizes.min()), int(sizes.max())],
                       "flops": float(np.sum(sizes.astype(float) ** 3) / 3), "batched_seconds": tb,
-                      "fields_per_s_batched": args.fields / tb, "looped_seconds_est": tl,
+                      "fields_per_s_batched": args.fields / tb, "batched_tflops": float(
+                          np.sum(sizes.astype(float) ** 3) / 3) / tb / 1e12,
+                      "batched_grad_seconds": tbg, "looped_seconds": tl,
                       "fields_per_s_looped": args.fields / tl, "speedup": tl / tb,
+                      "fields_not_spd": int(np.sum(~np.isfinite(out))),
                       "max_rel_diff_batched_vs_looped": err}), flush=True)
 
 
@@ -655,7 +666,121 @@ def ncu_traffic(kernel):
         return None, None
 
 
+def mode_batch_sharded(args):
+    """The batch workload sharded over the ranks of torchrun (NCCL): each
+    rank evaluates its LPT share of the fields (exageostat_b200.sharding.
+    ShardedBatch) and one all_gather hands every rank all log-likelihoods and
+    gradients.  Timed on the device between barriers, max over ranks; value =
+    all fields / that time."""
+    import datetime
+
+    import numpy as np
+    import torch
+    import torch.distributed as dist
+
+    import exageostat_b200 as xg
+    from exageostat_b200.sharding import ShardedBatch
+
+    rank, world = int(os.environ["RANK"]), int(os.environ["WORLD_SIZE"])
+    torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", "0")))
+    dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
+    xg.init(0)
+    rng = np.random.default_rng(args.seed)
+    xs, ys, zs, th = [], [], [], []
+    for f in range(args.fields):
+        n = int(rng.integers(500, 6001))
+        x, y = rng.random(n), rng.random(n)
+        t = [rng.uniform(0.5, 2.0), rng.uniform(0.02, 0.3), rng.uniform(0.3, 2.5)]
+        e = rng.standard_normal(n)
+        xs.append(x), ys.append(y), th.append(t), zs.append(e)
+    th = np.array(th)
+    # z_i = L_i e_i for this rank's fields only (the others are never read here)
+    sb = ShardedBatch(xs, ys, zs, ts=256)
+    for i in sb.mine:
+        with xg.Session(xs[i], ys[i], dts=256) as s:
+            s.zvg(th[i], zs[i])
+            zs[i] = s.z()
+    sb.close()
+    sb = ShardedBatch(xs, ys, zs, ts=256)
+    out = {}
+    for grad in (False, True):
+        for _ in range(max(args.warmup, 1)):
+            sb.loglik(th, grad=grad)
+        dist.barrier()
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        for _ in range(args.steps):
+            res = sb.loglik(th, grad=grad)
+        torch.cuda.synchronize()
+        dt = torch.tensor([(time.perf_counter() - t0) / args.steps], device="cuda", dtype=torch.float64)
+        dist.all_reduce(dt, op=dist.ReduceOp.MAX)
+        out["grad" if grad else "loglik"] = float(dt.item())
+    ll = res[0]
+    sb.close()
+    if rank == 0:
+        sizes = np.array([len(x) for x in xs])
+        print(json.dumps({"mode": "batch", "n_gpus": world, "fields": args.fields, "scaling": "strong",
+                          "sizes": [int(sizes.min()), int(sizes.max())],
+                          "batched_seconds": out["loglik"], "fields_per_s_batched": args.fields / out["loglik"],
+                          "batched_grad_seconds": out["grad"], "fields_not_spd": int(np.sum(~np.isfinite(ll))),
+                          "fields_per_rank": [len(p) for p in sb.parts]}), flush=True)
+    dist.barrier()
+    dist.destroy_process_group()
+
+
+def ingest_ncu(path, case, command):
+    """Writes profiles/ncu_traffic.json from the raw page of an ncu capture
+    (``ncu -i <rep> --page raw --csv``): per captured kernel, DRAM bytes
+    (dram__bytes_read.sum + dram__bytes_write.sum) per algorithmic operation,
+    the operations counted by the same capture -- INT8 tensor ops
+    (sm__ops_path_tensor_op_utcimma_src_int8.sum) or FP64 DMMA flops (1024 x
+    sm__inst_executed_pipe_tensor_subpipe_dmma)."""
+    import csv
+
+    with open(path, newline="") as f:
+        rows = list(csv.reader(f))
+    head = rows[0]
+    col = {name: i for i, name in enumerate(head)}
+
+    def num(r, name):
+        v = r[col[name]].replace(",", "") if name in col else ""
+        try:
+            return float(v)
+        except ValueError:
+            return None
+
+    per = {}
+    for r in rows[2:]:
+        if len(r) != len(head):
+            continue
+        name = r[col["Kernel Name"]].split("(")[0].split("<")[0].strip()
+        rd, wr = num(r, "dram__bytes_read.sum"), num(r, "dram__bytes_write.sum")
+        i8 = num(r, "sm__ops_path_tensor_op_utcimma_src_int8.sum")
+        dm = num(r, "sm__inst_executed_pipe_tensor_subpipe_dmma.sum")
+        ops = i8 if i8 else (1024.0 * dm if dm else None)
+        if rd is None or wr is None or not ops:
+            continue
+        per.setdefault(name, []).append((rd + wr, ops))
+    out_path = os.path.join(ROOT, "profiles", "ncu_traffic.json")
+    try:
+        with open(out_path) as f:
+            out = json.load(f)
+    except (OSError, ValueError):
+        out = {}
+    for name, v in per.items():
+        b = sum(x[0] for x in v)
+        o = sum(x[1] for x in v)
+        out[name] = {"dram_bytes_per_op": b / o, "launches": len(v), "dram_bytes": b, "ops": o, "case": case,
+                     "command": command}
+    with open(out_path, "w") as f:
+        json.dump(out, f, indent=1)
+    print(json.dumps(out, indent=1))
+
+
 def main():
+    if len(sys.argv) > 1 and sys.argv[1] == "--ingest-ncu":
+        ingest_ncu(sys.argv[2], sys.argv[3], sys.argv[4])
+        return
     args = parse()
     if args.impl == "reference":
         run_reference(args)

@@ -174,6 +174,7 @@ def lib():
                                               ctypes.POINTER(_VP)]),
         "exageostat_b200_batch_loglik": (_I, [_VP, _PD, _PD]),
         "exageostat_b200_batch_destroy": (_I, [_VP]),
+        "exageostat_b200_batch_loglik_grad": (_I, [_VP, _PD, _PD, _PD]),
         "exageostat_b200_set_sliced": (_I, [PM]),
         "exageostat_b200_dmle_host_sliced": (_I, [_I, _PD, _PD, _PD, _PD, _I, _I, _I, _PD]),
         "exageostat_b200_sliced_factor_dense": (_I, [_I, _PD, _PD, _PD, _I, _I, _I, _PD]),
@@ -597,9 +598,16 @@ class Batch:
             self.autotune_report = [(int(rep[2 * i]), float(rep[2 * i + 1])) for i in range(4) if rep[2 * i] > 0]
         self.h = h
 
-    def loglik(self, thetas) -> np.ndarray:
+    def loglik(self, thetas, grad: bool = False):
+        """Log-likelihood of every field (one row of parameters per field);
+        with grad=True also the gradients, an array of the same shape as the
+        parameters: (loglik, grad)."""
         th = _f64(thetas).reshape(len(self.n), self.nparams)
         out = np.empty(len(self.n))
+        if grad:
+            g = np.empty_like(th)
+            _check(self.L.exageostat_b200_batch_loglik_grad(self.h, _p(th), _p(out), _p(g)))
+            return out, g
         _check(self.L.exageostat_b200_batch_loglik(self.h, _p(th), _p(out)))
         return out
 

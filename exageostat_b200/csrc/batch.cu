@@ -3,16 +3,21 @@
  *
  * The reference evaluates one field per MLE_data; a study of many regions
  * loops over the exact path.  Here every field of a batch shares one lower-tile
- * store (fields packed one after the other, one TMA tensor over all of them)
- * and the factorisation runs tile step by tile step for all fields at once:
- * step k is one POTRF launch (one CTA per field with more than k tile rows),
- * one TRSM launch and one trailing-update launch whose CTAs each find their
- * field by a binary search in the step's block table.  Generation, the
- * ~3 * max(nt) step launches and the final reduction are captured once into a
- * CUDA graph; each evaluation uploads the fields' parameters (computed on the
- * host exactly as for a single field) and replays the graph.  Every field has
- * its own status word, so a field whose covariance is not positive definite
- * reports -inf without stopping the others.
+ * store (fields packed one after the other, one TMA tensor over all of them).
+ * Generation is one launch over every tile of every field; the whole
+ * factorisation (with the fused log-det and z solve) of all fields is ONE
+ * persistent launch driven by a device-resident tile scheduler
+ * (xg_batch_sched_kernel): the task list -- every POTRF, TRSM and trailing
+ * tile update of every field, in one topological order built here -- is
+ * taken by persistent CTAs, each task waiting (bounded) on per-tile
+ * dependency counters and publishing its completion, so the fields' steps
+ * interleave freely instead of proceeding in lock-step.  The reduction to
+ * log-likelihoods is a third launch.  The memsets and the three launches are
+ * captured once into a CUDA graph; each evaluation uploads the fields'
+ * parameters (computed on the host exactly as for a single field) and replays
+ * the graph.  Every field has its own status word, so a field whose
+ * covariance is not positive definite reports -inf without stopping the
+ * others.
  */
 #include <math.h>
 #include <stdlib.h>
@@ -27,6 +32,12 @@
 #include "xg_engine.h"
 #include "xg_kernels.h"
 
+#define XG_CU(call)                                                                                                    \
+    do {                                                                                                               \
+        cudaError_t _e = (call);                                                                                       \
+        if (_e != cudaSuccess) return xg_fail(XG_ERR_CUDA, "%s: %s", #call, cudaGetErrorString(_e));                   \
+    } while (0)
+
 struct XgBTable {
     std::vector<int> fields;
     std::vector<long long> start; /* nact + 1 */
@@ -36,7 +47,7 @@ struct XgBTable {
 
 struct XgBatch {
     int nfields = 0, ts = 0, kernel = 0, metric = 0, maxnt = 0;
-    long long total_tiles = 0, total_vec = 0, total_part = 0;
+    long long total_tiles = 0, total_vec = 0, total_part = 0, total_cnt = 0;
     std::vector<XgBField> F;
     XgBField *F_dev = nullptr, *F_pinned = nullptr;
     double *tiles = nullptr, *x = nullptr, *y = nullptr, *z = nullptr, *v = nullptr, *part = nullptr,
@@ -44,16 +55,42 @@ struct XgBatch {
     int *status = nullptr, *h_status = nullptr;
     void *table_buf = nullptr;
     XgBTable gen;
-    std::vector<XgBTable> potrf, trsm, gemm;
+    /* device tile scheduler: task list, counters, next-task index, abort flag */
+    int4 *tasks = nullptr;
+    long long ntasks = 0;
+    int *cnt = nullptr;
+    unsigned long long *next = nullptr;
+    int *abort_flag = nullptr;
+    double *dinv = nullptr; /* per scheduler CTA: ts x 32 inverted diagonal blocks */
     CUtensorMap map;
     cudaGraphExec_t graph = nullptr;
+    /* gradients (allocated on the first request): per stream an inverse-factor
+     * store for the largest field and contraction partials; per field a TMA
+     * view of its tiles; one (i, j) table per tile count; 4 sums per field */
+    static const int GS = 8;
+    cudaStream_t gst[GS] = {};
+    XgTileMatrix gX[GS];
+    double *gpart[GS] = {};
+    double *gout = nullptr, *h_gout = nullptr;
+    std::vector<CUtensorMap> fmap;
+    std::vector<int2 *> ij_by_nt;
 };
 
 static void xg_batch_free(XgBatch *b)
 {
     if (!b) return;
     if (b->graph) cudaGraphExecDestroy(b->graph);
-    void *dev[] = {b->F_dev, b->tiles, b->x, b->y, b->z, b->v, b->part, b->out, b->status, b->table_buf};
+    for (int s = 0; s < XgBatch::GS; ++s) {
+        xg_tm_free(b->gX[s]);
+        if (b->gpart[s]) cudaFree(b->gpart[s]);
+        if (b->gst[s]) cudaStreamDestroy(b->gst[s]);
+    }
+    for (int2 *p : b->ij_by_nt)
+        if (p) cudaFree(p);
+    if (b->gout) cudaFree(b->gout);
+    if (b->h_gout) cudaFreeHost(b->h_gout);
+    void *dev[] = {b->F_dev, b->tiles, b->x, b->y, b->z, b->v, b->part, b->out, b->status, b->table_buf,
+                   b->tasks, b->cnt, b->next, b->abort_flag, b->dinv};
     for (void *p : dev)
         if (p) cudaFree(p);
     if (b->F_pinned) cudaFreeHost(b->F_pinned);
@@ -102,9 +139,11 @@ extern "C" int exageostat_b200_batch_create(int nfields, const int *n, const dou
         fd.tile_off = b->total_tiles;
         fd.vec_off = b->total_vec;
         fd.part_off = b->total_part;
+        fd.sched_off = b->total_cnt;
         b->total_tiles += xg_num_lower_tiles(fd.nt);
         b->total_vec += (long long)fd.nt * b->ts;
         b->total_part += 2LL * fd.nt;
+        b->total_cnt += fd.nt + 2 * xg_num_lower_tiles(fd.nt);
         if (fd.nt > b->maxnt) b->maxnt = fd.nt;
     }
     const size_t tile = (size_t)b->ts * b->ts;
@@ -138,33 +177,43 @@ extern "C" int exageostat_b200_batch_create(int nfields, const int *n, const dou
     cudaMemcpy(b->x, hx.data(), b->total_vec * sizeof(double), cudaMemcpyHostToDevice);
     cudaMemcpy(b->y, hy.data(), b->total_vec * sizeof(double), cudaMemcpyHostToDevice);
     cudaMemcpy(b->z, hz.data(), b->total_vec * sizeof(double), cudaMemcpyHostToDevice);
-    /* launch tables */
-    const int bpt = b->ts / 128;
+    /* generation table: the CTAs of every field's tiles */
     std::vector<long long> cnt(nfields);
     for (int f = 0; f < nfields; ++f) cnt[f] = xg_num_lower_tiles(b->F[f].nt) * (b->ts / 8);
     xg_table_fill(b->gen, cnt);
-    b->potrf.resize(b->maxnt);
-    b->trsm.resize(b->maxnt);
-    b->gemm.resize(b->maxnt);
-    for (int k = 0; k < b->maxnt; ++k) {
-        for (int f = 0; f < nfields; ++f) cnt[f] = b->F[f].nt > k ? 1 : 0;
-        xg_table_fill(b->potrf[k], cnt);
-        for (int f = 0; f < nfields; ++f) cnt[f] = (long long)std::max(0, b->F[f].nt - k - 1) * (b->ts / 32);
-        xg_table_fill(b->trsm[k], cnt);
-        for (int f = 0; f < nfields; ++f) {
-            const long long T = std::max(0, b->F[f].nt - k - 1);
-            cnt[f] = T * (T + 1) / 2 * bpt * bpt;
+    /* the scheduler's task list in one topological order: step by step; in a
+     * step the POTRFs (largest fields first), the TRSMs, then the updates
+     * column by column, so the next step's panel column is ready first */
+    {
+        std::vector<int> order(nfields);
+        for (int f = 0; f < nfields; ++f) order[f] = f;
+        std::stable_sort(order.begin(), order.end(), [&](int a, int c) { return b->F[a].nt > b->F[c].nt; });
+        std::vector<int4> tl;
+        for (int k = 0; k < b->maxnt; ++k) {
+            for (int f : order)
+                if (b->F[f].nt > k) tl.push_back(make_int4(XG_TASK_POTRF | (f << 2), k, k, k));
+            for (int f : order)
+                for (int i = k + 1; i < b->F[f].nt; ++i) tl.push_back(make_int4(XG_TASK_TRSM | (f << 2), i, k, k));
+            for (int j = k + 1; j < b->maxnt; ++j)
+                for (int f : order)
+                    for (int i = j; i < b->F[f].nt; ++i) tl.push_back(make_int4(XG_TASK_GEMM | (f << 2), i, j, k));
         }
-        xg_table_fill(b->gemm[k], cnt);
+        b->ntasks = (long long)tl.size();
+        e = cudaMalloc(&b->tasks, tl.size() * sizeof(int4));
+        if (e == cudaSuccess) e = cudaMemcpy(b->tasks, tl.data(), tl.size() * sizeof(int4), cudaMemcpyHostToDevice);
+        if (e == cudaSuccess) e = cudaMalloc(&b->cnt, (size_t)b->total_cnt * sizeof(int));
+        if (e == cudaSuccess) e = cudaMalloc(&b->next, sizeof(unsigned long long));
+        if (e == cudaSuccess) e = cudaMalloc(&b->abort_flag, sizeof(int));
+        if (e == cudaSuccess) e = cudaMalloc(&b->dinv, (size_t)g_xg.sm_count * b->ts * 32 * sizeof(double));
+        if (e != cudaSuccess) {
+            xg_batch_free(b);
+            return xg_fail(XG_ERR_NO_MEMORY, "batch task list (%lld tasks): %s", (long long)tl.size(),
+                           cudaGetErrorString(e));
+        }
     }
-    /* one device buffer for every table: fields (int) then starts (long long) */
+    /* one device buffer for the table(s): fields (int) then starts (long long) */
     std::vector<XgBTable *> all;
     all.push_back(&b->gen);
-    for (int k = 0; k < b->maxnt; ++k) {
-        all.push_back(&b->potrf[k]);
-        all.push_back(&b->trsm[k]);
-        all.push_back(&b->gemm[k]);
-    }
     size_t bytes = 0;
     for (XgBTable *t : all) bytes += t->start.size() * sizeof(long long) + ((t->fields.size() * sizeof(int) + 7) & ~7ULL);
     std::vector<unsigned char> hbuf(bytes);
@@ -198,13 +247,20 @@ static void xg_batch_record(XgBatch *b, cudaStream_t st)
 {
     XgTileArgs base{b->tiles, b->ts, 0};
     cudaMemsetAsync(b->status, 0, 2 * (size_t)b->nfields * sizeof(int), st);
+    cudaMemsetAsync(b->cnt, 0, (size_t)b->total_cnt * sizeof(int), st);
+    cudaMemsetAsync(b->next, 0, sizeof(unsigned long long), st);
+    cudaMemsetAsync(b->abort_flag, 0, sizeof(int), st);
     cudaMemcpyAsync(b->v, b->z, b->total_vec * sizeof(double), cudaMemcpyDeviceToDevice, st);
     xg_launch_batch_gen(base, b->F_dev, b->gen.dev, b->gen.blocks, b->x, b->y, b->metric, st);
-    for (int k = 0; k < b->maxnt; ++k) {
-        xg_launch_batch_potrf(base, b->F_dev, b->potrf[k].dev, k, b->v, b->part, b->status, nullptr, st);
-        xg_launch_batch_trsm(base, b->F_dev, b->trsm[k].dev, b->trsm[k].blocks, k, b->v, b->status, st);
-        xg_launch_batch_gemm(b->map, base, b->F_dev, b->gemm[k].dev, b->gemm[k].blocks, k, b->status, st);
-    }
+    XgSched sch;
+    sch.tasks = b->tasks;
+    sch.ntasks = b->ntasks;
+    sch.next = b->next;
+    sch.abort = b->abort_flag;
+    sch.cnt = b->cnt;
+    sch.dinv = b->dinv;
+    const int ctas = (int)std::min<long long>(g_xg.sm_count, b->ntasks);
+    xg_launch_batch_sched(b->map, base, b->F_dev, sch, ctas, b->v, b->part, b->status, st);
     xg_launch_batch_finalize(b->F_dev, b->nfields, b->part, b->out, st);
 }
 
@@ -256,6 +312,86 @@ extern "C" int exageostat_b200_batch_loglik(void *handle, const double *theta, d
     }
     if (failed) xg_fail(XG_ERR_NOT_SPD, "%d of %d fields are not positive definite (their loglik is -inf)", failed,
                         b->nfields);
+    return XG_OK;
+}
+
+/* gradient workspace of a batch (first gradient request) */
+static int xg_batch_grad_workspace(XgBatch *b)
+{
+    if (b->gout) return XG_OK;
+    const int ts = b->ts;
+    long long maxblocks = 0;
+    b->ij_by_nt.assign(b->maxnt + 1, nullptr);
+    for (int nt = 1; nt <= b->maxnt; ++nt) {
+        const long long ntl = xg_num_lower_tiles(nt);
+        std::vector<int2> h(ntl);
+        for (int j = 0; j < nt; ++j)
+            for (int i = j; i < nt; ++i) h[xg_tile_index(i, j, nt)] = make_int2(i, j);
+        XG_CU(cudaMalloc(&b->ij_by_nt[nt], sizeof(int2) * ntl));
+        XG_CU(cudaMemcpy(b->ij_by_nt[nt], h.data(), sizeof(int2) * ntl, cudaMemcpyHostToDevice));
+        maxblocks = std::max(maxblocks, xg_grad_contract_blocks(ntl, ts));
+    }
+    for (int s = 0; s < XgBatch::GS; ++s) {
+        int rc = xg_tm_alloc(b->gX[s], b->maxnt * ts, ts);
+        if (rc) return rc;
+        XG_CU(cudaMalloc(&b->gpart[s], 4 * (size_t)maxblocks * sizeof(double)));
+        XG_CU(cudaStreamCreateWithFlags(&b->gst[s], cudaStreamNonBlocking));
+    }
+    b->fmap.resize(b->nfields);
+    for (int f = 0; f < b->nfields; ++f) {
+        const XgBField &fd = b->F[f];
+        int rc = xg_encode_tiles(&b->fmap[f], b->tiles + fd.tile_off * (long long)ts * ts, xg_num_lower_tiles(fd.nt),
+                                 ts);
+        if (rc) return rc;
+    }
+    XG_CU(cudaMalloc(&b->gout, 4 * (size_t)b->nfields * sizeof(double)));
+    XG_CU(cudaMallocHost(&b->h_gout, 4 * (size_t)b->nfields * sizeof(double)));
+    return XG_OK;
+}
+
+/* Log-likelihoods and their gradients of every field: the batched
+ * factorisation (the graph of exageostat_b200_batch_loglik), then per field,
+ * round-robin over eight streams, the adjoint of the single-field path on
+ * that field's tiles -- alpha = L^-T v by backward tile solves, X = L^-T,
+ * Sigma^-1 = X X^T over the factor, and the fused contraction with the
+ * on-the-fly dSigma/dtheta tiles.  A field that is not positive definite
+ * gets loglik -inf and a NaN gradient. */
+extern "C" int exageostat_b200_batch_loglik_grad(void *handle, const double *theta, double *loglik, double *grad)
+{
+    XgBatch *b = (XgBatch *)handle;
+    if (!b || !theta || !loglik || !grad) return xg_fail(XG_ERR_BAD_ARGUMENT, "NULL argument");
+    int rc = xg_batch_grad_workspace(b);
+    if (rc) return rc;
+    rc = exageostat_b200_batch_loglik(handle, theta, loglik);
+    if (rc) return rc;
+    const int ts = b->ts;
+    const int np = b->kernel == 1 ? 4 : 3;
+    for (int f = 0; f < b->nfields; ++f) {
+        if (!std::isfinite(loglik[f])) continue;
+        const XgBField &fd = b->F[f];
+        const int s = f % XgBatch::GS;
+        cudaStream_t st = b->gst[s];
+        XgTileArgs T{b->tiles + fd.tile_off * (long long)ts * ts, ts, fd.nt};
+        double *vf = b->v + fd.vec_off;
+        int *stf = b->status + 2 * f;
+        for (int k = fd.nt - 1; k >= 0; --k) xg_launch_trsv_lower_t_step(T, k, vf, stf, st);
+        xg_launch_inverse_factor(b->gX[s].map, b->fmap[f], b->gX[s].d, T.data, fd.nt, ts, stf, st);
+        xg_launch_inverse_syrk(b->gX[s].map, T.data, fd.nt, ts, stf, st);
+        const double dlogcon = -(log(2.0) + xg_digamma(fd.p.nu));
+        xg_launch_grad_contract(T.data, b->ij_by_nt[fd.nt], xg_num_lower_tiles(fd.nt), fd.nt, ts, b->x + fd.vec_off,
+                                b->y + fd.vec_off, vf, fd.N, fd.p, b->kernel, b->metric, dlogcon, b->gpart[s],
+                                b->gout + 4 * (size_t)f, st);
+    }
+    XG_CU(cudaGetLastError());
+    for (int s = 0; s < XgBatch::GS; ++s) XG_CU(cudaStreamSynchronize(b->gst[s]));
+    XG_CU(cudaMemcpy(b->h_gout, b->gout, 4 * (size_t)b->nfields * sizeof(double), cudaMemcpyDeviceToHost));
+    XG_CU(cudaMemcpy(b->h_status, b->status, 2 * (size_t)b->nfields * sizeof(int), cudaMemcpyDeviceToHost));
+    for (int f = 0; f < b->nfields; ++f) {
+        const bool ok = std::isfinite(loglik[f]) && b->h_status[2 * f] == 0;
+        if (!ok && std::isfinite(loglik[f]) && (b->h_status[2 * f] & XG_ST_TIMEOUT))
+            return xg_fail(XG_ERR_TIMEOUT, "field %d: a device wait timed out", f);
+        for (int i = 0; i < np; ++i) grad[(size_t)f * np + i] = ok ? b->h_gout[4 * (size_t)f + i] : NAN;
+    }
     return XG_OK;
 }
 

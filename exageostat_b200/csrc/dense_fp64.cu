@@ -94,6 +94,18 @@ __global__ void __launch_bounds__(256) xg_gen_matern_batch_kernel(XgTileArgs bas
 }
 
 /* ========================================================================== */
+/* Loads of tile data.  COH = false: ordinary loads (the data was written by   */
+/* an earlier launch).  COH = true: the bodies run inside the persistent       */
+/* scheduler, where other CTAs of the same launch wrote the data: the loads go */
+/* to L2 (ld.global.cg), never to a line this SM's L1 kept from an earlier     */
+/* task.                                                                      */
+/* ========================================================================== */
+
+template <bool COH> __device__ __forceinline__ double xg_ldt(const double *p) { return COH ? __ldcg(p) : *p; }
+template <bool COH> __device__ __forceinline__ double2 xg_ldt2(const double2 *p) { return COH ? __ldcg(p) : *p; }
+template <bool COH> __device__ __forceinline__ double xg_ldro(const double *p) { return COH ? __ldcg(p) : __ldg(p); }
+
+/* ========================================================================== */
 /* POTRF of a diagonal tile, fused with log-det and the z block solve         */
 /* ========================================================================== */
 
@@ -102,7 +114,7 @@ __global__ void __launch_bounds__(256) xg_gen_matern_batch_kernel(XgTileArgs bas
  * wavefront but the DMMA fragment loads are conflict-free. */
 #define XG_POTRF_THREADS 512
 
-template <int NB>
+template <int NB, bool COH = false>
 __device__ __forceinline__ void xg_potrf_body(const XgTileArgs &T, int k, double *__restrict__ v,
                                               double *__restrict__ part_logdet, double *__restrict__ part_dot,
                                               int with_rhs, int *status, int *info)
@@ -123,14 +135,14 @@ __device__ __forceinline__ void xg_potrf_body(const XgTileArgs &T, int k, double
         s_logdet = 0.0;
     }
     if (with_rhs)
-        for (int r = tid; r < ts; r += blockDim.x) vs[r] = vk[r];
+        for (int r = tid; r < ts; r += blockDim.x) vs[r] = xg_ldt<COH>(vk + r);
     double logdet_lane = 0.0;
     for (int c0 = 0; c0 < ts; c0 += NB) {
         const int rows = ts - c0;
         __syncthreads();
         for (int idx = tid; idx < rows * NB; idx += blockDim.x) {
             const int r = idx / NB, c = idx - r * NB;
-            P[r * LDP + c] = A[(long long)(c0 + r) * ts + c0 + c];
+            P[r * LDP + c] = xg_ldt<COH>(A + (long long)(c0 + r) * ts + c0 + c);
         }
         __syncthreads();
         /* unblocked Cholesky of the NB x NB diagonal block, one lane per row */
@@ -213,7 +225,7 @@ __device__ __forceinline__ void xg_potrf_body(const XgTileArgs &T, int k, double
             const int g = lane >> 2, tq = lane & 3;
             const double *Pb = P + NB * LDP;
             double *At = A + (long long)(c0 + NB) * ts + (c0 + NB);
-            for (int blk = warp; blk < nblk; blk += XG_POTRF_THREADS / 32) {
+            for (int blk = warp; blk < nblk; blk += (int)(blockDim.x >> 5)) {
                 int bi = (int)((sqrtf(8.0f * blk + 1.0f) - 1.0f) * 0.5f);
                 while ((bi + 1) * (bi + 2) / 2 <= blk) ++bi;
                 while (bi * (bi + 1) / 2 > blk) --bi;
@@ -257,7 +269,7 @@ __device__ __forceinline__ void xg_potrf_body(const XgTileArgs &T, int k, double
                             const int rr = r0 + mi * 16 + g + 8 * h;
                             if (rr < R && cc < R) {
                                 double2 *pc = reinterpret_cast<double2 *>(At + (long long)rr * ts + cc);
-                                double2 cv = *pc;
+                                double2 cv = xg_ldt2<COH>(pc);
                                 cv.x -= acc[mi][ni][2 * h];
                                 cv.y -= acc[mi][ni][2 * h + 1];
                                 *pc = cv;
@@ -325,28 +337,35 @@ __global__ void __launch_bounds__(XG_POTRF_THREADS) xg_potrf_diag_batch_kernel(X
 /* Inverses of the 32 x 32 diagonal blocks of L_kk (for the panel TRSM)       */
 /* ========================================================================== */
 
-/* One warp per diagonal block b: lane c forms column c of the inverse by
- * forward substitution, z_i = (delta_ic - sum_{q<i} L_iq z_q) / L_ii, and
- * writes T.dinv[(32 b + i) * 32 + c] = z_i (lower triangular). */
-__global__ void __launch_bounds__(32) xg_diag_inv_kernel(XgTileArgs T, int k, const int *status)
+/* One warp inverts the 32 x 32 lower-triangular block LB (shared memory,
+ * row stride 33): lane c forms column c by forward substitution,
+ * z_i = (delta_ic - sum_{q<i} L_iq z_q) / L_ii, and stores D[i * 32 + c] = z_i.
+ * The per-field and the batched paths share this arithmetic exactly. */
+__device__ __forceinline__ void xg_lower32_inverse(const double *LB, int lane, double *D)
 {
-    if (*(volatile const int *)status) return;
-    __shared__ double LB[32][33];
-    const int ts = T.ts, b = blockIdx.x, lane = threadIdx.x;
-    const double *L = T.data + xg_slot64(T, k, k) * (long long)ts * ts + (long long)(b * 32) * ts + b * 32;
-    for (int r = 0; r < 32; ++r) LB[r][lane] = L[(long long)r * ts + lane];
-    __syncwarp();
     double z[32];
 #pragma unroll
     for (int i = 0; i < 32; ++i) {
         double s = (i == lane) ? 1.0 : 0.0;
 #pragma unroll
-        for (int q = 0; q < i; ++q) s -= LB[i][q] * z[q];
-        z[i] = s / LB[i][i];
+        for (int q = 0; q < i; ++q) s -= LB[i * 33 + q] * z[q];
+        z[i] = s / LB[i * 33 + i];
     }
-    double *D = T.dinv + (long long)(b * 32) * 32;
 #pragma unroll
     for (int i = 0; i < 32; ++i) D[i * 32 + lane] = z[i];
+}
+
+/* One warp per diagonal block b of L_kk: T.dinv[(32 b + i) * 32 + c] =
+ * (L_bb^-1)_ic (lower triangular). */
+__global__ void __launch_bounds__(32) xg_diag_inv_kernel(XgTileArgs T, int k, const int *status)
+{
+    if (*(volatile const int *)status) return;
+    __shared__ double LB[32 * 33];
+    const int ts = T.ts, b = blockIdx.x, lane = threadIdx.x;
+    const double *L = T.data + xg_slot64(T, k, k) * (long long)ts * ts + (long long)(b * 32) * ts + b * 32;
+    for (int r = 0; r < 32; ++r) LB[r * 33 + lane] = L[(long long)r * ts + lane];
+    __syncwarp();
+    xg_lower32_inverse(LB, lane, T.dinv + (long long)(b * 32) * 32);
 }
 
 /* ========================================================================== */
@@ -356,6 +375,7 @@ __global__ void __launch_bounds__(32) xg_diag_inv_kernel(XgTileArgs T, int k, co
 #define XG_TRSM_THREADS 512
 #define XG_TRSM_SR 32 /* rows of A_ik per CTA */
 
+template <bool COH = false>
 __device__ __forceinline__ void xg_trsm_body(const XgTileArgs &T, int k, double *__restrict__ v, int with_rhs,
                                              const int *status, long long bid)
 {
@@ -373,19 +393,19 @@ __device__ __forceinline__ void xg_trsm_body(const XgTileArgs &T, int k, double 
     const double *L = T.data + xg_slot64(T, k, k) * (long long)ts * ts;
     for (int idx = tid; idx < XG_TRSM_SR * ts; idx += blockDim.x) {
         const int r = idx / ts, c = idx - r * ts;
-        S[r * LDS + c] = B[(long long)r * ts + c];
+        S[r * LDS + c] = xg_ldt<COH>(B + (long long)r * ts + c);
     }
     for (int cb = 0; cb < ts; cb += 32) {
         if (T.dinv) {
             /* the inverse D of this 32 x 32 diagonal block (xg_diag_inv_kernel) */
             for (int idx = tid; idx < 32 * 32; idx += blockDim.x) {
                 const int r = idx >> 5, c = idx & 31;
-                LD[r * 33 + c] = T.dinv[(cb + r) * 32 + c];
+                LD[r * 33 + c] = xg_ldt<COH>(T.dinv + (cb + r) * 32 + c);
             }
         } else {
             for (int idx = tid; idx < 32 * 32; idx += blockDim.x) {
                 const int r = idx >> 5, c = idx & 31;
-                LD[r * 33 + c] = L[(long long)(cb + r) * ts + cb + c];
+                LD[r * 33 + c] = xg_ldt<COH>(L + (long long)(cb + r) * ts + cb + c);
             }
         }
         __syncthreads();
@@ -438,7 +458,7 @@ __device__ __forceinline__ void xg_trsm_body(const XgTileArgs &T, int k, double 
         /* S[:, cb+32:] -= S[:, cb:cb+32] L[cb+32:, cb:cb+32]^T, 32-column groups */
         const int ncol = ts - cb - 32;
         const int ngrp = ncol / 32;
-        for (int grp = warp; grp < ngrp; grp += XG_TRSM_THREADS / 32) {
+        for (int grp = warp; grp < ngrp; grp += (int)(blockDim.x >> 5)) {
             const int c0 = cb + 32 + grp * 32;
             double acc[2][4][4];
 #pragma unroll
@@ -456,7 +476,7 @@ __device__ __forceinline__ void xg_trsm_body(const XgTileArgs &T, int k, double 
                     a[mi][1] = S[(mi * 16 + g + 8) * LDS + cb + p0 + tq];
                 }
 #pragma unroll
-                for (int ni = 0; ni < 4; ++ni) b[ni] = __ldg(L + (long long)(c0 + ni * 8 + g) * ts + cb + p0 + tq);
+                for (int ni = 0; ni < 4; ++ni) b[ni] = xg_ldro<COH>(L + (long long)(c0 + ni * 8 + g) * ts + cb + p0 + tq);
 #pragma unroll
                 for (int mi = 0; mi < 2; ++mi)
 #pragma unroll
@@ -484,11 +504,11 @@ __device__ __forceinline__ void xg_trsm_body(const XgTileArgs &T, int k, double 
     if (with_rhs) {
         const double *vk = v + (long long)k * ts;
         double *vi = v + (long long)i * ts + strip * XG_TRSM_SR;
-        for (int r = warp; r < XG_TRSM_SR; r += XG_TRSM_THREADS / 32) {
+        for (int r = warp; r < XG_TRSM_SR; r += (int)(blockDim.x >> 5)) {
             double s = 0.0;
-            for (int c = lane; c < ts; c += 32) s += S[r * LDS + c] * vk[c];
+            for (int c = lane; c < ts; c += 32) s += S[r * LDS + c] * xg_ldt<COH>(vk + c);
             for (int off = 16; off > 0; off >>= 1) s += __shfl_xor_sync(0xffffffffu, s, off);
-            if (lane == 0) vi[r] -= s;
+            if (lane == 0) vi[r] = xg_ldt<COH>(vi + r) - s;
         }
     }
 }
@@ -531,6 +551,7 @@ __global__ void __launch_bounds__(XG_TRSM_THREADS) xg_trsm_panel_batch_kernel(Xg
 /* Updates the tiles (i, j), j0 <= j <= i < nt, with panel column k.  With
  * single_col the launch covers column j0 only (the lookahead split: the next
  * panel's column first, the rest of the trailing matrix in a second launch). */
+template <bool COH = false>
 __device__ __forceinline__ void xg_gemm_body(const CUtensorMap &map, const XgTileArgs &T, int k, int j0,
                                              int single_col, int *status, long long bid)
 {
@@ -578,7 +599,18 @@ __device__ __forceinline__ void xg_gemm_body(const CUtensorMap &map, const XgTil
     const int rowB = T.band ? j * ts + bj * XG_G_BM
                             : (int)((T.tile_off + xg_tile_index(j, k, T.nt)) * ts + bj * XG_G_BM);
     int issued = 0;
+    __shared__ int s_gfail;
+    if (COH) {
+        /* each thread orders its earlier generic shared-memory writes (an
+         * earlier task used this memory) before the TMA writes into it */
+        xg_fence_proxy_async();
+        if (tid == 0) s_gfail = 0;
+        __syncthreads();
+    }
     if (tid == 0) {
+        /* the operand tiles may have been written by other CTAs of this launch
+         * through ordinary stores: order them before the async-proxy reads */
+        if (COH) asm volatile("fence.proxy.async.global;" ::: "memory");
         xg_prefetch_tensormap(&map);
         for (; issued < XG_G_STAGES && issued < KT; ++issued) {
             unsigned char *sa = smem + issued * XG_G_STAGE_BYTES;
@@ -601,15 +633,21 @@ __device__ __forceinline__ void xg_gemm_body(const CUtensorMap &map, const XgTil
             for (int h = 0; h < 2; ++h) {
                 const int r = wm * 64 + mi * 16 + g + 8 * h;
                 const int c = wn * 32 + ni * 8 + 2 * tq;
-                const double2 cv = *reinterpret_cast<const double2 *>(C + (long long)r * ts + c);
+                const double2 cv = xg_ldt2<COH>(reinterpret_cast<const double2 *>(C + (long long)r * ts + c));
                 acc[mi][ni][2 * h] = -cv.x;
                 acc[mi][ni][2 * h + 1] = -cv.y;
             }
     bool ok = true;
     for (int kb = 0; kb < KT; ++kb) {
         const int s = kb % XG_G_STAGES;
-        if (!xg_mbar_wait(&full[s], (kb / XG_G_STAGES) & 1)) {
+        if (COH && __shfl_sync(0xffffffffu, *(volatile int *)&s_gfail, 0)) { /* warp-uniform */
             ok = false;
+            break;
+        }
+        const bool landed = xg_mbar_wait(&full[s], (kb / XG_G_STAGES) & 1);
+        if (COH ? !__all_sync(0xffffffffu, landed) : !landed) {
+            ok = false;
+            if (COH) s_gfail = 1;
             break;
         }
         const unsigned char *sa = smem + s * XG_G_STAGE_BYTES;
@@ -655,10 +693,17 @@ __device__ __forceinline__ void xg_gemm_body(const CUtensorMap &map, const XgTil
                 ++issued;
             } else {
                 ok = false;
+                if (COH) s_gfail = 1;
             }
         }
         __syncwarp();
+        if (COH) ok = ok && !__shfl_sync(0xffffffffu, *(volatile int *)&s_gfail, 0);
         if (!ok) break;
+    }
+    if (COH) {
+        /* a failed wait anywhere makes every warp leave together */
+        __syncthreads();
+        ok = s_gfail == 0;
     }
     if (!ok) {
         atomicOr(status, XG_ST_TIMEOUT);
@@ -702,6 +747,157 @@ __global__ void __launch_bounds__(XG_G_THREADS, 1) xg_syrk_gemm_batch_kernel(con
     T.nt = fd.nt;
     T.tile_off = fd.tile_off;
     xg_gemm_body(map, T, k, k + 1, 0, status + 2 * f, local);
+}
+
+/* ========================================================================== */
+/* Batched factorisation in one persistent launch (device tile scheduler)     */
+/* ========================================================================== */
+
+__device__ __forceinline__ int xg_ld_acquire(const int *p)
+{
+    int v;
+    asm volatile("ld.acquire.gpu.global.b32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+    return v;
+}
+
+__device__ __forceinline__ void xg_add_release(int *p, int v)
+{
+    asm volatile("red.release.gpu.global.add.s32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
+}
+
+/* thread 0: waits until *p >= target; false when the wall-time limit passes
+ * or another CTA aborted the launch */
+__device__ __forceinline__ bool xg_sched_wait(const int *p, int target, const int *abort, uint64_t t0)
+{
+    while (xg_ld_acquire(p) < target) {
+        if (*(volatile const int *)abort) return false;
+        if (xg_globaltimer_ns() - t0 > 2000000000ull) return false;
+        __nanosleep(256);
+    }
+    return true;
+}
+
+/* Persistent CTAs (one per SM, 256 threads) run the task list of XgSched:
+ * thread 0 takes the next task, waits for its dependency counters, the CTA
+ * runs the task body (the POTRF, TRSM and DMMA update bodies of the per-step
+ * kernels, with L2-coherent loads), and thread 0 publishes it (release).
+ * Tasks are taken in a topological order, so every task waited on was taken
+ * earlier by a CTA that is running: the launch cannot deadlock.  A wait that
+ * times out sets the field's XG_ST_TIMEOUT bit and the abort flag; a field
+ * whose pivot fails skips its remaining bodies (status word) but still
+ * publishes them, so no other field waits on it. */
+template <int NB>
+__global__ void __launch_bounds__(XG_G_THREADS, 1)
+    xg_batch_sched_kernel(const __grid_constant__ CUtensorMap map, XgTileArgs base, const XgBField *__restrict__ F,
+                          XgSched sch, double *v, double *part, int *status)
+{
+    __shared__ int4 s_task;
+    __shared__ int s_go;
+    const int tid = threadIdx.x;
+    const int ts = base.ts;
+    for (;;) {
+        __syncthreads(); /* the previous task is finished by every thread */
+        if (tid == 0) {
+            int4 t = make_int4(-1, 0, 0, 0);
+            if (!*(volatile int *)sch.abort) {
+                const unsigned long long q = atomicAdd(sch.next, 1ULL);
+                if (q < (unsigned long long)sch.ntasks) t = sch.tasks[q];
+            }
+            s_task = t;
+        }
+        __syncthreads();
+        const int4 tk = s_task;
+        if (tk.x < 0) break;
+        const int type = tk.x & 3, f = tk.x >> 2, i = tk.y, j = tk.z, k = tk.w;
+        const XgBField &fd = F[f];
+        XgTileArgs T = base;
+        T.data = base.data + fd.tile_off * (long long)ts * ts;
+        T.nt = fd.nt;
+        T.tile_off = fd.tile_off;
+        int *stf = status + 2 * f;
+        int *pdone = sch.cnt + fd.sched_off;
+        int *tdone = pdone + fd.nt;
+        int *ucnt = tdone + xg_num_lower_tiles(fd.nt);
+        if (tid == 0) {
+            const uint64_t t0 = xg_globaltimer_ns();
+            bool ok;
+            if (type == XG_TASK_POTRF)
+                ok = xg_sched_wait(ucnt + xg_tile_index(k, k, fd.nt), k, sch.abort, t0);
+            else if (type == XG_TASK_TRSM)
+                ok = xg_sched_wait(pdone + k, 1, sch.abort, t0) &&
+                     xg_sched_wait(ucnt + xg_tile_index(i, k, fd.nt), k, sch.abort, t0);
+            else
+                ok = xg_sched_wait(tdone + xg_tile_index(i, k, fd.nt), 1, sch.abort, t0) &&
+                     xg_sched_wait(tdone + xg_tile_index(j, k, fd.nt), 1, sch.abort, t0) &&
+                     xg_sched_wait(ucnt + xg_tile_index(i, j, fd.nt), k, sch.abort, t0);
+            if (!ok) {
+                atomicOr(stf, XG_ST_TIMEOUT);
+                atomicExch(sch.abort, 1);
+            }
+            s_go = ok ? 1 : 0;
+        }
+        __syncthreads();
+        if (s_go) {
+            if (type == XG_TASK_POTRF) {
+                xg_potrf_body<NB, true>(T, k, v + fd.vec_off, part + fd.part_off, part + fd.part_off + fd.nt, 1, stf,
+                                        stf + 1);
+            } else if (type == XG_TASK_TRSM) {
+                /* the inverted diagonal blocks of L_kk into this CTA's scratch
+                 * (warp w: blocks w, w + 8, ...), then the tile's row strips;
+                 * done even for a field that has failed (its strips then skip),
+                 * so every thread takes the same path */
+                {
+                    extern __shared__ __align__(16) double xg_smem_d[];
+                    const int warp = tid >> 5, lane = tid & 31;
+                    double *LB = xg_smem_d + warp * (32 * 33);
+                    double *D = sch.dinv + (long long)blockIdx.x * ts * 32;
+                    const double *Lkk = T.data + xg_tile_index(k, k, fd.nt) * (long long)ts * ts;
+                    for (int bb = warp; bb < ts / 32; bb += XG_G_THREADS / 32) {
+                        const double *Lb = Lkk + (long long)(bb * 32) * ts + bb * 32;
+                        for (int r = 0; r < 32; ++r) LB[r * 33 + lane] = __ldcg(Lb + (long long)r * ts + lane);
+                        __syncwarp();
+                        xg_lower32_inverse(LB, lane, D + (long long)(bb * 32) * 32);
+                        __syncwarp();
+                    }
+                    T.dinv = D;
+                }
+                __syncthreads();
+                const int strips = ts / XG_TRSM_SR;
+                for (int sp = 0; sp < strips; ++sp)
+                    xg_trsm_body<true>(T, k, v + fd.vec_off, 1, stf, (long long)(i - k - 1) * strips + sp);
+            } else {
+                const int bpt = ts / XG_G_BM;
+                for (int b = 0; b < bpt * bpt; ++b)
+                    xg_gemm_body<true>(map, T, k, j, 1, stf, (long long)(i - j) * bpt * bpt + b);
+            }
+        }
+        __syncthreads();
+        if (tid == 0) {
+            __threadfence();
+            if (type == XG_TASK_POTRF)
+                xg_add_release(pdone + k, 1);
+            else if (type == XG_TASK_TRSM)
+                xg_add_release(tdone + xg_tile_index(i, k, fd.nt), 1);
+            else
+                xg_add_release(ucnt + xg_tile_index(i, j, fd.nt), 1);
+        }
+    }
+}
+
+static size_t xg_sched_smem_bytes(int ts)
+{
+    size_t b = xg_gemm_smem_bytes();
+    b = b > xg_potrf_smem_bytes(ts) ? b : xg_potrf_smem_bytes(ts);
+    b = b > xg_trsm_smem_bytes(ts) ? b : xg_trsm_smem_bytes(ts);
+    return b;
+}
+
+void xg_launch_batch_sched(const CUtensorMap &map, const XgTileArgs &base, const XgBField *F, const XgSched &sch,
+                           int ctas, double *v, double *part, int *status, cudaStream_t st)
+{
+    if (sch.ntasks <= 0 || ctas <= 0) return;
+    xg_batch_sched_kernel<32><<<ctas, XG_G_THREADS, xg_sched_smem_bytes(base.ts), st>>>(map, base, F, sch, v, part,
+                                                                                          status);
 }
 
 /* ========================================================================== */
@@ -774,6 +970,9 @@ cudaError_t xg_kernels_configure()
     if (e != cudaSuccess) return e;
     e = cudaFuncSetAttribute(xg_syrk_gemm_batch_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
                              (int)xg_gemm_smem_bytes());
+    if (e != cudaSuccess) return e;
+    e = cudaFuncSetAttribute(xg_batch_sched_kernel<32>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             (int)xg_sched_smem_bytes(XG_MAX_TS));
     return e;
 }
 

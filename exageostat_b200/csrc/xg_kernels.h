@@ -78,9 +78,33 @@ struct XgBField {
     long long tile_off; /* first packed tile of the field in the batch store */
     long long vec_off;  /* first entry of its vectors (x, y, z, v); a multiple of ts */
     long long part_off; /* first entry of its partial sums (2 nt) */
+    long long sched_off; /* first of its scheduler counters (nt + 2 lower tiles) */
     int N, nt;
     int kernel, pad_;
     XgMaternParams p;   /* this evaluation's parameters */
+};
+
+/* Device-resident tile scheduler of a batch (xg_batch_sched_kernel).  The
+ * task list holds every POTRF(k), TRSM(i, k) and update (i, j) <- step k of
+ * every field in one topological order; persistent CTAs take tasks in list
+ * order (one atomic counter), wait (bounded) on the task's dependency
+ * counters, run it and publish its completion.  Per field, at sched_off:
+ *   pdone[k]            POTRF(k) done
+ *   tdone[tile (i, k)]  TRSM(i, k) done
+ *   ucount[tile (i, j)] updates applied to tile (i, j) (final at min(i, j))
+ * Dependencies: POTRF(k) <- ucount(k, k) = k; TRSM(i, k) <- pdone(k),
+ * ucount(i, k) = k; update (i, j, k) <- tdone(i, k), tdone(j, k),
+ * ucount(i, j) = k (the updates of a tile are applied in k order). */
+#define XG_TASK_POTRF 0
+#define XG_TASK_TRSM 1
+#define XG_TASK_GEMM 2
+struct XgSched {
+    const int4 *tasks;         /* x = type | field << 2, y = i, z = j, w = k */
+    long long ntasks;
+    unsigned long long *next;  /* index of the next task to take */
+    int *abort;                /* set after a wait that timed out: no CTA takes another task */
+    int *cnt;                  /* the counters of every field */
+    double *dinv;              /* per CTA, ts x 32: the inverted diagonal blocks of its TRSM task's L_kk */
 };
 
 /* The fields taking part in one batched launch and the CTA ranges they own. */
@@ -185,6 +209,10 @@ void xg_launch_batch_trsm(const XgTileArgs &base, const XgBField *F, const XgBSt
 void xg_launch_batch_gemm(const CUtensorMap &map, const XgTileArgs &base, const XgBField *F, const XgBStep &S,
                           long long blocks, int k, int *status, cudaStream_t st);
 void xg_launch_batch_finalize(const XgBField *F, int nfields, const double *part, double *out, cudaStream_t st);
+/* the whole batched factorisation (with the fused log-det and solve) in one
+ * persistent launch of `ctas` CTAs driven by the task list of `sch` */
+void xg_launch_batch_sched(const CUtensorMap &map, const XgTileArgs &base, const XgBField *F, const XgSched &sch,
+                           int ctas, double *v, double *part, int *status, cudaStream_t st);
 
 /* solve.cu */
 void xg_launch_trmv_lower(const XgTileArgs &T, const double *e, double *z, const int *status, cudaStream_t st);

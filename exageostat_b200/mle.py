@@ -138,8 +138,8 @@ def _tr_step(g, B, delta, lo, hi):
     return np.clip(d, lo, hi)
 
 
-def fit_trust_region(loglik_grad, theta0, lb, ub, max_iter=60, gtol=1e-3, delta0=0.5, delta_max=2.0, log=None,
-                     state=None):
+def fit_trust_region(loglik_grad, theta0, lb, ub, max_iter=60, gtol=1e-3, delta0=0.5, delta_max=1.0, log=None,
+                     state=None, ftol=0.0):
     """Gradient-based maximiser of f on the box [lb, ub] (lb > 0), for an
     objective whose value and adjoint gradient come from one call
     (loglik_grad(theta) -> (f, grad)).
@@ -156,8 +156,10 @@ def fit_trust_region(loglik_grad, theta0, lb, ub, max_iter=60, gtol=1e-3, delta0
     delta0 and never exceeds delta_max (a factor e^2 per step).
 
     Stops when the scaled projected gradient max_k |d f / d log theta_k| over
-    the free coordinates is at most gtol, or when the radius falls below
-    1e-8, or after max_iter iterations.  Returns (theta, f, evaluations,
+    the free coordinates is at most gtol, when the gain the model predicts
+    for its next step is below ftol (an objective whose values carry noise of
+    that size cannot resolve more), when the radius falls below 1e-8, or
+    after max_iter iterations.  Returns (theta, f, evaluations,
     history) with one (theta, f) pair per accepted step.  state (a dict, may
     be None): state["B"], when present, is the initial Hessian model in phi,
     and receives the final one."""
@@ -183,8 +185,10 @@ def fit_trust_region(loglik_grad, theta0, lb, ub, max_iter=60, gtol=1e-3, delta0
     if not np.isfinite(f):
         raise RuntimeError("the objective fails at the start point %s" % list(th))
     B = -np.eye(n) * max(np.max(np.abs(gphi)) / delta0, 1.0)
+    first_update = True
     if state is not None and state.get("B") is not None:
         B = np.array(state["B"], dtype=np.float64)
+        first_update = False
     delta = delta0
     history = [(th.copy(), f)]
 
@@ -197,6 +201,8 @@ def fit_trust_region(loglik_grad, theta0, lb, ub, max_iter=60, gtol=1e-3, delta0
             break
         d = _tr_step(gphi, B, delta, plo - phi, phi_hi - phi)
         pred = gphi @ d + 0.5 * d @ B @ d
+        if 0.0 < pred < ftol and it > 0:
+            break
         if pred <= 0.0 or np.linalg.norm(d) == 0.0:
             B = -np.eye(n) * max(np.max(np.abs(gphi)) / delta, 1.0)
             delta *= 0.25
@@ -209,6 +215,11 @@ def fit_trust_region(loglik_grad, theta0, lb, ub, max_iter=60, gtol=1e-3, delta0
             s, y = d, gc - gphi
             sy = s @ y
             if sy < -1e-12 * np.linalg.norm(s) * np.linalg.norm(y):
+                if first_update:
+                    # the scaled identity of the first step is replaced by
+                    # the curvature seen along it (y.y / s.y, Shanno-Phua)
+                    B = np.eye(n) * ((y @ y) / sy)
+                    first_update = False
                 Bs = B @ s
                 B = B - np.outer(Bs, Bs) / (s @ Bs) + np.outer(y, y) / sy
         if rho >= 0.1:
@@ -229,27 +240,92 @@ def fit_trust_region(loglik_grad, theta0, lb, ub, max_iter=60, gtol=1e-3, delta0
     return np.exp(phi), f, evals, history
 
 
-def fit_mixed(session, lb, ub, theta0=None, gtol=1e-2, polish_gtol=1e-3, polish_iter=0, log=None):
-    """Mixed-precision adjoint-gradient MLE: the trust-region maximiser on the
-    INT8-sliced objective and its sliced adjoint gradient (precision 3) from
-    theta0 (default: the lower bounds, where the reference's driver starts,
-    examples/examples.c:263-264), then, when polish_iter > 0, at most
-    polish_iter FP64 gradient steps from its end point that reuse the sliced
-    run's Hessian model.  Leaves the session in FP64.  Returns (theta_hat,
-    loglik, sliced evaluations, FP64 evaluations, theta after the sliced
-    stage)."""
-    start = np.asarray(lb if theta0 is None else theta0, dtype=np.float64)
+def start_point(loglik, z, lb, ub, nbeta=7):
+    """A start for the gradient drivers: sigma^2 = the sample variance of z,
+    nu = 1/2 (both clipped to the box), and the range beta that maximises
+    loglik over nbeta values spaced geometrically across [lb, ub] (nbeta
+    evaluations; a failing one counts as -inf).  Returns (theta, evaluations)."""
+    lb = np.asarray(lb, dtype=np.float64)
+    ub = np.asarray(ub, dtype=np.float64)
+    th = np.clip(np.array([float(np.var(z)), np.sqrt(lb[1] * ub[1]), 0.5] + list(lb[3:])), lb, ub)
+    best, fbest = th.copy(), -np.inf
+    for b in np.geomspace(lb[1], ub[1], nbeta):
+        t = th.copy()
+        t[1] = b
+        try:
+            fv = loglik(t)
+        except Exception:
+            fv = -np.inf
+        if np.isfinite(fv) and fv > fbest:
+            best, fbest = t, fv
+    return best, nbeta
+
+
+def ridge_polish(loglik, theta, B, lb, ub, h=0.05):
+    """One parabolic line search along the flattest direction u of the
+    Hessian model B (in phi = log theta): the likelihood at phi and phi +- h u
+    fixes a parabola whose vertex (at most 2 h away, inside the box) is the
+    new point.  On the sigma^2-beta ridge of the Matern likelihood the
+    gradient-based stop leaves the largest error along u, and three values
+    of the objective resolve it far better than a gradient of the same
+    precision.  Returns (theta, loglik at theta or the start value when the
+    parabola is not concave, evaluations)."""
+    lb = np.asarray(lb, dtype=np.float64)
+    ub = np.asarray(ub, dtype=np.float64)
+    phi = np.log(np.asarray(theta, dtype=np.float64))
+    w, V = np.linalg.eigh(np.asarray(B, dtype=np.float64))
+    u = V[:, int(np.argmax(w))]  # B is negative definite: the largest eigenvalue is the flattest
+    f0 = loglik(np.exp(phi))
+    fp = loglik(np.exp(np.clip(phi + h * u, np.log(lb), np.log(ub))))
+    fm = loglik(np.exp(np.clip(phi - h * u, np.log(lb), np.log(ub))))
+    c = fp - 2.0 * f0 + fm
+    if not (np.isfinite(c) and c < 0.0):
+        return np.exp(phi), f0, 3
+    t = float(np.clip(h * (fm - fp) / (2.0 * c), -2.0 * h, 2.0 * h))
+    th = np.exp(np.clip(phi + t * u, np.log(lb), np.log(ub)))
+    f1 = loglik(th)
+    if not (np.isfinite(f1) and f1 >= f0):
+        return np.exp(phi), f0, 4
+    return th, f1, 4
+
+
+def fit_mixed(session, lb, ub, theta0=None, gtol=0.1, ftol=1e-4, log=None):
+    """Mixed-precision adjoint-gradient MLE, entirely on the INT8-sliced
+    objective (precision 3): a start from start_point (unless theta0 is
+    given), the trust-region maximiser driven by the sliced adjoint gradient
+    (stopping at gtol / ftol, the noise level of that gradient), then
+    ridge_polish with sliced log-likelihood values.  Leaves the session in
+    FP64.  Returns (theta_hat, loglik, sliced evaluations (log-likelihood and
+    gradient), sliced log-likelihood-only evaluations, theta after the
+    gradient stage)."""
     session.set_sliced()
+    z = session.z()
+    if theta0 is None:
+        start, ne = start_point(lambda t: session.loglik(t), z, lb, ub)
+    else:
+        start, ne = np.asarray(theta0, dtype=np.float64), 0
     st = {}
-    th1, f1, ev1, _ = fit_trust_region(lambda t: session.loglik(t, grad=True), start, lb, ub, gtol=gtol, log=log,
-                                       state=st)
+    th1, f1, ev1, _ = fit_trust_region(lambda t: session.loglik(t, grad=True), start, lb, ub, gtol=gtol, ftol=ftol,
+                                       log=log, state=st)
     if log:
-        log("sliced stage: %d evaluations, theta %s, loglik %.12g" % (ev1, list(th1), f1))
+        log("sliced gradient stage: %d evaluations, theta %s, loglik %.12g" % (ev1, list(th1), f1))
+    th, f, ne2 = ridge_polish(lambda t: session.loglik(t), th1, st["B"], lb, ub)
+    if log:
+        log("sliced ridge search: %d evaluations, theta %s, loglik %.12g" % (ne2, list(th), f))
     session.set_fp64()
-    if polish_iter <= 0:
-        return th1, f1, ev1, 0, th1
-    th, f, ev2, _ = fit_trust_region(lambda t: session.loglik(t, grad=True), th1, lb, ub, max_iter=polish_iter,
-                                     gtol=polish_gtol, delta0=0.05, log=log, state=st)
-    if log:
-        log("FP64 polish: %d evaluations, theta %s, loglik %.12g" % (ev2, list(th), f))
-    return th, f, ev1, ev2, th1
+    return th, f, ev1, ne + ne2, th1
+
+
+def fit_fp64(session, lb, ub, theta0=None, gtol=1e-3, ftol=1e-7, log=None):
+    """The same gradient driver in plain FP64 (start_point with FP64 values,
+    the trust region on the FP64 adjoint gradient).  Returns (theta_hat,
+    loglik, gradient evaluations, log-likelihood-only evaluations)."""
+    session.set_fp64()
+    z = session.z()
+    if theta0 is None:
+        start, ne = start_point(lambda t: session.loglik(t), z, lb, ub)
+    else:
+        start, ne = np.asarray(theta0, dtype=np.float64), 0
+    th, f, ev, _ = fit_trust_region(lambda t: session.loglik(t, grad=True), start, lb, ub, gtol=gtol, ftol=ftol,
+                                    log=log)
+    return th, f, ev, ne

@@ -552,6 +552,11 @@ int exageostat_b200_batch_create(int nfields, const int *n, const double *x, con
  * definite; the call then still returns 0 and exageostat_last_error() says
  * how many failed). */
 int exageostat_b200_batch_loglik(void *handle, const double *theta, double *loglik);
+/* The log-likelihoods and their gradients (nfields rows of 3, or 4 with the
+ * nugget) of every field at theta: the batched factorisation, then the
+ * adjoint of each field on its own tiles.  A field whose covariance is not
+ * positive definite gets loglik -inf and NaN gradient entries. */
+int exageostat_b200_batch_loglik_grad(void *handle, const double *theta, double *loglik, double *grad);
 int exageostat_b200_batch_destroy(void *handle);
 
 /* As exageostat_b200_batch_create with the tile size chosen by timing: the

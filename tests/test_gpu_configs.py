@@ -104,14 +104,25 @@ def test_c4_gradient_matches_oracle_central_differences(gpu, ora):
 
 
 def test_c1_theta_hat_matches_oracle_maximiser(gpu, ora):
+    """The reference's driver (derivative-free from the lower bounds) in FP64,
+    the gradient driver in FP64 and the mixed-precision gradient driver (INT8
+    sliced objective, gradient and ridge search) all land within 1e-3 of the
+    oracle's maximiser."""
+    from exageostat_b200.mle import fit_fp64, fit_mixed
+
     x, y, z, _ = ora.synthetic_field(1600, 0, [1.0, 0.1, 0.5])
     lb, ub = np.full(3, 0.01), np.full(3, 5.0)
     with gpu.Session(x, y, dts=320) as s:
         s.set_data(z=z)
         th_gpu, ll_gpu, _ = s.fit_bobyqa(lb, ub, ftol_abs=1e-9)
+    with gpu.Session(x, y, dts=128) as s:
+        s.set_data(z=z)
+        th_tr, _, _, _ = fit_fp64(s, lb, ub)
+        th_mx, _, _, _, _ = fit_mixed(s, lb, ub)
     th_ora, ll_ora = ora.maximise(x, y, z, lb, ub, [[0.5, 0.5, 0.5], [1.0, 0.1, 0.5]])
     assert ll_ora == pytest.approx(ll_gpu, abs=1e-6)
-    assert np.all(np.abs(th_gpu - th_ora) <= 1e-3 * np.abs(th_ora)), (th_gpu, th_ora)
+    for th in (th_gpu, th_tr, th_mx):
+        assert np.all(np.abs(th - th_ora) <= 1e-3 * np.abs(th_ora)), (th, th_ora)
 
 
 def test_c5_corner_fields_match_oracle(gpu, ora):
