@@ -254,13 +254,13 @@ def finalize() -> None:
 
 
 KERNELS = {0: b"univariate_matern_stationary", 1: b"univariate_matern_nuggets_stationary",
-           2: b"bivariate_matern_parsimonious"}
-NPARAMS = {0: 3, 1: 4, 2: 6}
+           2: b"bivariate_matern_parsimonious", 3: b"bivariate_matern_flexible"}
+NPARAMS = {0: 3, 1: 4, 2: 6, 3: 11}
 
 
 def _dim(x, kernel) -> int:
     """Matrix dimension: the locations, times 2 for the bivariate kernel."""
-    return x.size * (2 if kernel == 2 else 1)
+    return x.size * (2 if kernel in (2, 3) else 1)
 
 
 def bessel_knu(nu, x) -> np.ndarray:

@@ -383,7 +383,8 @@ int xg_small_spd_inverse(int n, const double *A, double *inv)
  * covariance store is overwritten (the next evaluation regenerates it). */
 int xg_field_fisher(XgField *f, const double *theta, int kernel, double *F, double *seconds)
 {
-    if (kernel == 2 || f->kernel == 2) return xg_fail(XG_ERR_UNSUPPORTED, "the Fisher matrix of a bivariate field");
+    if (xg_bivariate(kernel) || xg_bivariate(f->kernel))
+        return xg_fail(XG_ERR_UNSUPPORTED, "the Fisher matrix of a bivariate field");
     int rc = xg_check_theta(theta, kernel);
     if (rc) return rc;
     const int nt = f->C.nt, ts = f->C.ts, N = f->N;

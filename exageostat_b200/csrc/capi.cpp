@@ -45,8 +45,15 @@ static int xg_kernel_of(const MLE_data *data, int *kernel, int *nparams)
         *nparams = 6;
         return XG_OK;
     }
+    if (strcmp(k, "bivariate_matern_flexible") == 0) {
+        /* 11 parameters (examples/examples.c:221-223), N = 2 x the locations */
+        *kernel = 3;
+        *nparams = 11;
+        return XG_OK;
+    }
     return xg_fail(XG_ERR_UNSUPPORTED, "kernel_fun \"%s\" is not supported (univariate_matern_stationary, "
-                                       "univariate_matern_nuggets_stationary and bivariate_matern_parsimonious are)",
+                                       "univariate_matern_nuggets_stationary, bivariate_matern_parsimonious and "
+                                       "bivariate_matern_flexible are)",
                    k);
 }
 
@@ -244,8 +251,8 @@ extern "C" int exageostat_b200_loglik(MLE_data *data, const double *theta, doubl
     const int band = data->diag_thick > 0 ? data->diag_thick : 1;
     if (mixed && grad)
         return xg_fail(XG_ERR_UNSUPPORTED, "the gradient is computed with precision 0 or 3, not 2");
-    if (kernel == 2 && (mixed || grad))
-        return xg_fail(XG_ERR_UNSUPPORTED, "bivariate_matern_parsimonious: precision 0 or 3 without a gradient");
+    if (xg_bivariate(kernel) && (mixed || grad))
+        return xg_fail(XG_ERR_UNSUPPORTED, "bivariate kernels: precision 0 or 3 without a gradient");
     if (mixed && (!f->mx || f->mx->band != band)) {
         rc = xg_field_set_mixed(f, band, f->mx ? f->mx->passes : 3);
         if (rc) return rc;
@@ -364,7 +371,7 @@ extern "C" void EXAGEOSTAT_dmle_Predict_Allocate(MLE_data *data, int nZmiss, int
     }
     if (data->descC22) prediction_finalize(data);
     int kernel = 0, np = 0;
-    if (xg_kernel_of(data, &kernel, &np) == XG_OK && kernel == 2) {
+    if (xg_kernel_of(data, &kernel, &np) == XG_OK && xg_bivariate(kernel)) {
         /* the bivariate matrices have two rows per location (MLE_dexact.c:640-653) */
         nZobs *= 2;
         nZmiss *= 2;
@@ -407,7 +414,7 @@ extern "C" double EXAGEOSTAT_dmle_Predict_Tile(MLE_data *data, double *theta, in
     if (!q || q->nmiss != nZmiss || q->nobs != nZobs) {
         if (q) prediction_finalize(data);
         /* nZmiss / nZobs count matrix rows here; the allocation takes locations */
-        const int p = kernel == 2 ? 2 : 1;
+        const int p = xg_bivariate(kernel) ? 2 : 1;
         EXAGEOSTAT_dmle_Predict_Allocate(data, nZmiss / p, nZobs / p, 0, 1, 1, Zactual != NULL);
         q = (XgPredict *)data->descC22;
         if (!q) return -1;
@@ -430,7 +437,7 @@ extern "C" double EXAGEOSTAT_dmle_Predict_Tile(MLE_data *data, double *theta, in
     }
     data->mserror = mse;
     results.mse_pred = mse;
-    if (kernel == 2) { /* per-variable errors of the bivariate field (MLE_dexact.c:838-847, 859-860) */
+    if (xg_bivariate(kernel)) { /* per-variable errors of the bivariate field (MLE_dexact.c:838-847, 859-860) */
         data->mserror1 = parts[0];
         data->mserror2 = parts[1];
         results.mse_pred1 = parts[0];
@@ -467,7 +474,7 @@ extern "C" double *EXAGEOSTAT_Fisher_Tile(MLE_data *data, int N, double *initial
     (void)p_grid;
     (void)q_grid;
     XgField *f = xg_field_of(data);
-    if (f && f->kernel == 2) {
+    if (f && xg_bivariate(f->kernel)) {
         xg_fail(XG_ERR_UNSUPPORTED, "the Fisher matrix of a bivariate field");
         fprintf(stderr, "EXAGEOSTAT_Fisher_Tile: %s\n", exageostat_last_error());
         return NULL;
@@ -535,7 +542,7 @@ extern "C" void EXAGEOSTAT_dmle_mloe_mmom_Allocate(MLE_data *data, int nZmiss, i
     }
     int kernel = 0, np = 0;
     if (xg_kernel_of(data, &kernel, &np) ||
-        (kernel == 2 && xg_fail(XG_ERR_UNSUPPORTED, "MLOE / MMOM with bivariate_matern_parsimonious"))) {
+        (xg_bivariate(kernel) && xg_fail(XG_ERR_UNSUPPORTED, "MLOE / MMOM with a bivariate kernel"))) {
         fprintf(stderr, "EXAGEOSTAT_dmle_mloe_mmom_Allocate: %s\n", exageostat_last_error());
         return;
     }
@@ -585,7 +592,7 @@ static void xg_mloe_mmom(MLE_data *data, double *truth_theta, double *estimated_
 {
     int kernel = 0, np = 0;
     if (xg_kernel_of(data, &kernel, &np) ||
-        (kernel == 2 && xg_fail(XG_ERR_UNSUPPORTED, "MLOE / MMOM with bivariate_matern_parsimonious"))) {
+        (xg_bivariate(kernel) && xg_fail(XG_ERR_UNSUPPORTED, "MLOE / MMOM with a bivariate kernel"))) {
         fprintf(stderr, "EXAGEOSTAT_dmle_mloe_mmom_Tile: %s\n", exageostat_last_error());
         data->mloe = data->mmom = NAN;
         return;
@@ -678,7 +685,7 @@ extern "C" int exageostat_b200_mloe_mmom_host(int nmiss, const double *xmiss, co
 extern "C" int exageostat_b200_dmle_host(int n, const double *x, const double *y, const double *z,
                                          const double *theta, int kernel, int metric, int ts, double *out)
 {
-    if (kernel < 0 || kernel > 2) return xg_fail(XG_ERR_BAD_ARGUMENT, "kernel %d", kernel);
+    if (kernel < 0 || kernel > 3) return xg_fail(XG_ERR_BAD_ARGUMENT, "kernel %d", kernel);
     XgField *f = nullptr;
     int rc = xg_field_create(&f, n, ts, x, y, kernel, metric);
     if (rc) return rc;
@@ -726,7 +733,7 @@ extern "C" int exageostat_b200_set_sliced(MLE_data *data)
 extern "C" int exageostat_b200_dmle_host_sliced(int n, const double *x, const double *y, const double *z,
                                                 const double *theta, int kernel, int metric, int ts, double *out)
 {
-    if (kernel < 0 || kernel > 2) return xg_fail(XG_ERR_BAD_ARGUMENT, "kernel %d", kernel);
+    if (kernel < 0 || kernel > 3) return xg_fail(XG_ERR_BAD_ARGUMENT, "kernel %d", kernel);
     XgField *f = nullptr;
     int rc = xg_field_create(&f, n, ts, x, y, kernel, metric);
     if (rc) return rc;

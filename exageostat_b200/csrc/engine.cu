@@ -185,6 +185,42 @@ XgMaternParams xg_params(const double *theta, int kernel)
     XgMaternParams p;
     p.bivariate = 0;
     p.sigma2b = p.nu2 = p.con2 = p.nu12 = p.con12 = p.cross0 = 0.0;
+    p.beta2 = p.beta12 = 0.0;
+    if (kernel == 3) {
+        /* theta = (a_1, a_2, ., ., nu_1, nu_2, ., ., ., ., .): the constants of
+         * core_dcmg_bivariate_flexible (core_zcmg.c:1524-1556), in its order;
+         * at zero distance the reference stores theta[0], theta[1] and rho
+         * (:1565-1568) */
+        const double scale1 = theta[0], scale2 = theta[1], nu1 = theta[4], nu2 = theta[5];
+        const double scale12 = pow(0.5 * (pow(scale1, -2) + pow(scale2, -2)) + theta[2] * (1 - theta[3]), -0.5);
+        const double nu12 = 0.5 * (nu1 + nu2) + theta[6] * (1 - theta[7]);
+        const double rho = theta[8] * theta[9] * theta[10] * pow(scale12, 2 * theta[6] + (nu1 + nu2)) *
+                           tgamma(0.5 * (nu1 + nu2) + 1) * tgamma(nu12) / tgamma(nu12 + 1);
+        const double s11 = theta[8] * theta[8] * pow(scale1, 2 * theta[6] + nu1 + nu1) * tgamma(nu1);
+        const double s22 = theta[9] * theta[9] * pow(scale2, 2 * theta[6] + nu2 + nu2) * tgamma(nu2);
+        p.bivariate = 1;
+        p.sigma2 = theta[0];
+        p.sigma2b = theta[1];
+        p.cross0 = rho;
+        p.beta = scale1;
+        p.beta2 = scale2;
+        p.beta12 = scale12;
+        p.nu = nu1;
+        p.nu2 = nu2;
+        p.nu12 = nu12;
+        p.nugget = 0.0;
+        p.half_integer = -1;
+        double con1 = pow(2, (nu1 - 1)) * tgamma(nu1);
+        con1 = 1.0 / con1;
+        p.con = s11 * con1;
+        double con2 = pow(2, (nu2 - 1)) * tgamma(nu2);
+        con2 = 1.0 / con2;
+        p.con2 = s22 * con2;
+        double con12 = pow(2, (nu12 - 1)) * tgamma(nu12);
+        con12 = 1.0 / con12;
+        p.con12 = rho * con12;
+        return p;
+    }
     if (kernel == 2) {
         /* theta = (sigma_1^2, sigma_2^2, beta, nu_1, nu_2, rho): the constants of
          * core_dcmg_bivariate_parsimonious (core_zcmg.c:1637-1651), in its order */
@@ -210,6 +246,7 @@ XgMaternParams xg_params(const double *theta, int kernel)
         con12 = 1.0 / con12;
         p.con12 = rho * sqrt(theta[0] * theta[1]) * con12;
         p.cross0 = rho * sqrt(theta[0] * theta[1]);
+        p.beta2 = p.beta12 = p.beta;
         return p;
     }
     p.sigma2 = theta[0];
@@ -226,6 +263,16 @@ XgMaternParams xg_params(const double *theta, int kernel)
 
 int xg_check_theta(const double *theta, int kernel)
 {
+    if (kernel == 3) {
+        for (int i = 0; i < 11; ++i)
+            if (!isfinite(theta[i])) return xg_fail(XG_ERR_BAD_ARGUMENT, "theta[%d] is not finite", i);
+        const int pos[4] = {0, 1, 4, 5}; /* the two scales and smoothnesses */
+        for (int i : pos)
+            if (!(theta[i] > 0)) return xg_fail(XG_ERR_BAD_ARGUMENT, "theta[%d] = %g must be positive", i, theta[i]);
+        if (theta[4] > 25.0 || theta[5] > 25.0)
+            return xg_fail(XG_ERR_BAD_ARGUMENT, "smoothness above the supported maximum 25");
+        return XG_OK;
+    }
     if (kernel == 2) {
         for (int i = 0; i < 6; ++i)
             if (!isfinite(theta[i])) return xg_fail(XG_ERR_BAD_ARGUMENT, "theta[%d] is not finite", i);
@@ -354,7 +401,7 @@ static void xg_field_collect_profile(XgField *f)
 int xg_field_set_data(XgField *f, const double *x, const double *y, const double *z)
 {
     cudaStream_t st = g_xg.stream;
-    const int nloc = f->kernel == 2 ? f->N / 2 : f->N; /* bivariate: two variables per location */
+    const int nloc = xg_bivariate(f->kernel) ? f->N / 2 : f->N; /* bivariate: two variables per location */
     if (x) XG_CU(cudaMemcpyAsync(f->x, x, nloc * sizeof(double), cudaMemcpyHostToDevice, st));
     if (y) XG_CU(cudaMemcpyAsync(f->y, y, nloc * sizeof(double), cudaMemcpyHostToDevice, st));
     if (z) XG_CU(cudaMemcpyAsync(f->z, z, f->N * sizeof(double), cudaMemcpyHostToDevice, st));
@@ -407,10 +454,10 @@ int xg_field_create(XgField **out, int N, int ts, const double *x, const double 
     if (rc) return rc;
     if (N <= 0) return xg_fail(XG_ERR_BAD_ARGUMENT, "N = %d must be positive", N);
     if (!x || !y) return xg_fail(XG_ERR_BAD_ARGUMENT, "locations are NULL");
-    if (kernel == 2 && (N & 1))
+    if (xg_bivariate(kernel) && (N & 1))
         return xg_fail(XG_ERR_BAD_ARGUMENT, "bivariate kernel: N = %d must be 2 x the number of locations", N);
     /* bivariate: N / 2 locations, two variables each */
-    const int nloc = kernel == 2 ? N / 2 : N;
+    const int nloc = xg_bivariate(kernel) ? N / 2 : N;
     XgField *f = new XgField();
     f->N = N;
     f->kernel = kernel;
@@ -1342,7 +1389,7 @@ int xg_autotune_field(XgField **pf, const double *x, const double *y, const doub
                       int *ts_out, int *band_out, double *report)
 {
     XgField *f = *pf;
-    if (precision == 2 && f->kernel == 2)
+    if (precision == 2 && xg_bivariate(f->kernel))
         return xg_fail(XG_ERR_UNSUPPORTED, "banded mixed precision with bivariate_matern_parsimonious");
     const int N = f->N;
     std::vector<double> z(N);
@@ -1482,13 +1529,13 @@ int xg_predict_run(XgPredict *q, const double *theta, int kernel, int metric, co
 {
     int rc = xg_check_theta(theta, kernel);
     if (rc) return rc;
-    if (kernel == 2 && ((q->nmiss | q->nobs) & 1))
+    if (xg_bivariate(kernel) && ((q->nmiss | q->nobs) & 1))
         return xg_fail(XG_ERR_BAD_ARGUMENT, "bivariate kriging: nZmiss = %d and nZobs = %d must be even (2 x locations)",
                        q->nmiss, q->nobs);
     cudaStream_t st = g_xg.stream;
     const int nmiss = q->nmiss, nobs = q->nobs;
     /* bivariate: nmiss and nobs count matrix rows, two per location */
-    const int lmiss = kernel == 2 ? nmiss / 2 : nmiss, lobs = kernel == 2 ? nobs / 2 : nobs;
+    const int lmiss = xg_bivariate(kernel) ? nmiss / 2 : nmiss, lobs = xg_bivariate(kernel) ? nobs / 2 : nobs;
     XgTileArgs T{q->C22.d, q->C22.ts, q->C22.nt};
     const XgMaternParams p = xg_params(theta, kernel);
     const size_t Np = (size_t)q->C22.nt * q->C22.ts;

@@ -108,6 +108,10 @@ struct XgPredict {
     int *info() { return status + 1; }
 };
 
+/* kernels whose rows and columns interleave two variables per location:
+ * 2 bivariate parsimonious, 3 bivariate flexible Matern */
+inline bool xg_bivariate(int kernel) { return kernel == 2 || kernel == 3; }
+
 int xg_fail(int code, const char *fmt, ...);
 int xg_context_start(int dts);
 int xg_context_require();

@@ -71,6 +71,10 @@ struct XgMaternParams {
      * (core_zcmg.c:1628-1651) */
     int bivariate;
     double sigma2b, nu2, con2, nu12, con12, cross0;
+    /* scales of variable 1 and of the cross covariance (beta is variable 0's):
+     * all three equal beta for the parsimonious kernel; the flexible kernel
+     * (kernel 3, core_zcmg.c:1514-1580) has one per component */
+    double beta2, beta12;
 };
 
 /* One field of a batch of independent fields sharing one tile store. */

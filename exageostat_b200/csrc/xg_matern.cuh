@@ -41,17 +41,20 @@ __device__ inline double xg_matern_value(double d, const XgMaternParams &p)
     return xg_matern_general(r, p.nu, p.con);
 }
 
-/* Bivariate parsimonious Matern element between variable a of one location
- * and variable b of another (core_dcmg_bivariate_parsimonious,
+/* Bivariate Matern element between variable a of one location and variable
+ * b of another.  Parsimonious (core_dcmg_bivariate_parsimonious,
  * core_zcmg.c:1628-1726): Matern(sigma_a^2, beta, nu_a) on the diagonal
- * blocks, rho sqrt(sigma_1^2 sigma_2^2) Matern(1, beta, nu12) across, and the
- * values at d / beta == 0 exactly as the reference. */
+ * blocks, rho sqrt(sigma_1^2 sigma_2^2) Matern(1, beta, nu12) across.
+ * Flexible (core_dcmg_bivariate_flexible, core_zcmg.c:1514-1580): a scale,
+ * smoothness and constant per component.  The values at d / beta == 0 are the
+ * reference's (sigma2, sigma2b, cross0 as the host set them). */
 __device__ inline double xg_matern_value_biv(double d, const XgMaternParams &p, int a, int b)
 {
     const double r = d / p.beta;
-    if (a != b) return r == 0.0 ? p.cross0 : xg_matern_general(r, p.nu12, p.con12);
-    if (a == 0) return r == 0.0 ? p.sigma2 : xg_matern_general(r, p.nu, p.con);
-    return r == 0.0 ? p.sigma2b : xg_matern_general(r, p.nu2, p.con2);
+    if (r == 0.0) return a != b ? p.cross0 : (a == 0 ? p.sigma2 : p.sigma2b);
+    if (a != b) return xg_matern_general(d / p.beta12, p.nu12, p.con12);
+    if (a == 0) return xg_matern_general(r, p.nu, p.con);
+    return xg_matern_general(d / p.beta2, p.nu2, p.con2);
 }
 
 #endif

@@ -133,7 +133,7 @@ def covariance_lower(x, y, theta, kernel=0, metric=0) -> np.ndarray:
     bivariate kernel 2 the matrix is 2 n x 2 n (index 2 l + v)."""
     lib().ora_set_metric(int(metric))
     x, y, th = _f64(x), _f64(y), _f64(theta)
-    N = x.size * (2 if kernel == 2 else 1)
+    N = x.size * (2 if kernel in (2, 3) else 1)
     C = np.zeros((N, N))  # column-major buffer; transposed on return
     lib().ora_gen_lower_dense(_p(C), N, _p(x), _p(y), _p(th), int(kernel))
     return C.T.copy()
@@ -274,7 +274,7 @@ def dpredict(x_miss, y_miss, x_obs, y_obs, z_obs, z_actual, theta, kernel=0, met
     lib().ora_set_metric(int(metric))
     xm, ym, xo, yo, zo, th = (_f64(a) for a in (x_miss, y_miss, x_obs, y_obs, z_obs, theta))
     za = None if z_actual is None else _f64(z_actual)
-    nm = xm.size * (2 if kernel == 2 else 1)  # matrix rows: two per location for the bivariate kernel
+    nm = xm.size * (2 if kernel in (2, 3) else 1)  # matrix rows: two per location for the bivariate kernel
     zmiss = np.empty(nm)
     mse = lib().ora_dpredict(nm, zo.size, _p(xm), _p(ym), _p(xo), _p(yo), _p(zo),
                              None if za is None else _p(za), _p(th), int(kernel), _p(zmiss))
@@ -286,7 +286,7 @@ def synthetic_field(N: int, seed: int, theta, kernel=0, metric=0, locations=None
     e = dlarnv(3, {seed,seed,seed,1}), locations = GenerateXYLoc(N, seed),
     z = L(theta) e."""
     e = dlarnv(seed, N)
-    nloc = N // 2 if kernel == 2 else N  # N = p x locations (synthetic_dmle_test.c:134, 153)
+    nloc = N // 2 if kernel in (2, 3) else N  # N = p x locations (synthetic_dmle_test.c:134, 153)
     x, y = generate_xy_loc(nloc, seed) if locations is None else (_f64(locations[0]), _f64(locations[1]))
     z = dzvg(x, y, theta, e, kernel, metric)
     return x, y, z, e

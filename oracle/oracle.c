@@ -541,11 +541,50 @@ static double ora_matern_con(const double *theta)
     return theta[0] * con;
 }
 
-/* Bivariate parsimonious Matern (kernel 2, theta = (sigma_1^2, sigma_2^2,
- * beta, nu_1, nu_2, rho)): the constants of core_dcmg_bivariate_parsimonious
- * (core_zcmg.c:1637-1651) in its order, c[] = con1, con2, con12, rho, nu12. */
-static void ora_biv_consts(const double *theta, double *c)
+/* Bivariate Matern kernels, rows and columns interleaving the two variables.
+ * Per component (0: variable 1, 1: variable 2, 2: the cross covariance) the
+ * constant con, smoothness nu, scale and the value at zero distance.
+ *   kernel 2, parsimonious, theta = (sigma_1^2, sigma_2^2, beta, nu_1, nu_2,
+ *     rho): core_dcmg_bivariate_parsimonious (core_zcmg.c:1637-1651), one
+ *     scale beta for all three;
+ *   kernel 3, flexible, theta = (a_1, a_2, ., ., nu_1, nu_2, ., ., ., ., .):
+ *     core_dcmg_bivariate_flexible (core_zcmg.c:1524-1556), a scale per
+ *     component.  At zero distance the reference stores theta[0], theta[1] and
+ *     rho (:1565-1568) -- the scales, not the variances sigma_11, sigma_22 that
+ *     the Matern terms tend to -- and this restatement keeps that. */
+typedef struct {
+    double con[3], nu[3], scale[3], zero[3];
+} ora_biv_t;
+
+static void ora_biv_consts(const double *theta, int kernel, ora_biv_t *c)
 {
+    if (kernel == 3) {
+        const double scale1 = theta[0], scale2 = theta[1], nu1 = theta[4], nu2 = theta[5];
+        const double scale12 = pow(0.5 * (pow(scale1, -2) + pow(scale2, -2)) + theta[2] * (1 - theta[3]), -0.5);
+        const double nu12 = 0.5 * (nu1 + nu2) + theta[6] * (1 - theta[7]);
+        const double rho = theta[8] * theta[9] * theta[10] * pow(scale12, 2 * theta[6] + (nu1 + nu2)) *
+                           tgamma(0.5 * (nu1 + nu2) + 1) * tgamma(nu12) / tgamma(nu12 + 1);
+        const double s11 = theta[8] * theta[8] * pow(scale1, 2 * theta[6] + nu1 + nu1) * tgamma(nu1);
+        const double s22 = theta[9] * theta[9] * pow(scale2, 2 * theta[6] + nu2 + nu2) * tgamma(nu2);
+        double con1 = pow(2, (nu1 - 1)) * tgamma(nu1);
+        con1 = 1.0 / con1;
+        con1 = s11 * con1;
+        double con2 = pow(2, (nu2 - 1)) * tgamma(nu2);
+        con2 = 1.0 / con2;
+        con2 = s22 * con2;
+        double con12 = pow(2, (nu12 - 1)) * tgamma(nu12);
+        con12 = 1.0 / con12;
+        con12 = rho * con12;
+        const double con[3] = {con1, con2, con12}, nu[3] = {nu1, nu2, nu12};
+        const double sc[3] = {scale1, scale2, scale12}, zero[3] = {theta[0], theta[1], rho};
+        for (int t = 0; t < 3; ++t) {
+            c->con[t] = con[t];
+            c->nu[t] = nu[t];
+            c->scale[t] = sc[t];
+            c->zero[t] = zero[t];
+        }
+        return;
+    }
     double con1 = pow(2, (theta[3] - 1)) * tgamma(theta[3]);
     con1 = 1.0 / con1;
     con1 = theta[0] * con1;
@@ -559,26 +598,26 @@ static void ora_biv_consts(const double *theta, double *c)
     double con12 = pow(2, (nu12 - 1)) * tgamma(nu12);
     con12 = 1.0 / con12;
     con12 = rho * sqrt(theta[0] * theta[1]) * con12;
-    c[0] = con1;
-    c[1] = con2;
-    c[2] = con12;
-    c[3] = rho;
-    c[4] = nu12;
+    const double con[3] = {con1, con2, con12}, nu[3] = {theta[3], theta[4], nu12};
+    const double zero[3] = {theta[0], theta[1], rho * sqrt(theta[0] * theta[1])};
+    for (int t = 0; t < 3; ++t) {
+        c->con[t] = con[t];
+        c->nu[t] = nu[t];
+        c->scale[t] = theta[2];
+        c->zero[t] = zero[t];
+    }
 }
 
 /* Element between variable a of (x1, y1) and variable b of (x2, y2)
- * (core_zcmg.c:1656-1671: the 2 x 2 block of one location pair). */
-static inline double ora_biv_elem(double x1, double y1, double x2, double y2, int a, int b, const double *theta,
-                                  const double *c)
+ * (core_zcmg.c:1656-1671 and :1561-1576: the 2 x 2 block of one location
+ * pair; the zero-distance test is on the first component's scaled distance). */
+static inline double ora_biv_elem(double x1, double y1, double x2, double y2, int a, int b, const ora_biv_t *c)
 {
-    const double expr = ora_distance(x1, y1, x2, y2) / theta[2];
-    if (expr == 0) {
-        if (a != b) return c[3] * sqrt(theta[0] * theta[1]);
-        return a == 0 ? theta[0] : theta[1];
-    }
-    if (a != b) return c[2] * pow(expr, c[4]) * ora_bessel_knu(c[4], expr);
-    if (a == 0) return c[0] * pow(expr, theta[3]) * ora_bessel_knu(theta[3], expr);
-    return c[1] * pow(expr, theta[4]) * ora_bessel_knu(theta[4], expr);
+    const double d = ora_distance(x1, y1, x2, y2);
+    const int t = a != b ? 2 : a;
+    if (d / c->scale[0] == 0) return c->zero[t];
+    const double expr = d / c->scale[t];
+    return c->con[t] * pow(expr, c->nu[t]) * ora_bessel_knu(c->nu[t], expr);
 }
 
 /* core_dcmg: A (column-major, lda = m) = Sigma(l1[m0:m0+m], l2[n0:n0+n]).
@@ -587,15 +626,15 @@ static inline double ora_biv_elem(double x1, double y1, double x2, double y2, in
 void ora_core_dcmg(double *A, int m, int n, int m0, int n0, const double *x1, const double *y1, const double *x2,
                    const double *y2, const double *theta, int kernel)
 {
-    if (kernel == 2) {
-        double c[5];
-        ora_biv_consts(theta, c);
+    if (kernel == 2 || kernel == 3) {
+        ora_biv_t c;
+        ora_biv_consts(theta, kernel, &c);
 #pragma omp parallel for schedule(static)
         for (int j = 0; j < n; ++j)
             for (int i = 0; i < m; ++i) {
                 const int gi = m0 + i, gj = n0 + j;
                 A[i + (size_t)j * m] = ora_biv_elem(x1[gi / 2], y1[gi / 2], x2[gj / 2], y2[gj / 2], gi % 2, gj % 2,
-                                                    theta, c);
+                                                    &c);
             }
         return;
     }
@@ -675,13 +714,13 @@ void ora_dcmg_deriv(double *A, int m, int n, int m0, int n0, const double *x1, c
  * (codelet_zcmg.c:316-342); LAPACK dpotrf reads only the lower triangle. */
 static void ora_gen_lower(double *C, int N, const double *x, const double *y, const double *theta, int kernel)
 {
-    if (kernel == 2) {
-        double c[5];
-        ora_biv_consts(theta, c);
+    if (kernel == 2 || kernel == 3) {
+        ora_biv_t c;
+        ora_biv_consts(theta, kernel, &c);
 #pragma omp parallel for schedule(dynamic, 16)
         for (int j = 0; j < N; ++j)
             for (int i = j; i < N; ++i)
-                C[i + (size_t)j * N] = ora_biv_elem(x[i / 2], y[i / 2], x[j / 2], y[j / 2], i % 2, j % 2, theta, c);
+                C[i + (size_t)j * N] = ora_biv_elem(x[i / 2], y[i / 2], x[j / 2], y[j / 2], i % 2, j % 2, &c);
         return;
     }
     const double con = ora_matern_con(theta);

@@ -11,6 +11,7 @@ Functions (reference file:line):
   core_dcmg, calculateDistance, distanceEarth  exageostat_exact/cpu_core/compute/core_zcmg.c:30-92, 963-994
   core_dcmg_nuggets  exageostat_exact/cpu_core/compute/core_zcmg_nuggets.c:107-156
   core_dcmg_bivariate_parsimonious  exageostat_exact/cpu_core/compute/core_zcmg.c:1628-1726
+  core_dcmg_bivariate_flexible  exageostat_exact/cpu_core/compute/core_zcmg.c:1514-1580
   core_dcmg_matern_dsigma_square, _dbeta, _dnu  exageostat_exact/cpu_core/compute/core_zcmg.c:315-488
   core_dmdet  exageostat_exact/cpu_core/compute/core_zmdet.c:50-59
 K_nu inside the Matern kernels is the oracle's (GSL is absent; see
@@ -64,7 +65,7 @@ def lib():
         L.uniform_distribution.argtypes = [_D, _D]
         L.ref_pick_random_points.restype = None
         L.ref_pick_random_points.argtypes = [_I, _PD, _PD, _PD, _I] + [_PD] * 6
-        for name in ("core_dcmg", "core_dcmg_nuggets", "core_dcmg_bivariate_parsimonious",
+        for name in ("core_dcmg", "core_dcmg_nuggets", "core_dcmg_bivariate_parsimonious", "core_dcmg_bivariate_flexible",
                      "core_dcmg_matern_dsigma_square", "core_dcmg_matern_dbeta", "core_dcmg_matern_dnu"):
             f = getattr(L, name)
             f.restype = None
@@ -112,9 +113,11 @@ def _loc(x, y):
 def cmg(kernel: str, m, n, m0, n0, x1, y1, x2, y2, theta, metric=0) -> np.ndarray:
     """One tile of a reference generator, column-major m x n (A[i + j m]),
     returned as an (m, n) array.  kernel: "matern", "nuggets",
-    "bivariate_parsimonious", "dsigma_square", "dbeta", "dnu"."""
+    "bivariate_parsimonious", "bivariate_flexible", "dsigma_square", "dbeta",
+    "dnu"."""
     name = {"matern": "core_dcmg", "nuggets": "core_dcmg_nuggets",
             "bivariate_parsimonious": "core_dcmg_bivariate_parsimonious",
+            "bivariate_flexible": "core_dcmg_bivariate_flexible",
             "dsigma_square": "core_dcmg_matern_dsigma_square", "dbeta": "core_dcmg_matern_dbeta",
             "dnu": "core_dcmg_matern_dnu"}[kernel]
     l1, keep1 = _loc(x1, y1)

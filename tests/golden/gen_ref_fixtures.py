@@ -15,7 +15,8 @@ GenerateXYLoc's 2 N draws, then locations_obs_zsort_inplace :453-534) with z
 
 ref_fixtures.npz: 24 x 24 covariance tiles of core_dcmg (core_zcmg.c:963-994),
 core_dcmg_nuggets (core_zcmg_nuggets.c:107-156),
-core_dcmg_bivariate_parsimonious (core_zcmg.c:1628-1726), the great-circle
+core_dcmg_bivariate_parsimonious (core_zcmg.c:1628-1726),
+core_dcmg_bivariate_flexible (core_zcmg.c:1514-1580), the great-circle
 metric (distanceEarth, core_zcmg.c:51-60) and the derivative tiles
 core_dcmg_matern_dsigma_square / _dbeta / _dnu (core_zcmg.c:315-488) on the
 GenerateXYLoc(1600, 0) locations, and core_dmdet (core_zmdet.c:50-59) of a
@@ -48,6 +49,7 @@ COV_CASES = [
     ("matern_edge", "matern", [0.7, 4.9, 0.011], 0),
     ("nuggets", "nuggets", [1.0, 0.1, 1.0, 0.01], 0),
     ("bivariate", "bivariate_parsimonious", [1.0, 1.5, 0.1, 0.5, 1.2, 0.3], 0),
+    ("bivariate_flexible", "bivariate_flexible", [0.1, 0.15, 0.5, 0.5, 0.8, 1.2, 0.3, 0.5, 1.0, 1.1, 0.3], 0),
     ("great_circle", "matern", [1.0, 150.0, 0.73], 1),
     ("dsigma_square", "dsigma_square", [1.0, 0.1, 0.73], 0),
     ("dbeta", "dbeta", [1.0, 0.1, 0.73], 0),

@@ -109,3 +109,33 @@ def test_bivariate_holdout_and_kriging(gpu, ora):
     assert mse == pytest.approx(mse_ref, rel=1e-9)
     assert m1 == pytest.approx(np.mean((zact[0::2] - zm_ref[0::2]) ** 2), rel=1e-9)
     assert m2 == pytest.approx(np.mean((zact[1::2] - zm_ref[1::2]) ** 2), rel=1e-9)
+
+
+# kernel_fun = "bivariate_matern_flexible" (core_zcmg.c:1514-1580), 11
+# parameters; theta[8], theta[9] chosen so that the Matern terms tend to
+# theta[0], theta[1] at zero distance (the reference stores those there), which
+# keeps these covariances positive definite
+FLEX = [
+    [0.1, 0.15, 0.5, 0.5, 0.8, 1.2, 0.3, 0.5, 3.68961, 6.95741, 0.3],
+    [0.08, 0.12, 1.0, 0.2, 0.5, 1.0, 0.2, 0.8, 1.24479, 4.41137, -0.4],
+]
+
+
+@pytest.mark.parametrize("theta", FLEX)
+def test_flexible_bivariate_covariance_loglik_and_workflow(gpu, ora, theta):
+    nloc = 700
+    N = 2 * nloc
+    x, y, z_ref, e = ora.synthetic_field(N, 8, theta, kernel=3)
+    C = gpu.covariance_dense(x[:200], y[:200], theta, kernel=3, ts=128)
+    Co = np.tril(ora.covariance_full(x[:200], y[:200], theta, kernel=3))
+    assert np.abs(C - Co).max() < 1e-13 * np.abs(Co).max()
+    ref = ora.dmle(x, y, z_ref, theta, kernel=3)[0]
+    assert gpu.dmle_host(x, y, z_ref, theta, kernel=3, ts=256)[0] == pytest.approx(ref, rel=1e-10)
+    with gpu.Session(x, y, kernel=3, dts=128) as s:
+        assert s.N == N and s.nparams == 11
+        s.zvg(theta, e)
+        z = s.z()
+        assert np.abs(z - z_ref).max() < 1e-10 * np.abs(z_ref).max()
+        assert s.mle_alg(theta) == pytest.approx(ref, rel=1e-10)
+        s.set_sliced()
+        assert abs(s.mle_alg(theta) - ref) / abs(ref) < 1e-7

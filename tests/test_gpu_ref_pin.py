@@ -1,7 +1,7 @@
 """The GPU path against fixtures written by the reference's own C code
 (tests/golden/gen_ref_fixtures.py, from sources compiled unchanged into
 oracle/_ref): covariance tiles of the Matern, nugget, bivariate
-parsimonious and great-circle generators within 1e-13 relative (the device
+parsimonious and flexible, and great-circle generators within 1e-13 relative (the device
 has its own K_nu, pinned to mpmath to 1e-14), and the library's hold-out
 split (pick_random_points on the device's z) bit for bit."""
 import hashlib
@@ -14,7 +14,7 @@ import pytest
 pytestmark = pytest.mark.gpu
 
 GOLD = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden")
-KERNELS = {"matern": 0, "nuggets": 1, "bivariate_parsimonious": 2}
+KERNELS = {"matern": 0, "nuggets": 1, "bivariate_parsimonious": 2, "bivariate_flexible": 3}
 
 
 def _sha(a) -> str:

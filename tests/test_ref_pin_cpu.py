@@ -69,8 +69,8 @@ def test_oracle_hold_out_split_is_the_reference_bits(ora, meta):
 def _oracle_tile(ora, kern, theta, metric, m0, n0, x, y, t):
     if metric:
         x, y = _latlon(x, y)
-    if kern in ("matern", "nuggets", "bivariate_parsimonious"):
-        kernel = {"matern": 0, "nuggets": 1, "bivariate_parsimonious": 2}[kern]
+    if kern in ("matern", "nuggets", "bivariate_parsimonious", "bivariate_flexible"):
+        kernel = {"matern": 0, "nuggets": 1, "bivariate_parsimonious": 2, "bivariate_flexible": 3}[kern]
         return ora.core_dcmg(t, t, m0, n0, x, y, x, y, theta, kernel, metric)
     which = {"dsigma_square": 0, "dbeta": 1, "dnu": 2}[kern]
     return ora.dcmg_deriv(t, t, m0, n0, x, y, x, y, theta, which, metric)
