@@ -596,6 +596,25 @@ def mode_batch(args):
     t0 = time.perf_counter()
     loop = np.array([xg.dmle_host(x, y, z, t, ts=256)[0] for x, y, z, t in zip(xs, ys, zs, th)])
     tl = time.perf_counter() - t0
+    # single fields of the workload's sizes: plain FP64 vs INT8-sliced (CUDA events of the library)
+    per_field = []
+    for n in (1000, 3000, 6000):
+        i = int(np.argmin([abs(len(x) - n) for x in xs]))
+        row = {"n": len(xs[i])}
+        with xg.Session(xs[i], ys[i], dts=256) as s:
+            s.set_data(z=zs[i])
+            for name in ("fp64", "sliced"):
+                if name == "sliced":
+                    s.set_sliced()
+                for _ in range(2):
+                    s.loglik(th[i])
+                s.set_profiling(True)
+                for _ in range(5):
+                    s.loglik(th[i])
+                p = s.profile()
+                s.set_profiling(False)
+                row[name + "_seconds"] = p["t_total"] / p["evals"]
+        per_field.append(row)
     ok = np.isfinite(loop) & np.isfinite(out)
     err = float(np.max(np.abs(loop[ok] - out[ok]) / np.abs(loop[ok])))
     sizes = np.array([len(x) for x in xs])
@@ -606,6 +625,7 @@ def mode_batch(args):
                       "batched_grad_seconds": tbg, "looped_seconds": tl,
                       "fields_per_s_looped": args.fields / tl, "speedup": tl / tb,
                       "fields_not_spd": int(np.sum(~np.isfinite(out))),
+                      "single_field_sliced_vs_fp64": per_field,
                       "max_rel_diff_batched_vs_looped": err}), flush=True)
 
 
