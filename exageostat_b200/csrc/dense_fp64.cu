@@ -375,41 +375,42 @@ __global__ void __launch_bounds__(32) xg_diag_inv_kernel(XgTileArgs T, int k, co
 #define XG_TRSM_THREADS 512
 #define XG_TRSM_SR 32 /* rows of A_ik per CTA */
 
-template <bool COH = false>
-__device__ __forceinline__ void xg_trsm_body(const XgTileArgs &T, int k, double *__restrict__ v, int with_rhs,
-                                             const int *status, long long bid)
+/* One 32-row strip B (leading dimension ld, w columns) <- B L^-T for the
+ * lower-triangular w x w block L (same leading dimension), 32 columns at a
+ * time: with dinv (the inverted 32 x 32 diagonal blocks of L, [(cb + r) * 32
+ * + c]) each diagonal solve is a DMMA product, without it a serial
+ * substitution; the rest of each step is a DMMA update.  With vk != nullptr
+ * also vi[0:32] -= B_new vk[0:w].  Called by every CTA thread after the status
+ * check. */
+template <bool COH>
+__device__ __forceinline__ void xg_trsm_core(double *B, const double *L, int ld, int w, const double *dinv,
+                                             const double *vk, double *vi)
 {
-    const int ts = T.ts, LDS = ts + 4;
+    const int LDS = w + 4;
     extern __shared__ __align__(16) double xg_smem_d[];
-    double *S = xg_smem_d;                  /* [SR][LDS] */
-    double *LD = S + XG_TRSM_SR * LDS;      /* [32][33] */
-    if (xg_cta_should_skip(status)) return;
-    const int strips = ts / XG_TRSM_SR;
-    const int i = k + 1 + (int)(bid / strips);
-    const int strip = (int)(bid % strips);
+    double *S = xg_smem_d;             /* [SR][LDS] */
+    double *LD = S + XG_TRSM_SR * LDS; /* [32][33] */
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     const int g = lane >> 2, tq = lane & 3;
-    double *B = T.data + xg_slot64(T, i, k) * (long long)ts * ts + (long long)strip * XG_TRSM_SR * ts;
-    const double *L = T.data + xg_slot64(T, k, k) * (long long)ts * ts;
-    for (int idx = tid; idx < XG_TRSM_SR * ts; idx += blockDim.x) {
-        const int r = idx / ts, c = idx - r * ts;
-        S[r * LDS + c] = xg_ldt<COH>(B + (long long)r * ts + c);
+    for (int idx = tid; idx < XG_TRSM_SR * w; idx += blockDim.x) {
+        const int r = idx / w, c = idx - r * w;
+        S[r * LDS + c] = xg_ldt<COH>(B + (long long)r * ld + c);
     }
-    for (int cb = 0; cb < ts; cb += 32) {
-        if (T.dinv) {
+    for (int cb = 0; cb < w; cb += 32) {
+        if (dinv) {
             /* the inverse D of this 32 x 32 diagonal block (xg_diag_inv_kernel) */
             for (int idx = tid; idx < 32 * 32; idx += blockDim.x) {
                 const int r = idx >> 5, c = idx & 31;
-                LD[r * 33 + c] = xg_ldt<COH>(T.dinv + (cb + r) * 32 + c);
+                LD[r * 33 + c] = xg_ldt<COH>(dinv + (cb + r) * 32 + c);
             }
         } else {
             for (int idx = tid; idx < 32 * 32; idx += blockDim.x) {
                 const int r = idx >> 5, c = idx & 31;
-                LD[r * 33 + c] = xg_ldt<COH>(L + (long long)(cb + r) * ts + cb + c);
+                LD[r * 33 + c] = xg_ldt<COH>(L + (long long)(cb + r) * ld + cb + c);
             }
         }
         __syncthreads();
-        if (T.dinv) {
+        if (dinv) {
             /* S[:, cb:cb+32] <- S[:, cb:cb+32] D^T on DMMA: warp w < 4 computes
              * the 32 x 8 column block w (both 16-row halves); the results are
              * written after every warp has read its operands */
@@ -456,7 +457,7 @@ __device__ __forceinline__ void xg_trsm_body(const XgTileArgs &T, int k, double 
         }
         __syncthreads();
         /* S[:, cb+32:] -= S[:, cb:cb+32] L[cb+32:, cb:cb+32]^T, 32-column groups */
-        const int ncol = ts - cb - 32;
+        const int ncol = w - cb - 32;
         const int ngrp = ncol / 32;
         for (int grp = warp; grp < ngrp; grp += (int)(blockDim.x >> 5)) {
             const int c0 = cb + 32 + grp * 32;
@@ -476,7 +477,7 @@ __device__ __forceinline__ void xg_trsm_body(const XgTileArgs &T, int k, double 
                     a[mi][1] = S[(mi * 16 + g + 8) * LDS + cb + p0 + tq];
                 }
 #pragma unroll
-                for (int ni = 0; ni < 4; ++ni) b[ni] = xg_ldro<COH>(L + (long long)(c0 + ni * 8 + g) * ts + cb + p0 + tq);
+                for (int ni = 0; ni < 4; ++ni) b[ni] = xg_ldro<COH>(L + (long long)(c0 + ni * 8 + g) * ld + cb + p0 + tq);
 #pragma unroll
                 for (int mi = 0; mi < 2; ++mi)
 #pragma unroll
@@ -497,20 +498,33 @@ __device__ __forceinline__ void xg_trsm_body(const XgTileArgs &T, int k, double 
         }
         __syncthreads();
     }
-    for (int idx = tid; idx < XG_TRSM_SR * ts; idx += blockDim.x) {
-        const int r = idx / ts, c = idx - r * ts;
-        B[(long long)r * ts + c] = S[r * LDS + c];
+    for (int idx = tid; idx < XG_TRSM_SR * w; idx += blockDim.x) {
+        const int r = idx / w, c = idx - r * w;
+        B[(long long)r * ld + c] = S[r * LDS + c];
     }
-    if (with_rhs) {
-        const double *vk = v + (long long)k * ts;
-        double *vi = v + (long long)i * ts + strip * XG_TRSM_SR;
+    if (vk) {
         for (int r = warp; r < XG_TRSM_SR; r += (int)(blockDim.x >> 5)) {
             double s = 0.0;
-            for (int c = lane; c < ts; c += 32) s += S[r * LDS + c] * xg_ldt<COH>(vk + c);
+            for (int c = lane; c < w; c += 32) s += S[r * LDS + c] * xg_ldt<COH>(vk + c);
             for (int off = 16; off > 0; off >>= 1) s += __shfl_xor_sync(0xffffffffu, s, off);
             if (lane == 0) vi[r] = xg_ldt<COH>(vi + r) - s;
         }
     }
+}
+
+template <bool COH = false>
+__device__ __forceinline__ void xg_trsm_body(const XgTileArgs &T, int k, double *__restrict__ v, int with_rhs,
+                                             const int *status, long long bid)
+{
+    const int ts = T.ts;
+    if (xg_cta_should_skip(status)) return;
+    const int strips = ts / XG_TRSM_SR;
+    const int i = k + 1 + (int)(bid / strips);
+    const int strip = (int)(bid % strips);
+    double *B = T.data + xg_slot64(T, i, k) * (long long)ts * ts + (long long)strip * XG_TRSM_SR * ts;
+    const double *L = T.data + xg_slot64(T, k, k) * (long long)ts * ts;
+    xg_trsm_core<COH>(B, L, ts, ts, T.dinv, with_rhs ? v + (long long)k * ts : nullptr,
+                      with_rhs ? v + (long long)i * ts + strip * XG_TRSM_SR : nullptr);
 }
 
 __global__ void __launch_bounds__(XG_TRSM_THREADS) xg_trsm_panel_kernel(XgTileArgs T, int k, double *__restrict__ v,
@@ -551,38 +565,18 @@ __global__ void __launch_bounds__(XG_TRSM_THREADS) xg_trsm_panel_batch_kernel(Xg
 /* Updates the tiles (i, j), j0 <= j <= i < nt, with panel column k.  With
  * single_col the launch covers column j0 only (the lookahead split: the next
  * panel's column first, the rest of the trailing matrix in a second launch). */
-template <bool COH = false>
-__device__ __forceinline__ void xg_gemm_body(const CUtensorMap &map, const XgTileArgs &T, int k, int j0,
-                                             int single_col, int *status, long long bid)
+/* One 128 x 128 block C -= A B^T on DMMA: A and B are 128-row boxes of the
+ * TMA tensor `map` starting at rows rowA and rowB, K runs over KT 16-wide
+ * slabs from column kx0 (a multiple of 16), C has leading dimension ldc.
+ * Called by every CTA thread; the caller has done the status check. */
+template <bool COH>
+__device__ __forceinline__ void xg_gemm_core(const CUtensorMap &map, int rowA, int rowB, int kx0, int KT,
+                                             double *C, int ldc, int *status)
 {
     extern __shared__ __align__(1024) unsigned char xg_smem_raw[];
     unsigned char *smem = (unsigned char *)(((uintptr_t)xg_smem_raw + 1023) & ~(uintptr_t)1023);
     uint64_t *full = (uint64_t *)(smem + XG_G_STAGES * XG_G_STAGE_BYTES);
     uint64_t *empty = full + XG_G_STAGES;
-    const int ts = T.ts;
-    const int bpt = ts / XG_G_BM; /* blocks per tile side */
-    const long long pair = bid / (bpt * bpt);
-    const int blk = (int)(bid % (bpt * bpt));
-    const int bi = blk / bpt, bj = blk % bpt;
-    int i, j;
-    const int nb = T.band ? T.band : T.band_targets;
-    if (nb) {
-        /* band targets (i, j), 0 <= i - j < nb, j from j0 */
-        j = j0 + (int)(pair / nb);
-        i = j + (int)(pair % nb);
-        if (single_col && j != j0) i = T.nt; /* outside the launch */
-    } else {
-        int ii, jj;
-        if (single_col) {
-            ii = (int)pair;
-            jj = 0;
-        } else {
-            xg_pair_decode(pair, &ii, &jj);
-        }
-        i = j0 + ii;
-        j = j0 + jj;
-    }
-    if (xg_cta_should_skip(status, (i == j && bj > bi) || i >= T.nt)) return;
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     if (tid == 0) {
         for (int s = 0; s < XG_G_STAGES; ++s) {
@@ -592,12 +586,6 @@ __device__ __forceinline__ void xg_gemm_body(const CUtensorMap &map, const XgTil
         xg_fence_barrier_init();
     }
     __syncthreads();
-    const int KT = ts / XG_G_BK;
-    /* operands: packed tiles (i, k), (j, k), or rows of the FP64 panel copy in mixed mode */
-    const int rowA = T.band ? i * ts + bi * XG_G_BM
-                            : (int)((T.tile_off + xg_tile_index(i, k, T.nt)) * ts + bi * XG_G_BM);
-    const int rowB = T.band ? j * ts + bj * XG_G_BM
-                            : (int)((T.tile_off + xg_tile_index(j, k, T.nt)) * ts + bj * XG_G_BM);
     int issued = 0;
     __shared__ int s_gfail;
     if (COH) {
@@ -615,13 +603,12 @@ __device__ __forceinline__ void xg_gemm_body(const CUtensorMap &map, const XgTil
         for (; issued < XG_G_STAGES && issued < KT; ++issued) {
             unsigned char *sa = smem + issued * XG_G_STAGE_BYTES;
             xg_mbar_arrive_expect_tx(&full[issued], XG_G_STAGE_BYTES);
-            xg_tma_load_2d(sa, &map, issued * XG_G_BK, rowA, &full[issued]);
-            xg_tma_load_2d(sa + XG_G_BM * XG_G_BK * 8, &map, issued * XG_G_BK, rowB, &full[issued]);
+            xg_tma_load_2d(sa, &map, kx0 + issued * XG_G_BK, rowA, &full[issued]);
+            xg_tma_load_2d(sa + XG_G_BM * XG_G_BK * 8, &map, kx0 + issued * XG_G_BK, rowB, &full[issued]);
         }
     }
     const int wm = warp >> 2, wn = warp & 3;
     const int g = lane >> 2, tq = lane & 3;
-    double *C = T.data + xg_slot64(T, i, j) * (long long)ts * ts + (long long)(bi * XG_G_BM) * ts + bj * XG_G_BM;
     /* accumulators start at -C (loaded while the TMA ring fills), the main
      * loop adds L_ik L_jk^T and the epilogue stores -acc = C - L_ik L_jk^T */
     double acc[4][4][4];
@@ -633,7 +620,7 @@ __device__ __forceinline__ void xg_gemm_body(const CUtensorMap &map, const XgTil
             for (int h = 0; h < 2; ++h) {
                 const int r = wm * 64 + mi * 16 + g + 8 * h;
                 const int c = wn * 32 + ni * 8 + 2 * tq;
-                const double2 cv = xg_ldt2<COH>(reinterpret_cast<const double2 *>(C + (long long)r * ts + c));
+                const double2 cv = xg_ldt2<COH>(reinterpret_cast<const double2 *>(C + (long long)r * ldc + c));
                 acc[mi][ni][2 * h] = -cv.x;
                 acc[mi][ni][2 * h + 1] = -cv.y;
             }
@@ -688,8 +675,8 @@ __device__ __forceinline__ void xg_gemm_body(const CUtensorMap &map, const XgTil
             if (xg_mbar_wait(&empty[s], (kb / XG_G_STAGES) & 1)) {
                 unsigned char *sa = smem + s * XG_G_STAGE_BYTES;
                 xg_mbar_arrive_expect_tx(&full[s], XG_G_STAGE_BYTES);
-                xg_tma_load_2d(sa, &map, issued * XG_G_BK, rowA, &full[s]);
-                xg_tma_load_2d(sa + XG_G_BM * XG_G_BK * 8, &map, issued * XG_G_BK, rowB, &full[s]);
+                xg_tma_load_2d(sa, &map, kx0 + issued * XG_G_BK, rowA, &full[s]);
+                xg_tma_load_2d(sa + XG_G_BM * XG_G_BK * 8, &map, kx0 + issued * XG_G_BK, rowB, &full[s]);
                 ++issued;
             } else {
                 ok = false;
@@ -721,9 +708,46 @@ __device__ __forceinline__ void xg_gemm_body(const CUtensorMap &map, const XgTil
             for (int h = 0; h < 2; ++h) {
                 const int r = wm * 64 + mi * 16 + g + 8 * h;
                 const int c = wn * 32 + ni * 8 + 2 * tq;
-                *reinterpret_cast<double2 *>(C + (long long)r * ts + c) =
+                *reinterpret_cast<double2 *>(C + (long long)r * ldc + c) =
                     make_double2(-acc[mi][ni][2 * h], -acc[mi][ni][2 * h + 1]);
             }
+}
+
+template <bool COH = false>
+__device__ __forceinline__ void xg_gemm_body(const CUtensorMap &map, const XgTileArgs &T, int k, int j0,
+                                             int single_col, int *status, long long bid)
+{
+    const int ts = T.ts;
+    const int bpt = ts / XG_G_BM; /* blocks per tile side */
+    const long long pair = bid / (bpt * bpt);
+    const int blk = (int)(bid % (bpt * bpt));
+    const int bi = blk / bpt, bj = blk % bpt;
+    int i, j;
+    const int nb = T.band ? T.band : T.band_targets;
+    if (nb) {
+        /* band targets (i, j), 0 <= i - j < nb, j from j0 */
+        j = j0 + (int)(pair / nb);
+        i = j + (int)(pair % nb);
+        if (single_col && j != j0) i = T.nt; /* outside the launch */
+    } else {
+        int ii, jj;
+        if (single_col) {
+            ii = (int)pair;
+            jj = 0;
+        } else {
+            xg_pair_decode(pair, &ii, &jj);
+        }
+        i = j0 + ii;
+        j = j0 + jj;
+    }
+    if (xg_cta_should_skip(status, (i == j && bj > bi) || i >= T.nt)) return;
+    /* operands: packed tiles (i, k), (j, k), or rows of the FP64 panel copy in mixed mode */
+    const int rowA = T.band ? i * ts + bi * XG_G_BM
+                            : (int)((T.tile_off + xg_tile_index(i, k, T.nt)) * ts + bi * XG_G_BM);
+    const int rowB = T.band ? j * ts + bj * XG_G_BM
+                            : (int)((T.tile_off + xg_tile_index(j, k, T.nt)) * ts + bj * XG_G_BM);
+    double *C = T.data + xg_slot64(T, i, j) * (long long)ts * ts + (long long)(bi * XG_G_BM) * ts + bj * XG_G_BM;
+    xg_gemm_core<COH>(map, rowA, rowB, 0, ts / XG_G_BK, C, ts, status);
 }
 
 __global__ void __launch_bounds__(XG_G_THREADS, 1) xg_syrk_gemm_kernel(const __grid_constant__ CUtensorMap map,

@@ -612,6 +612,17 @@ double xg_digamma(double x)
     return r + log(x) - 0.5 / x - series;
 }
 
+/* Without a nugget the Matern covariance is linear in sigma^2
+ * (Sigma = sigma^2 R(beta, nu)), so dSigma/dsigma^2 = Sigma / sigma^2 and
+ *   dl/dsigma^2 = (z^T Sigma^-1 z - N) / (2 sigma^2)
+ * exactly, from the quadratic form of the evaluation itself; that component
+ * replaces the contraction's (on the INT8-sliced path the quadratic form is
+ * good to ~1e-9 while the trace of the sliced inverse is not). */
+static void xg_exact_sigma2_grad(const XgField *f, const double *theta, const double *res, double *grad)
+{
+    if (f->kernel == 0) grad[0] = 0.5 * (res[2] - (double)f->N) / theta[0];
+}
+
 /* The gradient's inverse-factor store and contraction partials, each
  * allocated on first use (the Fisher path allocates only the store). */
 static int xg_grad_workspace(XgField *f)
@@ -670,6 +681,7 @@ int xg_field_loglik_grad(XgField *f, const double *theta, double *res, double *g
     const int np = f->kernel == 1 ? 4 : 3;
     for (int i = 0; i < np; ++i) grad[i] = g4[i];
     /* the contraction kernel accumulates the nugget term in slot 3 */
+    xg_exact_sigma2_grad(f, theta, res, grad);
     return XG_OK;
 }
 
@@ -1356,6 +1368,7 @@ int xg_field_loglik_grad_sliced(XgField *f, const double *theta, double *res, do
     }
     const int np = f->kernel == 1 ? 4 : 3;
     for (int i = 0; i < np; ++i) grad[i] = g4[i];
+    xg_exact_sigma2_grad(f, theta, res, grad);
     return XG_OK;
 }
 

@@ -156,10 +156,10 @@ def fit_trust_region(loglik_grad, theta0, lb, ub, max_iter=60, gtol=1e-3, delta0
     delta0 and never exceeds delta_max (a factor e^2 per step).
 
     Stops when the scaled projected gradient max_k |d f / d log theta_k| over
-    the free coordinates is at most gtol, when the gain the model predicts
-    for its next step is below ftol (an objective whose values carry noise of
-    that size cannot resolve more), when the radius falls below 1e-8, or
-    after max_iter iterations.  Returns (theta, f, evaluations,
+    the free coordinates is at most gtol, when two accepted steps in a row
+    raise f by less than ftol (an objective whose values carry noise of that
+    size cannot resolve more), when the radius falls below 1e-8, or after
+    max_iter iterations.  Returns (theta, f, evaluations,
     history) with one (theta, f) pair per accepted step.  state (a dict, may
     be None): state["B"], when present, is the initial Hessian model in phi,
     and receives the final one."""
@@ -186,6 +186,7 @@ def fit_trust_region(loglik_grad, theta0, lb, ub, max_iter=60, gtol=1e-3, delta0
         raise RuntimeError("the objective fails at the start point %s" % list(th))
     B = -np.eye(n) * max(np.max(np.abs(gphi)) / delta0, 1.0)
     first_update = True
+    stalls = 0
     if state is not None and state.get("B") is not None:
         B = np.array(state["B"], dtype=np.float64)
         first_update = False
@@ -201,8 +202,6 @@ def fit_trust_region(loglik_grad, theta0, lb, ub, max_iter=60, gtol=1e-3, delta0
             break
         d = _tr_step(gphi, B, delta, plo - phi, phi_hi - phi)
         pred = gphi @ d + 0.5 * d @ B @ d
-        if 0.0 < pred < ftol and it > 0:
-            break
         if pred <= 0.0 or np.linalg.norm(d) == 0.0:
             B = -np.eye(n) * max(np.max(np.abs(gphi)) / delta, 1.0)
             delta *= 0.25
@@ -222,9 +221,18 @@ def fit_trust_region(loglik_grad, theta0, lb, ub, max_iter=60, gtol=1e-3, delta0
                     first_update = False
                 Bs = B @ s
                 B = B - np.outer(Bs, Bs) / (s @ Bs) + np.outer(y, y) / sy
+        if rho > 1.25 and np.linalg.norm(d) < 0.8 * delta:
+            # an interior step that gained more than the model promised: the
+            # model is too curved along it (the flat ridge); halve it so the
+            # next steps grow geometrically instead of crawling
+            B = 0.5 * B
         if rho >= 0.1:
+            small = 0.0 <= fc - f < ftol
             phi, f, gphi = cand_phi, fc, gc
             history.append((np.exp(phi), f))
+            stalls = stalls + 1 if small else 0
+            if stalls >= 2:
+                break
             if rho > 0.75 and np.linalg.norm(d) > 0.8 * delta:
                 delta = min(2.0 * delta, delta_max)
         else:
@@ -261,32 +269,62 @@ def start_point(loglik, z, lb, ub, nbeta=7):
     return best, nbeta
 
 
-def ridge_polish(loglik, theta, B, lb, ub, h=0.05):
-    """One parabolic line search along the flattest direction u of the
-    Hessian model B (in phi = log theta): the likelihood at phi and phi +- h u
-    fixes a parabola whose vertex (at most 2 h away, inside the box) is the
-    new point.  On the sigma^2-beta ridge of the Matern likelihood the
-    gradient-based stop leaves the largest error along u, and three values
-    of the objective resolve it far better than a gradient of the same
-    precision.  Returns (theta, loglik at theta or the start value when the
-    parabola is not concave, evaluations)."""
-    lb = np.asarray(lb, dtype=np.float64)
-    ub = np.asarray(ub, dtype=np.float64)
+def value_newton_polish(loglik, theta, B, lb, ub, signal=1e-2, rounds=2):
+    """Newton steps on a quadratic model fitted to values of the objective
+    only (in phi = log theta), for an objective whose gradient is less
+    accurate than its values -- the INT8-sliced path, whose log-likelihood is
+    good to ~1e-9 relative but whose adjoint gradient is good to ~1e-4 of
+    its largest entry.  The model is fitted in the eigenbasis u_i of the
+    Hessian model B, with steps h_i = sqrt(2 signal / |lambda_i|) so that every
+    sampled change of f is about `signal` (far above the values' noise):
+    f at the centre, at +- h_i u_i and at h_i u_i + h_j u_j (10 values for
+    three parameters) give the gradient, the diagonal and the cross
+    curvatures exactly for a quadratic.  The Newton step of that model (at
+    most 3 h_i along each direction, inside the box) is taken when it raises
+    f.  Returns (theta, f(theta), evaluations)."""
+    lo, hi = np.log(np.asarray(lb, dtype=np.float64)), np.log(np.asarray(ub, dtype=np.float64))
     phi = np.log(np.asarray(theta, dtype=np.float64))
     w, V = np.linalg.eigh(np.asarray(B, dtype=np.float64))
-    u = V[:, int(np.argmax(w))]  # B is negative definite: the largest eigenvalue is the flattest
-    f0 = loglik(np.exp(phi))
-    fp = loglik(np.exp(np.clip(phi + h * u, np.log(lb), np.log(ub))))
-    fm = loglik(np.exp(np.clip(phi - h * u, np.log(lb), np.log(ub))))
-    c = fp - 2.0 * f0 + fm
-    if not (np.isfinite(c) and c < 0.0):
-        return np.exp(phi), f0, 3
-    t = float(np.clip(h * (fm - fp) / (2.0 * c), -2.0 * h, 2.0 * h))
-    th = np.exp(np.clip(phi + t * u, np.log(lb), np.log(ub)))
-    f1 = loglik(th)
-    if not (np.isfinite(f1) and f1 >= f0):
-        return np.exp(phi), f0, 4
-    return th, f1, 4
+    n = phi.size
+
+    def f(p):
+        try:
+            v = loglik(np.exp(np.clip(p, lo, hi)))
+        except Exception:
+            return -np.inf
+        return v if np.isfinite(v) else -np.inf
+
+    f0 = f(phi)
+    evals = 1
+    for _ in range(rounds):
+        h = np.sqrt(2.0 * signal / np.maximum(np.abs(w), 1e-12))
+        h = np.minimum(h, 0.5)
+        D = V * h  # columns: the scaled sample directions
+        fp = np.array([f(phi + D[:, i]) for i in range(n)])
+        fm = np.array([f(phi - D[:, i]) for i in range(n)])
+        evals += 2 * n
+        g = (fp - fm) / 2.0
+        H = np.diag(fp - 2.0 * f0 + fm)
+        for i in range(n):
+            for j in range(i + 1, n):
+                fij = f(phi + D[:, i] + D[:, j])
+                evals += 1
+                H[i, j] = H[j, i] = fij - f0 - g[i] - g[j] - 0.5 * (H[i, i] + H[j, j])
+        if not (np.all(np.isfinite(H)) and np.all(np.isfinite(g))):
+            break
+        ev = np.linalg.eigvalsh(H)
+        if ev.max() >= 0.0:
+            break  # not concave at this scale: keep the point
+        x = np.clip(np.linalg.solve(H, -g), -3.0, 3.0)
+        cand = np.clip(phi + D @ x, lo, hi)
+        fc = f(cand)
+        evals += 1
+        if not fc > f0:
+            break
+        phi, f0 = cand, fc
+        if np.max(np.abs(x)) < 0.1:
+            break
+    return np.exp(phi), f0, evals
 
 
 def fit_mixed(session, lb, ub, theta0=None, gtol=0.1, ftol=1e-4, log=None):
@@ -294,7 +332,7 @@ def fit_mixed(session, lb, ub, theta0=None, gtol=0.1, ftol=1e-4, log=None):
     objective (precision 3): a start from start_point (unless theta0 is
     given), the trust-region maximiser driven by the sliced adjoint gradient
     (stopping at gtol / ftol, the noise level of that gradient), then
-    ridge_polish with sliced log-likelihood values.  Leaves the session in
+    value_newton_polish with sliced log-likelihood values.  Leaves the session in
     FP64.  Returns (theta_hat, loglik, sliced evaluations (log-likelihood and
     gradient), sliced log-likelihood-only evaluations, theta after the
     gradient stage)."""
@@ -309,9 +347,9 @@ def fit_mixed(session, lb, ub, theta0=None, gtol=0.1, ftol=1e-4, log=None):
                                        log=log, state=st)
     if log:
         log("sliced gradient stage: %d evaluations, theta %s, loglik %.12g" % (ev1, list(th1), f1))
-    th, f, ne2 = ridge_polish(lambda t: session.loglik(t), th1, st["B"], lb, ub)
+    th, f, ne2 = value_newton_polish(lambda t: session.loglik(t), th1, st["B"], lb, ub)
     if log:
-        log("sliced ridge search: %d evaluations, theta %s, loglik %.12g" % (ne2, list(th), f))
+        log("sliced value-based Newton polish: %d evaluations, theta %s, loglik %.12g" % (ne2, list(th), f))
     session.set_fp64()
     return th, f, ev1, ne + ne2, th1
 
