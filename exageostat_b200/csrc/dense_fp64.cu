@@ -114,22 +114,23 @@ template <bool COH> __device__ __forceinline__ double xg_ldro(const double *p) {
  * wavefront but the DMMA fragment loads are conflict-free. */
 #define XG_POTRF_THREADS 512
 
-template <int NB, bool COH = false>
-__device__ __forceinline__ void xg_potrf_body(const XgTileArgs &T, int k, double *__restrict__ v,
-                                              double *__restrict__ part_logdet, double *__restrict__ part_dot,
-                                              int with_rhs, int *status, int *info)
+/* Cholesky of the n x n block A (leading dimension lda; global memory or
+ * shared memory) by NB-wide panels staged in P ([n][NB + 4], shared), fused
+ * with the forward solve of vk (n entries, when with_rhs) using vs ([n],
+ * shared).  A receives L with its strict upper triangle zeroed; a non-positive
+ * pivot sets XG_ST_NOT_SPD and info = col0 + its 1-based column, and the call
+ * returns false (CTA-uniformly).  *logdet_out = sum log L_ii, *dot_out = |vk|^2
+ * after the solve (thread 0 / warp 0 write them). */
+template <int NB, bool COH>
+__device__ __forceinline__ bool xg_potrf_block(double *A, int n, int lda, double *vk, int with_rhs, long long col0,
+                                               int *status, int *info, double *logdet_out, double *dot_out,
+                                               double *P, double *vs)
 {
     constexpr int LDP = NB + 4;
-    extern __shared__ __align__(16) double xg_smem_d[];
-    double *P = xg_smem_d;                 /* [ts][LDP] */
-    double *vs = P + (size_t)T.ts * LDP;   /* [ts] */
     __shared__ int s_fail;
     __shared__ double s_logdet;
-    const int ts = T.ts;
+    const int ts = n;
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-    if (xg_cta_should_skip(status)) return;
-    double *A = T.data + xg_slot64(T, k, k) * (long long)ts * ts;
-    double *vk = v + (long long)k * ts;
     if (tid == 0) {
         s_fail = 0;
         s_logdet = 0.0;
@@ -142,7 +143,7 @@ __device__ __forceinline__ void xg_potrf_body(const XgTileArgs &T, int k, double
         __syncthreads();
         for (int idx = tid; idx < rows * NB; idx += blockDim.x) {
             const int r = idx / NB, c = idx - r * NB;
-            P[r * LDP + c] = xg_ldt<COH>(A + (long long)(c0 + r) * ts + c0 + c);
+            P[r * LDP + c] = xg_ldt<COH>(A + (long long)(c0 + r) * lda + c0 + c);
         }
         __syncthreads();
         /* unblocked Cholesky of the NB x NB diagonal block, one lane per row */
@@ -172,10 +173,10 @@ __device__ __forceinline__ void xg_potrf_body(const XgTileArgs &T, int k, double
         __syncthreads();
         if (s_fail) {
             if (tid == 0) {
-                atomicCAS(info, 0, k * ts + s_fail);
+                atomicCAS(info, 0, (int)(col0 + s_fail));
                 atomicOr(status, XG_ST_NOT_SPD);
             }
-            return;
+            return false;
         }
         /* rows below the diagonal block: X = B L_D^-T, one thread per row */
         for (int r = NB + tid; r < rows; r += blockDim.x) {
@@ -214,7 +215,7 @@ __device__ __forceinline__ void xg_potrf_body(const XgTileArgs &T, int k, double
             }
         for (int idx = tid; idx < rows * NB; idx += blockDim.x) {
             const int rr = idx / NB, c = idx - rr * NB;
-            A[(long long)(c0 + rr) * ts + c0 + c] = (rr < c) ? 0.0 : P[rr * LDP + c];
+            A[(long long)(c0 + rr) * lda + c0 + c] = (rr < c) ? 0.0 : P[rr * LDP + c];
         }
         /* trailing update of the tile: A[t][t] -= Pb Pb^T on the lower part,
          * 32 x 32 output blocks per warp iteration, DMMA m16n8k4 */
@@ -224,7 +225,7 @@ __device__ __forceinline__ void xg_potrf_body(const XgTileArgs &T, int k, double
             const int nblk = nbr * (nbr + 1) / 2;
             const int g = lane >> 2, tq = lane & 3;
             const double *Pb = P + NB * LDP;
-            double *At = A + (long long)(c0 + NB) * ts + (c0 + NB);
+            double *At = A + (long long)(c0 + NB) * lda + (c0 + NB);
             for (int blk = warp; blk < nblk; blk += (int)(blockDim.x >> 5)) {
                 int bi = (int)((sqrtf(8.0f * blk + 1.0f) - 1.0f) * 0.5f);
                 while ((bi + 1) * (bi + 2) / 2 <= blk) ++bi;
@@ -268,7 +269,7 @@ __device__ __forceinline__ void xg_potrf_body(const XgTileArgs &T, int k, double
                         for (int h = 0; h < 2; ++h) {
                             const int rr = r0 + mi * 16 + g + 8 * h;
                             if (rr < R && cc < R) {
-                                double2 *pc = reinterpret_cast<double2 *>(At + (long long)rr * ts + cc);
+                                double2 *pc = reinterpret_cast<double2 *>(At + (long long)rr * lda + cc);
                                 double2 cv = xg_ldt2<COH>(pc);
                                 cv.x -= acc[mi][ni][2 * h];
                                 cv.y -= acc[mi][ni][2 * h + 1];
@@ -284,7 +285,7 @@ __device__ __forceinline__ void xg_potrf_body(const XgTileArgs &T, int k, double
      * exactly L_kk and consumers may read it as a full tile */
     for (long long idx = tid; idx < (long long)ts * ts; idx += blockDim.x) {
         const int r = (int)(idx / ts), c = (int)(idx - (long long)r * ts);
-        if (c >= (r / NB + 1) * NB) A[idx] = 0.0;
+        if (c >= (r / NB + 1) * NB) A[(long long)r * lda + c] = 0.0;
     }
     __syncthreads();
     /* deterministic reductions: log-det over lanes of warp 0, dot over vs */
@@ -296,13 +297,29 @@ __device__ __forceinline__ void xg_potrf_body(const XgTileArgs &T, int k, double
     if (with_rhs)
         for (int rr = tid; rr < ts; rr += blockDim.x) vk[rr] = vs[rr];
     __syncthreads();
-    if (tid == 0) part_logdet[k] = s_logdet;
+    if (tid == 0) *logdet_out = s_logdet;
     if (with_rhs && warp == 0) {
         double s = 0.0;
         for (int rr = lane; rr < ts; rr += 32) s += vs[rr] * vs[rr];
         for (int off = 16; off > 0; off >>= 1) s += __shfl_xor_sync(0xffffffffu, s, off);
-        if (lane == 0) part_dot[k] = s;
+        if (lane == 0) *dot_out = s;
     }
+    return true;
+}
+
+template <int NB, bool COH = false>
+__device__ __forceinline__ void xg_potrf_body(const XgTileArgs &T, int k, double *__restrict__ v,
+                                              double *__restrict__ part_logdet, double *__restrict__ part_dot,
+                                              int with_rhs, int *status, int *info)
+{
+    extern __shared__ __align__(16) double xg_smem_d[];
+    const int ts = T.ts;
+    if (xg_cta_should_skip(status)) return;
+    double *A = T.data + xg_slot64(T, k, k) * (long long)ts * ts;
+    double *P = xg_smem_d;                     /* [ts][NB + 4] */
+    double *vs = P + (size_t)ts * (NB + 4);    /* [ts] */
+    xg_potrf_block<NB, COH>(A, ts, ts, v + (long long)k * ts, with_rhs, (long long)k * ts, status, info,
+                            part_logdet + k, part_dot + k, P, vs);
 }
 
 template <int NB>
@@ -355,18 +372,6 @@ __device__ __forceinline__ void xg_lower32_inverse(const double *LB, int lane, d
     for (int i = 0; i < 32; ++i) D[i * 32 + lane] = z[i];
 }
 
-/* One warp per diagonal block b of L_kk: T.dinv[(32 b + i) * 32 + c] =
- * (L_bb^-1)_ic (lower triangular). */
-__global__ void __launch_bounds__(32) xg_diag_inv_kernel(XgTileArgs T, int k, const int *status)
-{
-    if (*(volatile const int *)status) return;
-    __shared__ double LB[32 * 33];
-    const int ts = T.ts, b = blockIdx.x, lane = threadIdx.x;
-    const double *L = T.data + xg_slot64(T, k, k) * (long long)ts * ts + (long long)(b * 32) * ts + b * 32;
-    for (int r = 0; r < 32; ++r) LB[r * 33 + lane] = L[(long long)r * ts + lane];
-    __syncwarp();
-    xg_lower32_inverse(LB, lane, T.dinv + (long long)(b * 32) * 32);
-}
 
 /* ========================================================================== */
 /* Panel TRSM: L_ik = A_ik L_kk^-T, fused with v_i -= L_ik v_k                */
@@ -398,7 +403,7 @@ __device__ __forceinline__ void xg_trsm_core(double *B, const double *L, int ld,
     }
     for (int cb = 0; cb < w; cb += 32) {
         if (dinv) {
-            /* the inverse D of this 32 x 32 diagonal block (xg_diag_inv_kernel) */
+            /* the inverse D of this 32 x 32 diagonal block (xg_lower32_inverse) */
             for (int idx = tid; idx < 32 * 32; idx += blockDim.x) {
                 const int r = idx >> 5, c = idx & 31;
                 LD[r * 33 + c] = xg_ldt<COH>(dinv + (cb + r) * 32 + c);
@@ -774,6 +779,109 @@ __global__ void __launch_bounds__(XG_G_THREADS, 1) xg_syrk_gemm_batch_kernel(con
 }
 
 /* ========================================================================== */
+/* POTRF of a diagonal tile by 128 x 128 sub-blocks on several CTAs           */
+/* ========================================================================== */
+
+/* The one-CTA POTRF streams the whole ts x ts tile through one SM and updates
+ * it in global memory once per 32-wide panel (1.5 ms at ts = 512).  Here the
+ * tile is factored as a 4 x 4 (ts / 128 per side) grid of sub-blocks, right
+ * looking, with three launches per sub-step s:
+ *   xg_potrf_sub_kernel      L_ss = chol(A_ss) in shared memory (one CTA), the
+ *                            forward solve of v's segment, log-det, and the
+ *                            inverses of its four 32 x 32 diagonal blocks;
+ *   xg_potrf_sub_trsm_kernel A_is <- A_is L_ss^-T for the sub-blocks below
+ *                            (32-row strips, DMMA with the inverted blocks),
+ *                            v_i -= L_is v_s;
+ *   xg_potrf_sub_gemm_kernel A_ij -= L_is L_js^T for s < j <= i (TMA-fed DMMA,
+ *                            one 128 x 128 block per CTA, K = 128).
+ * The inverted diagonal blocks of the whole L_kk land in T.dinv on the way, so
+ * the panel TRSM that follows needs no separate inversion. */
+#define XG_SUB 128
+#define XG_SUB_LDS (XG_SUB + 4)
+#define XG_POTRF_SUB_SMEM ((size_t)(XG_SUB * XG_SUB_LDS + XG_SUB * 36 + XG_SUB + 4 * 32 * 33) * sizeof(double))
+
+__global__ void __launch_bounds__(XG_POTRF_THREADS) xg_potrf_sub_kernel(XgTileArgs T, int k, int s, double *v,
+                                                                        double *part_logdet, double *part_dot,
+                                                                        int with_rhs, int *status, int *info)
+{
+    extern __shared__ __align__(16) double xg_smem_d[];
+    double *SD = xg_smem_d;                /* [128][132] the sub-block */
+    double *P = SD + XG_SUB * XG_SUB_LDS;  /* [128][36] panel */
+    double *vs = P + XG_SUB * 36;          /* [128] */
+    double *LB = vs + XG_SUB;              /* [4][32 * 33] */
+    __shared__ double s_ld, s_dot;
+    if (xg_cta_should_skip(status)) return;
+    const int ts = T.ts, r0 = s * XG_SUB;
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    double *A = T.data + xg_slot64(T, k, k) * (long long)ts * ts;
+    double *vk = with_rhs ? v + (long long)k * ts : nullptr;
+    for (int idx = tid; idx < XG_SUB * XG_SUB; idx += blockDim.x) {
+        const int r = idx / XG_SUB, c = idx - r * XG_SUB;
+        SD[r * XG_SUB_LDS + c] = A[(long long)(r0 + r) * ts + r0 + c];
+    }
+    __syncthreads();
+    if (!xg_potrf_block<32, false>(SD, XG_SUB, XG_SUB_LDS, vk ? vk + r0 : nullptr, with_rhs, (long long)k * ts + r0,
+                                   status, info, &s_ld, &s_dot, P, vs))
+        return;
+    __syncthreads();
+    if (T.dinv && warp < XG_SUB / 32) {
+        double *lb = LB + warp * (32 * 33);
+        for (int r = 0; r < 32; ++r) lb[r * 33 + lane] = SD[(warp * 32 + r) * XG_SUB_LDS + warp * 32 + lane];
+        __syncwarp();
+        xg_lower32_inverse(lb, lane, T.dinv + (long long)(r0 + 32 * warp) * 32);
+    }
+    /* L_ss (zeros above its diagonal) back to the tile, and zeros to its right */
+    for (int idx = tid; idx < XG_SUB * XG_SUB; idx += blockDim.x) {
+        const int r = idx / XG_SUB, c = idx - r * XG_SUB;
+        A[(long long)(r0 + r) * ts + r0 + c] = SD[r * XG_SUB_LDS + c];
+    }
+    const int right = ts - r0 - XG_SUB;
+    for (int idx = tid; idx < XG_SUB * right; idx += blockDim.x) {
+        const int r = idx / right, c = idx - r * right;
+        A[(long long)(r0 + r) * ts + r0 + XG_SUB + c] = 0.0;
+    }
+    __syncthreads();
+    if (tid == 0) part_logdet[k] = (s == 0 ? 0.0 : part_logdet[k]) + s_ld;
+    if (with_rhs && r0 + XG_SUB == ts && warp == 0) {
+        /* |v_k|^2 over the whole tile, its segments all solved by now */
+        double sum = 0.0;
+        for (int rr = lane; rr < ts; rr += 32) {
+            const double x = vk[rr];
+            sum += x * x;
+        }
+        for (int off = 16; off > 0; off >>= 1) sum += __shfl_xor_sync(0xffffffffu, sum, off);
+        if (lane == 0) part_dot[k] = sum;
+    }
+}
+
+__global__ void __launch_bounds__(XG_TRSM_THREADS) xg_potrf_sub_trsm_kernel(XgTileArgs T, int k, int s, double *v,
+                                                                            int with_rhs, const int *status)
+{
+    if (xg_cta_should_skip(status)) return;
+    const int ts = T.ts, r0 = s * XG_SUB;
+    const int row = r0 + XG_SUB + (int)blockIdx.x * XG_TRSM_SR;
+    double *A = T.data + xg_slot64(T, k, k) * (long long)ts * ts;
+    double *vk = with_rhs ? v + (long long)k * ts : nullptr;
+    xg_trsm_core<false>(A + (long long)row * ts + r0, A + (long long)r0 * ts + r0, ts, XG_SUB,
+                        T.dinv ? T.dinv + (long long)r0 * 32 : nullptr, vk ? vk + r0 : nullptr,
+                        vk ? vk + row : nullptr);
+}
+
+__global__ void __launch_bounds__(XG_G_THREADS, 1) xg_potrf_sub_gemm_kernel(const __grid_constant__ CUtensorMap map,
+                                                                            XgTileArgs T, int k, int s, int *status)
+{
+    int ii, jj;
+    xg_pair_decode(blockIdx.x, &ii, &jj);
+    const int i = s + 1 + ii, j = s + 1 + jj;
+    if (xg_cta_should_skip(status)) return;
+    const int ts = T.ts;
+    const long long slot = T.tile_off + xg_tile_index(k, k, T.nt);
+    double *C = T.data + xg_slot64(T, k, k) * (long long)ts * ts + (long long)(i * XG_SUB) * ts + j * XG_SUB;
+    xg_gemm_core<false>(map, (int)(slot * ts + i * XG_SUB), (int)(slot * ts + j * XG_SUB), s * XG_SUB,
+                        XG_SUB / XG_G_BK, C, ts, status);
+}
+
+/* ========================================================================== */
 /* Batched factorisation in one persistent launch (device tile scheduler)     */
 /* ========================================================================== */
 
@@ -997,6 +1105,14 @@ cudaError_t xg_kernels_configure()
     if (e != cudaSuccess) return e;
     e = cudaFuncSetAttribute(xg_batch_sched_kernel<32>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                              (int)xg_sched_smem_bytes(XG_MAX_TS));
+    if (e != cudaSuccess) return e;
+    e = cudaFuncSetAttribute(xg_potrf_sub_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)XG_POTRF_SUB_SMEM);
+    if (e != cudaSuccess) return e;
+    e = cudaFuncSetAttribute(xg_potrf_sub_trsm_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             (int)xg_trsm_smem_bytes(XG_SUB));
+    if (e != cudaSuccess) return e;
+    e = cudaFuncSetAttribute(xg_potrf_sub_gemm_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             (int)xg_gemm_smem_bytes());
     return e;
 }
 
@@ -1021,11 +1137,25 @@ void xg_launch_potrf_diag(const XgTileArgs &T, int k, double *v, double *part_lo
                                                                      info);
 }
 
-void xg_launch_diag_inv(const XgTileArgs &T, int k, const int *status, cudaStream_t st)
+void xg_launch_potrf_tiled(const CUtensorMap &map, const XgTileArgs &T, int k, double *v, double *part_logdet,
+                           double *part_dot, int with_rhs, int *status, int *info, cudaStream_t st)
 {
-    if (!T.dinv) return;
-    xg_diag_inv_kernel<<<T.ts / 32, 32, 0, st>>>(T, k, status);
+    const int nb = T.ts / XG_SUB;
+    for (int s = 0; s < nb; ++s) {
+        xg_potrf_sub_kernel<<<1, XG_POTRF_THREADS, XG_POTRF_SUB_SMEM, st>>>(T, k, s, v, part_logdet, part_dot,
+                                                                           with_rhs, status, info);
+        const int m = nb - s - 1;
+        if (m > 0) {
+            xg_potrf_sub_trsm_kernel<<<m * (XG_SUB / XG_TRSM_SR), XG_TRSM_THREADS, xg_trsm_smem_bytes(XG_SUB), st>>>(
+                T, k, s, v, with_rhs, status);
+            xg_potrf_sub_gemm_kernel<<<m * (m + 1) / 2, XG_G_THREADS, xg_gemm_smem_bytes(), st>>>(map, T, k, s,
+                                                                                                 status);
+        }
+    }
 }
+
+int xg_potrf_tiled_launches(int ts) { return 3 * (ts / XG_SUB) - 2; }
+
 
 void xg_launch_trsm_panel(const XgTileArgs &T, int k, double *v, int with_rhs, const int *status, cudaStream_t st,
                           int i1)

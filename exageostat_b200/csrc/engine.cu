@@ -317,9 +317,8 @@ void xg_factor_lookahead(XgTileMatrix &M, double *v, double *part, int *status, 
     for (int k = 0; k < M.nt; ++k) {
         if (la) cudaStreamWaitEvent(sp, fs.ev_upd, 0);
         if (pev) cudaEventRecord(pev[5 * k], sp);
-        xg_launch_potrf_diag(T, k, v, part, part + M.nt, rhs, status, info, sp);
+        xg_launch_potrf_tiled(M.map, T, k, v, part, part + M.nt, rhs, status, info, sp);
         if (pev) cudaEventRecord(pev[5 * k + 1], sp);
-        xg_launch_diag_inv(T, k, status, sp);
         xg_launch_trsm_panel(T, k, v, rhs, status, sp);
         if (pev) cudaEventRecord(pev[5 * k + 2], sp);
         if (la) {
@@ -389,10 +388,11 @@ static void xg_field_collect_profile(XgField *f)
     }
     cudaEventElapsedTime(&ms, f->ev[0], f->ev[2]);
     f->prof[7] += ms * 1e-3;
-    /* launches: generation, POTRF per step, TRSM and two trailing launches per
-     * step but the last (the first trailing launch of the last step but one
-     * covers one column and the second is empty), finalize */
-    double launches = 1 + nt + 1;
+    /* launches: generation, the sub-block POTRF sequence per step, TRSM and two
+     * trailing launches per step but the last (the first trailing launch of
+     * the last step but one covers one column and the second is empty),
+     * finalize */
+    double launches = 1 + (double)nt * xg_potrf_tiled_launches(f->C.ts) + 1;
     for (int k = 0; k + 1 < nt; ++k) launches += 1 + 1 + (k + 2 < nt ? 1 : 0);
     f->prof[5] += launches;
     f->prof[6] += 1;
@@ -1144,9 +1144,8 @@ static void xg_factor_sliced(XgField *f, double *v, const XgFactorStreams &fs)
                              sp);
         }
         rec(j, 1, sp);
-        xg_launch_potrf_diag(T, j, v, f->part, f->part + nt, rhs, f->status, f->info, sp);
+        xg_launch_potrf_tiled(M.map, T, j, v, f->part, f->part + nt, rhs, f->status, f->info, sp);
         rec(j, 2, sp);
-        xg_launch_diag_inv(T, j, f->status, sp);
         xg_launch_trsm_panel(T, j, v, rhs, f->status, sp);
         if (j + 1 < nt) xg_launch_slice_panel(T, j, 0, sl->dig, sl->scale, plane, f->status, sp);
         rec(j, 3, sp);
@@ -1212,8 +1211,9 @@ static void xg_field_collect_profile_sliced(XgField *f, bool lookahead)
     }
     cudaEventElapsedTime(&ms, f->ev[0], f->ev[2]);
     f->prof[7] += ms * 1e-3;
-    /* generation, finalize; per column two update launches, POTRF, TRSM, slicing */
-    f->prof[5] += 2 + 5.0 * nt;
+    /* generation, finalize; per column two update launches, the sub-block POTRF
+     * sequence, TRSM, slicing */
+    f->prof[5] += 2 + (4.0 + xg_potrf_tiled_launches(f->C.ts)) * nt;
     f->prof[6] += 1;
 }
 

@@ -29,9 +29,9 @@ struct XgTileArgs {
      * 0 <= i - j < band_targets (the others go to the INT8-sliced kernel) */
     int band_targets = 0;
     /* optional: ts x 32 doubles receiving the inverses of the 32 x 32
-     * diagonal blocks of the current panel's L_kk (xg_launch_diag_inv); with
-     * it the panel TRSM applies them as DMMA products instead of a serial
-     * substitution */
+     * diagonal blocks of the current panel's L_kk (written by
+     * xg_launch_potrf_tiled); with it the panel TRSM applies them as DMMA
+     * products instead of a serial substitution */
     double *dinv = nullptr;
 };
 
@@ -156,8 +156,11 @@ void xg_launch_potrf_diag(const XgTileArgs &T, int k, double *v, double *part_lo
                           int *status, int *info, cudaStream_t st);
 void xg_launch_trsm_panel(const XgTileArgs &T, int k, double *v, int with_rhs, const int *status, cudaStream_t st,
                           int i1 = -1);
-/* T.dinv <- inverses of the 32 x 32 diagonal blocks of L_kk (no-op without T.dinv) */
-void xg_launch_diag_inv(const XgTileArgs &T, int k, const int *status, cudaStream_t st);
+/* POTRF(k, k) with the fused log-det and solve, by 128 x 128 sub-blocks on
+ * several CTAs (map: the TMA view of the tile store); fills T.dinv too */
+void xg_launch_potrf_tiled(const CUtensorMap &map, const XgTileArgs &T, int k, double *v, double *part_logdet,
+                           double *part_dot, int with_rhs, int *status, int *info, cudaStream_t st);
+int xg_potrf_tiled_launches(int ts);
 void xg_launch_syrk_gemm(const CUtensorMap &map, const XgTileArgs &T, int k, int *status, cudaStream_t st,
                          int part = 0);
 

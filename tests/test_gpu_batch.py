@@ -85,13 +85,15 @@ def test_batch_single_tile_fields_and_nugget(gpu, ora):
 
 
 def test_batch_equals_single_field_path(gpu, ora):
-    """The batched launch runs the single-field kernels over block tables, so
-    with the same tile size every field reproduces the one-field path."""
-    xs, ys, zs, th = _fields(ora, 10, 5, 400, 1500)
+    """The batched scheduler and the single-field path factor the diagonal
+    tiles in different block orders (one CTA per POTRF task against 128 x 128
+    sub-blocks on several CTAs), so on moderately conditioned fields they
+    agree to rounding, 1e-11 relative."""
+    xs, ys, zs, th = _fields(ora, 10, 5, 400, 1500, beta_max=0.1, nu_max=1.0)
     with gpu.Batch(xs, ys, zs, ts=256) as b:
         got = b.loglik(th)
     one = np.array([gpu.dmle_host(x, y, z, t, ts=256)[0] for x, y, z, t in zip(xs, ys, zs, th)])
-    assert np.allclose(got, one, rtol=1e-13, atol=0), np.abs(got - one) / np.abs(one)
+    assert np.allclose(got, one, rtol=1e-11, atol=0), np.abs(got - one) / np.abs(one)
 
 
 def test_batch_gradients_match_the_single_field_adjoint(gpu, ora):
@@ -113,7 +115,7 @@ def test_batch_gradients_match_the_single_field_adjoint(gpu, ora):
         with gpu.Session(xs[f], ys[f], dts=256) as s:
             s.set_data(z=zs[f])
             l1, g1 = s.loglik(th[f], grad=True)
-        assert ll[f] == pytest.approx(l1, rel=1e-12)
+        assert ll[f] == pytest.approx(l1, rel=1e-11)
         assert np.abs(g[f] - g1).max() <= 1e-9 * max(np.abs(g1).max(), 1.0), (f, g[f], g1)
     f = ok[0]
     t = np.asarray(th[f], dtype=float)
