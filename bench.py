@@ -47,6 +47,7 @@ def parse():
     ap.add_argument("--seed", type=int, default=0)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-mle", action="store_true", help="skip the time-to-MLE block (N = 40000) of the default line")
     ap.add_argument("--no-mixed-leg", action="store_true", help="skip the TF32 banded mixed-precision sub-result")
     ap.add_argument("--band", type=int, default=2, help="FP64 band width in tiles (mixed leg)")
     ap.add_argument("--mode", choices=["evals", "bands", "mle", "batch", "grad", "predict", "assess"], default="evals",
@@ -673,6 +674,44 @@ def c2_pair(xg, seed, ts):
     return out
 
 
+def mle_block(xg, seed, ts, n=C2_N, theta0=(1.0, 0.1, 0.5)):
+    """Time-to-MLE at the C2 size (N = 40 000, a field z = L e generated at
+    theta0), bounds [0.01, 5]^3, through the library's gradient drivers: the
+    mixed-precision driver (exageostat_b200.mle.fit_mixed: INT8-sliced
+    objective, sliced adjoint gradient, value-based Newton polish) against
+    the same driver in plain FP64 (fit_fp64).  Wall clock of each fit; theta-hat
+    compared with the FP64 one, and both optima evaluated in FP64."""
+    import numpy as np
+
+    from exageostat_b200.mle import fit_fp64, fit_mixed
+    from exageostat_b200.synthetic import dlarnv
+
+    x, y = xg.generate_xy_loc(n, seed)
+    lb, ub = [0.01] * 3, [5.0] * 3
+    out = {"n": n, "theta0": list(theta0), "bounds": [lb, ub]}
+    with xg.Session(x, y, dts=ts) as s:
+        s.zvg(list(theta0), dlarnv(seed, n))
+        s.loglik(list(theta0))  # warm-up of the FP64 path
+        t0 = time.perf_counter()
+        th64, _, ev64, ne64 = fit_fp64(s, lb, ub)
+        t64 = time.perf_counter() - t0
+        s.set_sliced()
+        s.loglik(list(theta0))  # warm-up of the sliced path
+        t0 = time.perf_counter()
+        thmx, _, evmx, nemx, _ = fit_mixed(s, lb, ub)
+        tmx = time.perf_counter() - t0
+        s.set_fp64()
+        l64 = s.loglik(list(th64))
+        lmx = s.loglik(list(thmx))
+    out["fp64"] = {"seconds": t64, "grad_evals": ev64, "loglik_evals": ne64, "theta": list(th64), "loglik": l64}
+    out["mixed"] = {"seconds": tmx, "grad_evals": evmx, "loglik_evals": nemx, "theta": list(thmx),
+                    "loglik_fp64_at_theta": lmx}
+    out["speedup"] = t64 / tmx
+    out["theta_max_rel_diff"] = float(np.max(np.abs(np.array(thmx) - np.array(th64)) / np.abs(np.array(th64))))
+    out["loglik_rel_diff"] = abs(lmx - l64) / abs(l64)
+    return out
+
+
 def ncu_traffic(kernel):
     """DRAM bytes per algorithmic operation of `kernel` from an ncu capture
     (profiles/ncu_traffic.json, written from the capture's raw CSV by
@@ -980,6 +1019,8 @@ def main():
                                                  "C2 pair")
         # the same baseline's speed-up over the extrapolated CPU time at this N, for reading beside the C2 pair
         line["cpu_baseline"]["gpu_speedup_extrapolated"] = value / line["cpu_baseline"]["value"]
+    if rank == 0 and world == 1 and not args.no_mle:
+        line["time_to_mle"] = mle_block(xg, args.seed, args.ts)
     if rank == 0:
         print(json.dumps(line), flush=True)
     if dist is not None:
