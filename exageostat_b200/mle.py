@@ -162,7 +162,8 @@ def fit_trust_region(loglik_grad, theta0, lb, ub, max_iter=60, gtol=1e-3, delta0
     max_iter iterations.  Returns (theta, f, evaluations,
     history) with one (theta, f) pair per accepted step.  state (a dict, may
     be None): state["B"], when present, is the initial Hessian model in phi,
-    and receives the final one."""
+    and receives the final one; state["stop"] receives the stop reason
+    ("gtol", "stall", "radius" or "max_iter")."""
     lb = np.asarray(lb, dtype=np.float64)
     ub = np.asarray(ub, dtype=np.float64)
     th = np.clip(np.asarray(theta0, dtype=np.float64), lb, ub)
@@ -197,8 +198,13 @@ def fit_trust_region(loglik_grad, theta0, lb, ub, max_iter=60, gtol=1e-3, delta0
         free = ~(((ph <= plo + 1e-12) & (gp < 0)) | ((ph >= phi_hi - 1e-12) & (gp > 0)))
         return np.max(np.abs(gp[free])) if np.any(free) else 0.0
 
+    stop = "max_iter"
     for it in range(max_iter):
-        if projected(gphi, phi) <= gtol or delta < 1e-8:
+        if projected(gphi, phi) <= gtol:
+            stop = "gtol"
+            break
+        if delta < 1e-8:
+            stop = "radius"
             break
         d = _tr_step(gphi, B, delta, plo - phi, phi_hi - phi)
         pred = gphi @ d + 0.5 * d @ B @ d
@@ -232,6 +238,7 @@ def fit_trust_region(loglik_grad, theta0, lb, ub, max_iter=60, gtol=1e-3, delta0
             history.append((np.exp(phi), f))
             stalls = stalls + 1 if small else 0
             if stalls >= 2:
+                stop = "stall"
                 break
             if rho > 0.75 and np.linalg.norm(d) > 0.8 * delta:
                 delta = min(2.0 * delta, delta_max)
@@ -242,9 +249,12 @@ def fit_trust_region(loglik_grad, theta0, lb, ub, max_iter=60, gtol=1e-3, delta0
         if log:
             log("trust region %d: theta %s f %.12g rho %.3g delta %.3g |g_phi| %.3g" % (
                 it, list(np.exp(phi)), f, rho, delta, projected(gphi, phi)))
+    if projected(gphi, phi) <= gtol:
+        stop = "gtol"
     if state is not None:
         state["B"] = B
         state["gphi"] = gphi
+        state["stop"] = stop
     return np.exp(phi), f, evals, history
 
 
@@ -331,8 +341,9 @@ def fit_mixed(session, lb, ub, theta0=None, gtol=0.1, ftol=1e-4, log=None):
     """Mixed-precision adjoint-gradient MLE, entirely on the INT8-sliced
     objective (precision 3): a start from start_point (unless theta0 is
     given), the trust-region maximiser driven by the sliced adjoint gradient
-    (stopping at gtol / ftol, the noise level of that gradient), then
-    value_newton_polish with sliced log-likelihood values.  Leaves the session in
+    (stopping at gtol / ftol, the noise level of that gradient), then, unless
+    the gradient itself reached gtol, value_newton_polish with sliced
+    log-likelihood values.  Leaves the session in
     FP64.  Returns (theta_hat, loglik, sliced evaluations (log-likelihood and
     gradient), sliced log-likelihood-only evaluations, theta after the
     gradient stage)."""
@@ -347,9 +358,14 @@ def fit_mixed(session, lb, ub, theta0=None, gtol=0.1, ftol=1e-4, log=None):
                                        log=log, state=st)
     if log:
         log("sliced gradient stage: %d evaluations, theta %s, loglik %.12g" % (ev1, list(th1), f1))
-    th, f, ne2 = value_newton_polish(lambda t: session.loglik(t), th1, st["B"], lb, ub)
+    if st["stop"] == "gtol":
+        # the sliced gradient itself reached the optimum to its noise level
+        th, f, ne2 = th1, f1, 0
+    else:
+        th, f, ne2 = value_newton_polish(lambda t: session.loglik(t), th1, st["B"], lb, ub)
     if log:
-        log("sliced value-based Newton polish: %d evaluations, theta %s, loglik %.12g" % (ne2, list(th), f))
+        log("sliced value-based Newton polish (%s stop): %d evaluations, theta %s, loglik %.12g" % (
+            st["stop"], ne2, list(th), f))
     session.set_fp64()
     return th, f, ev1, ne + ne2, th1
 
