@@ -114,6 +114,90 @@ template <bool COH> __device__ __forceinline__ double xg_ldro(const double *p) {
  * wavefront but the DMMA fragment loads are conflict-free. */
 #define XG_POTRF_THREADS 512
 
+/* Cholesky of the NB x NB block at P (leading dimension LDP, NB <= 32) by one
+ * warp with lane r holding row r in registers: per column j the pivot is
+ * broadcast from lane j, the column is scaled by the reciprocal of its square
+ * root (as LAPACK's dpotf2 scales by ONE / AJJ) and the lower trailing rows
+ * are updated with the column's entries broadcast lane by lane.  Writes L
+ * (zeros above the diagonal) back to P and 1 / L_jj to rdiag[j], adds log L_jj
+ * to lane j's logdet; returns the first column (1-based) whose pivot is not
+ * positive, or 0, the same value in every lane. */
+template <int NB, int LDP>
+__device__ __forceinline__ int xg_chol_warp(double *P, int lane, double &logdet_lane, double *rdiag)
+{
+    double row[NB];
+    const bool act = lane < NB;
+#pragma unroll
+    for (int c = 0; c < NB; ++c) row[c] = act ? P[lane * LDP + c] : 0.0;
+    int fail = 0;
+#pragma unroll
+    for (int j = 0; j < NB; ++j) {
+        double d = __shfl_sync(0xffffffffu, row[j], j);
+        if (!(d > 0.0)) {
+            if (!fail) fail = j + 1;
+            d = 1.0;
+        }
+        const double ljj = sqrt(d);
+        const double rj = 1.0 / ljj;
+        if (lane == j) {
+            row[j] = ljj;
+            logdet_lane += log(ljj);
+            rdiag[j] = rj;
+        } else if (lane > j) {
+            row[j] *= rj;
+        }
+        const double lrj = row[j];
+#pragma unroll
+        for (int c = 1; c < NB; ++c) {
+            if (c > j) {
+                const double lcj = __shfl_sync(0xffffffffu, lrj, c);
+                if (lane >= c) row[c] = fma(-lrj, lcj, row[c]);
+            }
+        }
+    }
+    if (act) {
+#pragma unroll
+        for (int c = 0; c < NB; ++c) P[lane * LDP + c] = c <= lane ? row[c] : 0.0;
+    }
+    return fail;
+}
+
+/* The same factorisation with the block left in shared memory (lane r
+ * updates row r in place), for kernels launched with 512 threads whose
+ * 128-register budget cannot hold a 32-double row: same results, same
+ * return value. */
+template <int NB, int LDP>
+__device__ __forceinline__ int xg_chol_warp_smem(double *P, int lane, double &logdet_lane, double *rdiag)
+{
+    int fail = 0;
+    for (int j = 0; j < NB; ++j) {
+        double d = P[j * LDP + j];
+        if (!(d > 0.0)) {
+            if (!fail) fail = j + 1;
+            d = 1.0;
+        }
+        const double ljj = sqrt(d);
+        const double rj = 1.0 / ljj;
+        __syncwarp();
+        if (lane == j) {
+            P[j * LDP + j] = ljj;
+            logdet_lane += log(ljj);
+            rdiag[j] = rj;
+        } else if (lane > j && lane < NB) {
+            P[lane * LDP + j] *= rj;
+        }
+        __syncwarp();
+        if (lane > j && lane < NB) {
+            const double lij = P[lane * LDP + j];
+            for (int c = j + 1; c <= lane; ++c) P[lane * LDP + c] = fma(-lij, P[c * LDP + j], P[lane * LDP + c]);
+        }
+        __syncwarp();
+    }
+    if (lane < NB)
+        for (int c = lane + 1; c < NB; ++c) P[lane * LDP + c] = 0.0;
+    return fail;
+}
+
 /* Cholesky of the n x n block A (leading dimension lda; global memory or
  * shared memory) by NB-wide panels staged in P ([n][NB + 4], shared), fused
  * with the forward solve of vk (n entries, when with_rhs) using vs ([n],
@@ -121,7 +205,7 @@ template <bool COH> __device__ __forceinline__ double xg_ldro(const double *p) {
  * pivot sets XG_ST_NOT_SPD and info = col0 + its 1-based column, and the call
  * returns false (CTA-uniformly).  *logdet_out = sum log L_ii, *dot_out = |vk|^2
  * after the solve (thread 0 / warp 0 write them). */
-template <int NB, bool COH>
+template <int NB, bool COH, bool REGCHOL = false>
 __device__ __forceinline__ bool xg_potrf_block(double *A, int n, int lda, double *vk, int with_rhs, long long col0,
                                                int *status, int *info, double *logdet_out, double *dot_out,
                                                double *P, double *vs)
@@ -129,6 +213,7 @@ __device__ __forceinline__ bool xg_potrf_block(double *A, int n, int lda, double
     constexpr int LDP = NB + 4;
     __shared__ int s_fail;
     __shared__ double s_logdet;
+    __shared__ double s_rdiag[NB]; /* 1 / L_jj of the panel's diagonal block */
     const int ts = n;
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     if (tid == 0) {
@@ -146,29 +231,11 @@ __device__ __forceinline__ bool xg_potrf_block(double *A, int n, int lda, double
             P[r * LDP + c] = xg_ldt<COH>(A + (long long)(c0 + r) * lda + c0 + c);
         }
         __syncthreads();
-        /* unblocked Cholesky of the NB x NB diagonal block, one lane per row */
+        /* unblocked Cholesky of the NB x NB diagonal block (warp 0, in registers) */
         if (warp == 0) {
-            for (int j = 0; j < NB; ++j) {
-                double d = 0.0;
-                if (lane == j) {
-                    d = P[j * LDP + j];
-                    if (!(d > 0.0)) {
-                        s_fail = c0 + j + 1;
-                        d = 1.0;
-                    }
-                    d = sqrt(d);
-                    P[j * LDP + j] = d;
-                    logdet_lane += log(d);
-                }
-                d = __shfl_sync(0xffffffffu, d, j);
-                if (lane > j && lane < NB) P[lane * LDP + j] /= d;
-                __syncwarp();
-                if (lane > j && lane < NB) {
-                    const double lij = P[lane * LDP + j];
-                    for (int c = j + 1; c <= lane; ++c) P[lane * LDP + c] -= lij * P[c * LDP + j];
-                }
-                __syncwarp();
-            }
+            const int f = REGCHOL ? xg_chol_warp<NB, LDP>(P, lane, logdet_lane, s_rdiag)
+                                  : xg_chol_warp_smem<NB, LDP>(P, lane, logdet_lane, s_rdiag);
+            if (f && lane == 0) s_fail = c0 + f;
         }
         __syncthreads();
         if (s_fail) {
@@ -178,7 +245,8 @@ __device__ __forceinline__ bool xg_potrf_block(double *A, int n, int lda, double
             }
             return false;
         }
-        /* rows below the diagonal block: X = B L_D^-T, one thread per row */
+        /* rows below the diagonal block: X = B L_D^-T, one thread per row
+         * (forward substitution, scaled by the reciprocals as dtrsm does) */
         for (int r = NB + tid; r < rows; r += blockDim.x) {
             double row[NB];
 #pragma unroll
@@ -188,7 +256,7 @@ __device__ __forceinline__ bool xg_potrf_block(double *A, int n, int lda, double
                 double s = row[j];
 #pragma unroll
                 for (int q = 0; q < j; ++q) s -= row[q] * P[j * LDP + q];
-                row[j] = s / P[j * LDP + j];
+                row[j] = s * s_rdiag[j];
             }
 #pragma unroll
             for (int j = 0; j < NB; ++j) P[r * LDP + j] = row[j];
@@ -307,7 +375,7 @@ __device__ __forceinline__ bool xg_potrf_block(double *A, int n, int lda, double
     return true;
 }
 
-template <int NB, bool COH = false>
+template <int NB, bool COH = false, bool REGCHOL = false>
 __device__ __forceinline__ void xg_potrf_body(const XgTileArgs &T, int k, double *__restrict__ v,
                                               double *__restrict__ part_logdet, double *__restrict__ part_dot,
                                               int with_rhs, int *status, int *info)
@@ -318,7 +386,7 @@ __device__ __forceinline__ void xg_potrf_body(const XgTileArgs &T, int k, double
     double *A = T.data + xg_slot64(T, k, k) * (long long)ts * ts;
     double *P = xg_smem_d;                     /* [ts][NB + 4] */
     double *vs = P + (size_t)ts * (NB + 4);    /* [ts] */
-    xg_potrf_block<NB, COH>(A, ts, ts, v + (long long)k * ts, with_rhs, (long long)k * ts, status, info,
+    xg_potrf_block<NB, COH, REGCHOL>(A, ts, ts, v + (long long)k * ts, with_rhs, (long long)k * ts, status, info,
                             part_logdet + k, part_dot + k, P, vs);
 }
 
@@ -798,9 +866,10 @@ __global__ void __launch_bounds__(XG_G_THREADS, 1) xg_syrk_gemm_batch_kernel(con
  * the panel TRSM that follows needs no separate inversion. */
 #define XG_SUB 128
 #define XG_SUB_LDS (XG_SUB + 4)
+#define XG_POTRF_SUB_THREADS 256 /* 255 registers a thread: the warp factor keeps its rows in registers */
 #define XG_POTRF_SUB_SMEM ((size_t)(XG_SUB * XG_SUB_LDS + XG_SUB * 36 + XG_SUB + 4 * 32 * 33) * sizeof(double))
 
-__global__ void __launch_bounds__(XG_POTRF_THREADS) xg_potrf_sub_kernel(XgTileArgs T, int k, int s, double *v,
+__global__ void __launch_bounds__(XG_POTRF_SUB_THREADS) xg_potrf_sub_kernel(XgTileArgs T, int k, int s, double *v,
                                                                         double *part_logdet, double *part_dot,
                                                                         int with_rhs, int *status, int *info)
 {
@@ -820,7 +889,7 @@ __global__ void __launch_bounds__(XG_POTRF_THREADS) xg_potrf_sub_kernel(XgTileAr
         SD[r * XG_SUB_LDS + c] = A[(long long)(r0 + r) * ts + r0 + c];
     }
     __syncthreads();
-    if (!xg_potrf_block<32, false>(SD, XG_SUB, XG_SUB_LDS, vk ? vk + r0 : nullptr, with_rhs, (long long)k * ts + r0,
+    if (!xg_potrf_block<32, false, true>(SD, XG_SUB, XG_SUB_LDS, vk ? vk + r0 : nullptr, with_rhs, (long long)k * ts + r0,
                                    status, info, &s_ld, &s_dot, P, vs))
         return;
     __syncthreads();
@@ -971,7 +1040,7 @@ __global__ void __launch_bounds__(XG_G_THREADS, 1)
         __syncthreads();
         if (s_go) {
             if (type == XG_TASK_POTRF) {
-                xg_potrf_body<NB, true>(T, k, v + fd.vec_off, part + fd.part_off, part + fd.part_off + fd.nt, 1, stf,
+                xg_potrf_body<NB, true, true>(T, k, v + fd.vec_off, part + fd.part_off, part + fd.part_off + fd.nt, 1, stf,
                                         stf + 1);
             } else if (type == XG_TASK_TRSM) {
                 /* the inverted diagonal blocks of L_kk into this CTA's scratch
@@ -1142,7 +1211,7 @@ void xg_launch_potrf_tiled(const CUtensorMap &map, const XgTileArgs &T, int k, d
 {
     const int nb = T.ts / XG_SUB;
     for (int s = 0; s < nb; ++s) {
-        xg_potrf_sub_kernel<<<1, XG_POTRF_THREADS, XG_POTRF_SUB_SMEM, st>>>(T, k, s, v, part_logdet, part_dot,
+        xg_potrf_sub_kernel<<<1, XG_POTRF_SUB_THREADS, XG_POTRF_SUB_SMEM, st>>>(T, k, s, v, part_logdet, part_dot,
                                                                            with_rhs, status, info);
         const int m = nb - s - 1;
         if (m > 0) {

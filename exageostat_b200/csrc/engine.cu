@@ -1115,6 +1115,23 @@ static int xg_panel_share(int j, int sms)
     return r;
 }
 
+/* How the SMs are divided between the panel chain and the split update.
+ * "static" (default): the split update runs as a persistent launch on
+ * sms - xg_panel_share(j) CTAs, leaving the rest to the panel chain.
+ * "dynamic" (EXAGEOSTAT_B200_SL_SHARE=dynamic): both updates launch one CTA
+ * per job, so CTAs retire throughout the update and the hardware hands each
+ * freed SM to the pending panel kernels first (higher stream priority), the
+ * SMs the chain does not need staying with the update. */
+static bool xg_sl_dynamic_share()
+{
+    static int v = -1;
+    if (v < 0) {
+        const char *e = getenv("EXAGEOSTAT_B200_SL_SHARE");
+        v = (e && strcmp(e, "dynamic") == 0) ? 1 : 0;
+    }
+    return v == 1;
+}
+
 static void xg_factor_sliced(XgField *f, double *v, const XgFactorStreams &fs)
 {
     XgSliced *sl = f->sl;
@@ -1132,13 +1149,15 @@ static void xg_factor_sliced(XgField *f, double *v, const XgFactorStreams &fs)
     };
     const int rhs = v != nullptr;
     const int sms = g_xg.sm_count;
+    const bool dyn = xg_sl_dynamic_share();
+    const int all = 1 << 30; /* one CTA per job */
     if (la) cudaEventRecord(sl->ev_a, fs.st); /* the generated matrix */
     for (int j = 0; j < nt; ++j) {
         if (la) cudaStreamWaitEvent(sp, sl->ev_a, 0); /* chunks k < j-1 of column j */
         rec(j, 0, sp);
         if (la) {
             if (j >= 1) xg_launch_sliced(sl->map_a, sl->map_b, sl->scale, sl->scale, T, factor_task(j, j - 1, j), pr,
-                                         xg_panel_share(j, sms), f->status, sp);
+                                         dyn ? all : xg_panel_share(j, sms), f->status, sp);
         } else {
             xg_launch_sliced(sl->map_a, sl->map_b, sl->scale, sl->scale, T, factor_task(j, 0, j), pr, sms, f->status,
                              sp);
@@ -1156,7 +1175,7 @@ static void xg_factor_sliced(XgField *f, double *v, const XgFactorStreams &fs)
             rec(j, 4, fs.st);
             if (j >= 1 && j + 1 < nt)
                 xg_launch_sliced(sl->map_a, sl->map_b, sl->scale, sl->scale, T, factor_task(j + 1, 0, j), pr,
-                                 sms - xg_panel_share(j, sms), f->status, fs.st);
+                                 dyn ? all : sms - xg_panel_share(j, sms), f->status, fs.st);
             rec(j, 5, fs.st);
             cudaEventRecord(sl->ev_a, fs.st);
         } else {
