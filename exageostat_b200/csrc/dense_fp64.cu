@@ -445,38 +445,42 @@ __device__ __forceinline__ void xg_lower32_inverse(const double *LB, int lane, d
 /* Panel TRSM: L_ik = A_ik L_kk^-T, fused with v_i -= L_ik v_k                */
 /* ========================================================================== */
 
-#define XG_TRSM_THREADS 512
-#define XG_TRSM_SR 32 /* rows of A_ik per CTA */
+#define XG_TRSM_THREADS 256 /* 255 registers a thread: a group's 32 L fragments are loaded before its DMMAs */
+#define XG_TRSM_SR 32       /* rows of A_ik per CTA */
 
 /* One 32-row strip B (leading dimension ld, w columns) <- B L^-T for the
  * lower-triangular w x w block L (same leading dimension), 32 columns at a
  * time: with dinv (the inverted 32 x 32 diagonal blocks of L, [(cb + r) * 32
- * + c]) each diagonal solve is a DMMA product, without it a serial
- * substitution; the rest of each step is a DMMA update.  With vk != nullptr
- * also vi[0:32] -= B_new vk[0:w].  Called by every CTA thread after the status
- * check. */
+ * + c]) each diagonal solve is a DMMA product -- warps 0-3 apply block b
+ * while warps 4-7 fetch block b + 1 into the other buffer -- without it a
+ * serial substitution; the rest of each step is a DMMA update in which each
+ * warp takes 32-column groups and loads the group's 32 x 32 block of L
+ * (32 fragments a thread) before its 64 DMMAs, so the L2 latency is paid
+ * once per group.  With vk != nullptr also vi[0:32] -= B_new vk[0:w].
+ * Called by every CTA thread after the status check. */
 template <bool COH>
 __device__ __forceinline__ void xg_trsm_core(double *B, const double *L, int ld, int w, const double *dinv,
                                              const double *vk, double *vi)
 {
     const int LDS = w + 4;
     extern __shared__ __align__(16) double xg_smem_d[];
-    double *S = xg_smem_d;             /* [SR][LDS] */
-    double *LD = S + XG_TRSM_SR * LDS; /* [32][33] */
+    double *S = xg_smem_d;              /* [SR][LDS] */
+    double *LDb = S + XG_TRSM_SR * LDS; /* [2][32][33] */
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    const int nwarps = (int)(blockDim.x >> 5);
     const int g = lane >> 2, tq = lane & 3;
     for (int idx = tid; idx < XG_TRSM_SR * w; idx += blockDim.x) {
         const int r = idx / w, c = idx - r * w;
         S[r * LDS + c] = xg_ldt<COH>(B + (long long)r * ld + c);
     }
-    for (int cb = 0; cb < w; cb += 32) {
-        if (dinv) {
-            /* the inverse D of this 32 x 32 diagonal block (xg_lower32_inverse) */
-            for (int idx = tid; idx < 32 * 32; idx += blockDim.x) {
-                const int r = idx >> 5, c = idx & 31;
-                LD[r * 33 + c] = xg_ldt<COH>(dinv + (cb + r) * 32 + c);
-            }
-        } else {
+    if (dinv)
+        for (int idx = tid; idx < 32 * 32; idx += blockDim.x) {
+            const int r = idx >> 5, c = idx & 31;
+            LDb[r * 33 + c] = xg_ldt<COH>(dinv + r * 32 + c);
+        }
+    for (int cb = 0, b = 0; cb < w; cb += 32, ++b) {
+        double *LD = LDb + (b & 1) * (32 * 33);
+        if (!dinv) {
             for (int idx = tid; idx < 32 * 32; idx += blockDim.x) {
                 const int r = idx >> 5, c = idx & 31;
                 LD[r * 33 + c] = xg_ldt<COH>(L + (long long)(cb + r) * ld + cb + c);
@@ -486,7 +490,8 @@ __device__ __forceinline__ void xg_trsm_core(double *B, const double *L, int ld,
         if (dinv) {
             /* S[:, cb:cb+32] <- S[:, cb:cb+32] D^T on DMMA: warp w < 4 computes
              * the 32 x 8 column block w (both 16-row halves); the results are
-             * written after every warp has read its operands */
+             * written after every warp has read its operands.  Warps 4.. fetch
+             * the next block's inverse meanwhile. */
             double acc[2][4];
 #pragma unroll
             for (int mi = 0; mi < 2; ++mi)
@@ -501,6 +506,12 @@ __device__ __forceinline__ void xg_trsm_core(double *B, const double *L, int ld,
                         xg_dmma_16x8x4(acc[mi][0], acc[mi][1], acc[mi][2], acc[mi][3],
                                        S[(mi * 16 + g) * LDS + cb + p0 + tq], S[(mi * 16 + g + 8) * LDS + cb + p0 + tq],
                                        b0);
+                }
+            } else if (cb + 32 < w) {
+                double *LN = LDb + ((b + 1) & 1) * (32 * 33);
+                for (int idx = tid - 128; idx < 32 * 32; idx += (int)blockDim.x - 128) {
+                    const int r = idx >> 5, c = idx & 31;
+                    LN[r * 33 + c] = xg_ldt<COH>(dinv + (cb + 32 + r) * 32 + c);
                 }
             }
             __syncthreads();
@@ -532,8 +543,13 @@ __device__ __forceinline__ void xg_trsm_core(double *B, const double *L, int ld,
         /* S[:, cb+32:] -= S[:, cb:cb+32] L[cb+32:, cb:cb+32]^T, 32-column groups */
         const int ncol = w - cb - 32;
         const int ngrp = ncol / 32;
-        for (int grp = warp; grp < ngrp; grp += (int)(blockDim.x >> 5)) {
+        for (int grp = warp; grp < ngrp; grp += nwarps) {
             const int c0 = cb + 32 + grp * 32;
+            double bl[8][4];
+#pragma unroll
+            for (int p = 0; p < 8; ++p)
+#pragma unroll
+                for (int ni = 0; ni < 4; ++ni) bl[p][ni] = xg_ldro<COH>(L + (long long)(c0 + ni * 8 + g) * ld + cb + p * 4 + tq);
             double acc[2][4][4];
 #pragma unroll
             for (int mi = 0; mi < 2; ++mi)
@@ -542,21 +558,19 @@ __device__ __forceinline__ void xg_trsm_core(double *B, const double *L, int ld,
 #pragma unroll
                     for (int e = 0; e < 4; ++e) acc[mi][ni][e] = 0.0;
 #pragma unroll
-            for (int p0 = 0; p0 < 32; p0 += 4) {
-                double a[2][2], b[4];
+            for (int p = 0; p < 8; ++p) {
+                double a[2][2];
 #pragma unroll
                 for (int mi = 0; mi < 2; ++mi) {
-                    a[mi][0] = S[(mi * 16 + g) * LDS + cb + p0 + tq];
-                    a[mi][1] = S[(mi * 16 + g + 8) * LDS + cb + p0 + tq];
+                    a[mi][0] = S[(mi * 16 + g) * LDS + cb + p * 4 + tq];
+                    a[mi][1] = S[(mi * 16 + g + 8) * LDS + cb + p * 4 + tq];
                 }
-#pragma unroll
-                for (int ni = 0; ni < 4; ++ni) b[ni] = xg_ldro<COH>(L + (long long)(c0 + ni * 8 + g) * ld + cb + p0 + tq);
 #pragma unroll
                 for (int mi = 0; mi < 2; ++mi)
 #pragma unroll
                     for (int ni = 0; ni < 4; ++ni)
                         xg_dmma_16x8x4(acc[mi][ni][0], acc[mi][ni][1], acc[mi][ni][2], acc[mi][ni][3], a[mi][0],
-                                       a[mi][1], b[ni]);
+                                       a[mi][1], bl[p][ni]);
             }
 #pragma unroll
             for (int mi = 0; mi < 2; ++mi)
@@ -569,14 +583,14 @@ __device__ __forceinline__ void xg_trsm_core(double *B, const double *L, int ld,
                         ps[1] -= acc[mi][ni][2 * h + 1];
                     }
         }
-        __syncthreads();
     }
+    __syncthreads();
     for (int idx = tid; idx < XG_TRSM_SR * w; idx += blockDim.x) {
         const int r = idx / w, c = idx - r * w;
         B[(long long)r * ld + c] = S[r * LDS + c];
     }
     if (vk) {
-        for (int r = warp; r < XG_TRSM_SR; r += (int)(blockDim.x >> 5)) {
+        for (int r = warp; r < XG_TRSM_SR; r += nwarps) {
             double s = 0.0;
             for (int c = lane; c < w; c += 32) s += S[r * LDS + c] * xg_ldt<COH>(vk + c);
             for (int off = 16; off > 0; off >>= 1) s += __shfl_xor_sync(0xffffffffu, s, off);
@@ -600,13 +614,13 @@ __device__ __forceinline__ void xg_trsm_body(const XgTileArgs &T, int k, double 
                       with_rhs ? v + (long long)i * ts + strip * XG_TRSM_SR : nullptr);
 }
 
-__global__ void __launch_bounds__(XG_TRSM_THREADS) xg_trsm_panel_kernel(XgTileArgs T, int k, double *__restrict__ v,
+__global__ void __launch_bounds__(XG_TRSM_THREADS, 1) xg_trsm_panel_kernel(XgTileArgs T, int k, double *__restrict__ v,
                                                                         int with_rhs, const int *status)
 {
     xg_trsm_body(T, k, v, with_rhs, status, blockIdx.x);
 }
 
-__global__ void __launch_bounds__(XG_TRSM_THREADS) xg_trsm_panel_batch_kernel(XgTileArgs base,
+__global__ void __launch_bounds__(XG_TRSM_THREADS, 1) xg_trsm_panel_batch_kernel(XgTileArgs base,
                                                                               const XgBField *__restrict__ F,
                                                                               XgBStep S, int k, double *v,
                                                                               const int *status)
@@ -923,7 +937,7 @@ __global__ void __launch_bounds__(XG_POTRF_SUB_THREADS) xg_potrf_sub_kernel(XgTi
     }
 }
 
-__global__ void __launch_bounds__(XG_TRSM_THREADS) xg_potrf_sub_trsm_kernel(XgTileArgs T, int k, int s, double *v,
+__global__ void __launch_bounds__(XG_TRSM_THREADS, 1) xg_potrf_sub_trsm_kernel(XgTileArgs T, int k, int s, double *v,
                                                                             int with_rhs, const int *status)
 {
     if (xg_cta_should_skip(status)) return;
@@ -1148,7 +1162,7 @@ __global__ void xg_finalize_batch_kernel(const XgBField *__restrict__ F, int nfi
 static int xg_potrf_nb(int ts) { return ts > 512 ? 16 : 32; }
 
 size_t xg_potrf_smem_bytes(int ts) { return ((size_t)ts * (xg_potrf_nb(ts) + 4) + ts) * sizeof(double); }
-size_t xg_trsm_smem_bytes(int ts) { return ((size_t)XG_TRSM_SR * (ts + 4) + 32 * 33) * sizeof(double); }
+size_t xg_trsm_smem_bytes(int ts) { return ((size_t)XG_TRSM_SR * (ts + 4) + 2 * 32 * 33) * sizeof(double); }
 size_t xg_gemm_smem_bytes() { return (size_t)XG_G_STAGES * XG_G_STAGE_BYTES + 2 * XG_G_STAGES * 8 + 1024; }
 
 cudaError_t xg_kernels_configure()
