@@ -25,6 +25,8 @@
 
 #include <algorithm>
 #include <chrono>
+#include <functional>
+#include <queue>
 #include <vector>
 
 #include "../../include/exageostat_b200.h"
@@ -112,6 +114,172 @@ static void xg_table_fill(XgBTable &t, const std::vector<long long> &cnt)
     t.blocks = t.start.back();
 }
 
+/* ------------------------------------------------------------------------- */
+/* task order of the device scheduler                                        */
+/* ------------------------------------------------------------------------- */
+
+/* Relative durations of the scheduler's task bodies on one SM (units of a
+ * tile update, 2 ts^3 DMMA flops): a TRSM task solves the tile's ts / 32 row
+ * strips one after the other; a POTRF task is latency-bound. */
+#define XG_PLAN_GEMM 1.0
+#define XG_PLAN_TRSM 1.05
+#define XG_PLAN_POTRF 0.5
+
+/* Bottom levels (longest path to the end of the field's DAG, the task's own
+ * duration included) of every task of a tile Cholesky with nt tiles per side,
+ * under the scheduler's dependencies: POTRF(k) <- the k updates of (k, k);
+ * TRSM(i, k) <- POTRF(k) and the k updates of (i, k); update (i, j) <- k <-
+ * TRSM(i, k), TRSM(j, k) and the update (i, j) <- k - 1. */
+struct XgPlanLevels {
+    int nt = 0;
+    std::vector<double> p, t, g; /* p[k], t[i * nt + k], g[(i * nt + j) * nt + k] */
+};
+
+static void xg_plan_levels(int nt, XgPlanLevels &L)
+{
+    L.nt = nt;
+    L.p.assign(nt, 0.0);
+    L.t.assign((size_t)nt * nt, 0.0);
+    L.g.assign((size_t)nt * nt * nt, 0.0);
+    auto G = [&](int i, int j, int k) -> double & { return L.g[((size_t)i * nt + j) * nt + k]; };
+    auto T = [&](int i, int k) -> double & { return L.t[(size_t)i * nt + k]; };
+    for (int k = nt - 1; k >= 0; --k) {
+        for (int j = k + 1; j < nt; ++j)
+            for (int i = j; i < nt; ++i) {
+                const double next = k + 1 < j ? G(i, j, k + 1) : (i == j ? L.p[j] : T(i, j));
+                G(i, j, k) = XG_PLAN_GEMM + next;
+            }
+        for (int i = k + 1; i < nt; ++i) {
+            double m = 0.0;
+            for (int j = k + 1; j <= i; ++j) m = std::max(m, G(i, j, k));
+            for (int i2 = i; i2 < nt; ++i2) m = std::max(m, G(i2, i, k));
+            T(i, k) = XG_PLAN_TRSM + m;
+        }
+        double m = 0.0;
+        for (int i = k + 1; i < nt; ++i) m = std::max(m, T(i, k));
+        L.p[k] = XG_PLAN_POTRF + m;
+    }
+}
+
+/* The task list of a batch for `workers` persistent CTAs that take tasks in
+ * list order: a list-scheduling simulation in which every free worker starts
+ * the ready task of largest bottom level (critical path first), with the
+ * durations above; the list is the order in which tasks start.  A task
+ * starts only after every task it waits on has finished, so the list is a
+ * topological order and the device scheduler cannot deadlock on it. */
+static void xg_batch_plan(const std::vector<int> &nts, int workers, std::vector<int4> &tl)
+{
+    struct Task {
+        int f, type, i, j, k;
+        double bl;
+    };
+    const int nf = (int)nts.size();
+    std::vector<const XgPlanLevels *> lev(nf);
+    std::vector<XgPlanLevels> cache;
+    {
+        std::vector<int> distinct(nts.begin(), nts.end());
+        std::sort(distinct.begin(), distinct.end());
+        distinct.erase(std::unique(distinct.begin(), distinct.end()), distinct.end());
+        cache.resize(distinct.size());
+        for (size_t d = 0; d < distinct.size(); ++d) xg_plan_levels(distinct[d], cache[d]);
+        for (int f = 0; f < nf; ++f)
+            lev[f] = &cache[std::lower_bound(distinct.begin(), distinct.end(), nts[f]) - distinct.begin()];
+    }
+    /* per field: update counts and TRSM completion per lower tile, POTRF completion per step */
+    std::vector<long long> off(nf + 1, 0);
+    for (int f = 0; f < nf; ++f) off[f + 1] = off[f] + xg_num_lower_tiles(nts[f]);
+    std::vector<int> ucnt(off[nf], 0);
+    std::vector<char> tdone(off[nf], 0);
+    std::vector<long long> poff(nf + 1, 0);
+    for (int f = 0; f < nf; ++f) poff[f + 1] = poff[f] + nts[f];
+    std::vector<char> pdone(poff[nf], 0);
+
+    std::vector<Task> tasks;
+    auto cmp = [&](int a, int b) { /* max-heap on bottom level, then the earlier task */
+        if (tasks[a].bl != tasks[b].bl) return tasks[a].bl < tasks[b].bl;
+        return a > b;
+    };
+    std::priority_queue<int, std::vector<int>, decltype(cmp)> ready(cmp);
+    auto push = [&](int f, int type, int i, int j, int k) {
+        const XgPlanLevels &L = *lev[f];
+        const int nt = L.nt;
+        double bl = type == XG_TASK_POTRF ? L.p[k]
+                    : type == XG_TASK_TRSM ? L.t[(size_t)i * nt + k]
+                                           : L.g[((size_t)i * nt + j) * nt + k];
+        tasks.push_back(Task{f, type, i, j, k, bl});
+        ready.push((int)tasks.size() - 1);
+    };
+    for (int f = 0; f < nf; ++f) push(f, XG_TASK_POTRF, 0, 0, 0);
+    typedef std::pair<double, int> Ev; /* finish time, task */
+    std::priority_queue<Ev, std::vector<Ev>, std::greater<Ev>> running;
+    double now = 0.0;
+    int idle = workers;
+    tl.clear();
+    while (!ready.empty() || !running.empty()) {
+        while (idle > 0 && !ready.empty()) {
+            const int id = ready.top();
+            ready.pop();
+            const Task &t = tasks[id];
+            tl.push_back(make_int4(t.type | (t.f << 2), t.i, t.j, t.k));
+            const double d = t.type == XG_TASK_POTRF ? XG_PLAN_POTRF : t.type == XG_TASK_TRSM ? XG_PLAN_TRSM
+                                                                                                 : XG_PLAN_GEMM;
+            running.push(Ev(now + d, id));
+            --idle;
+        }
+        if (running.empty()) break;
+        /* complete the next task and release what it unblocks */
+        const Ev ev = running.top();
+        running.pop();
+        now = ev.first;
+        ++idle;
+        const Task t = tasks[ev.second];
+        const int f = t.f, nt = nts[f];
+        auto U = [&](int i, int j) -> int & { return ucnt[off[f] + xg_tile_index(i, j, nt)]; };
+        auto TD = [&](int i, int j) -> char & { return tdone[off[f] + xg_tile_index(i, j, nt)]; };
+        if (t.type == XG_TASK_POTRF) {
+            pdone[poff[f] + t.k] = 1;
+            for (int i = t.k + 1; i < nt; ++i)
+                if (U(i, t.k) == t.k) push(f, XG_TASK_TRSM, i, t.k, t.k);
+        } else if (t.type == XG_TASK_TRSM) {
+            const int i = t.i, k = t.k;
+            TD(i, k) = 1;
+            for (int j = k + 1; j <= i; ++j) /* update (i, j) <- k: A operand L_ik, B operand L_jk */
+                if (TD(j, k) && U(i, j) == k) push(f, XG_TASK_GEMM, i, j, k);
+            for (int i2 = i + 1; i2 < nt; ++i2) /* update (i2, i) <- k: B operand L_ik */
+                if (TD(i2, k) && U(i2, i) == k) push(f, XG_TASK_GEMM, i2, i, k);
+        } else {
+            const int i = t.i, j = t.j, k = t.k;
+            const int u = ++U(i, j);
+            if (u < j) {
+                if (TD(i, u) && TD(j, u)) push(f, XG_TASK_GEMM, i, j, u);
+            } else if (i == j) {
+                push(f, XG_TASK_POTRF, j, j, j);
+            } else if (pdone[poff[f] + j]) {
+                push(f, XG_TASK_TRSM, i, j, j);
+            }
+        }
+    }
+}
+
+/* The planned task list of a batch of fields with nt[f] tiles per side, for
+ * `workers` CTAs: writes 4 ints per task (type | field << 2, i, j, k) to out
+ * when out is not null and returns the number of tasks.  Host-only. */
+extern "C" long long exageostat_b200_batch_plan(int nfields, const int *nt, int workers, int *out)
+{
+    if (nfields <= 0 || !nt || workers <= 0) return 0;
+    std::vector<int> nts(nt, nt + nfields);
+    std::vector<int4> tl;
+    xg_batch_plan(nts, workers, tl);
+    if (out)
+        for (size_t q = 0; q < tl.size(); ++q) {
+            out[4 * q] = tl[q].x;
+            out[4 * q + 1] = tl[q].y;
+            out[4 * q + 2] = tl[q].z;
+            out[4 * q + 3] = tl[q].w;
+        }
+    return (long long)tl.size();
+}
+
 extern "C" int exageostat_b200_batch_create(int nfields, const int *n, const double *x, const double *y,
                                             const double *z, int kernel, int metric, int ts, void **handle)
 {
@@ -181,23 +349,13 @@ extern "C" int exageostat_b200_batch_create(int nfields, const int *n, const dou
     std::vector<long long> cnt(nfields);
     for (int f = 0; f < nfields; ++f) cnt[f] = xg_num_lower_tiles(b->F[f].nt) * (b->ts / 8);
     xg_table_fill(b->gen, cnt);
-    /* the scheduler's task list in one topological order: step by step; in a
-     * step the POTRFs (largest fields first), the TRSMs, then the updates
-     * column by column, so the next step's panel column is ready first */
+    /* the scheduler's task list: a critical-path-first list schedule over
+     * every field's tasks for the launch's CTAs (xg_batch_plan) */
     {
-        std::vector<int> order(nfields);
-        for (int f = 0; f < nfields; ++f) order[f] = f;
-        std::stable_sort(order.begin(), order.end(), [&](int a, int c) { return b->F[a].nt > b->F[c].nt; });
+        std::vector<int> nts(nfields);
+        for (int f = 0; f < nfields; ++f) nts[f] = b->F[f].nt;
         std::vector<int4> tl;
-        for (int k = 0; k < b->maxnt; ++k) {
-            for (int f : order)
-                if (b->F[f].nt > k) tl.push_back(make_int4(XG_TASK_POTRF | (f << 2), k, k, k));
-            for (int f : order)
-                for (int i = k + 1; i < b->F[f].nt; ++i) tl.push_back(make_int4(XG_TASK_TRSM | (f << 2), i, k, k));
-            for (int j = k + 1; j < b->maxnt; ++j)
-                for (int f : order)
-                    for (int i = j; i < b->F[f].nt; ++i) tl.push_back(make_int4(XG_TASK_GEMM | (f << 2), i, j, k));
-        }
+        xg_batch_plan(nts, g_xg.sm_count, tl);
         b->ntasks = (long long)tl.size();
         e = cudaMalloc(&b->tasks, tl.size() * sizeof(int4));
         if (e == cudaSuccess) e = cudaMemcpy(b->tasks, tl.data(), tl.size() * sizeof(int4), cudaMemcpyHostToDevice);

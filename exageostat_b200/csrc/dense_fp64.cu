@@ -114,50 +114,79 @@ template <bool COH> __device__ __forceinline__ double xg_ldro(const double *p) {
  * wavefront but the DMMA fragment loads are conflict-free. */
 #define XG_POTRF_THREADS 512
 
+/* dst[r][c] = src[r][c] for r < rows, c < cols (leading dimensions ldd and
+ * lds), by all threads of the CTA with U loads in flight per thread before
+ * any store (the loads of a plain loop would wait one by one where the
+ * compiler cannot tell dst and src apart). */
+template <bool COH, int U = 8>
+__device__ __forceinline__ void xg_stage_rows(double *dst, int ldd, const double *src, long long lds, int rows,
+                                              int cols)
+{
+    const int total = rows * cols, step = (int)blockDim.x;
+    for (int base = (int)threadIdx.x; base < total; base += U * step) {
+        double t[U];
+#pragma unroll
+        for (int u = 0; u < U; ++u) {
+            const int idx = base + u * step;
+            if (idx < total) {
+                const int r = idx / cols, c = idx - r * cols;
+                t[u] = xg_ldt<COH>(src + (long long)r * lds + c);
+            }
+        }
+#pragma unroll
+        for (int u = 0; u < U; ++u) {
+            const int idx = base + u * step;
+            if (idx < total) {
+                const int r = idx / cols, c = idx - r * cols;
+                dst[r * ldd + c] = t[u];
+            }
+        }
+    }
+}
+
 /* Cholesky of the NB x NB block at P (leading dimension LDP, NB <= 32) by one
- * warp with lane r holding row r in registers: per column j the pivot is
- * broadcast from lane j, the column is scaled by the reciprocal of its square
- * root (as LAPACK's dpotf2 scales by ONE / AJJ) and the lower trailing rows
- * are updated with the column's entries broadcast lane by lane.  Writes L
- * (zeros above the diagonal) back to P and 1 / L_jj to rdiag[j], adds log L_jj
- * to lane j's logdet; returns the first column (1-based) whose pivot is not
- * positive, or 0, the same value in every lane. */
+ * warp, lane r holding the part of row r still to be factored in registers:
+ * at step j, w[t] is element (r, j + t), so the pivot column is always w[0]
+ * and the loop over j stays rolled (one copy of the square root and the
+ * division).  Per step the pivot is broadcast from lane j, the column is
+ * scaled by the reciprocal of its square root (as LAPACK's dpotf2 scales by
+ * ONE / AJJ) and stored, the lower trailing elements are updated with the
+ * column's entries broadcast lane by lane, and the window shifts by one.
+ * Writes L (zeros above the diagonal) back to P and 1 / L_jj to rdiag[j],
+ * adds log L_rr to lane r's logdet; returns the first column (1-based) whose
+ * pivot is not positive, or 0, the same value in every lane. */
 template <int NB, int LDP>
 __device__ __forceinline__ int xg_chol_warp(double *P, int lane, double &logdet_lane, double *rdiag)
 {
-    double row[NB];
+    double w[NB];
     const bool act = lane < NB;
 #pragma unroll
-    for (int c = 0; c < NB; ++c) row[c] = act ? P[lane * LDP + c] : 0.0;
+    for (int c = 0; c < NB; ++c) w[c] = act ? P[lane * LDP + c] : 0.0;
     int fail = 0;
-#pragma unroll
+#pragma unroll 1
     for (int j = 0; j < NB; ++j) {
-        double d = __shfl_sync(0xffffffffu, row[j], j);
+        double d = __shfl_sync(0xffffffffu, w[0], j);
         if (!(d > 0.0)) {
             if (!fail) fail = j + 1;
             d = 1.0;
         }
         const double ljj = sqrt(d);
         const double rj = 1.0 / ljj;
-        if (lane == j) {
-            row[j] = ljj;
-            logdet_lane += log(ljj);
-            rdiag[j] = rj;
-        } else if (lane > j) {
-            row[j] *= rj;
-        }
-        const double lrj = row[j];
+        const double l = lane == j ? ljj : w[0] * rj; /* L(lane, j) for lane >= j */
+        if (lane == j) rdiag[j] = rj;
+        if (act && lane >= j) P[lane * LDP + j] = l;
 #pragma unroll
-        for (int c = 1; c < NB; ++c) {
-            if (c > j) {
-                const double lcj = __shfl_sync(0xffffffffu, lrj, c);
-                if (lane >= c) row[c] = fma(-lrj, lcj, row[c]);
-            }
+        for (int t = 1; t < NB; ++t) {
+            const double lcj = __shfl_sync(0xffffffffu, l, (j + t) & 31);
+            if (t < NB - j && lane >= j + t) w[t] = fma(-l, lcj, w[t]);
         }
+#pragma unroll
+        for (int t = 0; t < NB - 1; ++t) w[t] = w[t + 1];
+        w[NB - 1] = 0.0;
     }
     if (act) {
-#pragma unroll
-        for (int c = 0; c < NB; ++c) P[lane * LDP + c] = c <= lane ? row[c] : 0.0;
+        for (int c = lane + 1; c < NB; ++c) P[lane * LDP + c] = 0.0;
+        logdet_lane += log(P[lane * LDP + lane]);
     }
     return fail;
 }
@@ -226,10 +255,7 @@ __device__ __forceinline__ bool xg_potrf_block(double *A, int n, int lda, double
     for (int c0 = 0; c0 < ts; c0 += NB) {
         const int rows = ts - c0;
         __syncthreads();
-        for (int idx = tid; idx < rows * NB; idx += blockDim.x) {
-            const int r = idx / NB, c = idx - r * NB;
-            P[r * LDP + c] = xg_ldt<COH>(A + (long long)(c0 + r) * lda + c0 + c);
-        }
+        xg_stage_rows<COH>(P, LDP, A + (long long)c0 * lda + c0, lda, rows, NB);
         __syncthreads();
         /* unblocked Cholesky of the NB x NB diagonal block (warp 0, in registers) */
         if (warp == 0) {
@@ -880,7 +906,7 @@ __global__ void __launch_bounds__(XG_G_THREADS, 1) xg_syrk_gemm_batch_kernel(con
  * the panel TRSM that follows needs no separate inversion. */
 #define XG_SUB 128
 #define XG_SUB_LDS (XG_SUB + 4)
-#define XG_POTRF_SUB_THREADS 256 /* 255 registers a thread: the warp factor keeps its rows in registers */
+#define XG_POTRF_SUB_THREADS 512
 #define XG_POTRF_SUB_SMEM ((size_t)(XG_SUB * XG_SUB_LDS + XG_SUB * 36 + XG_SUB + 4 * 32 * 33) * sizeof(double))
 
 __global__ void __launch_bounds__(XG_POTRF_SUB_THREADS) xg_potrf_sub_kernel(XgTileArgs T, int k, int s, double *v,
@@ -898,10 +924,7 @@ __global__ void __launch_bounds__(XG_POTRF_SUB_THREADS) xg_potrf_sub_kernel(XgTi
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     double *A = T.data + xg_slot64(T, k, k) * (long long)ts * ts;
     double *vk = with_rhs ? v + (long long)k * ts : nullptr;
-    for (int idx = tid; idx < XG_SUB * XG_SUB; idx += blockDim.x) {
-        const int r = idx / XG_SUB, c = idx - r * XG_SUB;
-        SD[r * XG_SUB_LDS + c] = A[(long long)(r0 + r) * ts + r0 + c];
-    }
+    xg_stage_rows<false>(SD, XG_SUB_LDS, A + (long long)r0 * ts + r0, ts, XG_SUB, XG_SUB);
     __syncthreads();
     if (!xg_potrf_block<32, false, true>(SD, XG_SUB, XG_SUB_LDS, vk ? vk + r0 : nullptr, with_rhs, (long long)k * ts + r0,
                                    status, info, &s_ld, &s_dot, P, vs))

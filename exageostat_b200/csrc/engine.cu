@@ -1107,9 +1107,21 @@ static XgSlTask factor_task(int col, int k0, int k1)
  * per column the chain needs about 8 / (8 + j) of the machine (measured
  * costs at tile 512: a TRSM strip of 32 rows ~63 us, a 128 x 128 job-chunk of
  * the update ~9 us); clamped to [XG_PANEL_SMS, sms - XG_PANEL_SMS]. */
+static int xg_panel_k()
+{
+    static int v = -1;
+    if (v < 0) {
+        const char *e = getenv("EXAGEOSTAT_B200_PANEL_K");
+        v = e ? atoi(e) : 0;
+        if (v < 1 || v > 64) v = 8;
+    }
+    return v;
+}
+
 static int xg_panel_share(int j, int sms)
 {
-    int r = (int)((long long)sms * 8 / (8 + j));
+    const int K = xg_panel_k(); /* EXAGEOSTAT_B200_PANEL_K overrides the 8 */
+    int r = (int)((long long)sms * K / (K + j));
     if (r < XG_PANEL_SMS) r = XG_PANEL_SMS;
     if (r > sms - XG_PANEL_SMS) r = sms - XG_PANEL_SMS;
     return r;
