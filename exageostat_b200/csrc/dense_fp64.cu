@@ -495,15 +495,8 @@ __device__ __forceinline__ void xg_trsm_core(double *B, const double *L, int ld,
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     const int nwarps = (int)(blockDim.x >> 5);
     const int g = lane >> 2, tq = lane & 3;
-    for (int idx = tid; idx < XG_TRSM_SR * w; idx += blockDim.x) {
-        const int r = idx / w, c = idx - r * w;
-        S[r * LDS + c] = xg_ldt<COH>(B + (long long)r * ld + c);
-    }
-    if (dinv)
-        for (int idx = tid; idx < 32 * 32; idx += blockDim.x) {
-            const int r = idx >> 5, c = idx & 31;
-            LDb[r * 33 + c] = xg_ldt<COH>(dinv + r * 32 + c);
-        }
+    xg_stage_rows<COH>(S, LDS, B, ld, XG_TRSM_SR, w);
+    if (dinv) xg_stage_rows<COH, 4>(LDb, 33, dinv, 32, 32, 32);
     for (int cb = 0, b = 0; cb < w; cb += 32, ++b) {
         double *LD = LDb + (b & 1) * (32 * 33);
         if (!dinv) {
