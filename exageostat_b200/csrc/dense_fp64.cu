@@ -880,6 +880,208 @@ __global__ void __launch_bounds__(XG_G_THREADS, 1) xg_syrk_gemm_batch_kernel(con
 }
 
 /* ========================================================================== */
+/* Panel TRSM by 128-column blocks: TMA-fed DMMA GEMMs + in-block solves      */
+/* ========================================================================== */
+
+/* L_ik = A_ik L_kk^-T for one 128-row block of A_ik per CTA, by the 128-column
+ * blocks c of L_kk in order:
+ *   T_c = A_c - sum_{q < c} X_q L_cq^T       (xg_gemm_core: K = 128 c, TMA-fed DMMA)
+ *   X_c = T_c L_cc^-T                         (xg_block_trsm128: 4 steps of 32
+ *                                              columns, each a DMMA product with the
+ *                                              inverted 32 x 32 diagonal block and a
+ *                                              DMMA update of the columns to its right)
+ * so three quarters of the flops run at the trailing update's rate instead of
+ * in 32-row strips.  The X_q read by the GEMM of step c are this CTA's own
+ * stores of the steps before (ordered before the TMA reads by the proxy
+ * fences of xg_gemm_core's coherent mode).  The rounding is that of the
+ * strip TRSM up to the order of the sums: the solves use the same 32 x 32
+ * inverses.  Fused: v_i -= L_ik v_k for the block's rows. */
+#define XG_TB 128                                           /* rows of A_ik per CTA, columns per block */
+#define XG_TB_S_BYTES ((size_t)XG_TB * XG_TB * sizeof(double)) /* the block, swizzled: fits the GEMM ring */
+
+/* element (r, c) of the 128 x 128 staged block: each group of four rows is
+ * shifted by a different multiple of four columns, so a DMMA fragment read
+ * (rows g, columns tq of a 4-aligned column group) hits 32 distinct banks */
+__device__ __forceinline__ int xg_tb_idx(int r, int c) { return r * XG_TB + (c ^ ((r & 3) << 2)); }
+
+/* X = S L^-T in place for the staged 128 x 128 block S (xg_tb_idx layout),
+ * L the 128 x 128 lower block (global, leading dimension ld), dinv its four
+ * inverted 32 x 32 diagonal blocks ([(32 b + r) * 32 + c]); LDb: 2 x 32 x 33
+ * doubles of shared memory.  256 threads. */
+template <bool COH>
+__device__ __forceinline__ void xg_block_trsm128(double *S, double *LDb, const double *L, int ld, const double *dinv)
+{
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    const int g = lane >> 2, tq = lane & 3;
+    xg_stage_rows<COH, 4>(LDb, 33, dinv, 32, 32, 32);
+    for (int cb = 0; cb < XG_TB / 32; ++cb) {
+        const double *LD = LDb + (cb & 1) * (32 * 33);
+        /* the next block's inverse, loaded now and stored after the barrier */
+        double nd[4];
+        const bool more = cb + 1 < XG_TB / 32;
+        if (more)
+#pragma unroll
+            for (int u = 0; u < 4; ++u) {
+                const int idx = tid + u * 256;
+                nd[u] = xg_ldt<COH>(dinv + (long long)(cb + 1) * 32 * 32 + idx);
+            }
+        __syncthreads(); /* S and LD[cb & 1] are complete */
+        /* S[:, 32 cb : 32 cb + 32] <- that block D^T: warp w, rows 16 w .. + 15 */
+        double acc[4][4];
+#pragma unroll
+        for (int ni = 0; ni < 4; ++ni)
+#pragma unroll
+            for (int e = 0; e < 4; ++e) acc[ni][e] = 0.0;
+        const int r0 = 16 * warp;
+#pragma unroll
+        for (int p = 0; p < 8; ++p) {
+            const int c = 32 * cb + 4 * p + tq;
+            const double a0 = S[xg_tb_idx(r0 + g, c)], a1 = S[xg_tb_idx(r0 + g + 8, c)];
+#pragma unroll
+            for (int ni = 0; ni < 4; ++ni)
+                xg_dmma_16x8x4(acc[ni][0], acc[ni][1], acc[ni][2], acc[ni][3], a0, a1, LD[(ni * 8 + g) * 33 + 4 * p + tq]);
+        }
+        __syncthreads(); /* every read of the block's columns is done */
+#pragma unroll
+        for (int ni = 0; ni < 4; ++ni)
+#pragma unroll
+            for (int h = 0; h < 2; ++h) {
+                const int r = r0 + g + 8 * h, c = 32 * cb + ni * 8 + 2 * tq;
+                *reinterpret_cast<double2 *>(&S[xg_tb_idx(r, c)]) = make_double2(acc[ni][2 * h], acc[ni][2 * h + 1]);
+            }
+        if (more) {
+            double *LN = LDb + ((cb + 1) & 1) * (32 * 33);
+#pragma unroll
+            for (int u = 0; u < 4; ++u) {
+                const int idx = tid + u * 256;
+                LN[(idx >> 5) * 33 + (idx & 31)] = nd[u];
+            }
+        }
+        __syncthreads();
+        /* columns to the right: S[:, c0 : c0 + 32] -= S[:, 32 cb : +32] L[c0 : c0 + 32, 32 cb : +32]^T,
+         * items = (32-row tile, 32-column group), the group's L fragments loaded first */
+        const int ngrp = XG_TB / 32 - 1 - cb;
+        for (int item = warp; item < 4 * ngrp; item += 8) {
+            const int rt = item & 3, c0 = 32 * (cb + 1 + (item >> 2));
+            double bl[8][4];
+#pragma unroll
+            for (int p = 0; p < 8; ++p)
+#pragma unroll
+                for (int ni = 0; ni < 4; ++ni)
+                    bl[p][ni] = xg_ldro<COH>(L + (long long)(c0 + ni * 8 + g) * ld + 32 * cb + 4 * p + tq);
+            double ac[2][4][4];
+#pragma unroll
+            for (int mi = 0; mi < 2; ++mi)
+#pragma unroll
+                for (int ni = 0; ni < 4; ++ni)
+#pragma unroll
+                    for (int e = 0; e < 4; ++e) ac[mi][ni][e] = 0.0;
+#pragma unroll
+            for (int p = 0; p < 8; ++p) {
+                const int c = 32 * cb + 4 * p + tq;
+#pragma unroll
+                for (int mi = 0; mi < 2; ++mi) {
+                    const int r = 32 * rt + 16 * mi + g;
+                    const double a0 = S[xg_tb_idx(r, c)], a1 = S[xg_tb_idx(r + 8, c)];
+#pragma unroll
+                    for (int ni = 0; ni < 4; ++ni)
+                        xg_dmma_16x8x4(ac[mi][ni][0], ac[mi][ni][1], ac[mi][ni][2], ac[mi][ni][3], a0, a1, bl[p][ni]);
+                }
+            }
+#pragma unroll
+            for (int mi = 0; mi < 2; ++mi)
+#pragma unroll
+                for (int ni = 0; ni < 4; ++ni)
+#pragma unroll
+                    for (int h = 0; h < 2; ++h) {
+                        const int r = 32 * rt + 16 * mi + g + 8 * h, c = c0 + ni * 8 + 2 * tq;
+                        double2 *ps = reinterpret_cast<double2 *>(&S[xg_tb_idx(r, c)]);
+                        double2 v = *ps;
+                        v.x -= ac[mi][ni][2 * h];
+                        v.y -= ac[mi][ni][2 * h + 1];
+                        *ps = v;
+                    }
+        }
+    }
+    __syncthreads();
+}
+
+__global__ void __launch_bounds__(XG_G_THREADS, 1)
+    xg_trsm_gemm_kernel(const __grid_constant__ CUtensorMap map, XgTileArgs T, int k, double *v, int with_rhs,
+                        int *status)
+{
+    extern __shared__ __align__(1024) unsigned char xg_smem_raw[];
+    unsigned char *smem = (unsigned char *)(((uintptr_t)xg_smem_raw + 1023) & ~(uintptr_t)1023);
+    double *S = (double *)smem; /* aliases the GEMM ring, used between the GEMMs */
+    double *LDb = (double *)(smem + XG_G_STAGES * XG_G_STAGE_BYTES + 1024);
+    double *vacc = LDb + 2 * 32 * 33;
+    __shared__ int s_stop;
+    if (xg_cta_should_skip(status)) return;
+    const int ts = T.ts, nb = ts / XG_TB, tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    const int i = k + 1 + (int)blockIdx.x / nb, rb = (int)blockIdx.x % nb;
+    const long long slot_i = T.tile_off + xg_tile_index(i, k, T.nt), slot_k = T.tile_off + xg_tile_index(k, k, T.nt);
+    double *B = T.data + xg_slot64(T, i, k) * (long long)ts * ts + (long long)(rb * XG_TB) * ts;
+    const double *Lkk = T.data + xg_slot64(T, k, k) * (long long)ts * ts;
+    const double *vk = v + (long long)k * ts;
+    if (with_rhs)
+        for (int r = tid; r < XG_TB; r += blockDim.x) vacc[r] = 0.0;
+    for (int c = 0; c < nb; ++c) {
+        double *Bc = B + c * XG_TB;
+        if (c > 0) {
+            xg_gemm_core<true>(map, (int)(slot_i * ts + rb * XG_TB), (int)(slot_k * ts + c * XG_TB), 0,
+                               c * XG_TB / XG_G_BK, Bc, ts, status);
+            __syncthreads();
+            if (tid == 0) s_stop = *(volatile int *)status != 0;
+            __syncthreads();
+            if (s_stop) return;
+        }
+        /* stage T_c (this CTA's own stores, or the tile as the update left it) */
+        {
+            constexpr int U = 8;
+            for (int base = tid; base < XG_TB * XG_TB / 2; base += U * 256) {
+                double2 t[U];
+#pragma unroll
+                for (int u = 0; u < U; ++u) {
+                    const int idx = base + u * 256, r = idx >> 6, c2 = idx & 63;
+                    t[u] = __ldcg(reinterpret_cast<const double2 *>(Bc + (long long)r * ts) + c2);
+                }
+#pragma unroll
+                for (int u = 0; u < U; ++u) {
+                    const int idx = base + u * 256, r = idx >> 6, c2 = idx & 63;
+                    *reinterpret_cast<double2 *>(&S[xg_tb_idx(r, 2 * c2)]) = t[u];
+                }
+            }
+        }
+        xg_block_trsm128<true>(S, LDb, Lkk + (long long)(c * XG_TB) * ts + c * XG_TB, ts,
+                               T.dinv + (long long)(c * XG_TB) * 32);
+        /* X_c back to the tile; v_i -= X_c v_k[c block] (row sums per warp) */
+        for (int idx = tid; idx < XG_TB * XG_TB / 2; idx += 256) {
+            const int r = idx >> 6, c2 = idx & 63;
+            *(reinterpret_cast<double2 *>(Bc + (long long)r * ts) + c2) =
+                *reinterpret_cast<const double2 *>(&S[xg_tb_idx(r, 2 * c2)]);
+        }
+        if (with_rhs) {
+            for (int r = warp; r < XG_TB; r += 8) {
+                double sum = 0.0;
+                for (int cc = lane; cc < XG_TB; cc += 32) sum += S[xg_tb_idx(r, cc)] * __ldcg(vk + c * XG_TB + cc);
+                for (int off = 16; off > 0; off >>= 1) sum += __shfl_xor_sync(0xffffffffu, sum, off);
+                if (lane == 0) vacc[r] += sum;
+            }
+        }
+        __syncthreads(); /* S is read by everyone before the next GEMM's TMA writes the ring */
+    }
+    if (with_rhs) {
+        double *vi = v + (long long)i * ts + rb * XG_TB;
+        for (int r = tid; r < XG_TB; r += blockDim.x) vi[r] -= vacc[r];
+    }
+}
+
+static size_t xg_trsm_gemm_smem_bytes()
+{
+    return 1024 + XG_G_STAGES * XG_G_STAGE_BYTES + 1024 + (2 * 32 * 33 + XG_TB) * sizeof(double);
+}
+
+/* ========================================================================== */
 /* POTRF of a diagonal tile by 128 x 128 sub-blocks on several CTAs           */
 /* ========================================================================== */
 
@@ -1212,6 +1414,9 @@ cudaError_t xg_kernels_configure()
     if (e != cudaSuccess) return e;
     e = cudaFuncSetAttribute(xg_potrf_sub_gemm_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
                              (int)xg_gemm_smem_bytes());
+    if (e != cudaSuccess) return e;
+    e = cudaFuncSetAttribute(xg_trsm_gemm_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             (int)xg_trsm_gemm_smem_bytes());
     return e;
 }
 
@@ -1265,6 +1470,15 @@ void xg_launch_trsm_panel(const XgTileArgs &T, int k, double *v, int with_rhs, c
     if (n <= 0) return;
     xg_trsm_panel_kernel<<<n * (T.ts / XG_TRSM_SR), XG_TRSM_THREADS, xg_trsm_smem_bytes(T.ts), st>>>(T, k, v, with_rhs,
                                                                                                    status);
+}
+
+void xg_launch_trsm_gemm(const CUtensorMap &map, const XgTileArgs &T, int k, double *v, int with_rhs, int *status,
+                         cudaStream_t st)
+{
+    const int n = T.nt - k - 1;
+    if (n <= 0) return;
+    xg_trsm_gemm_kernel<<<n * (T.ts / XG_TB), XG_G_THREADS, xg_trsm_gemm_smem_bytes(), st>>>(map, T, k, v, with_rhs,
+                                                                                          status);
 }
 
 void xg_launch_syrk_gemm(const CUtensorMap &map, const XgTileArgs &T, int k, int *status, cudaStream_t st, int part)

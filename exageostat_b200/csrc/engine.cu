@@ -319,7 +319,10 @@ void xg_factor_lookahead(XgTileMatrix &M, double *v, double *part, int *status, 
         if (pev) cudaEventRecord(pev[5 * k], sp);
         xg_launch_potrf_tiled(M.map, T, k, v, part, part + M.nt, rhs, status, info, sp);
         if (pev) cudaEventRecord(pev[5 * k + 1], sp);
-        xg_launch_trsm_panel(T, k, v, rhs, status, sp);
+        if (T.dinv)
+            xg_launch_trsm_gemm(M.map, T, k, v, rhs, status, sp);
+        else
+            xg_launch_trsm_panel(T, k, v, rhs, status, sp);
         if (pev) cudaEventRecord(pev[5 * k + 2], sp);
         if (la) {
             cudaEventRecord(fs.ev_panel, sp);
@@ -1177,7 +1180,10 @@ static void xg_factor_sliced(XgField *f, double *v, const XgFactorStreams &fs)
         rec(j, 1, sp);
         xg_launch_potrf_tiled(M.map, T, j, v, f->part, f->part + nt, rhs, f->status, f->info, sp);
         rec(j, 2, sp);
-        xg_launch_trsm_panel(T, j, v, rhs, f->status, sp);
+        if (T.dinv)
+            xg_launch_trsm_gemm(M.map, T, j, v, rhs, f->status, sp);
+        else
+            xg_launch_trsm_panel(T, j, v, rhs, f->status, sp);
         if (j + 1 < nt) xg_launch_slice_panel(T, j, 0, sl->dig, sl->scale, plane, f->status, sp);
         rec(j, 3, sp);
         if (la) {

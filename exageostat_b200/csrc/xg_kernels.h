@@ -173,6 +173,10 @@ struct XgMixedMaps {
 cudaError_t xg_mixed_kernels_configure();
 void xg_launch_gen_mixed(const XgTileArgs &T, const int2 *tile_ij, long long ntiles, const double *x, const double *y,
                          int n, const XgMaternParams &p, int metric, cudaStream_t st);
+/* panel TRSM of column k by 128-column blocks (TMA-fed DMMA GEMMs and in-block
+ * solves with the inverted 32 x 32 diagonal blocks in T.dinv); ts a multiple of 128 */
+void xg_launch_trsm_gemm(const CUtensorMap &map, const XgTileArgs &T, int k, double *v, int with_rhs, int *status,
+                         cudaStream_t st);
 void xg_launch_trsm_panel32(const XgTileArgs &T, int k, double *v, int with_rhs, const int *status, cudaStream_t st);
 void xg_launch_panel_prep(const XgTileArgs &T, int k, double *p64, float *phi, float *plo, int passes,
                           const int *status, cudaStream_t st);
