@@ -1105,29 +1105,53 @@ static XgSlTask factor_task(int col, int k0, int k1)
 }
 
 /* SMs given to the panel chain of column j (last-chunk update, POTRF, TRSM,
- * slicing) while the split update of column j+1 runs on the others.  The
- * chain's work grows like nt - j and the split update's like j (nt - j), so
- * per column the chain needs about 8 / (8 + j) of the machine (measured
- * costs at tile 512: a TRSM strip of 32 rows ~63 us, a 128 x 128 job-chunk of
- * the update ~9 us); clamped to [XG_PANEL_SMS, sms - XG_PANEL_SMS]. */
+ * slicing) while the split update of column j+1 runs on the others: the
+ * smallest share s for which the chain, P + W_chain / s, is no longer than
+ * the update, W_upd / (sms - s).  Costs per SM in units of one tile-chunk of
+ * the sliced update (a 512 x 512 target tile times one panel chunk, ~0.16 ms
+ * on one SM): the last-chunk update 1 per tile, the TRSM of a tile
+ * XG_SHARE_TRSM (the 128-column-block kernel at ~56 % of the DMMA rate), the
+ * POTRF a latency of XG_SHARE_POTRF; W_upd = j (nt - j - 1).  With
+ * EXAGEOSTAT_B200_PANEL_K=K set, the older rule s = sms K / (K + j) is used
+ * instead.  Clamped to [XG_PANEL_MIN, sms - XG_PANEL_MIN]. */
+#define XG_SHARE_TRSM 6.2
+#define XG_SHARE_POTRF 4.7
+#define XG_PANEL_MIN 6
+
 static int xg_panel_k()
 {
     static int v = -1;
     if (v < 0) {
         const char *e = getenv("EXAGEOSTAT_B200_PANEL_K");
         v = e ? atoi(e) : 0;
-        if (v < 1 || v > 64) v = 8;
+        if (v < 1 || v > 64) v = 0;
     }
     return v;
 }
 
-static int xg_panel_share(int j, int sms)
+static int xg_panel_share(int j, int nt, int sms)
 {
-    const int K = xg_panel_k(); /* EXAGEOSTAT_B200_PANEL_K overrides the 8 */
-    int r = (int)((long long)sms * K / (K + j));
-    if (r < XG_PANEL_SMS) r = XG_PANEL_SMS;
-    if (r > sms - XG_PANEL_SMS) r = sms - XG_PANEL_SMS;
-    return r;
+    const int lo = XG_PANEL_MIN, hi = sms - XG_PANEL_MIN;
+    const int K = xg_panel_k();
+    if (K > 0) {
+        int r = (int)((long long)sms * K / (K + j));
+        return r < XG_PANEL_SMS ? XG_PANEL_SMS : (r > sms - XG_PANEL_SMS ? sms - XG_PANEL_SMS : r);
+    }
+    const double chain = (double)(nt - j) + XG_SHARE_TRSM * (nt - j - 1);
+    const double upd = (double)j * (nt - j - 1);
+    if (upd <= 0.0) return hi;
+    auto longer = [&](int s) { return XG_SHARE_POTRF + chain / s > upd / (sms - s); }; /* chain still longer */
+    if (!longer(lo)) return lo;
+    if (longer(hi)) return hi;
+    int a = lo, b = hi; /* longer(a), !longer(b) */
+    while (b - a > 1) {
+        const int m = (a + b) / 2;
+        if (longer(m))
+            a = m;
+        else
+            b = m;
+    }
+    return b;
 }
 
 /* How the SMs are divided between the panel chain and the split update.
@@ -1172,7 +1196,7 @@ static void xg_factor_sliced(XgField *f, double *v, const XgFactorStreams &fs)
         rec(j, 0, sp);
         if (la) {
             if (j >= 1) xg_launch_sliced(sl->map_a, sl->map_b, sl->scale, sl->scale, T, factor_task(j, j - 1, j), pr,
-                                         dyn ? all : xg_panel_share(j, sms), f->status, sp);
+                                         dyn ? all : xg_panel_share(j, nt, sms), f->status, sp);
         } else {
             xg_launch_sliced(sl->map_a, sl->map_b, sl->scale, sl->scale, T, factor_task(j, 0, j), pr, sms, f->status,
                              sp);
@@ -1193,7 +1217,7 @@ static void xg_factor_sliced(XgField *f, double *v, const XgFactorStreams &fs)
             rec(j, 4, fs.st);
             if (j >= 1 && j + 1 < nt)
                 xg_launch_sliced(sl->map_a, sl->map_b, sl->scale, sl->scale, T, factor_task(j + 1, 0, j), pr,
-                                 dyn ? all : sms - xg_panel_share(j, sms), f->status, fs.st);
+                                 dyn ? all : sms - xg_panel_share(j, nt, sms), f->status, fs.st);
             rec(j, 5, fs.st);
             cudaEventRecord(sl->ev_a, fs.st);
         } else {
