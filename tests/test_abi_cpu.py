@@ -77,6 +77,29 @@ def test_device_bessel_code_compiled_for_host_matches_mpmath(tmp_path):
     assert max(rel) < 1e-14, max(rel)
 
 
+def test_device_matern_element_compiled_for_host_matches_mpmath(tmp_path):
+    """The Matern element of the covariance generators (xg_matern_general:
+    Temme's series with the order constants and r^nu from its own power for
+    r <= 2, the trapezoidal rule, the asymptotic expansion for r >= 20),
+    compiled for the host, against mpmath's r^nu K_nu(r) on a grid of orders
+    and distances that crosses every branch boundary."""
+    mpmath = pytest.importorskip("mpmath")
+    mpmath.mp.dps = 30
+    src = tmp_path / "m.cpp"
+    src.write_text('#include <cstdio>\n#include "kbessel.cuh"\nint main(){double a,b;'
+                   'while(scanf("%lf %lf",&a,&b)==2)printf("%.17g\\n",xg_matern_general(b,a,1.0));}\n')
+    exe = tmp_path / "m"
+    subprocess.run(["g++", "-O2", "-I", os.path.join(ROOT, "exageostat_b200", "csrc"), str(src), "-o", str(exe)],
+                   check=True)
+    pts = [(nu, float(r)) for nu in (0.01, 0.3, 0.5, 0.73, 1.0, 1.37, 2.5, 3.3, 4.99, 5.0, 5.5)
+           for r in list(np.geomspace(1e-4, 2.0, 9)) + [2.0000001, 3.0, 7.0, 12.5, 19.99, 20.0, 20.01, 25.0, 40.0,
+                                                         80.0, 200.0]]
+    out = subprocess.run([str(exe)], input="\n".join("%r %r" % p for p in pts), capture_output=True, text=True,
+                         check=True).stdout.split()
+    rel = [abs(float(v) / float(mpmath.power(r, nu) * mpmath.besselk(nu, r)) - 1.0) for (nu, r), v in zip(pts, out)]
+    assert len(rel) == len(pts) and max(rel) < 2e-14, max(rel)
+
+
 def test_product_fails_loudly_without_library(xg, monkeypatch):
     monkeypatch.setattr(xg, "_lib", None)
     monkeypatch.setattr(xg, "LIB_PATH", "/nonexistent/libexageostat_b200.so")
