@@ -1006,9 +1006,13 @@ __device__ __forceinline__ void xg_block_trsm128(double *S, double *LDb, const d
     __syncthreads();
 }
 
-__global__ void __launch_bounds__(XG_G_THREADS, 1)
-    xg_trsm_gemm_kernel(const __grid_constant__ CUtensorMap map, XgTileArgs T, int k, double *v, int with_rhs,
-                        int *status)
+/* The TRSM of the 128-row block rb of panel tile (i, k); called by all 256
+ * threads of a CTA after its status check.  Returns false (CTA-uniformly)
+ * when a GEMM wait timed out.  Under the device scheduler (COH) the tiles and
+ * inverses were written by other CTAs of the launch. */
+template <bool COH>
+__device__ __forceinline__ bool xg_trsm_gemm_body(const CUtensorMap &map, const XgTileArgs &T, int k, int i, int rb,
+                                                  double *v, int with_rhs, int *status)
 {
     extern __shared__ __align__(1024) unsigned char xg_smem_raw[];
     unsigned char *smem = (unsigned char *)(((uintptr_t)xg_smem_raw + 1023) & ~(uintptr_t)1023);
@@ -1016,9 +1020,7 @@ __global__ void __launch_bounds__(XG_G_THREADS, 1)
     double *LDb = (double *)(smem + XG_G_STAGES * XG_G_STAGE_BYTES + 1024);
     double *vacc = LDb + 2 * 32 * 33;
     __shared__ int s_stop;
-    if (xg_cta_should_skip(status)) return;
     const int ts = T.ts, nb = ts / XG_TB, tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-    const int i = k + 1 + (int)blockIdx.x / nb, rb = (int)blockIdx.x % nb;
     const long long slot_i = T.tile_off + xg_tile_index(i, k, T.nt), slot_k = T.tile_off + xg_tile_index(k, k, T.nt);
     double *B = T.data + xg_slot64(T, i, k) * (long long)ts * ts + (long long)(rb * XG_TB) * ts;
     const double *Lkk = T.data + xg_slot64(T, k, k) * (long long)ts * ts;
@@ -1033,9 +1035,9 @@ __global__ void __launch_bounds__(XG_G_THREADS, 1)
             __syncthreads();
             if (tid == 0) s_stop = *(volatile int *)status != 0;
             __syncthreads();
-            if (s_stop) return;
+            if (s_stop) return false;
         }
-        /* stage T_c (this CTA's own stores, or the tile as the update left it) */
+        /* stage T_c (this CTA's own stores, or the tile as the updates left it) */
         {
             constexpr int U = 8;
             for (int base = tid; base < XG_TB * XG_TB / 2; base += U * 256) {
@@ -1052,8 +1054,8 @@ __global__ void __launch_bounds__(XG_G_THREADS, 1)
                 }
             }
         }
-        xg_block_trsm128<true>(S, LDb, Lkk + (long long)(c * XG_TB) * ts + c * XG_TB, ts,
-                               T.dinv + (long long)(c * XG_TB) * 32);
+        xg_block_trsm128<COH>(S, LDb, Lkk + (long long)(c * XG_TB) * ts + c * XG_TB, ts,
+                              T.dinv + (long long)(c * XG_TB) * 32);
         /* X_c back to the tile; v_i -= X_c v_k[c block] (row sums per warp) */
         for (int idx = tid; idx < XG_TB * XG_TB / 2; idx += 256) {
             const int r = idx >> 6, c2 = idx & 63;
@@ -1072,8 +1074,18 @@ __global__ void __launch_bounds__(XG_G_THREADS, 1)
     }
     if (with_rhs) {
         double *vi = v + (long long)i * ts + rb * XG_TB;
-        for (int r = tid; r < XG_TB; r += blockDim.x) vi[r] -= vacc[r];
+        for (int r = tid; r < XG_TB; r += blockDim.x) vi[r] = xg_ldt<COH>(vi + r) - vacc[r];
     }
+    return true;
+}
+
+__global__ void __launch_bounds__(XG_G_THREADS, 1)
+    xg_trsm_gemm_kernel(const __grid_constant__ CUtensorMap map, XgTileArgs T, int k, double *v, int with_rhs,
+                        int *status)
+{
+    if (xg_cta_should_skip(status)) return;
+    const int nb = T.ts / XG_TB;
+    xg_trsm_gemm_body<false>(map, T, k, k + 1 + (int)blockIdx.x / nb, (int)blockIdx.x % nb, v, with_rhs, status);
 }
 
 static size_t xg_trsm_gemm_smem_bytes()
@@ -1295,9 +1307,11 @@ __global__ void __launch_bounds__(XG_G_THREADS, 1)
                     T.dinv = D;
                 }
                 __syncthreads();
-                const int strips = ts / XG_TRSM_SR;
-                for (int sp = 0; sp < strips; ++sp)
-                    xg_trsm_body<true>(T, k, v + fd.vec_off, 1, stf, (long long)(i - k - 1) * strips + sp);
+                /* the tile's 128-row blocks one after the other (xg_trsm_gemm_body;
+                 * a field that has failed skips them uniformly) */
+                if (!xg_cta_should_skip(stf))
+                    for (int rb = 0; rb < ts / XG_TB; ++rb)
+                        if (!xg_trsm_gemm_body<true>(map, T, k, i, rb, v + fd.vec_off, 1, stf)) break;
             } else {
                 const int bpt = ts / XG_G_BM;
                 for (int b = 0; b < bpt * bpt; ++b)
@@ -1319,7 +1333,8 @@ __global__ void __launch_bounds__(XG_G_THREADS, 1)
 
 static size_t xg_sched_smem_bytes(int ts)
 {
-    size_t b = xg_gemm_smem_bytes();
+    size_t b = xg_trsm_gemm_smem_bytes();
+    b = b > xg_gemm_smem_bytes() ? b : xg_gemm_smem_bytes();
     b = b > xg_potrf_smem_bytes(ts) ? b : xg_potrf_smem_bytes(ts);
     b = b > xg_trsm_smem_bytes(ts) ? b : xg_trsm_smem_bytes(ts);
     return b;
