@@ -163,7 +163,8 @@ def fit_trust_region(loglik_grad, theta0, lb, ub, max_iter=60, gtol=1e-3, delta0
     history) with one (theta, f) pair per accepted step.  state (a dict, may
     be None): state["B"], when present, is the initial Hessian model in phi,
     and receives the final one; state["stop"] receives the stop reason
-    ("gtol", "stall", "radius" or "max_iter")."""
+    ("gtol", "stall", "radius" or "max_iter"), state["gphi"] the final
+    gradient in phi and state["updates"] the number of BFGS updates."""
     lb = np.asarray(lb, dtype=np.float64)
     ub = np.asarray(ub, dtype=np.float64)
     th = np.clip(np.asarray(theta0, dtype=np.float64), lb, ub)
@@ -188,6 +189,7 @@ def fit_trust_region(loglik_grad, theta0, lb, ub, max_iter=60, gtol=1e-3, delta0
     B = -np.eye(n) * max(np.max(np.abs(gphi)) / delta0, 1.0)
     first_update = True
     stalls = 0
+    updates = 0
     if state is not None and state.get("B") is not None:
         B = np.array(state["B"], dtype=np.float64)
         first_update = False
@@ -227,6 +229,7 @@ def fit_trust_region(loglik_grad, theta0, lb, ub, max_iter=60, gtol=1e-3, delta0
                     first_update = False
                 Bs = B @ s
                 B = B - np.outer(Bs, Bs) / (s @ Bs) + np.outer(y, y) / sy
+                updates += 1
         if rho > 1.25 and np.linalg.norm(d) < 0.8 * delta:
             # an interior step that gained more than the model promised: the
             # model is too curved along it (the flat ridge); halve it so the
@@ -255,6 +258,7 @@ def fit_trust_region(loglik_grad, theta0, lb, ub, max_iter=60, gtol=1e-3, delta0
         state["B"] = B
         state["gphi"] = gphi
         state["stop"] = stop
+        state["updates"] = updates
     return np.exp(phi), f, evals, history
 
 
@@ -337,13 +341,29 @@ def value_newton_polish(loglik, theta, B, lb, ub, signal=1e-2, rounds=2):
     return np.exp(phi), f0, evals
 
 
-def fit_mixed(session, lb, ub, theta0=None, gtol=0.1, ftol=1e-4, log=None):
+def _newton_step_size(state):
+    """max |d log theta| of the Newton step -B^-1 g of the trust region's
+    final model; inf when the model is singular or has seen fewer BFGS
+    updates than twice the parameters (a model that has not learned the flat
+    ridge misjudges the step along it)."""
+    if state.get("updates", 0) < 2 * len(state.get("gphi", ())):
+        return np.inf
+    try:
+        return float(np.max(np.abs(np.linalg.solve(state["B"], state["gphi"]))))
+    except (np.linalg.LinAlgError, KeyError, TypeError):
+        return np.inf
+
+
+def fit_mixed(session, lb, ub, theta0=None, gtol=0.1, ftol=1e-4, log=None, newton_tol=5e-4):
     """Mixed-precision adjoint-gradient MLE, entirely on the INT8-sliced
     objective (precision 3): a start from start_point (unless theta0 is
     given), the trust-region maximiser driven by the sliced adjoint gradient
-    (stopping at gtol / ftol, the noise level of that gradient), then, unless
-    the gradient itself reached gtol, value_newton_polish with sliced
-    log-likelihood values.  Leaves the session in
+    (stopping at gtol / ftol, the noise level of that gradient), then
+    value_newton_polish with sliced log-likelihood values -- skipped when the
+    gradient itself reached gtol and the Newton step of the trust region's
+    model (learned over at least 2 n BFGS updates) would move log theta by
+    at most newton_tol: along a flat ridge a gradient at its noise level can
+    still leave theta 1e-3 away.  Leaves the session in
     FP64.  Returns (theta_hat, loglik, sliced evaluations (log-likelihood and
     gradient), sliced log-likelihood-only evaluations, theta after the
     gradient stage)."""
@@ -358,8 +378,9 @@ def fit_mixed(session, lb, ub, theta0=None, gtol=0.1, ftol=1e-4, log=None):
                                        log=log, state=st)
     if log:
         log("sliced gradient stage: %d evaluations, theta %s, loglik %.12g" % (ev1, list(th1), f1))
-    if st["stop"] == "gtol":
-        # the sliced gradient itself reached the optimum to its noise level
+    if st["stop"] == "gtol" and _newton_step_size(st) <= newton_tol:
+        # the sliced gradient reached the optimum to its noise level and the
+        # model's Newton step from there moves theta by less than newton_tol
         th, f, ne2 = th1, f1, 0
     else:
         th, f, ne2 = value_newton_polish(lambda t: session.loglik(t), th1, st["B"], lb, ub)

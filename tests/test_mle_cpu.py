@@ -53,3 +53,68 @@ def test_newton_polish_treats_failing_evaluations_as_minus_infinity():
     assert f >= guarded(opt * np.array([1.02, 1.01, 1.0]))[0]
     th2, f2, ev2 = newton_polish(guarded, opt * np.array([1.0, 1.0, 1.01]), lb, ub)
     assert f2 == -np.inf and ev2 == 1
+
+
+def _ridge2(th):
+    """A ridge with the curvatures of a Matern likelihood near its optimum
+    (across the ridge 2000, along it 20, in nu 200, in log theta): a gradient
+    stop at |g| = 0.1 leaves theta ~3e-3 along the ridge."""
+    s, b, n = th
+    u = np.log(s) - 2 * np.log(b) - 1.0
+    v = np.log(b) + 2.0
+    w = np.log(n / 0.5)
+    f = -2000 * u * u - 20 * v * v - 200 * w * w
+    g = np.array([-4000 * u / s, (8000 * u - 40 * v) / b, -400 * w / n])
+    return f, g
+
+
+class _FakeSession:
+    """The calls fit_mixed makes of a Session, on _ridge2 (no GPU)."""
+
+    def __init__(self):
+        self.values = 0
+
+    def set_sliced(self):
+        pass
+
+    def set_fp64(self):
+        pass
+
+    def z(self):
+        return np.array([1.0, -1.0])
+
+    def loglik(self, th, grad=False):
+        f, g = _ridge2(np.asarray(th, dtype=float))
+        if grad:
+            return f, g
+        self.values += 1
+        return f
+
+
+def test_fit_mixed_polishes_along_a_flat_ridge_after_a_loose_gradient_stop():
+    """A gradient stop at the loose tolerance of the sliced gradient can leave
+    theta ~3e-3 along the flat ridge: the trust region's Newton step says so,
+    the value-based polish runs and lands on the optimum."""
+    from exageostat_b200.mle import fit_mixed
+
+    lb, ub = [0.01] * 3, [5.0] * 3
+    b0 = np.exp(-2.0)
+    opt = np.array([np.e * b0 * b0, b0, 0.5])
+    th, f, ev, nvals, th1 = fit_mixed(_FakeSession(), lb, ub, theta0=opt * np.array([1.8, 0.7, 1.4]), gtol=0.1)
+    assert np.max(np.abs(th1 - opt) / opt) > 1e-3
+    assert nvals > 0 and np.max(np.abs(th - opt) / opt) < 1e-6
+
+
+def test_fit_mixed_skips_the_polish_when_the_newton_step_is_tiny():
+    """A gradient stop whose learned model puts the optimum within 5e-4 in log
+    theta spends no polish values; a stop before the model has seen 2 n
+    updates always polishes."""
+    from exageostat_b200.mle import fit_mixed
+
+    lb, ub = [0.01] * 3, [5.0] * 3
+    b0 = np.exp(-2.0)
+    opt = np.array([np.e * b0 * b0, b0, 0.5])
+    th, f, ev, nvals, th1 = fit_mixed(_FakeSession(), lb, ub, theta0=opt * np.array([1.3, 1.14, 1.0]), gtol=0.1)
+    assert nvals == 0 and np.array_equal(th, th1) and np.max(np.abs(th - opt) / opt) < 1e-4
+    th, f, ev, nvals, th1 = fit_mixed(_FakeSession(), lb, ub, theta0=opt * (1 + 1e-6), gtol=0.1)
+    assert ev == 1 and nvals > 0
