@@ -236,7 +236,7 @@ def measured_dgemm_tflops(torch):
 
 
 def peak_bf16_tflops():
-    """Measured dense bf16 peak from MEASURED_PEAKS.json (driver-written), if present."""
+    """Measured dense bf16 peak from MEASURED_PEAKS.json, if present."""
     p = os.path.join(ROOT, "MEASURED_PEAKS.json")
     try:
         with open(p) as f:
