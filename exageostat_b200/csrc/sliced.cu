@@ -44,14 +44,6 @@
  *                           epilogue (FP64 combine per chunk into 64 sums per thread,
  *                           one C -= update per job); setmaxnreg moves the registers of
  *                           warpgroup 0 to the epilogue.
- *                           The four levels fill TMEM, so each chunk runs in two MMA
- *                           passes over K: levels 0-1 (the pairs (0,0), (0,1), (1,0),
- *                           digits 0-1 only), then levels 2-3 (the other seven pairs).
- *                           The epilogue reads levels 0-1 while the second pass runs and
- *                           levels 2-3 while the next chunk's first pass runs, releasing
- *                           each pair of levels (its own mbarrier) as soon as it is read,
- *                           so the TMEM reads hide under the MMAs; digits 0-1 cross from
- *                           L2 twice per chunk (1.5x the operand bytes).
  *                           The MMA computes the transposed block so that a TMEM lane
  *                           holds a column of C and the accesses to C are coalesced.
  */
@@ -73,10 +65,10 @@
  * 128 x 40 + 256 x 232 = 64,512 */
 #define XG_SL_REG_LOW 40
 #define XG_SL_REG_HIGH 232
-#define XG_SL_STAGES 6
-#define XG_SL_ABOX_BYTES (XG_SL_BM * XG_SL_BK)                 /* one digit plane, 128 rows */
-#define XG_SL_BBOX_BYTES (XG_SL_BN * XG_SL_BK)                 /* one digit plane, 128 rows */
-#define XG_SL_STAGE_BYTES (2 * (XG_SL_ABOX_BYTES + XG_SL_BBOX_BYTES)) /* two digit planes of A and B: 32 KB */
+#define XG_SL_STAGES 3
+#define XG_SL_ABOX_BYTES (XG_SL_BM * XG_SL_BK)                                  /* one digit plane, 128 rows */
+#define XG_SL_BBOX_BYTES (XG_SL_BN * XG_SL_BK)                                  /* one digit plane, 128 rows */
+#define XG_SL_STAGE_BYTES (XG_SL_SLICES * (XG_SL_ABOX_BYTES + XG_SL_BBOX_BYTES)) /* 64 KB */
 /* per panel chunk, the 128 A-row and 128 B-row scales, double-buffered */
 #define XG_SL_SCALE_BYTES (2 * 2 * 128 * 8)
 #define XG_SL_SMEM (XG_SL_STAGES * XG_SL_STAGE_BYTES + XG_SL_SCALE_BYTES + 1024 + 256)
@@ -240,9 +232,9 @@ __global__ void __launch_bounds__(XG_SL_THREADS, 1)
     double *sscale = (double *)(smem + XG_SL_STAGES * XG_SL_STAGE_BYTES); /* [2][A 128 | B 128] */
     uint64_t *full = (uint64_t *)(smem + XG_SL_STAGES * XG_SL_STAGE_BYTES + XG_SL_SCALE_BYTES);
     uint64_t *empty = full + XG_SL_STAGES;
-    uint64_t *acc_full = empty + XG_SL_STAGES; /* [2]: levels 0-1 / 2-3 of a chunk are complete */
-    uint64_t *acc_empty = acc_full + 2;        /* [2]: the epilogue has read them */
-    uint64_t *drain = acc_empty + 2;
+    uint64_t *acc_full = empty + XG_SL_STAGES;
+    uint64_t *acc_empty = acc_full + 1;
+    uint64_t *drain = acc_empty + 1;
     uint64_t *sfull = drain + 1;  /* [2] the chunk's row scales have landed */
     uint64_t *sempty = sfull + 2; /* [2] the epilogue is done with them */
     uint32_t *tmem_slot = (uint32_t *)(sempty + 2);
@@ -254,13 +246,13 @@ __global__ void __launch_bounds__(XG_SL_THREADS, 1)
             xg_mbar_init(&full[s], 1);
             xg_mbar_init(&empty[s], 1);
         }
+        xg_mbar_init(acc_full, 1);
+        xg_mbar_init(acc_empty, XG_SL_EPI_WARPS);
+        xg_mbar_init(drain, 1);
         for (int b = 0; b < 2; ++b) {
-            xg_mbar_init(&acc_full[b], 1);
-            xg_mbar_init(&acc_empty[b], XG_SL_EPI_WARPS);
             xg_mbar_init(&sfull[b], 1);
             xg_mbar_init(&sempty[b], XG_SL_EPI_WARPS);
         }
-        xg_mbar_init(drain, 1);
         xg_fence_barrier_init();
     }
     if (warp == 1) xg_tmem_alloc(tmem_slot, 512); /* four 128-lane x 128-column S32 levels */
@@ -276,29 +268,11 @@ __global__ void __launch_bounds__(XG_SL_THREADS, 1)
     if (warp == 0) {
         /* ---- TMA producer: per panel chunk the 128 + 128 row scales of the
          * job's A and B blocks (one bulk copy each, into a double buffer the
-         * epilogue reads), then pass 1: per K slab a stage with digits 0-1 of
-         * A and B; pass 2: per K slab a stage with digits 0-1 and one with
-         * digits 2-3 ---- */
+         * epilogue reads), then per stage the four A and four B digit boxes ---- */
         if (lane == 0) {
             xg_prefetch_tensormap(&map_a);
             xg_prefetch_tensormap(&map_b);
             long long it = 0, cs = 0;
-            auto load_stage = [&](int kb, int d0, int rowA, int rowB) -> bool {
-                const int s = (int)(it % XG_SL_STAGES);
-                if (it >= XG_SL_STAGES && !xg_mbar_wait(&empty[s], (uint32_t)((it / XG_SL_STAGES) - 1) & 1))
-                    return false;
-                unsigned char *st = smem + s * XG_SL_STAGE_BYTES;
-                xg_mbar_arrive_expect_tx(&full[s], XG_SL_STAGE_BYTES);
-#pragma unroll
-                for (int t = 0; t < 2; ++t) {
-                    xg_tma_load_2d(st + t * XG_SL_ABOX_BYTES, &map_a, kb * XG_SL_BK, (d0 + t) * plane_rows + rowA,
-                                   &full[s]);
-                    xg_tma_load_2d(st + 2 * XG_SL_ABOX_BYTES + t * XG_SL_BBOX_BYTES, &map_b, kb * XG_SL_BK,
-                                   (d0 + t) * plane_rows + rowB, &full[s]);
-                }
-                ++it;
-                return true;
-            };
             for (long long job = blockIdx.x; job < njobs && ok; job += gridDim.x) {
                 XgSlJob J;
                 if (!xg_sl_job(S, job, nt, ts, J)) continue;
@@ -318,8 +292,23 @@ __global__ void __launch_bounds__(XG_SL_THREADS, 1)
                         xg_bulk_load(sscale + sb * 256 + 128, scale_b + slot_b * ts + J.bn * XG_SL_BN, XG_SL_BN * 8,
                                      &sfull[sb]);
                     }
-                    for (int kb = 0; kb < KT && ok; ++kb) ok = load_stage(kb, 0, rowA, rowB);
-                    for (int kb = 0; kb < KT && ok; ++kb) ok = load_stage(kb, 0, rowA, rowB) && load_stage(kb, 2, rowA, rowB);
+                    for (int kb = 0; kb < KT; ++kb, ++it) {
+                        const int s = (int)(it % XG_SL_STAGES);
+                        if (it >= XG_SL_STAGES &&
+                            !xg_mbar_wait(&empty[s], (uint32_t)((it / XG_SL_STAGES) - 1) & 1)) {
+                            ok = false;
+                            break;
+                        }
+                        unsigned char *st = smem + s * XG_SL_STAGE_BYTES;
+                        xg_mbar_arrive_expect_tx(&full[s], XG_SL_STAGE_BYTES);
+#pragma unroll
+                        for (int t = 0; t < XG_SL_SLICES; ++t) {
+                            xg_tma_load_2d(st + t * XG_SL_ABOX_BYTES, &map_a, kb * XG_SL_BK, t * plane_rows + rowA,
+                                           &full[s]);
+                            xg_tma_load_2d(st + XG_SL_SLICES * XG_SL_ABOX_BYTES + t * XG_SL_BBOX_BYTES, &map_b,
+                                           kb * XG_SL_BK, t * plane_rows + rowB, &full[s]);
+                        }
+                    }
                 }
             }
             if (!ok) atomicOr(status, XG_ST_TIMEOUT);
@@ -330,102 +319,50 @@ __global__ void __launch_bounds__(XG_SL_THREADS, 1)
             for (long long q = cs > 2 ? cs - 2 : 0; q < cs; ++q) xg_mbar_wait(&sfull[q & 1], (uint32_t)(q >> 1) & 1);
         }
     } else if (warp == 1) {
-        /* ---- MMA issuer: per (job, panel chunk) pass 1 accumulates the digit
-         * pairs of levels 0-1, pass 2 those of levels 2-3, each pass behind
-         * the epilogue's release of the same two levels of the previous chunk ---- */
+        /* ---- MMA issuer: one accumulation (4 levels) per (job, panel chunk) ---- */
         if (lane == 0) {
             constexpr uint32_t idesc = xg_idesc_i8(XG_SL_BN, XG_SL_BM); /* M = 128 (C columns), N = 128 (C rows) */
             const uint32_t sbase = xg_smem_u32(smem);
             long long it = 0, cc = 0;
-            auto take = [&](uint32_t &sa) -> bool { /* next stage: wait until it landed */
-                const int s = (int)(it % XG_SL_STAGES);
-                if (!xg_mbar_wait(&full[s], (uint32_t)(it / XG_SL_STAGES) & 1)) return false;
-                xg_tc_fence_after();
-                sa = sbase + s * XG_SL_STAGE_BYTES;
-                return true;
-            };
-            auto release = [&]() {
-                xg_umma_commit(&empty[it % XG_SL_STAGES]);
-                ++it;
-            };
             for (long long job = blockIdx.x; job < njobs && ok; job += gridDim.x) {
                 XgSlJob J;
                 if (!xg_sl_job(S, job, nt, ts, J)) continue;
                 for (int k = J.k0; k < J.k1 && ok; ++k, ++cc) {
-                    /* pass 1: levels 0 (0,0) and 1 (0,1), (1,0) */
-                    if (cc >= 1 && !xg_mbar_wait(&acc_empty[0], (uint32_t)(cc - 1) & 1)) {
+                    if (cc >= 1 && !xg_mbar_wait(acc_empty, (uint32_t)(cc - 1) & 1)) {
                         ok = false;
                         break;
                     }
                     xg_tc_fence_after();
-                    for (int kb = 0; kb < KT; ++kb) {
-                        uint32_t sa;
-                        if (!take(sa)) {
+                    const uint32_t dt = tmem;
+                    for (int kb = 0; kb < KT; ++kb, ++it) {
+                        const int s = (int)(it % XG_SL_STAGES);
+                        if (!xg_mbar_wait(&full[s], (uint32_t)(it / XG_SL_STAGES) & 1)) {
                             ok = false;
                             break;
                         }
-                        const uint32_t sb = sa + 2 * XG_SL_ABOX_BYTES;
+                        xg_tc_fence_after();
+                        const uint32_t sa = sbase + s * XG_SL_STAGE_BYTES;
+                        const uint32_t sb = sa + XG_SL_SLICES * XG_SL_ABOX_BYTES;
 #pragma unroll
                         for (int kk = 0; kk < XG_SL_BK / 32; ++kk) {
-                            const uint32_t acc = (kb | kk) != 0;
-                            const uint64_t a0 = xg_umma_desc_sw64(sa + kk * 32), a1 = xg_umma_desc_sw64(sa + XG_SL_ABOX_BYTES + kk * 32);
-                            const uint64_t b0 = xg_umma_desc_sw64(sb + kk * 32), b1 = xg_umma_desc_sw64(sb + XG_SL_BBOX_BYTES + kk * 32);
-                            /* the transposed block E_b D_a^T: TMEM lane = column of C, TMEM column = row of C */
-                            xg_umma_i8(tmem, b0, a0, idesc, acc);
-                            xg_umma_i8(tmem + XG_SL_BM, b1, a0, idesc, acc);
-                            xg_umma_i8(tmem + XG_SL_BM, b0, a1, idesc, 1);
-                        }
-                        release();
-                    }
-                    if (!ok) break;
-                    xg_umma_commit(&acc_full[0]);
-                    /* pass 2: level 2 (0,2), (1,1), (2,0) and level 3 (0,3), (1,2), (2,1), (3,0) */
-                    if (cc >= 1 && !xg_mbar_wait(&acc_empty[1], (uint32_t)(cc - 1) & 1)) {
-                        ok = false;
-                        break;
-                    }
-                    xg_tc_fence_after();
-                    for (int kb = 0; kb < KT; ++kb) {
-                        uint32_t s01, s23;
-                        if (!take(s01)) {
-                            ok = false;
-                            break;
-                        }
-                        const long long it01 = it;
-                        ++it; /* the digit 2-3 stage follows */
-                        if (!take(s23)) {
-                            ok = false;
-                            break;
-                        }
-                        uint32_t ad[4], bd[4];
-                        ad[0] = s01;
-                        ad[1] = s01 + XG_SL_ABOX_BYTES;
-                        ad[2] = s23;
-                        ad[3] = s23 + XG_SL_ABOX_BYTES;
-                        bd[0] = s01 + 2 * XG_SL_ABOX_BYTES;
-                        bd[1] = bd[0] + XG_SL_BBOX_BYTES;
-                        bd[2] = s23 + 2 * XG_SL_ABOX_BYTES;
-                        bd[3] = bd[2] + XG_SL_BBOX_BYTES;
+                            /* K = 32 int8 = 32 bytes per MMA inside the 64-byte swizzled row */
 #pragma unroll
-                        for (int kk = 0; kk < XG_SL_BK / 32; ++kk) {
-                            const uint32_t acc = (kb | kk) != 0;
-                            const uint32_t t2 = tmem + 2 * XG_SL_BM, t3 = tmem + 3 * XG_SL_BM;
-#define XG_SL_MMA(lvl_t, a, b, accf)                                                                                   \
-    xg_umma_i8(lvl_t, xg_umma_desc_sw64(bd[b] + kk * 32), xg_umma_desc_sw64(ad[a] + kk * 32), idesc, accf)
-                            XG_SL_MMA(t2, 0, 2, acc);
-                            XG_SL_MMA(t2, 1, 1, 1);
-                            XG_SL_MMA(t2, 2, 0, 1);
-                            XG_SL_MMA(t3, 0, 3, acc);
-                            XG_SL_MMA(t3, 1, 2, 1);
-                            XG_SL_MMA(t3, 2, 1, 1);
-                            XG_SL_MMA(t3, 3, 0, 1);
-#undef XG_SL_MMA
+                            for (int p = 0; p < 10; ++p) {
+                                int a, b;
+                                xg_sl_pair(p, a, b);
+                                const uint64_t ad = xg_umma_desc_sw64(sa + a * XG_SL_ABOX_BYTES + kk * 32);
+                                const uint64_t bd = xg_umma_desc_sw64(sb + b * XG_SL_BBOX_BYTES + kk * 32);
+                                const bool starts = (p == 0 || p == 1 || p == 3 || p == 6);
+                                /* the transposed block E_b D_a^T: TMEM lane = column of
+                                 * C, TMEM column = row of C */
+                                xg_umma_i8(dt + (uint32_t)((a + b) * XG_SL_BM), bd, ad, idesc,
+                                           (kb | kk) != 0 || !starts);
+                            }
                         }
-                        xg_umma_commit(&empty[it01 % XG_SL_STAGES]);
-                        release();
+                        xg_umma_commit(&empty[s]);
                     }
                     if (!ok) break;
-                    xg_umma_commit(&acc_full[1]);
+                    xg_umma_commit(acc_full);
                 }
             }
             if (!ok) atomicOr(status, XG_ST_TIMEOUT);
@@ -438,10 +375,8 @@ __global__ void __launch_bounds__(XG_SL_THREADS, 1)
         /* ---- epilogue: warps 4-11.  Thread (quarter q = warp % 4, lane l) owns
          * C column 32 q + l of the job's block (TMEM lane 32 q + l) and the 64
          * rows h * 64 .. + 63, h = (warp - 4) / 4 (TMEM columns of each level).
-         * Per chunk k it adds s_A(row) s_B(col) 254^-3 (254^2 hi + lo) to 64
-         * FP64 sums: hi = L0 254 + L1 as soon as levels 0-1 are complete (then
-         * they are released to the next chunk's first pass), lo = L2 254 + L3
-         * once levels 2-3 are; after the last chunk C -= sums. ---- */
+         * Per chunk k it adds s_A(row) s_B(col) sum_t 254^-t level_t to 64 FP64
+         * sums; after the last chunk C -= sums. ---- */
         const int q = warp & 3, h = (warp - 4) >> 2;
         long long cc = 0;
         for (long long job = blockIdx.x; job < njobs && ok; job += gridDim.x) {
@@ -460,91 +395,73 @@ __global__ void __launch_bounds__(XG_SL_THREADS, 1)
                 asm volatile("prefetch.global.L2 [%0];" ::"l"(pf + ts));
                 asm volatile("prefetch.global.L2 [%0];" ::"l"(pf + ts + 16));
             }
-            const uint32_t base = tmem + ((uint32_t)(q * 32) << 16) + (uint32_t)(h * 64);
             double res[64];
 #pragma unroll
             for (int u = 0; u < 64; ++u) res[u] = 0.0;
             for (int k = J.k0; k < J.k1; ++k, ++cc) {
                 const int sb = (int)(cc & 1);
-                if (!xg_mbar_wait(&sfull[sb], (uint32_t)(cc >> 1) & 1) ||
-                    !xg_mbar_wait(&acc_full[0], (uint32_t)cc & 1)) {
+                if (!xg_mbar_wait(&sfull[sb], (uint32_t)(cc >> 1) & 1) || !xg_mbar_wait(acc_full, (uint32_t)cc & 1)) {
                     if (lane == 0) atomicOr(status, XG_ST_TIMEOUT);
                     ok = false;
                     break;
                 }
                 xg_tc_fence_after();
-                /* s_B (this thread's column) with 254^-3 and the sign folded in;
-                 * the row scales come from the shared-memory copy the producer
-                 * staged for this chunk */
+                /* s_B (this thread's column) with 254^-3 folded in: the levels are
+                 * combined as the exact integer v = L0 254^3 + L1 254^2 + L2 254 + L3
+                 * (|v| < 2^48) and converted once.  The row scales come from the
+                 * shared-memory copy the producer staged for this chunk. */
                 const double sc = sscale[sb * 256 + 128 + q * 32 + lane] * (S.sign * XG_SL_INV_RADIX3);
-                const double sc_hi = sc * 64516.0; /* 254^2, exact */
                 const double2 *sr2 = reinterpret_cast<const double2 *>(sscale + sb * 256 + h * 64);
-                /* levels 0-1: res += s_A s_B 254^-1 (L0 254 + L1); |L0 254 + L1| < 2^31 for ts <= 512 */
+                const uint32_t base = tmem + ((uint32_t)(q * 32) << 16) + (uint32_t)(h * 64);
+                /* 8 batches per chunk: (columns c * 16 .. + 15, levels 0-1 or 2-3),
+                 * software-pipelined -- the next batch's TMEM loads are issued
+                 * before the current one is processed, so every wait::ld covers
+                 * a load issued one batch earlier */
+                uint32_t A0[16], A1[16], B0[16], B1[16];
+                int hi[16];
+                xg_tmem_ld_32x32b_x16(base + 0u, A0);
+                xg_tmem_ld_32x32b_x16(base + (uint32_t)XG_SL_BM, A1);
+                xg_tmem_ld_wait();
 #pragma unroll
-                for (int half = 0; half < 2; ++half) {
-                    uint32_t R0[2][16], R1[2][16];
-#pragma unroll
-                    for (int g = 0; g < 2; ++g) {
-                        const int c = (2 * half + g) * 16;
-                        xg_tmem_ld_32x32b_x16(base + (uint32_t)c, R0[g]);
-                        xg_tmem_ld_32x32b_x16(base + (uint32_t)(XG_SL_BM + c), R1[g]);
+                for (int b = 0; b < 8; ++b) {
+                    const int c = b >> 1, half = b & 1;
+                    uint32_t(&C0)[16] = (b & 1) ? B0 : A0; /* current batch */
+                    uint32_t(&C1)[16] = (b & 1) ? B1 : A1;
+                    uint32_t(&N0)[16] = (b & 1) ? A0 : B0; /* next batch */
+                    uint32_t(&N1)[16] = (b & 1) ? A1 : B1;
+                    if (b < 7) {
+                        const int nc = (b + 1) >> 1, nl = 2 * ((b + 1) & 1);
+                        xg_tmem_ld_32x32b_x16(base + (uint32_t)(nl * XG_SL_BM + nc * 16), N0);
+                        xg_tmem_ld_32x32b_x16(base + (uint32_t)((nl + 1) * XG_SL_BM + nc * 16), N1);
                     }
-                    xg_tmem_ld_wait();
-                    if (half == 1) {
-                        /* levels 0-1 are read: the next chunk's first pass may start */
-                        xg_tc_fence_before();
-                        __syncwarp();
-                        if (lane == 0) xg_mbar_arrive(&acc_empty[0]);
-                    }
+                    if (half == 0) {
+                        /* |L0| <= 127^2 ts, |L1| <= 2 127^2 ts: L0 254 + L1 fits int32 for ts <= 512 */
 #pragma unroll
-                    for (int g = 0; g < 2; ++g)
+                        for (int w = 0; w < 16; ++w) hi[w] = (int)C0[w] * 254 + (int)C1[w];
+                    } else {
 #pragma unroll
-                        for (int w = 0; w < 16; w += 2) {
-                            const int u0 = (2 * half + g) * 16 + w;
-                            const double2 s2 = sr2[u0 >> 1]; /* same address in every lane: a broadcast */
+                        for (int u = 0; u < 16; u += 2) {
+                            const double2 s2 = sr2[(c * 16 + u) >> 1]; /* same address in every lane: a broadcast */
 #pragma unroll
                             for (int e = 0; e < 2; ++e) {
-                                const long long v = (long long)((int)R0[g][w + e] * 254 + (int)R1[g][w + e]);
-                                res[u0 + e] = fma((e ? s2.y : s2.x) * sc_hi, xg_i64_to_f64(v), res[u0 + e]);
+                                const int w = u + e;
+                                /* v = (L0 254 + L1) 254^2 + L2 254 + L3, exact in int64 (< 2^48) */
+                                const long long v =
+                                    (long long)hi[w] * 64516 + ((long long)(int)C0[w] * 254 + (int)C1[w]);
+                                const double sr = e ? s2.y : s2.x;
+                                res[c * 16 + w] = fma(sr * sc, xg_i64_to_f64(v), res[c * 16 + w]);
                             }
                         }
-                }
-                /* levels 2-3: res += s_A s_B 254^-3 (L2 254 + L3) */
-                if (!xg_mbar_wait(&acc_full[1], (uint32_t)cc & 1)) {
-                    if (lane == 0) atomicOr(status, XG_ST_TIMEOUT);
-                    ok = false;
-                    break;
-                }
-                xg_tc_fence_after();
-#pragma unroll
-                for (int half = 0; half < 2; ++half) {
-                    uint32_t R2[2][16], R3[2][16];
-#pragma unroll
-                    for (int g = 0; g < 2; ++g) {
-                        const int c = (2 * half + g) * 16;
-                        xg_tmem_ld_32x32b_x16(base + (uint32_t)(2 * XG_SL_BM + c), R2[g]);
-                        xg_tmem_ld_32x32b_x16(base + (uint32_t)(3 * XG_SL_BM + c), R3[g]);
                     }
-                    xg_tmem_ld_wait();
-                    if (half == 1) {
-                        /* every TMEM load of the chunk is complete: levels 2-3 are free */
+                    if (b < 7) xg_tmem_ld_wait();
+                    if (b == 6) {
+                        /* every TMEM load of this chunk is complete: the
+                         * accumulators are free for the next chunk while the
+                         * last batch is combined */
                         xg_tc_fence_before();
                         __syncwarp();
-                        if (lane == 0) xg_mbar_arrive(&acc_empty[1]);
+                        if (lane == 0) xg_mbar_arrive(acc_empty);
                     }
-#pragma unroll
-                    for (int g = 0; g < 2; ++g)
-#pragma unroll
-                        for (int w = 0; w < 16; w += 2) {
-                            const int u0 = (2 * half + g) * 16 + w;
-                            const double2 s2 = sr2[u0 >> 1];
-#pragma unroll
-                            for (int e = 0; e < 2; ++e) {
-                                /* |L2 254 + L3| < 2^34: exact in int64 */
-                                const long long v = (long long)(int)R2[g][w + e] * 254 + (int)R3[g][w + e];
-                                res[u0 + e] = fma((e ? s2.y : s2.x) * sc, xg_i64_to_f64(v), res[u0 + e]);
-                            }
-                        }
                 }
                 /* this chunk's scale buffer may be refilled */
                 __syncwarp();
@@ -552,9 +469,10 @@ __global__ void __launch_bounds__(XG_SL_THREADS, 1)
             }
             if (!ok) break;
             /* C += sign U (or C = sign U): each warp instruction touches 32
-             * consecutive doubles of a row; 16 rows are loaded before any is
-             * stored; L2-only accesses (.cg): the few KB of L1 left beside the
-             * shared-memory stages would only thrash */
+             * consecutive doubles of a row; 16 rows are loaded before any is stored, so 16 loads per
+             * thread are in flight (a load after a store through the same
+             * pointer would wait for it); L2-only accesses (.cg): the few KB
+             * of L1 left beside the shared-memory stages would only thrash */
 #pragma unroll
             for (int u0 = 0; u0 < 64; u0 += 16) {
                 double cv[16];
