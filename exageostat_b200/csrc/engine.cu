@@ -1133,16 +1133,11 @@ static int xg_panel_k()
     return v;
 }
 
-static int xg_panel_share(int j, int nt, int sms)
+/* the balance itself: chain = tiles of the last-chunk update + XG_SHARE_TRSM
+ * x tiles of the TRSM (per-SM units), upd = tile-chunks of the split update */
+static int xg_share_balance(double chain, double upd, int sms)
 {
     const int lo = XG_PANEL_MIN, hi = sms - XG_PANEL_MIN;
-    const int K = xg_panel_k();
-    if (K > 0) {
-        int r = (int)((long long)sms * K / (K + j));
-        return r < XG_PANEL_SMS ? XG_PANEL_SMS : (r > sms - XG_PANEL_SMS ? sms - XG_PANEL_SMS : r);
-    }
-    const double chain = (double)(nt - j) + XG_SHARE_TRSM * (nt - j - 1);
-    const double upd = (double)j * (nt - j - 1);
     if (upd <= 0.0) return hi;
     auto longer = [&](int s) { return XG_SHARE_POTRF + chain / s > upd / (sms - s); }; /* chain still longer */
     if (!longer(lo)) return lo;
@@ -1156,6 +1151,16 @@ static int xg_panel_share(int j, int nt, int sms)
             b = m;
     }
     return b;
+}
+
+static int xg_panel_share(int j, int nt, int sms)
+{
+    const int K = xg_panel_k();
+    if (K > 0) {
+        int r = (int)((long long)sms * K / (K + j));
+        return r < XG_PANEL_SMS ? XG_PANEL_SMS : (r > sms - XG_PANEL_SMS ? sms - XG_PANEL_SMS : r);
+    }
+    return xg_share_balance((double)(nt - j) + XG_SHARE_TRSM * (nt - j - 1), (double)j * (nt - j - 1), sms);
 }
 
 /* How the SMs are divided between the panel chain and the split update.
@@ -1390,19 +1395,49 @@ int xg_field_loglik_grad_sliced(XgField *f, const double *theta, double *res, do
     XG_CU(cudaEventRecord(f->ev[0], st));
     for (int k = nt - 1; k >= 0; --k) xg_launch_trsv_lower_t_step(T, k, f->v, f->status, st);
     xg_launch_identity_x(f->X.d, nt, ts, st);
+    /* X = L^-T column by column, with the lookahead of the factorisation: the
+     * chain of column b (its last chunk c = b - 1, the FP64 solve with L_bb,
+     * the slicing) on the high-priority stream, beside the update of column
+     * b + 1 from the chunks c < b (columns already sliced) on the main stream */
+    auto inverse_task = [](int col, int k0, int k1) {
+        XgSlTask S;
+        S.mode = XG_SL_INVERSE;
+        S.col = col;
+        S.k0 = k0;
+        S.k1 = k1;
+        S.sign = -1.0;
+        S.overwrite = 0;
+        return S;
+    };
+    cudaStream_t sp = g_xg.stream_hi ? g_xg.stream_hi : st;
+    const bool la = sp != st;
+    const int sms = g_xg.sm_count;
+    if (la) cudaEventRecord(sl->ev_a, st); /* X initialised, alpha solved */
     for (int b = 0; b < nt; ++b) {
-        if (b >= 1) {
-            XgSlTask S;
-            S.mode = XG_SL_INVERSE;
-            S.col = b;
-            S.k0 = 0;
-            S.k1 = b;
-            S.sign = -1.0;
-            S.overwrite = 0;
-            xg_launch_sliced(sl->xmap, sl->map_b, sl->xscale, sl->scale, TX, S, pr, g_xg.sm_count, f->status, st);
+        /* per-SM costs as in the factorisation's share: the strip solve of a
+         * tile counts twice the factorisation's TRSM */
+        const int share = xg_share_balance((double)b + 2.0 * XG_SHARE_TRSM * (b + 1), 0.5 * b * (b + 1.0), sms);
+        if (la) cudaStreamWaitEvent(sp, sl->ev_a, 0); /* chunks c < b - 1 of column b */
+        if (b >= 1)
+            xg_launch_sliced(sl->xmap, sl->map_b, sl->xscale, sl->scale, TX, la ? inverse_task(b, b - 1, b)
+                                                                                 : inverse_task(b, 0, b),
+                             pr, la ? share : sms, f->status, sp);
+        xg_launch_xtrsm(f->X.d, f->C.d, nt, ts, b, f->status, sp);
+        xg_launch_slice_panel(TX, b, 1, sl->xdig, sl->xscale, (long long)plane, f->status, sp);
+        if (la) {
+            cudaEventRecord(sl->ev_p[b & 1], sp);
+            /* chunks c < b of column b + 1, behind the slicing of column b - 1 */
+            if (b >= 1 && b + 1 < nt) {
+                cudaStreamWaitEvent(st, sl->ev_p[(b - 1) & 1], 0);
+                xg_launch_sliced(sl->xmap, sl->map_b, sl->xscale, sl->scale, TX, inverse_task(b + 1, 0, b), pr,
+                                 sms - share, f->status, st);
+            }
+            cudaEventRecord(sl->ev_a, st);
         }
-        xg_launch_xtrsm(f->X.d, f->C.d, nt, ts, b, f->status, st);
-        xg_launch_slice_panel(TX, b, 1, sl->xdig, sl->xscale, (long long)plane, f->status, st);
+    }
+    if (la) {
+        cudaEventRecord(f->ev_panel, sp);
+        cudaStreamWaitEvent(st, f->ev_panel, 0);
     }
     XgSlTask S;
     S.mode = XG_SL_SYRK;
