@@ -1395,49 +1395,25 @@ int xg_field_loglik_grad_sliced(XgField *f, const double *theta, double *res, do
     XG_CU(cudaEventRecord(f->ev[0], st));
     for (int k = nt - 1; k >= 0; --k) xg_launch_trsv_lower_t_step(T, k, f->v, f->status, st);
     xg_launch_identity_x(f->X.d, nt, ts, st);
-    /* X = L^-T column by column, with the lookahead of the factorisation: the
-     * chain of column b (its last chunk c = b - 1, the FP64 solve with L_bb,
-     * the slicing) on the high-priority stream, beside the update of column
-     * b + 1 from the chunks c < b (columns already sliced) on the main stream */
-    auto inverse_task = [](int col, int k0, int k1) {
-        XgSlTask S;
-        S.mode = XG_SL_INVERSE;
-        S.col = col;
-        S.k0 = k0;
-        S.k1 = k1;
-        S.sign = -1.0;
-        S.overwrite = 0;
-        return S;
-    };
-    cudaStream_t sp = g_xg.stream_hi ? g_xg.stream_hi : st;
-    const bool la = sp != st;
-    const int sms = g_xg.sm_count;
-    if (la) cudaEventRecord(sl->ev_a, st); /* X initialised, alpha solved */
+    /* X = L^-T column by column: the update of column b from the finished
+     * columns c < b (INT8-sliced), the FP64 solve with L_bb, the slicing of
+     * column b.  (Overlapping the solve and slicing of column b with the
+     * update of column b + 1 on two streams, as the factorisation does, was
+     * measured at the same 5.87 s per gradient at N = 100 000: the update
+     * dominates each column.) */
     for (int b = 0; b < nt; ++b) {
-        /* per-SM costs as in the factorisation's share: the strip solve of a
-         * tile counts twice the factorisation's TRSM */
-        const int share = xg_share_balance((double)b + 2.0 * XG_SHARE_TRSM * (b + 1), 0.5 * b * (b + 1.0), sms);
-        if (la) cudaStreamWaitEvent(sp, sl->ev_a, 0); /* chunks c < b - 1 of column b */
-        if (b >= 1)
-            xg_launch_sliced(sl->xmap, sl->map_b, sl->xscale, sl->scale, TX, la ? inverse_task(b, b - 1, b)
-                                                                                 : inverse_task(b, 0, b),
-                             pr, la ? share : sms, f->status, sp);
-        xg_launch_xtrsm(f->X.d, f->C.d, nt, ts, b, f->status, sp);
-        xg_launch_slice_panel(TX, b, 1, sl->xdig, sl->xscale, (long long)plane, f->status, sp);
-        if (la) {
-            cudaEventRecord(sl->ev_p[b & 1], sp);
-            /* chunks c < b of column b + 1, behind the slicing of column b - 1 */
-            if (b >= 1 && b + 1 < nt) {
-                cudaStreamWaitEvent(st, sl->ev_p[(b - 1) & 1], 0);
-                xg_launch_sliced(sl->xmap, sl->map_b, sl->xscale, sl->scale, TX, inverse_task(b + 1, 0, b), pr,
-                                 sms - share, f->status, st);
-            }
-            cudaEventRecord(sl->ev_a, st);
+        if (b >= 1) {
+            XgSlTask S;
+            S.mode = XG_SL_INVERSE;
+            S.col = b;
+            S.k0 = 0;
+            S.k1 = b;
+            S.sign = -1.0;
+            S.overwrite = 0;
+            xg_launch_sliced(sl->xmap, sl->map_b, sl->xscale, sl->scale, TX, S, pr, g_xg.sm_count, f->status, st);
         }
-    }
-    if (la) {
-        cudaEventRecord(f->ev_panel, sp);
-        cudaStreamWaitEvent(st, f->ev_panel, 0);
+        xg_launch_xtrsm(f->X.d, f->C.d, nt, ts, b, f->status, st);
+        xg_launch_slice_panel(TX, b, 1, sl->xdig, sl->xscale, (long long)plane, f->status, st);
     }
     XgSlTask S;
     S.mode = XG_SL_SYRK;
