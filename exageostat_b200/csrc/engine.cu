@@ -18,6 +18,7 @@
 #include <string.h>
 #include <sys/time.h>
 
+#include <algorithm>
 #include <mutex>
 #include <string>
 #include <vector>
@@ -1163,6 +1164,43 @@ static int xg_panel_share(int j, int nt, int sms)
     return xg_share_balance((double)(nt - j) + XG_SHARE_TRSM * (nt - j - 1), (double)j * (nt - j - 1), sms);
 }
 
+/* CTAs of the split update of column j + 1 (jobs of 128 x 128, j chunks
+ * each, in rounds over the CTAs of a persistent launch) and of the
+ * last-chunk update of column j, with the round count in the balance: the
+ * share s minimises max(chain(s), rounds(s) j) in job-chunk units, and the
+ * update then takes only as many CTAs as its rounds need, leaving the rest to
+ * the chain (a last round that is only partly full costs the update nothing
+ * when the SMs it would leave idle go to the panel chain instead). */
+static void xg_split_ctas(int j, int nt, int ts, int sms, int *band_ctas, int *upd_ctas)
+{
+    const int K = xg_panel_k();
+    if (K > 0 || j < 1 || j + 1 >= nt) {
+        const int s = xg_panel_share(j, nt, sms);
+        *band_ctas = s;
+        *upd_ctas = sms - s;
+        return;
+    }
+    const int bpt = ts / 128;
+    const double per_tile = (double)bpt * bpt;
+    const long long jobs = (long long)(nt - j - 1) * bpt * bpt - (long long)bpt * (bpt - 1) / 2;
+    const double chain_work = per_tile * ((double)(nt - j) + XG_SHARE_TRSM * (nt - j - 1));
+    const double lat = per_tile * XG_SHARE_POTRF;
+    int best = XG_PANEL_MIN;
+    double best_t = 1e300;
+    for (int s = XG_PANEL_MIN; s <= sms - XG_PANEL_MIN; ++s) {
+        const long long rounds = (jobs + (sms - s) - 1) / (sms - s);
+        const double t = std::max(lat + chain_work / s, (double)rounds * j);
+        if (t < best_t) {
+            best_t = t;
+            best = s;
+        }
+    }
+    const long long rounds = (jobs + (sms - best) - 1) / (sms - best);
+    const int upd = (int)((jobs + rounds - 1) / rounds);
+    *upd_ctas = upd;
+    *band_ctas = sms - upd;
+}
+
 /* How the SMs are divided between the panel chain and the split update.
  * "static" (default): the split update runs as a persistent launch on
  * sms - xg_panel_share(j) CTAs, leaving the rest to the panel chain.
@@ -1203,9 +1241,11 @@ static void xg_factor_sliced(XgField *f, double *v, const XgFactorStreams &fs)
     for (int j = 0; j < nt; ++j) {
         if (la) cudaStreamWaitEvent(sp, sl->ev_a, 0); /* chunks k < j-1 of column j */
         rec(j, 0, sp);
+        int band_ctas = sms, upd_ctas = sms;
+        xg_split_ctas(j, nt, M.ts, sms, &band_ctas, &upd_ctas);
         if (la) {
             if (j >= 1) xg_launch_sliced(sl->map_a, sl->map_b, sl->scale, sl->scale, T, factor_task(j, j - 1, j), pr,
-                                         dyn ? all : xg_panel_share(j, nt, sms), f->status, sp);
+                                         dyn ? all : band_ctas, f->status, sp);
         } else {
             xg_launch_sliced(sl->map_a, sl->map_b, sl->scale, sl->scale, T, factor_task(j, 0, j), pr, sms, f->status,
                              sp);
@@ -1226,7 +1266,7 @@ static void xg_factor_sliced(XgField *f, double *v, const XgFactorStreams &fs)
             rec(j, 4, fs.st);
             if (j >= 1 && j + 1 < nt)
                 xg_launch_sliced(sl->map_a, sl->map_b, sl->scale, sl->scale, T, factor_task(j + 1, 0, j), pr,
-                                 dyn ? all : sms - xg_panel_share(j, nt, sms), f->status, fs.st);
+                                 dyn ? all : upd_ctas, f->status, fs.st);
             rec(j, 5, fs.st);
             cudaEventRecord(sl->ev_a, fs.st);
         } else {
