@@ -1110,95 +1110,33 @@ static XgSlTask factor_task(int col, int k0, int k1)
 }
 
 /* SMs given to the panel chain of column j (last-chunk update, POTRF, TRSM,
- * slicing) while the split update of column j+1 runs on the others: the
- * smallest share s for which the chain, P + W_chain / s, is no longer than
- * the update, W_upd / (sms - s).  Costs per SM in units of one tile-chunk of
- * the sliced update (a 512 x 512 target tile times one panel chunk, ~0.16 ms
- * on one SM): the last-chunk update 1 per tile, the TRSM of a tile
- * XG_SHARE_TRSM (the 128-column-block kernel at ~56 % of the DMMA rate), the
- * POTRF a latency of XG_SHARE_POTRF; W_upd = j (nt - j - 1).  With
- * EXAGEOSTAT_B200_PANEL_K=K set, the older rule s = sms K / (K + j) is used
- * instead.  Clamped to [XG_PANEL_MIN, sms - XG_PANEL_MIN]. */
-#define XG_SHARE_TRSM 6.2
-#define XG_SHARE_POTRF 4.7
-#define XG_PANEL_MIN 6
-
+ * slicing) while the split update of column j+1 runs on the others.  The
+ * chain's work grows like nt - j and the split update's like j (nt - j), so
+ * the chain gets sms K / (K + j), clamped to [XG_PANEL_SMS, sms -
+ * XG_PANEL_SMS].  K = 4 (EXAGEOSTAT_B200_PANEL_K overrides it) measured best
+ * at N = 100 000 with the 128-column-block TRSM: 1.589-1.644 s per
+ * evaluation against 1.614-1.665 s for K = 2, 3, 6, 8, 1.624 s for a cost
+ * model balancing the chain against the update, and 1.639 s for that model
+ * with the update's round count in it (each compared within one GPU
+ * session; the sessions differ by up to 3 %). */
 static int xg_panel_k()
 {
     static int v = -1;
     if (v < 0) {
         const char *e = getenv("EXAGEOSTAT_B200_PANEL_K");
         v = e ? atoi(e) : 0;
-        if (v < 1 || v > 64) v = 0;
+        if (v < 1 || v > 64) v = 4;
     }
     return v;
 }
 
-/* the balance itself: chain = tiles of the last-chunk update + XG_SHARE_TRSM
- * x tiles of the TRSM (per-SM units), upd = tile-chunks of the split update */
-static int xg_share_balance(double chain, double upd, int sms)
-{
-    const int lo = XG_PANEL_MIN, hi = sms - XG_PANEL_MIN;
-    if (upd <= 0.0) return hi;
-    auto longer = [&](int s) { return XG_SHARE_POTRF + chain / s > upd / (sms - s); }; /* chain still longer */
-    if (!longer(lo)) return lo;
-    if (longer(hi)) return hi;
-    int a = lo, b = hi; /* longer(a), !longer(b) */
-    while (b - a > 1) {
-        const int m = (a + b) / 2;
-        if (longer(m))
-            a = m;
-        else
-            b = m;
-    }
-    return b;
-}
-
-static int xg_panel_share(int j, int nt, int sms)
+static int xg_panel_share(int j, int sms)
 {
     const int K = xg_panel_k();
-    if (K > 0) {
-        int r = (int)((long long)sms * K / (K + j));
-        return r < XG_PANEL_SMS ? XG_PANEL_SMS : (r > sms - XG_PANEL_SMS ? sms - XG_PANEL_SMS : r);
-    }
-    return xg_share_balance((double)(nt - j) + XG_SHARE_TRSM * (nt - j - 1), (double)j * (nt - j - 1), sms);
-}
-
-/* CTAs of the split update of column j + 1 (jobs of 128 x 128, j chunks
- * each, in rounds over the CTAs of a persistent launch) and of the
- * last-chunk update of column j, with the round count in the balance: the
- * share s minimises max(chain(s), rounds(s) j) in job-chunk units, and the
- * update then takes only as many CTAs as its rounds need, leaving the rest to
- * the chain (a last round that is only partly full costs the update nothing
- * when the SMs it would leave idle go to the panel chain instead). */
-static void xg_split_ctas(int j, int nt, int ts, int sms, int *band_ctas, int *upd_ctas)
-{
-    const int K = xg_panel_k();
-    if (K > 0 || j < 1 || j + 1 >= nt) {
-        const int s = xg_panel_share(j, nt, sms);
-        *band_ctas = s;
-        *upd_ctas = sms - s;
-        return;
-    }
-    const int bpt = ts / 128;
-    const double per_tile = (double)bpt * bpt;
-    const long long jobs = (long long)(nt - j - 1) * bpt * bpt - (long long)bpt * (bpt - 1) / 2;
-    const double chain_work = per_tile * ((double)(nt - j) + XG_SHARE_TRSM * (nt - j - 1));
-    const double lat = per_tile * XG_SHARE_POTRF;
-    int best = XG_PANEL_MIN;
-    double best_t = 1e300;
-    for (int s = XG_PANEL_MIN; s <= sms - XG_PANEL_MIN; ++s) {
-        const long long rounds = (jobs + (sms - s) - 1) / (sms - s);
-        const double t = std::max(lat + chain_work / s, (double)rounds * j);
-        if (t < best_t) {
-            best_t = t;
-            best = s;
-        }
-    }
-    const long long rounds = (jobs + (sms - best) - 1) / (sms - best);
-    const int upd = (int)((jobs + rounds - 1) / rounds);
-    *upd_ctas = upd;
-    *band_ctas = sms - upd;
+    int r = (int)((long long)sms * K / (K + j));
+    if (r < XG_PANEL_SMS) r = XG_PANEL_SMS;
+    if (r > sms - XG_PANEL_SMS) r = sms - XG_PANEL_SMS;
+    return r;
 }
 
 /* How the SMs are divided between the panel chain and the split update.
@@ -1241,8 +1179,7 @@ static void xg_factor_sliced(XgField *f, double *v, const XgFactorStreams &fs)
     for (int j = 0; j < nt; ++j) {
         if (la) cudaStreamWaitEvent(sp, sl->ev_a, 0); /* chunks k < j-1 of column j */
         rec(j, 0, sp);
-        int band_ctas = sms, upd_ctas = sms;
-        xg_split_ctas(j, nt, M.ts, sms, &band_ctas, &upd_ctas);
+        const int band_ctas = xg_panel_share(j, sms), upd_ctas = sms - band_ctas;
         if (la) {
             if (j >= 1) xg_launch_sliced(sl->map_a, sl->map_b, sl->scale, sl->scale, T, factor_task(j, j - 1, j), pr,
                                          dyn ? all : band_ctas, f->status, sp);
