@@ -1019,7 +1019,7 @@ def main():
                        "band_tiles": args.band, "scheme": args.scheme,
                        "tf32_passes": None if sliced else passes,
                        "sm_share": os.environ.get("EXAGEOSTAT_B200_SL_SHARE", "static"),
-                       "panel_k": int(os.environ.get("EXAGEOSTAT_B200_PANEL_K", "8")),
+                       "panel_k": int(os.environ.get("EXAGEOSTAT_B200_PANEL_K", "4")),
                        "parallelism": "replicas" if world > 1 else "single-gpu",
                        "l2": "inputs larger than L2 (20-40 GB of covariance tiles per step)",
                        "loglik_reduced": llsmx[-1], "loglik_fp64": lls64[-1], "rel_err_vs_fp64": rel_err,
