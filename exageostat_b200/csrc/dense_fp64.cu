@@ -37,12 +37,104 @@
 /* One CTA fills XG_GEN_ROWS rows of one tile; threads stride the columns so
  * the row-major stores and the column-location loads are coalesced. */
 #define XG_GEN_ROWS 8
+/* General-order univariate elements, grouped by K_nu branch: the lanes of a
+ * warp would otherwise mix Temme's series, two trapezoid lengths and the
+ * asymptotic series (unsorted locations) and run every branch they hold.
+ * Each warp takes 32 columns x XG_GEN_ROWS rows at a time: every lane
+ * computes r for its 8 elements and files them by branch in a per-warp
+ * index list (ballots), the warp then evaluates the list branch by branch,
+ * one element per lane, and stores its 8 x 32 block row by row (coalesced).
+ * Each element is computed by the same function as the ungrouped path, so
+ * the values are the same bit for bit. */
+__device__ __forceinline__ void xg_gen_body_grouped(double *tile, int ts, int2 ij, int strip,
+                                                    const double *__restrict__ xr, const double *__restrict__ yr,
+                                                    const double *__restrict__ xc, const double *__restrict__ yc,
+                                                    int n_rows, int n_cols, const XgMaternParams &p, int metric,
+                                                    int identity_pad)
+{
+    __shared__ double s_val[8][32 * XG_GEN_ROWS];
+    __shared__ unsigned short s_idx[8][32 * XG_GEN_ROWS];
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarps = (int)(blockDim.x >> 5);
+    double *val = s_val[warp];
+    unsigned short *idx = s_idx[warp];
+    const unsigned lt = (1u << lane) - 1u;
+    for (int g = warp; g * 32 < ts; g += nwarps) {
+        const int c = g * 32 + lane;
+        const int C = ij.y * ts + c;
+        const bool col_ok = C < n_cols;
+        const double x2 = col_ok ? xc[C] : 0.0, y2 = col_ok ? yc[C] : 0.0;
+        int q_of[XG_GEN_ROWS];
+#pragma unroll
+        for (int rr = 0; rr < XG_GEN_ROWS; ++rr) {
+            const int R = ij.x * ts + strip * XG_GEN_ROWS + rr;
+            double v;
+            int q = -1;
+            if (R < n_rows && col_ok) {
+                const double d = xg_distance(xr[R], yr[R], x2, y2, metric);
+                const double r = d / p.beta;
+                if (r == 0.0) {
+                    v = p.sigma2 + p.nugget;
+                } else {
+                    q = xg_matern_branch(r, p.nu);
+                    v = r;
+                }
+            } else {
+                v = (identity_pad && R == C) ? 1.0 : 0.0;
+            }
+            val[rr * 32 + lane] = v; /* r for the listed elements, the value otherwise */
+            q_of[rr] = q;
+        }
+        int start[5];
+        start[0] = 0;
+#pragma unroll
+        for (int q = 0; q < 4; ++q) {
+            int n = 0;
+#pragma unroll
+            for (int rr = 0; rr < XG_GEN_ROWS; ++rr) n += __popc(__ballot_sync(0xffffffffu, q_of[rr] == q));
+            start[q + 1] = start[q] + n;
+        }
+        {
+            int pos[4] = {start[0], start[1], start[2], start[3]};
+#pragma unroll
+            for (int rr = 0; rr < XG_GEN_ROWS; ++rr)
+#pragma unroll
+                for (int q = 0; q < 4; ++q) {
+                    const unsigned m = __ballot_sync(0xffffffffu, q_of[rr] == q);
+                    if (q_of[rr] == q) idx[pos[q] + __popc(m & lt)] = (unsigned short)(rr * 32 + lane);
+                    pos[q] += __popc(m);
+                }
+        }
+        __syncwarp();
+        for (int i = start[0] + lane; i < start[1]; i += 32) {
+            const int e = idx[i];
+            val[e] = xg_matern_small_c(val[e], p.con, p.tm);
+        }
+        for (int i = start[1] + lane; i < start[3]; i += 32) {
+            const int e = idx[i];
+            val[e] = xg_matern_trap(val[e], p.nu, p.con);
+        }
+        for (int i = start[3] + lane; i < start[4]; i += 32) {
+            const int e = idx[i];
+            val[e] = xg_matern_asym(val[e], p.nu, p.con);
+        }
+        __syncwarp();
+#pragma unroll
+        for (int rr = 0; rr < XG_GEN_ROWS; ++rr)
+            tile[(long long)(strip * XG_GEN_ROWS + rr) * ts + c] = val[rr * 32 + lane];
+        __syncwarp();
+    }
+}
+
 __device__ __forceinline__ void xg_gen_body(const XgTileArgs &T, long long t, int2 ij, int strip,
                                             const double *__restrict__ xr, const double *__restrict__ yr,
                                             const double *__restrict__ xc, const double *__restrict__ yc, int n_rows,
                                             int n_cols, const XgMaternParams &p, int metric, int identity_pad)
 {
     double *tile = T.data + t * (long long)T.ts * T.ts;
+    if (!p.bivariate && p.half_integer < 0) {
+        xg_gen_body_grouped(tile, T.ts, ij, strip, xr, yr, xc, yc, n_rows, n_cols, p, metric, identity_pad);
+        return;
+    }
     /* bivariate: matrix index 2 l + v -> location l, variable v */
     const int sh = p.bivariate ? 1 : 0;
     for (int rr = 0; rr < XG_GEN_ROWS; ++rr) {

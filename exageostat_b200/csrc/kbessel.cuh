@@ -216,18 +216,38 @@ XG_HD inline double xg_bessel_knu(double nu, double x)
  * r^nu = r^n 2^mu / (2/r)^mu reuses the series' own power; the large-r
  * branches fold r^nu e^-r into one exp so it neither overflows nor
  * underflows early. */
+/* the three branches, also called one by one by the generators that group
+ * elements by branch (xg_matern_branch) */
+XG_HD inline double xg_matern_small_c(double r, double con, const XgTemme &tc) /* 0 < r <= 2 */
+{
+    double pw;
+    const double k = xg_knu_small_c(tc, r, nullptr, &pw);
+    double rn = 1.0;
+    for (int j = 0; j < tc.n; ++j) rn *= r;
+    return con * (rn * tc.two_mu / pw) * k;
+}
+XG_HD inline double xg_matern_asym(double r, double nu, double con) /* r >= 20, nu <= 5 */
+{
+    return con * XG_SQRT_HALF_PI * exp((nu - 0.5) * log(r) - r) * xg_knu_asym_sum(nu, r);
+}
+XG_HD inline double xg_matern_trap(double r, double nu, double con) /* r > 2 */
+{
+    return con * exp(nu * log(r) - r) * xg_knu_scaled_trap(nu, r);
+}
+/* branch of r > 0: 0 Temme (r <= 2), 1 and 2 the trapezoidal rule (r <= 6,
+ * beyond: fewer nodes), 3 the asymptotic expansion */
+XG_HD inline int xg_matern_branch(double r, double nu)
+{
+    if (r <= 2.0) return 0;
+    if (r >= XG_KNU_ASYM_X && nu <= XG_KNU_ASYM_NU) return 3;
+    return r <= 6.0 ? 1 : 2;
+}
+
 XG_HD inline double xg_matern_general_c(double r, double nu, double con, const XgTemme &tc)
 {
-    if (r <= 2.0) {
-        double pw;
-        const double k = xg_knu_small_c(tc, r, nullptr, &pw);
-        double rn = 1.0;
-        for (int j = 0; j < tc.n; ++j) rn *= r;
-        return con * (rn * tc.two_mu / pw) * k;
-    }
-    if (r >= XG_KNU_ASYM_X && nu <= XG_KNU_ASYM_NU)
-        return con * XG_SQRT_HALF_PI * exp((nu - 0.5) * log(r) - r) * xg_knu_asym_sum(nu, r);
-    return con * exp(nu * log(r) - r) * xg_knu_scaled_trap(nu, r);
+    if (r <= 2.0) return xg_matern_small_c(r, con, tc);
+    if (r >= XG_KNU_ASYM_X && nu <= XG_KNU_ASYM_NU) return xg_matern_asym(r, nu, con);
+    return xg_matern_trap(r, nu, con);
 }
 
 XG_HD inline double xg_matern_general(double r, double nu, double con)
