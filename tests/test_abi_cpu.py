@@ -100,6 +100,27 @@ def test_device_matern_element_compiled_for_host_matches_mpmath(tmp_path):
     assert len(rel) == len(pts) and max(rel) < 2e-14, max(rel)
 
 
+def test_branch_grouped_generation_gives_the_same_bits(tmp_path):
+    """The generators that group elements by K_nu branch (xg_matern_branch,
+    then xg_matern_small_c / _trap / _asym) must give the same bits as the
+    one-call element (xg_matern_general_c) for every r and order."""
+    src = tmp_path / "b.cpp"
+    src.write_text('#include <cstdio>\n#include <cstring>\n#include "kbessel.cuh"\n'
+                   'int main(){double nu,r;int bad=0,n=0;while(scanf("%lf %lf",&nu,&r)==2){++n;'
+                   'XgTemme tc=xg_temme_consts(nu);double con=1.7;double a=xg_matern_general_c(r,nu,con,tc);'
+                   'int q=xg_matern_branch(r,nu);double b=q==0?xg_matern_small_c(r,con,tc):'
+                   'q==3?xg_matern_asym(r,nu,con):xg_matern_trap(r,nu,con);'
+                   'if(memcmp(&a,&b,8))++bad;}printf("%d %d\\n",n,bad);}\n')
+    exe = tmp_path / "b"
+    subprocess.run(["g++", "-O2", "-I", os.path.join(ROOT, "exageostat_b200", "csrc"), str(src), "-o", str(exe)],
+                   check=True)
+    pts = ["%r %r" % (nu, float(r)) for nu in (0.01, 0.37, 0.5, 0.73, 1.0, 2.2, 4.99, 5.0, 5.5)
+           for r in np.concatenate([np.geomspace(1e-5, 2.0, 40), [2.0, 6.0, 19.999, 20.0]], axis=None).tolist()
+           + np.geomspace(2.0001, 600.0, 60).tolist()]
+    out = subprocess.run([str(exe)], input="\n".join(pts), capture_output=True, text=True, check=True).stdout.split()
+    assert int(out[0]) == len(pts) and int(out[1]) == 0
+
+
 def test_product_fails_loudly_without_library(xg, monkeypatch):
     monkeypatch.setattr(xg, "_lib", None)
     monkeypatch.setattr(xg, "LIB_PATH", "/nonexistent/libexageostat_b200.so")
