@@ -793,7 +793,7 @@ def mode_batch_sharded(args):
     dist.destroy_process_group()
 
 
-def ingest_ncu(path, case, command):
+def ingest_ncu(path, case, command, out_path=None):
     """Writes profiles/ncu_traffic.json from the raw page of an ncu capture
     (``ncu -i <rep> --page raw --csv``): per captured kernel, DRAM bytes
     (dram__bytes_read.sum + dram__bytes_write.sum, scaled by the unit row of
@@ -834,7 +834,7 @@ def ingest_ncu(path, case, command):
         if rd is None or wr is None or not ops:
             continue
         per.setdefault(name, []).append((rd + wr, ops))
-    out_path = os.path.join(ROOT, "profiles", "ncu_traffic.json")
+    out_path = out_path or os.path.join(ROOT, "profiles", "ncu_traffic.json")
     try:
         with open(out_path) as f:
             out = json.load(f)
