@@ -568,6 +568,14 @@ int exageostat_b200_batch_autotune(int nfields, const int *n, const double *x, c
                                    int kernel, int metric, const double *theta, int *ts, double *report,
                                    void **handle);
 
+/* The device scheduler's task list for fields of nt[f] tiles per side and
+ * `workers` persistent CTAs (host only, no GPU needed): writes 4 ints per
+ * task -- type | field << 2 (type 0 POTRF(k), 1 TRSM(i, k), 2 the update
+ * (i, j) <- k), i, j, k -- to out when out is not NULL, and returns the
+ * number of tasks.  exageostat_b200_batch_create builds its list this way;
+ * exposed so the order can be checked (complete, topological). */
+long long exageostat_b200_batch_plan(int nfields, const int *nt, int workers, int *out);
+
 /* ---- diagnostics used by the parity tests (no counterpart in the reference; all run on the GPU) ---- */
 /* Runs the bounded-wait path of the kernels on purpose: one thread waits on
  * a shared-memory barrier that nothing arrives on, gives up after limit_us
